@@ -1,0 +1,128 @@
+"""Procedural inputs for the drape workloads (host-side set-up, numpy).
+
+`quad_grid` restates the reference's generator
+(crates/vistio-mesh/src/generators.rs:28-100) in float32 with the same
+operation order, so meshes are bit-identical to the reference's.  The
+scenario builders follow crates/vistio-bench/src/scenarios.rs:84-147 with the
+parameter mapping of the drape workloads:
+
+* hanging_sheet: 1 m x 1 m, 20x20 cells, rotated into XZ at y = 1.0, the
+  first 21 vertices pinned, no contact.
+* sphere_drape: 1.5 m x 1.5 m, 64x64 cells, sheet plane y = 0.5, sphere at the
+  origin r = 0.3, ground y = -0.3 (runner.rs:77-81).
+* self_fold: 0.2 m x 2.0 m, 40x400 cells, rotated 45 degrees about x with the
+  lowest point at y = 0.5, ground y = 0, self contact.
+* batched sheets: hanging sheets of random side / size / material.
+
+The reference is Y-up (gravity (0, -9.81, 0)); a "z" in the workload text
+means the reference's y.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+SEED = 20261203
+
+
+def quad_grid(cols: int, rows: int, width: float, height: float):
+    """Flat grid in the XY plane with checkerboard diagonals (generators.rs:28)."""
+    f32 = np.float32
+    vx, vy = cols + 1, rows + 1
+    hw, hh = f32(width) / f32(2.0), f32(height) / f32(2.0)
+    i = np.arange(vx, dtype=np.float32)
+    j = np.arange(vy, dtype=np.float32)
+    u = (i / f32(cols)).astype(np.float32)
+    v = (j / f32(rows)).astype(np.float32)
+    x = (-hw + u * f32(width)).astype(np.float32)
+    y = (hh - v * f32(height)).astype(np.float32)
+    px = np.tile(x, vy).astype(np.float32)
+    py = np.repeat(y, vx).astype(np.float32)
+    pz = np.zeros(vx * vy, dtype=np.float32)
+    jj, ii = np.meshgrid(np.arange(rows, dtype=np.int64), np.arange(cols, dtype=np.int64), indexing="ij")
+    tl = (jj * vx + ii).ravel()
+    tr, bl = tl + 1, tl + vx
+    br = bl + 1
+    even = ((ii + jj) % 2 == 0).ravel()
+    t_even = np.stack([tl, bl, tr, tr, bl, br], axis=1)
+    t_odd = np.stack([tl, bl, br, tl, br, tr], axis=1)
+    tris = np.where(even[:, None], t_even, t_odd).reshape(-1, 3).astype(np.uint32)
+    return px, py, pz, tris
+
+
+@dataclasses.dataclass
+class Mesh:
+    px: np.ndarray
+    py: np.ndarray
+    pz: np.ndarray
+    tris: np.ndarray  # (T, 3) uint32
+    pinned: np.ndarray  # (V,) uint8
+
+    @property
+    def nv(self) -> int:
+        return int(self.px.shape[0])
+
+    @property
+    def nt(self) -> int:
+        return int(self.tris.shape[0])
+
+
+def hanging_sheet(side: int = 20, length: float = 1.0, height: float = 1.0) -> Mesh:
+    """scenarios.rs:84-114: rotate into XZ at y = height, pin the first row."""
+    px, py, pz, tris = quad_grid(side, side, length, length)
+    pz = py.copy()
+    py = np.full_like(px, np.float32(height))
+    pinned = np.zeros(px.shape[0], dtype=np.uint8)
+    pinned[: side + 1] = 1
+    return Mesh(px, py, pz, tris, pinned)
+
+
+def sphere_drape(side: int = 64, length: float = 1.5, height: float = 0.5) -> Mesh:
+    """scenarios.rs:120-147 with the sheet plane at y = 0.5; nothing pinned."""
+    px, py, pz, tris = quad_grid(side, side, length, length)
+    pz = py.copy()
+    py = np.full_like(px, np.float32(height))
+    return Mesh(px, py, pz, tris, np.zeros(px.shape[0], dtype=np.uint8))
+
+
+def self_fold(cols: int = 40, rows: int = 400, width: float = 0.2, height: float = 2.0,
+              lowest: float = 0.5) -> Mesh:
+    """Ribbon rotated 45 degrees about x, lowest point at y = `lowest`."""
+    px, py, pz, tris = quad_grid(cols, rows, width, height)
+    c = np.float32(math.cos(math.pi / 4))
+    s = np.float32(math.sin(math.pi / 4))
+    ny = (py * c - pz * s).astype(np.float32)
+    nz = (py * s + pz * c).astype(np.float32)
+    ny = (ny + (np.float32(lowest) - ny.min())).astype(np.float32)
+    return Mesh(px, ny, nz, tris, np.zeros(px.shape[0], dtype=np.uint8))
+
+
+@dataclasses.dataclass
+class SheetSpec:
+    side: int
+    length: float
+    stretch: float   # element stiffness k (N/m): weight = k * area
+    bending: float   # hinge stiffness k_b (N m): weight = k_b * edge length
+    density_gsm: float
+
+
+def batched_specs(n_instances: int = 512, n_topologies: int = 8, side_lo: int = 16, side_hi: int = 128,
+                  seed: int = SEED):
+    """The batched workload: 8 grid sides drawn once and assigned round-robin;
+    per instance a side length in [0.5, 2] m, stretch log-uniform in
+    [2e2, 5e3] N/m, bending log-uniform in [1e-5, 1e-3] N m and density
+    uniform in [0.08, 0.30] kg/m^2."""
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(side_lo, side_hi + 1, size=n_topologies)
+    specs = []
+    for k in range(n_instances):
+        specs.append(SheetSpec(
+            side=int(sides[k % n_topologies]),
+            length=float(rng.uniform(0.5, 2.0)),
+            stretch=float(math.exp(rng.uniform(math.log(2e2), math.log(5e3)))),
+            bending=float(math.exp(rng.uniform(math.log(1e-5), math.log(1e-3)))),
+            density_gsm=float(rng.uniform(0.08, 0.30) * 1000.0),
+        ))
+    return specs
