@@ -1,0 +1,242 @@
+/*
+ * vistio_cuda.h — C ABI of the B200 (sm_100a) Projective Dynamics + IPC drape
+ * solver. Plain C types only; every call returns a vistio_status.
+ *
+ * Each group of entry points replaces one interface of the reference
+ * (Rust, MTawhid7/Vistio). Paths cite files inside that project:
+ *
+ *   vistio_solver_init*        SolverStrategy::init            crates/vistio-solver/src/strategy.rs:42-56
+ *                              ProjectiveDynamicsSolver::init  crates/vistio-solver/src/pd_solver.rs:221-257
+ *                              ::init_with_material            pd_solver.rs:106-143
+ *                              ::init_with_material_tier3/4    pd_solver.rs:152-211
+ *   vistio_solver_lumped_masses  ::lumped_masses               pd_solver.rs:95-97
+ *   vistio_solver_set/get_state  SimulationState fields        crates/vistio-solver/src/state.rs:23-140
+ *   vistio_step                SolverStrategy::step            strategy.rs:57-64, pd_solver.rs:259-476
+ *   vistio_step_with_ipc       ::step_with_ipc                 pd_solver.rs:549-1157, with the handler
+ *                              IpcCollisionHandler             pd_solver.rs:483-489 implemented inside
+ *                              the library as CollisionPipeline::detect_ipc_contacts / compute_ccd_step
+ *                              crates/vistio-contact/src/collision_pipeline.rs:207-400
+ *   vistio_sparse_factorize/solve  SparseSolver                crates/vistio-math/src/sparse.rs:110-120,
+ *                              FaerSolver                      crates/vistio-math/src/faer_solver.rs:25-129
+ *   vistio_broadphase_pairs    BroadPhase::update + query_triangle_pairs  crates/vistio-contact/src/broad.rs:39-56
+ *   vistio_ccd_hits            compute_max_step_size           crates/vistio-contact/src/ccd.rs:238-292
+ *   vistio_batch_*             (no counterpart: the reference steps one garment at a time)
+ *
+ * Threading: a context is used from one host thread at a time. Device work
+ * runs on the context's stream; the calls that return host data synchronise.
+ */
+#ifndef VISTIO_CUDA_H
+#define VISTIO_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: VistioError variants (crates/vistio-types/src/error.rs:9-44)
+ * plus the device-side conditions. */
+typedef enum vistio_status {
+  VISTIO_OK = 0,
+  VISTIO_ERR_INVALID_MESH = 1,      /* VistioError::InvalidMesh */
+  VISTIO_ERR_INVALID_MATERIAL = 2,  /* VistioError::InvalidMaterial */
+  VISTIO_ERR_INVALID_CONFIG = 3,    /* VistioError::InvalidConfig (also: not initialised) */
+  VISTIO_ERR_IO = 4,                /* VistioError::Io */
+  VISTIO_ERR_SERIALIZATION = 5,     /* VistioError::Serialization */
+  VISTIO_ERR_GPU = 6,               /* VistioError::Gpu: a CUDA call failed */
+  VISTIO_ERR_SOLVER_DIVERGENCE = 7, /* VistioError::SolverDivergence: non-finite state */
+  VISTIO_ERR_INVARIANT = 8,         /* VistioError::InvariantViolation */
+  VISTIO_ERR_TIMEOUT = 9,           /* a bounded device wait gave up */
+  VISTIO_ERR_OOM = 10,              /* device allocation failed / over the memory budget */
+  VISTIO_ERR_NOT_SPD = 11,          /* Cholesky pivot <= 0 (reported by the reference as InvalidConfig) */
+  VISTIO_ERR_CAPACITY = 12          /* an output buffer is too small */
+} vistio_status;
+
+typedef struct vistio_ctx vistio_ctx;
+typedef struct vistio_solver vistio_solver;
+typedef struct vistio_batch vistio_batch;
+typedef struct vistio_factor vistio_factor;
+
+/* TriangleMesh (crates/vistio-mesh/src/mesh.rs): SoA positions + u32 indices. */
+typedef struct vistio_mesh_desc {
+  uint32_t vertex_count;
+  uint32_t triangle_count;
+  const float* pos_x;
+  const float* pos_y;
+  const float* pos_z;
+  const uint32_t* indices; /* 3 * triangle_count */
+} vistio_mesh_desc;
+
+/* Live fields of SolverConfig (crates/vistio-solver/src/config.rs:10-129).
+ * Fields the reference declares but never reads on this path
+ * (contact_weight, chebyshev_acceleration, spectral_radius,
+ * self_collision_d_hat, cloth_thickness, ccd_enabled, material_name) are
+ * not carried. */
+typedef struct vistio_solver_config {
+  uint32_t max_iterations;
+  uint32_t al_max_iterations;
+  double tolerance;
+  float gravity[3];
+  float damping;
+  float stretch_weight;
+  float bending_weight;
+  float rayleigh_mass_damping;
+  float barrier_d_hat;   /* squared-distance activation threshold */
+  float barrier_kappa;   /* 0 = estimate (barrier.rs:97) */
+  float al_mu_initial;
+  float al_mu_growth;
+  float al_tolerance;
+  float friction_coefficient;
+  float contact_damping;
+  float compliant_d_hat_scale;
+  float contact_damping_max;
+  float contact_velocity_threshold;
+  int32_t compliant_contact;
+  int32_t adaptive_contact_damping;
+} vistio_solver_config;
+
+/* FabricProperties (crates/vistio-material/src/properties.rs:23-58). */
+typedef struct vistio_material_desc {
+  float density;                 /* g/m^2 */
+  float stretch_stiffness_warp;
+  float stretch_stiffness_weft;
+  float shear_stiffness;         /* carried, unused by the reference's PD path */
+  float bending_stiffness_warp;
+  float bending_stiffness_weft;
+  float thickness;
+  float friction;
+  float damping;
+} vistio_material_desc;
+
+/* ConstitutiveModel implementations (crates/vistio-material/src/traits.rs:36-56). */
+typedef enum vistio_model_kind {
+  VISTIO_MODEL_ARAP = 0,         /* ElementData::project, the `init` path (element.rs:127) */
+  VISTIO_MODEL_COROTATIONAL = 1, /* CoRotationalModel (corotational.rs:50) */
+  VISTIO_MODEL_ORTHOTROPIC = 2,  /* OrthotropicLinearModel (orthotropic.rs:50) */
+  VISTIO_MODEL_ANISOTROPIC = 3,  /* AnisotropicCoRotationalModel (anisotropic.rs:77) */
+  VISTIO_MODEL_ISOTROPIC_LINEAR = 4 /* IsotropicLinearModel (isotropic.rs:41) */
+} vistio_model_kind;
+
+typedef struct vistio_model_desc {
+  int32_t kind;          /* vistio_model_kind */
+  float warp_stiffness;  /* ORTHOTROPIC / ANISOTROPIC */
+  float weft_stiffness;
+} vistio_model_desc;
+
+typedef enum vistio_bending_kind {
+  VISTIO_BENDING_NONE = 0,
+  VISTIO_BENDING_DIHEDRAL = 1,       /* BendingData (bending.rs:44) */
+  VISTIO_BENDING_DISCRETE_SHELLS = 2,/* DiscreteShellsBendingData (discrete_shells.rs:81) */
+  VISTIO_BENDING_DISCRETE_SHELLS_ANISOTROPIC = 3
+} vistio_bending_kind;
+
+/* The explicit form every init path reduces to. */
+typedef struct vistio_setup_desc {
+  int32_t model;          /* vistio_model_kind */
+  int32_t bending;        /* vistio_bending_kind */
+  float stiffness;        /* element weight = stiffness * rest area */
+  float bend_stiffness;   /* hinge weight = bend_stiffness * rest edge length */
+  float density_gsm;      /* lumped-mass area density, g/m^2 */
+  float warp_stiffness, weft_stiffness;
+  float bend_warp, bend_weft;
+  float matrix_dt;        /* dt of the system matrix; the reference always uses 1/60 */
+} vistio_setup_desc;
+
+/* What the reference's RunnerIpcHandler wires into the CollisionPipeline
+ * (crates/vistio-bench/src/runner.rs:48-99,190-204). */
+typedef struct vistio_contact_desc {
+  int32_t has_ground;
+  float ground_height;       /* y of the ground plane (Y-up) */
+  int32_t has_sphere;
+  float sphere_center[3];
+  float sphere_radius;
+  int32_t self_collision;    /* triangle self contact, 1-ring exclusion */
+  float kappa;               /* barrier stiffness; <= 0 estimates it from avg vertex mass */
+  float thickness;           /* C-IPC thickness for self contacts (runner: 1.5 * d_hat) */
+} vistio_contact_desc;
+
+/* StepResult (strategy.rs:15-24) plus contact diagnostics. */
+typedef struct vistio_step_result {
+  uint32_t iterations;
+  int32_t converged;
+  double final_residual;
+  double wall_time;          /* seconds, host clock around the call */
+  uint32_t al_iterations;
+  uint32_t active_contacts;
+  float last_alpha;
+  int32_t status;
+} vistio_step_result;
+
+/* ---- context ---- */
+vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out);
+vistio_status vistio_ctx_destroy(vistio_ctx* ctx);
+const char* vistio_status_string(vistio_status s);
+const char* vistio_last_error(const vistio_ctx* ctx);
+vistio_status vistio_sync(vistio_ctx* ctx);
+
+/* ---- solver (one garment) ---- */
+vistio_status vistio_solver_init(vistio_ctx* ctx, const vistio_mesh_desc* mesh, const vistio_solver_config* cfg,
+                                 const uint8_t* pinned, vistio_solver** out);
+vistio_status vistio_solver_init_with_material(vistio_ctx* ctx, const vistio_mesh_desc* mesh,
+                                               const vistio_solver_config* cfg, const vistio_material_desc* material,
+                                               const vistio_model_desc* model, int32_t bending_kind,
+                                               const uint8_t* pinned, vistio_solver** out);
+vistio_status vistio_solver_init_explicit(vistio_ctx* ctx, const vistio_mesh_desc* mesh,
+                                          const vistio_solver_config* cfg, const vistio_setup_desc* setup,
+                                          const uint8_t* pinned, vistio_solver** out);
+vistio_status vistio_solver_destroy(vistio_solver* s);
+const char* vistio_solver_name(const vistio_solver* s); /* "ProjectiveDynamics" */
+vistio_status vistio_solver_info(const vistio_solver* s, uint32_t* nv, uint32_t* nt, uint32_t* nh,
+                                 uint64_t* nnz_a, uint64_t* nnz_l, uint32_t* nsupernodes, uint32_t* nlevels);
+vistio_status vistio_solver_lumped_masses(const vistio_solver* s, float* out);
+vistio_status vistio_solver_set_ground(vistio_solver* s, int32_t has_ground, float height);
+vistio_status vistio_solver_set_state(vistio_solver* s, const float* px, const float* py, const float* pz,
+                                      const float* vx, const float* vy, const float* vz);
+vistio_status vistio_solver_get_state(vistio_solver* s, float* px, float* py, float* pz, float* vx, float* vy,
+                                      float* vz);
+vistio_status vistio_step(vistio_solver* s, float dt, vistio_step_result* res);
+vistio_status vistio_step_with_ipc(vistio_solver* s, float dt, const vistio_contact_desc* contact,
+                                   vistio_step_result* res);
+
+/* ---- batches: many garments advanced together from HBM-resident ragged SoA ---- */
+vistio_status vistio_batch_create(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch** out);
+vistio_status vistio_batch_destroy(vistio_batch* b);
+/* Advances every instance `nsteps` steps of size dt; contact may be NULL. Asynchronous. */
+vistio_status vistio_batch_step(vistio_batch* b, float dt, uint32_t nsteps, const vistio_contact_desc* contact);
+vistio_status vistio_batch_set_state(vistio_batch* b, uint32_t k, const float* px, const float* py, const float* pz,
+                                     const float* vx, const float* vy, const float* vz);
+vistio_status vistio_batch_get_state(vistio_batch* b, uint32_t k, float* px, float* py, float* pz, float* vx,
+                                     float* vy, float* vz);
+/* Whole-batch positions in instance order (3 * total vertices, interleaved xyz), one copy each way. */
+vistio_status vistio_batch_upload_positions(vistio_batch* b, const float* xyz);
+vistio_status vistio_batch_download_positions(vistio_batch* b, float* xyz);
+vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, uint64_t* total_vertices,
+                                uint64_t* total_triangles, uint64_t* total_hinges, uint64_t* factor_bytes,
+                                uint64_t* device_bytes);
+/* Kernel launches in one batch step (graph nodes), for launch accounting. */
+vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* launches);
+/* The stream the batch runs on (cudaStream_t as void*), for event timing. */
+void* vistio_batch_stream(vistio_batch* b);
+
+/* ---- SparseSolver mirror ---- */
+vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
+                                      const float* values, vistio_factor** out);
+vistio_status vistio_sparse_solve(vistio_factor* f, const float* rhs, float* solution);
+vistio_status vistio_sparse_destroy(vistio_factor* f);
+
+/* ---- contact boundary queries ---- */
+/* Candidate triangle pairs (ta < tb) whose AABBs inflated by `margin` overlap,
+ * computed on the GPU (LBVH). Writes up to `cap` pairs sorted; *count = total. */
+vistio_status vistio_broadphase_pairs(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py, const float* pz,
+                                      uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs, uint64_t cap,
+                                      uint64_t* count);
+/* Vertex-triangle CCD over candidate pairs on the GPU: sorted unique
+ * (vertex, triangle) hits and the minimum safe TOI. */
+vistio_status vistio_ccd_hits(vistio_ctx* ctx, uint32_t nv, const float* p0, const float* p1, uint32_t nt,
+                              const uint32_t* tris, uint64_t npairs, const uint32_t* pairs, uint32_t* hits,
+                              uint64_t cap, uint64_t* nhits, float* min_toi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VISTIO_CUDA_H */

@@ -1,0 +1,131 @@
+// CPU check of the host-side set-up (vistio_b200/csrc/setup.cpp): builds a
+// quad-grid instance, then replays the GPU sweep schedule of k_solve (level
+// by level: pull-forward through the panel row lists, inverted diagonal
+// blocks, panel-transpose backward) on the CPU and reports the relative
+// residual of A x = b. Prints one JSON object.
+//
+// usage: factor_check cols rows width [bending] [pinned_row]
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <vector>
+
+#include "../../vistio_b200/csrc/setup.h"
+
+using namespace vistio;
+
+template <class T>
+static void sweep(const Factor& F, const std::vector<T>& vals, std::vector<T>& Y) {
+  uint32_t n = F.n;
+  std::vector<T> Tm(n);
+  for (uint32_t l = 0; l < F.nlevels; ++l) {
+    for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
+      uint32_t r = F.level_rows[i];
+      T t = Y[r];
+      for (uint32_t q = F.fwd_ptr[r]; q < F.fwd_ptr[r + 1]; ++q) {
+        const Supernode& S = F.sn[F.fwd_sn[q]];
+        const T* pr = vals.data() + S.panel_off + uint64_t(F.fwd_pos[q]) * S.ncols;
+        for (uint32_t c = 0; c < S.ncols; ++c) t -= pr[c] * Y[S.first + c];
+      }
+      Tm[r] = t;
+    }
+    for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
+      uint32_t r = F.level_rows[i];
+      const Supernode& S = F.sn[F.row_sn[r]];
+      uint32_t c = r - S.first, s = S.ncols;
+      const T* D = vals.data() + S.diag_off;
+      T y = 0;
+      for (uint32_t c2 = 0; c2 <= c; ++c2) y += D[uint64_t(c2) * s + c] * Tm[S.first + c2];
+      Y[r] = y;
+    }
+  }
+  for (int l = int(F.nlevels) - 1; l >= 0; --l) {
+    for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
+      uint32_t r = F.level_rows[i];
+      const Supernode& S = F.sn[F.row_sn[r]];
+      uint32_t c = r - S.first, s = S.ncols;
+      T t = Y[r];
+      const T* pc = vals.data() + S.panel_off + c;
+      const uint32_t* rr = F.rows.data() + S.rows_off;
+      for (uint32_t j = 0; j < S.nrows; ++j) t -= pc[uint64_t(j) * s] * Y[rr[j]];
+      Tm[r] = t;
+    }
+    for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
+      uint32_t r = F.level_rows[i];
+      const Supernode& S = F.sn[F.row_sn[r]];
+      uint32_t c = r - S.first, s = S.ncols;
+      const T* D = vals.data() + S.diag_off + uint64_t(c) * s;
+      T x = 0;
+      for (uint32_t c2 = c; c2 < s; ++c2) x += D[c2] * Tm[S.first + c2];
+      Y[r] = x;
+    }
+  }
+}
+
+int main(int argc, char** argv) {
+  uint32_t cols = argc > 1 ? atoi(argv[1]) : 20, rows = argc > 2 ? atoi(argv[2]) : 20;
+  float width = argc > 3 ? float(atof(argv[3])) : 1.f;
+  int bending = argc > 4 ? atoi(argv[4]) : BEND_DIHEDRAL;
+  int pin_row = argc > 5 ? atoi(argv[5]) : 1;
+  uint32_t vx = cols + 1, vy = rows + 1, nv = vx * vy;
+  std::vector<float> px(nv), py(nv), pz(nv);
+  float height = width * float(rows) / float(cols);
+  for (uint32_t j = 0; j < vy; ++j)
+    for (uint32_t i = 0; i < vx; ++i) {
+      uint32_t k = j * vx + i;
+      px[k] = -width / 2 + float(i) / float(cols) * width;
+      pz[k] = height / 2 - float(j) / float(rows) * height;
+      py[k] = 1.0f;
+    }
+  std::vector<uint32_t> tris;
+  for (uint32_t j = 0; j < rows; ++j)
+    for (uint32_t i = 0; i < cols; ++i) {
+      uint32_t tl = j * vx + i, tr = tl + 1, bl = tl + vx, br = bl + 1;
+      if ((i + j) % 2 == 0) tris.insert(tris.end(), {tl, bl, tr, tr, bl, br});
+      else tris.insert(tris.end(), {tl, bl, br, tl, br, tr});
+    }
+  std::vector<uint8_t> pinned(nv, 0);
+  if (pin_row)
+    for (uint32_t i = 0; i < vx; ++i) pinned[i] = 1;
+  SetupParams p;
+  p.bending = bending;
+  p.stiffness = 1000.f;
+  p.bend_stiffness = 1e-4f;
+  p.density_gsm = 150.f;
+  InstanceSetup I;
+  int st = 0;
+  std::string err = build_instance(nv, px.data(), py.data(), pz.data(), uint32_t(tris.size() / 3), tris.data(),
+                                   pinned.data(), p, I, &st);
+  if (!err.empty()) {
+    printf("{\"error\": \"%s\", \"status\": %d}\n", err.c_str(), st);
+    return 1;
+  }
+  const Factor& F = I.factor;
+  std::mt19937_64 rng(20261203);
+  std::normal_distribution<double> nd;
+  std::vector<double> b(nv), yd(nv);
+  for (auto& v : b) v = nd(rng);
+  for (uint32_t i = 0; i < nv; ++i) yd[F.iperm[i]] = b[i];
+  std::vector<float> yf(yd.begin(), yd.end());
+  std::vector<float> valsf(F.vals.begin(), F.vals.end());
+  sweep<double>(F, F.vals, yd);
+  sweep<float>(F, valsf, yf);
+  auto resid = [&](auto& y) {
+    double rn = 0, bn = 0;
+    for (uint32_t i = 0; i < nv; ++i) {
+      double s = b[i];
+      for (uint32_t q = I.A_ptr[i]; q < I.A_ptr[i + 1]; ++q) s -= I.A_val[q] * double(y[F.iperm[I.A_col[q]]]);
+      rn += s * s;
+      bn += b[i] * b[i];
+    }
+    return std::sqrt(rn / bn);
+  };
+  uint32_t maxs = 0;
+  for (auto& S : F.sn) maxs = std::max(maxs, S.ncols);
+  printf("{\"nv\": %u, \"nh\": %u, \"nnz_a\": %zu, \"nnz_l\": %llu, \"stored\": %llu, \"supernodes\": %zu, "
+         "\"levels\": %u, \"max_snode\": %u, \"fwd_entries\": %zu, \"resid64\": %.3e, \"resid32\": %.3e}\n",
+         nv, I.nh, I.A_col.size(), (unsigned long long)F.nnz_L, (unsigned long long)F.nnz_stored, F.sn.size(),
+         F.nlevels, maxs, F.fwd_sn.size(), resid(yd), resid(yf));
+  return 0;
+}

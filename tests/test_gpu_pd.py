@@ -1,0 +1,167 @@
+"""GPU parity of the plain PD step (SolverStrategy::step) against the oracle.
+
+Tolerances (positions, metres; the sheet spans about 1 m):
+* one step from an identical state: relative L2 error <= 1e-5 against the
+  FP64 oracle and against the FP32 reference restatement;
+* a full 120-step hanging_sheet run: max |x_gpu - x_fp64| <= 1e-4 m.
+"""
+import numpy as np
+import pytest
+
+import oracle_api as O
+from vistio_b200 import api, scenarios
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 60.0
+
+
+def sheet_pair(side=20, length=1.0, stiffness=1e3, bend=1e-4, density=150.0, iters=10, model=0, bending=1,
+               warp=0.0, weft=0.0, bend_warp=0.0, bend_weft=0.0, precision=1):
+    mesh = scenarios.hanging_sheet(side, length)
+    cfg = api.drape_config(max_iterations=iters)
+    setup = api.SetupDesc(model=model, bending=bending, stiffness=stiffness, bend_stiffness=bend, density_gsm=density,
+                          warp_stiffness=warp, weft_stiffness=weft, bend_warp=bend_warp, bend_weft=bend_weft)
+    gpu = api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
+    p = O.init_params(stiffness=stiffness, bend_stiffness=bend, density_gsm=density, model=model, bending=bending,
+                      warp=warp, weft=weft, bend_warp=bend_warp, bend_weft=bend_weft)
+    ref = O.OracleSim(mesh, p, O.default_config(max_iterations=iters), precision=precision)
+    return mesh, gpu, ref
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_lumped_masses_match_oracle():
+    mesh, gpu, ref = sheet_pair()
+    assert np.array_equal(gpu.lumped_masses(), ref.masses())
+
+
+def test_one_step_from_rest_matches_fp64_and_ref32():
+    mesh, gpu, ref64 = sheet_pair(precision=1)
+    _, _, ref32 = sheet_pair(precision=0)
+    r = gpu.step(DT)
+    ref64.step(DT)
+    ref32.step(DT)
+    pg, vg = gpu.state()
+    p64, v64 = ref64.state()
+    p32, _ = ref32.state()
+    assert r.iterations == 10
+    assert rel(pg, p64) <= 1e-5, rel(pg, p64)
+    assert rel(pg, p32) <= 1e-5, rel(pg, p32)
+    assert np.abs(vg - v64).max() <= 1e-3  # velocities = dx / dt
+    # pinned vertices stay where they are (solver_tests.rs:419-450)
+    pin = mesh.pinned.astype(bool)
+    x0 = np.stack([mesh.px, mesh.py, mesh.pz], 1)
+    assert np.abs(pg[pin] - x0[pin]).max() <= 1e-6
+
+
+def test_per_step_parity_along_a_trajectory():
+    """At checkpoints of an oracle trajectory, one GPU step from the oracle's
+    state stays within 1e-5 relative of the oracle's next state."""
+    mesh, gpu, ref = sheet_pair(precision=1)
+    worst = 0.0
+    for s in range(60):
+        if s % 10 == 5:
+            p, v = ref.state()
+            gpu.set_state(p, v)
+            ref.step(DT)
+            gpu.step(DT)
+            worst = max(worst, rel(gpu.state()[0], ref.state()[0]))
+        else:
+            ref.step(DT)
+    assert worst <= 1e-5, worst
+
+
+def test_full_hanging_sheet_run_within_1e4_m_of_fp64():
+    """hanging_sheet, 120 steps, 10 iterations: the GPU run stays within 1e-4 m
+    of the FP64 run; gravity lowers the centroid (solver_tests.rs:453-483)."""
+    mesh, gpu, ref = sheet_pair(precision=1)
+    for _ in range(120):
+        gpu.step(DT)
+        ref.step(DT)
+    pg, _ = gpu.state()
+    pr, _ = ref.state()
+    err = float(np.abs(pg - pr).max())
+    print(f"120-step hanging_sheet: max |x_gpu - x_fp64| = {err:.3e} m")
+    assert err <= 1e-4, err
+    assert pg[:, 1].mean() < mesh.py.mean() - 0.1
+
+
+@pytest.mark.parametrize("model,bending,warp,weft", [
+    (api.MODEL_COROTATIONAL, api.BENDING_DIHEDRAL, 0.0, 0.0),
+    (api.MODEL_ORTHOTROPIC, api.BENDING_DISCRETE_SHELLS, 1e3, 6e2),
+    (api.MODEL_ANISOTROPIC, api.BENDING_DISCRETE_SHELLS_ANISOTROPIC, 0.8, 0.3),
+    (api.MODEL_ISOTROPIC_LINEAR, api.BENDING_DISCRETE_SHELLS, 0.0, 0.0),
+    (api.MODEL_ARAP, api.BENDING_NONE, 0.0, 0.0),
+])
+def test_material_models_one_step(model, bending, warp, weft):
+    mesh, gpu, ref = sheet_pair(side=16, length=0.8, model=model, bending=bending, warp=warp, weft=weft,
+                                bend_warp=0.02, bend_weft=0.01)
+    for _ in range(3):
+        p, v = ref.state()
+        gpu.set_state(p, v)
+        ref.step(DT)
+        gpu.step(DT)
+        assert rel(gpu.state()[0], ref.state()[0]) <= 1e-5
+
+
+def test_batch_equals_individual_solvers_bitwise():
+    """Instances advanced together in one ragged batch give exactly the
+    results they give alone."""
+    specs = [(12, 0.7, 400.0, 2e-5, 90.0), (20, 1.3, 3000.0, 5e-4, 250.0), (9, 0.5, 900.0, 1e-4, 150.0)]
+    cfg = api.drape_config(max_iterations=10)
+    solo, grouped = [], []
+    for side, length, k, kb, rho in specs:
+        mesh = scenarios.hanging_sheet(side, length)
+        setup = api.SetupDesc(stiffness=k, bend_stiffness=kb, density_gsm=rho)
+        solo.append(api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned))
+        grouped.append(api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned))
+    batch = api.Batch(grouped)
+    batch.step(DT, 5)
+    for k, s in enumerate(solo):
+        for _ in range(5):
+            s.step(DT)
+        assert np.array_equal(s.state()[0], batch.state(k)[0])
+
+
+def test_sparse_solver_reference_cases():
+    """The reference's FaerSolver tests (math_tests.rs:115-273) through the
+    SparseSolver mirror."""
+    s = api.SparseSolver()
+    assert not s.is_factorized()
+    s.factorize([0, 1, 2, 3], [0, 1, 2], [1.0, 1.0, 1.0], 3)
+    assert s.is_factorized()
+    assert np.abs(s.solve([3.0, 7.0, -2.0]) - [3.0, 7.0, -2.0]).max() < 1e-5
+    s = api.SparseSolver()
+    s.factorize([0, 2, 5, 7], [0, 1, 0, 1, 2, 1, 2], [4, 1, 1, 3, 1, 1, 2], 3)
+    x = s.solve([1.0, 2.0, 3.0])
+    A = np.array([[4, 1, 0], [1, 3, 1], [0, 1, 2]], np.float64)
+    assert np.abs(A @ x - [1, 2, 3]).max() < 1e-4
+    s = api.SparseSolver()
+    s.factorize([0, 1, 2, 3], [0, 1, 2], [2.0, 3.0, 5.0], 3)
+    assert np.abs(s.solve([4.0, 9.0, 25.0]) - [2, 3, 5]).max() < 1e-5
+    assert np.abs(s.solve([1.0, 1.0, 1.0]) - [0.5, 1 / 3, 0.2]).max() < 1e-5
+    n = 100
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        for j, v in ((i - 1, -1.0), (i, 2.1), (i + 1, -1.0)):
+            if 0 <= j < n:
+                rows.append(i); cols.append(j); vals.append(v)
+    rp = np.searchsorted(rows, np.arange(n + 1))
+    s = api.SparseSolver()
+    s.factorize(rp, cols, vals, n)
+    x = s.solve(np.ones(n))
+    A = np.zeros((n, n))
+    A[rows, cols] = vals
+    assert np.abs(A @ x - 1.0).max() < 1e-3
+    with pytest.raises(Exception):
+        api.SparseSolver().solve([1.0])
+
+
+def test_not_spd_is_reported():
+    s = api.SparseSolver()
+    with pytest.raises(api.L.VistioError) as e:
+        s.factorize([0, 1, 2], [0, 1], [1.0, -1.0], 2)
+    assert e.value.status == 11

@@ -1,0 +1,251 @@
+// sm_100a kernels of the IPC contact path: collider barriers (ground plane,
+// sphere), the CCD step bound, the line-search update and the
+// Augmented-Lagrangian bookkeeping of step_with_ipc
+// (crates/vistio-solver/src/pd_solver.rs:549-1157).
+#pragma once
+#include "pd_kernels.cuh"
+
+namespace vistio {
+
+// barrier_gradient (crates/vistio-contact/src/barrier.rs:35-46): squared
+// distances, FP64 inside as in the reference.
+__device__ __forceinline__ float barrier_grad_dev(float d, float d_hat) {
+  float dc = fminf(fmaxf(d, d_hat * 1e-3f), d_hat);
+  if (dc >= d_hat) return 0.f;
+  double d64 = dc, dh = d_hat, diff = d64 - dh;
+  double ln_ratio = log(d64 / dh);
+  return float(-(diff) * (2.0 * ln_ratio + diff / d64));
+}
+// scaled_barrier_gradient (barrier.rs:78-87)
+__device__ __forceinline__ float scaled_barrier_grad_dev(float d, float d_hat, float kappa) {
+  float r = kappa * barrier_grad_dev(d, d_hat);
+  if (isfinite(r)) return r;
+  return signbit(r) ? -1e6f : 1e6f;
+}
+
+__device__ __forceinline__ void warp_sum_u32(uint32_t& v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+}
+
+// Ground and sphere barriers of CollisionPipeline::detect_ipc_contacts
+// (collision_pipeline.rs:207-352, ground_plane.rs:68-109, sphere.rs:102-175).
+// mode 0: the detect at the start of an AL pass (writes grad / in_contact,
+//         records ever-in-contact normals, clears multipliers off contact);
+// mode 1: the re-detect after the inner loop (writes grad_up / in_contact_up,
+//         reduces active count and max violation).
+__global__ void __launch_bounds__(256) k_detect(BatchDev B, int mode) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  const StepParams& P = *B.prm;
+  InstRed& R = B.red[ch.x];
+  if (R.al_done) return;
+  const InstDev I = B.inst[ch.x];
+  uint32_t active = 0;
+  float viol = 0.f;
+  if ((int)threadIdx.x < ch.z) {
+    uint32_t g = uint32_t(ch.y) + threadIdx.x;
+    float4 x = B.pos[g];
+    float3 gr = make_float3(0.f, 0.f, 0.f);
+    if (P.self_collision)  // self-contact gradients were accumulated by k_self_grad before this kernel
+      gr = f3(mode == 0 ? B.grad[g] : B.grad_up[g]);
+    float3 n = make_float3(0.f, 0.f, 0.f);
+    bool inc = false;
+    if (P.self_collision) {
+      float gsq = dot3(gr, gr);
+      if (gsq > 1e-12f) { float gl = sqrtf(gsq); n = gr * (1.f / gl); inc = true; }
+    }
+    const float dh = P.d_hat, kap = P.kappa;
+    if (P.has_ground) {
+      float ds = x.y - P.ground_h;
+      if (ds <= 0.f) {
+        viol = fmaxf(viol, -ds);
+        float dc = fmaxf(-ds, 1e-6f);
+        active++;
+        gr.y += scaled_barrier_grad_dev(dc * dc, dh, kap) * 2.f * dc;
+      } else if (ds * ds < dh) {
+        active++;
+        gr.y += scaled_barrier_grad_dev(ds * ds, dh, kap) * 2.f * ds;
+      }
+      if (ds * ds < dh || ds <= 0.f) { n.y += 1.f; inc = true; }
+    }
+    if (P.has_sphere) {
+      float dx = x.x - P.sphere_c[0], dy = x.y - P.sphere_c[1], dz = x.z - P.sphere_c[2];
+      float r = sqrtf(dx * dx + dy * dy + dz * dz);
+      float ds = r - P.sphere_r;
+      if (ds <= 0.f) {
+        viol = fmaxf(viol, -ds);
+        float dc = fmaxf(-ds, 1e-6f);
+        active++;
+        float bg = scaled_barrier_grad_dev(dc * dc, dh, kap);
+        if (r > 1e-6f) {
+          float f = bg * 2.f * dc;
+          gr.x += f * (dx / r); gr.y += f * (dy / r); gr.z += f * (dz / r);
+        } else {
+          gr.y += bg * 2.f * dc;
+        }
+      } else if (ds * ds < dh) {
+        active++;
+        float f = scaled_barrier_grad_dev(ds * ds, dh, kap) * 2.f * ds;
+        gr.x += f * (dx / r); gr.y += f * (dy / r); gr.z += f * (dz / r);
+      }
+      if (ds * ds < dh || ds <= 0.f) {
+        if (r > 1e-6f) { n.x += dx / r; n.y += dy / r; n.z += dz / r; }
+        inc = true;
+      }
+    }
+    if (inc) {
+      float ls = dot3(n, n);
+      if (ls > 1e-12f) n = n * (1.f / sqrtf(ls));
+    }
+    float4 g4 = make_float4(gr.x, gr.y, gr.z, 0.f);
+    if (mode == 0) {
+      B.grad[g] = g4;
+      B.in_contact[g] = inc;
+      if (inc) { B.ever[g] = 1; B.fin_n[g] = make_float4(n.x, n.y, n.z, 0.f); }
+      else B.lam[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      B.grad_up[g] = g4;
+      B.in_contact_up[g] = inc;
+      if (inc) { B.ever[g] = 1; B.fin_n[g] = make_float4(n.x, n.y, n.z, 0.f); }
+    }
+  }
+  if (mode == 1) {
+    warp_sum_u32(active);
+    for (int o = 16; o > 0; o >>= 1) viol = fmaxf(viol, __shfl_down_sync(0xffffffffu, viol, o));
+    if ((threadIdx.x & 31) == 0) {
+      if (active) atomicAdd(&R.active, active);
+      if (viol > 0.f) atomicMax(&R.maxviol_bits, __float_as_uint(viol));
+    }
+  }
+  (void)I;
+}
+
+// CCD step bound for the colliders (ground_plane.rs:112-134, sphere.rs:178-224)
+// and the backtracking sum grad . d over free vertices (pd_solver.rs:915-925).
+__global__ void __launch_bounds__(256) k_ccd(BatchDev B) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  const StepParams& P = *B.prm;
+  InstRed& R = B.red[ch.x];
+  if (R.al_done) return;
+  const InstDev I = B.inst[ch.x];
+  float toi = 1.f;
+  double gdd = 0.0;
+  if ((int)threadIdx.x < ch.z) {
+    uint32_t g = uint32_t(ch.y) + threadIdx.x;
+    float4 x0 = B.pos[g];
+    float4 d = B.Y[I.vbase + B.perm_local[g]];
+    float3 x1 = make_float3(x0.x + d.x, x0.y + d.y, x0.z + d.z);
+    if (P.has_ground) {
+      float y0 = x0.y, y1 = x1.y, h = P.ground_h;
+      if (y0 > h && y1 < h) {
+        float t = (h - y0) / (y1 - y0);
+        if (t >= 0.f && t <= 1.f) toi = fminf(toi, t * 0.9f);
+      }
+    }
+    if (P.has_sphere) {
+      float r2 = P.sphere_r * P.sphere_r;
+      float px0 = x0.x - P.sphere_c[0], py0 = x0.y - P.sphere_c[1], pz0 = x0.z - P.sphere_c[2];
+      float px1 = x1.x - P.sphere_c[0], py1 = x1.y - P.sphere_c[1], pz1 = x1.z - P.sphere_c[2];
+      if (!(px0 * px0 + py0 * py0 + pz0 * pz0 < r2)) {
+        float vx = px1 - px0, vy = py1 - py0, vz = pz1 - pz0;
+        float a = vx * vx + vy * vy + vz * vz;
+        float b = 2.f * (px0 * vx + py0 * vy + pz0 * vz);
+        float c = px0 * px0 + py0 * py0 + pz0 * pz0 - r2;
+        if (a > 1e-8f) {
+          float disc = b * b - 4.f * a * c;
+          if (disc >= 0.f) {
+            float t = (-b - sqrtf(disc)) / (2.f * a);
+            if (t >= 0.f && t <= 1.f) toi = fminf(toi, t * 0.9f);
+          }
+        }
+      }
+    }
+    if (!B.pinned[g]) {
+      float4 gr = B.grad[g];
+      gdd = double(gr.x * d.x + gr.y * d.y + gr.z * d.z);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    toi = fminf(toi, __shfl_down_sync(0xffffffffu, toi, o));
+    gdd += __shfl_down_sync(0xffffffffu, gdd, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (toi < 1.f) atomicMin(&R.toi_bits, __float_as_uint(fmaxf(toi, 0.f)));
+    if (gdd != 0.0) atomicAdd(&R.gdd, gdd);
+  }
+}
+
+// Step-size selection (pd_solver.rs:896-932) and x <- x + alpha d on free vertices.
+__global__ void __launch_bounds__(256) k_ipc_update(BatchDev B) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  InstRed& R = B.red[ch.x];
+  if (R.al_done) return;
+  const InstDev I = B.inst[ch.x];
+  float max_alpha = fmaxf(__uint_as_float(R.toi_bits), 1e-6f);
+  if (max_alpha < 1.f) max_alpha *= 0.8f;
+  max_alpha = fminf(max_alpha, 1.f);
+  float alpha = max_alpha;
+  for (int bt = 0; bt < 4; ++bt) {
+    if (alpha < 0.1f) break;
+    if (R.gdd * double(R.mu) > double(1e-4f) * R.diff_sq * 100.0) alpha *= 0.5f;
+    else break;
+  }
+  if (threadIdx.x == 0 && ch.y == int(I.vbase)) R.alpha = alpha;
+  if ((int)threadIdx.x >= ch.z) return;
+  uint32_t g = uint32_t(ch.y) + threadIdx.x;
+  if (B.pinned[g]) return;
+  float4 d = B.Y[I.vbase + B.perm_local[g]];
+  float4 x = B.pos[g];
+  x.x += alpha * d.x; x.y += alpha * d.y; x.z += alpha * d.z;
+  B.pos[g] = x;
+}
+
+// Clears the re-detect reductions before the inner loop of an AL pass.
+__global__ void k_al_begin(BatchDev B, uint32_t ninst) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ninst) return;
+  InstRed& R = B.red[k];
+  if (R.al_done) return;
+  R.active = 0;
+  R.maxviol_bits = 0;
+}
+
+// lambda += mu * grad_up on re-detected contacts when the AL pass did not
+// converge (pd_solver.rs:1005-1018).
+__global__ void __launch_bounds__(256) k_al_end(BatchDev B) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  const StepParams& P = *B.prm;
+  InstRed& R = B.red[ch.x];
+  if (R.al_done) return;
+  if ((int)threadIdx.x >= ch.z) return;
+  if (__uint_as_float(R.maxviol_bits) < P.al_tolerance) return;
+  uint32_t g = uint32_t(ch.y) + threadIdx.x;
+  if (!B.in_contact_up[g]) return;
+  float4 gu = B.grad_up[g], la = B.lam[g];
+  float mu = R.mu;
+  la.x += mu * gu.x; la.y += mu * gu.y; la.z += mu * gu.z;
+  B.lam[g] = la;
+}
+
+// Per instance: count the pass, record the active contacts, stop or grow mu.
+__global__ void k_al_finish(BatchDev B, uint32_t ninst) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ninst) return;
+  const StepParams& P = *B.prm;
+  InstRed& R = B.red[k];
+  if (R.al_done) return;
+  R.al_iters += 1;
+  R.last_active = R.active;
+  if (__uint_as_float(R.maxviol_bits) < P.al_tolerance) R.al_done = 1;
+  else R.mu *= P.al_mu_growth;
+}
+
+// Zeroes the gradient accumulators before a detect (self-contact adds into them).
+__global__ void __launch_bounds__(256) k_clear_grad(BatchDev B, int mode) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  if (B.red[ch.x].al_done) return;
+  if ((int)threadIdx.x >= ch.z) return;
+  uint32_t g = uint32_t(ch.y) + threadIdx.x;
+  (mode == 0 ? B.grad : B.grad_up)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+}  // namespace vistio

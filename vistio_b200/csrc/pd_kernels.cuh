@@ -1,0 +1,561 @@
+// sm_100a kernels of the Projective Dynamics iteration.
+//
+// Layout (ragged SoA over every instance of a batch): per-vertex float4
+// (x, y, z, -) arrays indexed by a global vertex id; triangles and hinges
+// hold global vertex ids; each kernel over elements or vertices runs one
+// block per "chunk" (instance, first element, count <= blockDim) so a block
+// always sees a single instance and its constants.
+//
+// The iteration is written in delta form: with A the constant PD matrix
+// (M/h^2 + sum w S^T S + sum w_b L^T L) and b the reference's right-hand side
+// (assembly.rs:157-240), the solve computes d = A^-1 (b - A x) and sets
+// x <- x + d, which equals the reference's x <- A^-1 b in exact arithmetic.
+// b - A x collapses per element to w g_k . (F_target - F) for a triangle and
+// to w s_k s . (target - x) for a hinge, so the residual is formed from small
+// differences and FP32 sweeps lose accuracy relative to |d|, not to |x|.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vistio {
+
+struct InstDev {
+  uint32_t vbase, nv;
+  uint32_t lvl_base, nlvl;
+  int32_t model;
+  float warp, weft;
+  float inv_hmat2;   // 1 / matrix_dt^2
+  int32_t has_ground;
+  float ground_h;
+  uint32_t sn_base, nsn;
+};
+
+struct SnDev {
+  uint32_t first;    // first column (instance-local permuted row)
+  uint32_t ncols;
+  uint32_t nrows;
+  uint32_t rows_off; // into rows pool (instance-local rows)
+  uint64_t panel_off;
+  uint64_t diag_off;
+};
+
+// Per-step constants read from device memory so a captured graph stays valid
+// when dt or the contact set-up change.
+struct StepParams {
+  float dt, inv_dt2;
+  float gravity[3];
+  float damping;
+  float rayleigh;          // alpha_M
+  int32_t ipc;             // step_with_ipc semantics
+  // contact
+  int32_t has_ground;
+  float ground_h;
+  int32_t has_sphere;
+  float sphere_c[3];
+  float sphere_r;
+  int32_t self_collision;
+  float kappa;
+  float thickness;
+  float d_hat;             // effective (compliant) d_hat
+  float max_vel;           // velocity clamp (0 = off)
+  float al_tolerance, al_mu_growth, al_mu_initial;
+  float friction, contact_damping, contact_damping_max, contact_vthresh;
+  int32_t adaptive_damping;
+};
+
+// Per-instance device scalars of the IPC outer loop and reductions.
+struct InstRed {
+  double diff_sq, norm_sq;   // residual sums of the last solve
+  double gdd;                // sum over free vertices of grad . d
+  uint32_t toi_bits;         // min CCD time of impact (float bits, >= 0)
+  uint32_t active;           // active contacts of the last detect
+  uint32_t maxviol_bits;     // max violation (float bits)
+  uint32_t al_done;
+  float mu;
+  float alpha;
+  uint32_t last_active;      // active contacts of the last re-detect
+  uint32_t al_iters;
+  uint32_t iters;
+  uint32_t pad;
+};
+
+struct BatchDev {
+  const InstDev* inst;
+  const int4* tri_chunks;
+  const int4* hinge_chunks;
+  const int4* vtx_chunks;
+  // state
+  float4* pos;
+  float4* vel;
+  float4* prev;
+  float4* pred;
+  const float* mass;       // solver lumped masses (pinned = 1e8)
+  const uint8_t* pinned;
+  // elements
+  const uint4* tri_idx;    // global vertex ids
+  const float4* tri_dm;
+  const float* tri_w;
+  float* tri_out;          // 9 floats per triangle: the three vertex contributions
+  const uint4* hinge_idx;
+  const float4* hinge_st;
+  const float2* hinge_wr;  // (weight, rest angle)
+  float4* hinge_out;       // w * s . (target - x)
+  // vertex incidence (CSR over global vertex ids)
+  const uint32_t* vtri_ptr;
+  const uint32_t* vtri;    // (triangle << 2) | slot
+  const uint32_t* vhinge_ptr;
+  const uint32_t* vhinge;  // (hinge << 2) | slot
+  // solve
+  const uint32_t* perm_local;  // vertex -> instance-local permuted row
+  const uint32_t* row_vertex;  // global row -> instance-local vertex
+  float4* Y;               // rhs / y / delta, indexed by vbase + row
+  float4* T;               // scratch of the sweeps
+  const SnDev* sn;
+  const uint32_t* rows;
+  const float* vals;
+  const uint32_t* level_ptr;
+  const uint32_t* level_rows;
+  const uint32_t* row_sn;      // global row -> global supernode
+  const uint32_t* fwd_ptr;     // global row -> offsets
+  const uint2* fwd;            // (global supernode, panel row)
+  // contact / IPC
+  float4* grad;            // barrier gradient of the detect at the start of the AL pass
+  float4* grad_up;         // gradient of the re-detect
+  float4* lam;             // AL multipliers
+  float4* fin_n;           // final contact normal (ever in contact)
+  uint8_t* in_contact;     // of the detect at the start of the AL pass
+  uint8_t* in_contact_up;  // of the re-detect
+  uint8_t* ever;
+  InstRed* red;
+  const StepParams* prm;
+  uint32_t* status;        // bit 0: non-finite state
+};
+
+// ------------------------------------------------------------ math helpers
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float len3(float3 a) { return sqrtf(dot3(a, a)); }
+
+struct M32 { float3 c0, c1; };
+
+__device__ __forceinline__ M32 mul2(const M32& f, float a, float b, float c, float d) {
+  // f * [[a, c], [b, d]] (column-major [a, b, c, d], mat3x2.rs:62)
+  M32 r;
+  r.c0 = f.c0 * a + f.c1 * b;
+  r.c1 = f.c0 * c + f.c1 * d;
+  return r;
+}
+
+// polar_decomposition_3x2 (crates/vistio-math/src/decomposition.rs:76-138).
+struct PolarD {
+  M32 rot;
+  float s0, s1;
+  float2 v0, v1;
+};
+__device__ __forceinline__ PolarD polar_dev(const M32& f) {
+  float a = dot3(f.c0, f.c0), b = dot3(f.c0, f.c1), d = dot3(f.c1, f.c1);
+  float ht = 0.5f * (a + d), hd = 0.5f * (a - d);
+  float disc = sqrtf(hd * hd + b * b);
+  float l0 = fmaxf(ht + disc, 0.f), l1 = fmaxf(ht - disc, 0.f);
+  float s0 = sqrtf(l0), s1 = sqrtf(l1);
+  const float eps = 1.0e-10f;
+  PolarD p;
+  if (s0 < eps) {
+    p.rot.c0 = make_float3(1.f, 0.f, 0.f);
+    p.rot.c1 = make_float3(0.f, 1.f, 0.f);
+    p.s0 = p.s1 = 0.f;
+    p.v0 = make_float2(1.f, 0.f);
+    p.v1 = make_float2(0.f, 1.f);
+    return p;
+  }
+  float2 v0, v1;
+  if (fabsf(b) > eps) {
+    float vx = l0 - d, vy = b;
+    float r = 1.f / sqrtf(vx * vx + vy * vy);
+    v0 = make_float2(vx * r, vy * r);
+    v1 = make_float2(-v0.y, v0.x);
+  } else if (a >= d) {
+    v0 = make_float2(1.f, 0.f); v1 = make_float2(0.f, 1.f);
+  } else {
+    v0 = make_float2(0.f, 1.f); v1 = make_float2(1.f, 0.f);
+  }
+  float is0 = 1.f / s0, is1 = s1 > eps ? 1.f / s1 : 0.f;
+  float si00 = v0.x * v0.x * is0 + v1.x * v1.x * is1;
+  float si01 = v0.x * v0.y * is0 + v1.x * v1.y * is1;
+  float si11 = v0.y * v0.y * is0 + v1.y * v1.y * is1;
+  p.rot = mul2(f, si00, si01, si01, si11);
+  p.s0 = s0; p.s1 = s1; p.v0 = v0; p.v1 = v1;
+  return p;
+}
+
+// Target deformation gradient of the membrane model
+// (element.rs:127-174 and crates/vistio-material/src/*.rs).
+__device__ __forceinline__ M32 model_target(int model, const M32& F, float warp, float weft) {
+  if (model == 4) {  // IsotropicLinearModel: identity (isotropic.rs:42-57)
+    M32 r; r.c0 = make_float3(1.f, 0.f, 0.f); r.c1 = make_float3(0.f, 1.f, 0.f); return r;
+  }
+  PolarD p = polar_dev(F);
+  if (model == 0) return p.rot;  // ARAP: R
+  float s0t, s1t;
+  if (model == 1) {  // co-rotational, tension field: min(sigma, 1) (decomposition.rs:50-66)
+    s0t = fminf(p.s0, 1.f); s1t = fminf(p.s1, 1.f);
+  } else if (model == 2) {  // orthotropic (orthotropic.rs:51-79)
+    float mk = fmaxf(fmaxf(warp, weft), 1e-6f);
+    float kw = warp / mk, kf = weft / mk;
+    s0t = p.s0 + (1.f - p.s0) * kw;
+    s1t = p.s1 + (1.f - p.s1) * kf;
+  } else {  // anisotropic co-rotational (anisotropic.rs:78-143)
+    float kw = fminf(fmaxf(warp, 0.f), 1.f), kf = fminf(fmaxf(weft, 0.f), 1.f);
+    float cos2 = p.v0.x * p.v0.x, sin2 = p.v0.y * p.v0.y;
+    float k0 = kw * cos2 + kf * sin2, k1 = kw * sin2 + kf * cos2;
+    s0t = p.s0 > 1.f ? 1.f + (p.s0 - 1.f) * (1.f - k0) : p.s0;
+    s1t = p.s1 > 1.f ? 1.f + (p.s1 - 1.f) * (1.f - k1) : p.s1;
+  }
+  float t00 = p.v0.x * p.v0.x * s0t + p.v1.x * p.v1.x * s1t;
+  float t01 = p.v0.x * p.v0.y * s0t + p.v1.x * p.v1.y * s1t;
+  float t11 = p.v0.y * p.v0.y * s0t + p.v1.y * p.v1.y * s1t;
+  return mul2(p.rot, t00, t01, t01, t11);
+}
+
+// ------------------------------------------------------------- kernels
+// Local membrane step: per triangle, w * g_k . (F_target - F) for k = 0..2.
+__global__ void __launch_bounds__(256) k_tri(BatchDev B) {
+  int4 ch = B.tri_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  uint32_t t = uint32_t(ch.y) + threadIdx.x;
+  const InstDev I = B.inst[ch.x];
+  uint4 id = B.tri_idx[t];
+  float4 dm = B.tri_dm[t];
+  float w = B.tri_w[t];
+  float3 p0 = f3(B.pos[id.x]), p1 = f3(B.pos[id.y]), p2 = f3(B.pos[id.z]);
+  M32 ds; ds.c0 = p1 - p0; ds.c1 = p2 - p0;
+  M32 F = mul2(ds, dm.x, dm.y, dm.z, dm.w);
+  float det = dm.x * dm.w - dm.y * dm.z;
+  float3 d0 = make_float3(0.f, 0.f, 0.f), d1 = d0;
+  if (fabsf(det) > 1e-12f) {  // element.rs:192-202: degenerate rest shape keeps p
+    M32 Ft = model_target(I.model, F, I.warp, I.weft);
+    d0 = (Ft.c0 - F.c0) * w;
+    d1 = (Ft.c1 - F.c1) * w;
+  }
+  // g = [[-(a+b), -(c+d)], [a, c], [b, d]] (assembly.rs:77-81)
+  float g00 = -(dm.x + dm.y), g01 = -(dm.z + dm.w);
+  float3 c0 = d0 * g00 + d1 * g01;
+  float3 c1 = d0 * dm.x + d1 * dm.z;
+  float3 c2 = d0 * dm.y + d1 * dm.w;
+  float* o = B.tri_out + 9ull * t;
+  o[0] = c0.x; o[1] = c0.y; o[2] = c0.z;
+  o[3] = c1.x; o[4] = c1.y; o[5] = c1.z;
+  o[6] = c2.x; o[7] = c2.y; o[8] = c2.z;
+}
+
+// Rotation of v = p - centre about `axis` by angle minus v itself:
+// (axis (axis . v) - v)(1 - cos) + (axis x v) sin (bending.rs:231-239).
+__device__ __forceinline__ float3 rot_delta(float3 v, float3 axis, float ang) {
+  float s = sinf(ang);
+  float h = sinf(0.5f * ang);
+  float omc = 2.f * h * h;  // 1 - cos, without cancellation
+  float dt = dot3(axis, v);
+  return (axis * dt - v) * omc + cross3(axis, v) * s;
+}
+
+// Local bending step: per hinge, w * s . (target - x); only the wings move
+// (bending.rs:182-227, discrete_shells.rs:285-337).
+__global__ void __launch_bounds__(256) k_hinge(BatchDev B) {
+  int4 ch = B.hinge_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  uint32_t h = uint32_t(ch.y) + threadIdx.x;
+  uint4 id = B.hinge_idx[h];
+  float4 st = B.hinge_st[h];
+  float2 wr = B.hinge_wr[h];
+  float3 p0 = f3(B.pos[id.x]), p1 = f3(B.pos[id.y]), pa = f3(B.pos[id.z]), pb = f3(B.pos[id.w]);
+  float3 out = make_float3(0.f, 0.f, 0.f);
+  float3 e = p1 - p0;
+  float el = len3(e);
+  if (el >= 1e-10f) {
+    float3 ed = e * (1.f / el);
+    float3 ta = pa - p0, tb = pb - p0;
+    float3 qa = ta - ed * dot3(ta, ed), qb = tb - ed * dot3(tb, ed);
+    float la = len3(qa), lb = len3(qb);
+    const float PI = 3.14159265358979323846f;
+    float ang = PI;
+    if (la >= 1e-10f && lb >= 1e-10f) {
+      float c = dot3(qa * (1.f / la), qb * (1.f / lb));
+      ang = acosf(fminf(fmaxf(c, -1.f), 1.f));
+    }
+    float diff = ang - wr.y;
+    if (fabsf(diff) >= 1e-8f) {
+      float sign = dot3(cross3(qa, qb), ed) >= 0.f ? 1.f : -1.f;
+      float half = diff * 0.5f * sign;
+      float3 mid = (p0 + p1) * 0.5f;
+      float3 da = rot_delta(pa - mid, ed, half);
+      float3 db = rot_delta(pb - mid, ed, -half);
+      out = (da * st.z + db * st.w) * wr.x;
+    }
+  }
+  B.hinge_out[h] = make_float4(out.x, out.y, out.z, 0.f);
+}
+
+// Residual gather: r_i = m_i (pred_i / dt^2 - x_i / h^2) + sum of element
+// terms [- (mu grad_i + lambda_i)], written in solve (permuted) order.
+__global__ void __launch_bounds__(256) k_gather(BatchDev B) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  const InstDev I = B.inst[ch.x];
+  uint32_t g = uint32_t(ch.y) + threadIdx.x;
+  const StepParams& P = *B.prm;
+  InstRed& R = B.red[ch.x];
+  if (P.ipc && R.al_done) return;
+  float m = B.mass[g];
+  float3 x = f3(B.pos[g]), q = f3(B.pred[g]);
+  float cm = m * I.inv_hmat2, cr = m * P.inv_dt2;
+  float3 r = (q - x) * cm + q * (cr - cm);
+  for (uint32_t e = B.vtri_ptr[g], ee = B.vtri_ptr[g + 1]; e < ee; ++e) {
+    uint32_t code = B.vtri[e];
+    const float* o = B.tri_out + 9ull * (code >> 2) + 3 * (code & 3u);
+    r.x += o[0]; r.y += o[1]; r.z += o[2];
+  }
+  for (uint32_t e = B.vhinge_ptr[g], ee = B.vhinge_ptr[g + 1]; e < ee; ++e) {
+    uint32_t code = B.vhinge[e];
+    uint32_t h = code >> 2, k = code & 3u;
+    float4 st = B.hinge_st[h];
+    float s = k == 0 ? st.x : k == 1 ? st.y : k == 2 ? st.z : st.w;
+    float4 o = B.hinge_out[h];
+    r.x += s * o.x; r.y += s * o.y; r.z += s * o.z;
+  }
+  if (P.ipc) {  // assemble_barrier_rhs (assembly.rs:272-282)
+    float mu = R.mu;
+    float4 gr = B.grad[g], la = B.lam[g];
+    r.x -= mu * gr.x + la.x; r.y -= mu * gr.y + la.y; r.z -= mu * gr.z + la.z;
+  }
+  B.Y[I.vbase + B.perm_local[g]] = make_float4(r.x, r.y, r.z, 0.f);
+}
+
+__device__ __forceinline__ void f4_fms(float4& t, float a, float4 y) {
+  t.x -= a * y.x; t.y -= a * y.y; t.z -= a * y.z;
+}
+
+// Supernodal forward + back substitution for one instance per block, on
+// P A P^T = L L^T with inv(L_kk) stored per supernode; then (plain step) the
+// position update, pin reset, ground clamp and residual sums.
+// Levels of the supernodal elimination tree are separated by __syncthreads.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
+  const uint32_t inst = blockIdx.x;
+  const InstDev I = B.inst[inst];
+  const StepParams& P = *B.prm;
+  InstRed& R = B.red[inst];
+  if (P.ipc && R.al_done) return;
+  const uint32_t vb = I.vbase;
+  float4* Y = B.Y + vb;
+  float4* T = B.T + vb;
+  const uint32_t* lp = B.level_ptr + I.lvl_base;
+  // forward: y = L^-1 r
+  for (uint32_t l = 0; l < I.nlvl; ++l) {
+    uint32_t b = lp[l], e = lp[l + 1];
+    for (uint32_t i = b + threadIdx.x; i < e; i += NT) {
+      uint32_t r = B.level_rows[i];
+      uint32_t g = vb + r;
+      float4 t = Y[r];
+      for (uint32_t q = B.fwd_ptr[g], qe = B.fwd_ptr[g + 1]; q < qe; ++q) {
+        uint2 f = B.fwd[q];
+        SnDev S = B.sn[f.x];
+        const float* pr = B.vals + S.panel_off + uint64_t(f.y) * S.ncols;
+        const float4* yy = Y + S.first;
+        for (uint32_t c = 0; c < S.ncols; ++c) f4_fms(t, pr[c], yy[c]);
+      }
+      T[r] = t;
+    }
+    __syncthreads();
+    for (uint32_t i = b + threadIdx.x; i < e; i += NT) {
+      uint32_t r = B.level_rows[i];
+      SnDev S = B.sn[B.row_sn[vb + r]];
+      uint32_t c = r - S.first, s = S.ncols;
+      const float* D = B.vals + S.diag_off;
+      float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (uint32_t c2 = 0; c2 <= c; ++c2) {
+        float a = D[uint64_t(c2) * s + c];
+        float4 tt = T[S.first + c2];
+        y.x += a * tt.x; y.y += a * tt.y; y.z += a * tt.z;
+      }
+      Y[r] = y;
+    }
+    __syncthreads();
+  }
+  // backward: d = L^-T y
+  for (int l = int(I.nlvl) - 1; l >= 0; --l) {
+    uint32_t b = lp[l], e = lp[l + 1];
+    for (uint32_t i = b + threadIdx.x; i < e; i += NT) {
+      uint32_t r = B.level_rows[i];
+      SnDev S = B.sn[B.row_sn[vb + r]];
+      uint32_t c = r - S.first, s = S.ncols;
+      float4 t = Y[r];
+      const float* pc = B.vals + S.panel_off + c;
+      const uint32_t* rr = B.rows + S.rows_off;
+      for (uint32_t j = 0; j < S.nrows; ++j) f4_fms(t, pc[uint64_t(j) * s], Y[rr[j]]);
+      T[r] = t;
+    }
+    __syncthreads();
+    for (uint32_t i = b + threadIdx.x; i < e; i += NT) {
+      uint32_t r = B.level_rows[i];
+      SnDev S = B.sn[B.row_sn[vb + r]];
+      uint32_t c = r - S.first, s = S.ncols;
+      const float* D = B.vals + S.diag_off + uint64_t(c) * s;
+      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (uint32_t c2 = c; c2 < s; ++c2) {
+        float a = D[c2];
+        float4 tt = T[S.first + c2];
+        x.x += a * tt.x; x.y += a * tt.y; x.z += a * tt.z;
+      }
+      Y[r] = x;
+    }
+    __syncthreads();
+  }
+  // residual sums (pd_solver.rs:403-421) and, for the plain step, the update.
+  double dsq = 0.0, nsq = 0.0;
+  bool bad = false;
+  for (uint32_t v = threadIdx.x; v < I.nv; v += NT) {
+    uint32_t g = vb + v;
+    float4 d = Y[B.perm_local[g]];
+    float4 x = B.pos[g];
+    dsq += double(d.x) * d.x + double(d.y) * d.y + double(d.z) * d.z;
+    nsq += double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z;
+    if (!(isfinite(d.x) && isfinite(d.y) && isfinite(d.z))) bad = true;
+    if (do_update) {
+      float4 nx;
+      if (B.pinned[g]) nx = B.prev[g];
+      else {
+        nx = make_float4(x.x + d.x, x.y + d.y, x.z + d.z, 0.f);
+        if (I.has_ground && nx.y < I.ground_h) nx.y = I.ground_h;  // state.rs:180-189
+      }
+      B.pos[g] = nx;
+    }
+  }
+  __shared__ double s_a[NT / 32], s_b[NT / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    dsq += __shfl_down_sync(0xffffffffu, dsq, o);
+    nsq += __shfl_down_sync(0xffffffffu, nsq, o);
+  }
+  if ((threadIdx.x & 31) == 0) { s_a[threadIdx.x >> 5] = dsq; s_b[threadIdx.x >> 5] = nsq; }
+  if (bad) atomicOr(B.status, 1u);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, bb = 0.0;
+    for (int k = 0; k < NT / 32; ++k) { a += s_a[k]; bb += s_b[k]; }
+    R.diff_sq = a;
+    R.norm_sq = bb;
+    R.iters += 1;
+    // reset the per-iteration reductions of the IPC line search
+    R.toi_bits = __float_as_uint(1.0f);
+    R.gdd = 0.0;
+  }
+}
+
+// save_previous + (IPC) velocity clamp + predict + x <- pred (state.rs:145-169,
+// pd_solver.rs:273-283 and 566-603).
+__global__ void __launch_bounds__(256) k_predict(BatchDev B) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  const InstDev I = B.inst[ch.x];
+  const StepParams& P = *B.prm;
+  if (threadIdx.x == 0 && ch.y == int(I.vbase)) {
+    InstRed& R = B.red[ch.x];
+    R.iters = 0;
+    R.al_iters = 0;
+    R.al_done = 0;
+    R.mu = P.al_mu_initial;
+    R.last_active = 0;
+    R.alpha = 1.f;
+  }
+  if ((int)threadIdx.x >= ch.z) return;
+  uint32_t g = uint32_t(ch.y) + threadIdx.x;
+  float4 x = B.pos[g];
+  float4 v = B.vel[g];
+  B.prev[g] = x;
+  bool pin = B.pinned[g] != 0;
+  bool ground = P.ipc ? P.has_ground : I.has_ground;
+  float gh = P.ipc ? P.ground_h : I.ground_h;
+  if (P.ipc) {
+    if (!pin && P.max_vel > 0.f) {
+      float vsq = v.x * v.x + v.y * v.y + v.z * v.z;
+      if (vsq > P.max_vel * P.max_vel) {
+        float sc = P.max_vel / sqrtf(vsq);
+        v.x *= sc; v.y *= sc; v.z *= sc;
+        B.vel[g] = v;
+      }
+    }
+    B.ever[g] = 0;
+    B.fin_n[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  float4 q = x;
+  if (!pin) {
+    float dt = P.dt, dt2 = dt * dt;
+    q.x = x.x + dt * v.x + dt2 * P.gravity[0];
+    q.y = x.y + dt * v.y + dt2 * P.gravity[1];
+    q.z = x.z + dt * v.z + dt2 * P.gravity[2];
+    if (ground && q.y < gh) q.y = gh;
+  }
+  B.pred[g] = q;
+  B.pos[g] = q;
+}
+
+// update_velocities, (IPC) inelastic velocity filter, ground velocities,
+// damping and Rayleigh damping (pd_solver.rs:447-466 and 1027-1147).
+__global__ void __launch_bounds__(256) k_finalize(BatchDev B) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  const InstDev I = B.inst[ch.x];
+  const StepParams& P = *B.prm;
+  uint32_t g = uint32_t(ch.y) + threadIdx.x;
+  float4 x = B.pos[g], pv = B.prev[g];
+  float inv_dt = 1.f / P.dt;
+  float3 v = make_float3((x.x - pv.x) * inv_dt, (x.y - pv.y) * inv_dt, (x.z - pv.z) * inv_dt);
+  bool pin = B.pinned[g] != 0;
+  bool ground = P.ipc ? P.has_ground : I.has_ground;
+  float gh = P.ipc ? P.ground_h : I.ground_h;
+  if (P.ipc) {
+    const InstRed& R = B.red[ch.x];
+    if (!pin && B.ever[g]) {
+      float4 n4 = B.fin_n[g];
+      float3 n = f3(n4);
+      if (dot3(n, n) >= 0.5f) {
+        float vdn = dot3(v, n);
+        v = v - n * vdn;
+        float vn = fabsf(vdn);
+        float vt = len3(v);
+        if (vt > 1e-8f) {
+          float fi = P.friction * vn;
+          if (fi >= vt) v = make_float3(0.f, 0.f, 0.f);
+          else v = v * (1.f - fi / vt);
+        }
+        float cd = P.contact_damping;
+        if (P.adaptive_damping) {
+          float vm = len3(v);
+          float tt = fminf(fmaxf(1.f - vm / fmaxf(P.contact_vthresh, 1e-6f), 0.f), 1.f);
+          float ad = cd + tt * (P.contact_damping_max - cd);
+          v = v * (1.f - ad);
+        } else {
+          v = v * (1.f - cd);
+        }
+      }
+    }
+    if (R.last_active > 0) v = v * (1.f - 0.05f);
+  }
+  if (ground && !pin && x.y <= gh) {  // state.rs:195-213
+    if (v.y < 0.f) v.y = 0.f;
+    pv.y = gh;
+    B.prev[g] = pv;
+    v.x *= 0.5f; v.z *= 0.5f;
+  }
+  v = v * (1.f - P.damping);
+  if (P.rayleigh > 0.f && !pin) v = v * (1.f / (1.f + P.rayleigh * P.dt));
+  B.vel[g] = make_float4(v.x, v.y, v.z, 0.f);
+}
+
+}  // namespace vistio

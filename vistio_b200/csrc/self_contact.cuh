@@ -1,0 +1,581 @@
+// sm_100a self-contact path of the IPC step: triangle broad phase, the
+// vertex-triangle / edge-edge barrier gradients and vertex-triangle CCD.
+//
+// Broad phase. The reference rebuilds a median-split BVH every tenth update
+// and refits it otherwise (crates/vistio-contact/src/bvh.rs:122-373). Here
+// each garment's triangles, in mesh index order, are the leaves of an
+// implicit balanced binary tree: node (l, i) bounds leaves [i 2^l, (i+1) 2^l).
+// Mesh order keeps every subtree an intrinsically compact patch of cloth, so
+// the tree stays tight when the cloth folds, and a refit is all a detect
+// needs. A node's leaf range is known from its position, so the traversal
+// for leaf i skips every subtree whose leaves are all <= i and emits exactly
+// the pairs (i < j) whose inflated AABBs overlap: the complete candidate set,
+// independent of tree shape. Pairs are produced in a count / scan / write
+// sequence so their order (and every sum over them) is deterministic.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "contact_kernels.cuh"
+#include "../../include/vistio_cuda.h"
+
+struct vistio_solver;
+
+namespace vistio {
+
+struct SelfInst {
+  uint32_t tbase, nt;      // global triangle range
+  uint32_t box_base;       // first box of this garment's tree
+  uint32_t nlevels;        // tree levels including the leaf level
+  uint32_t lvl_off[28];    // box offset of each level relative to box_base
+  uint32_t lvl_cnt[28];    // boxes on each level
+};
+
+struct SelfContactDev {
+  bool ready = false;
+  uint32_t ninst = 0;
+  uint64_t T = 0;
+  uint64_t pair_cap = 0;
+  SelfInst* inst = nullptr;      // per garment
+  uint32_t* tri_inst = nullptr;  // triangle -> garment
+  float4* box_min = nullptr;     // all tree levels
+  float4* box_max = nullptr;
+  uint32_t* cnt = nullptr;       // per triangle pair counts, then exclusive offsets
+  uint32_t* block_sums = nullptr;
+  uint2* pairs = nullptr;        // global (ta, tb)
+  uint32_t* npairs = nullptr;    // [0] pair count, [1] overflow flag
+  uint32_t* adj_ptr = nullptr;   // 1-ring exclusion lists (sorted, include the vertex itself)
+  uint32_t* adj = nullptr;
+  uint32_t scan_blocks = 0;
+  void release() {
+    cudaFree(inst); cudaFree(tri_inst); cudaFree(box_min); cudaFree(box_max); cudaFree(cnt);
+    cudaFree(block_sums); cudaFree(pairs); cudaFree(npairs); cudaFree(adj_ptr); cudaFree(adj);
+    inst = nullptr; tri_inst = nullptr; box_min = box_max = nullptr; cnt = block_sums = nullptr;
+    pairs = nullptr; npairs = nullptr; adj_ptr = adj = nullptr; ready = false;
+  }
+  ~SelfContactDev() { release(); }
+};
+
+constexpr int kScanBlock = 1024;
+
+// ---------------------------------------------------------------- trees
+// Leaf boxes (bvh.rs:29-43, inflated by the margin) and the level-by-level
+// refit, one block per garment.
+__global__ void __launch_bounds__(1024) k_self_boxes(BatchDev B, SelfContactDev S, float margin_arg) {
+  const SelfInst I = S.inst[blockIdx.x];
+  if (B.prm->ipc && B.red[blockIdx.x].al_done) return;
+  const float margin = margin_arg >= 0.f ? margin_arg : B.prm->thickness;
+  float4* mn = S.box_min + I.box_base;
+  float4* mx = S.box_max + I.box_base;
+  for (uint32_t i = threadIdx.x; i < I.nt; i += blockDim.x) {
+    uint4 id = B.tri_idx[I.tbase + i];
+    float4 a = B.pos[id.x], b = B.pos[id.y], c = B.pos[id.z];
+    mn[i] = make_float4(fminf(fminf(a.x, b.x), c.x) - margin, fminf(fminf(a.y, b.y), c.y) - margin,
+                        fminf(fminf(a.z, b.z), c.z) - margin, 0.f);
+    mx[i] = make_float4(fmaxf(fmaxf(a.x, b.x), c.x) + margin, fmaxf(fmaxf(a.y, b.y), c.y) + margin,
+                        fmaxf(fmaxf(a.z, b.z), c.z) + margin, 0.f);
+  }
+  __syncthreads();
+  for (uint32_t l = 1; l < I.nlevels; ++l) {
+    uint32_t n = I.lvl_cnt[l], nprev = I.lvl_cnt[l - 1];
+    const float4* cmn = mn + I.lvl_off[l - 1];
+    const float4* cmx = mx + I.lvl_off[l - 1];
+    float4* pmn = mn + I.lvl_off[l];
+    float4* pmx = mx + I.lvl_off[l];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      float4 a0 = cmn[2 * i], a1 = cmx[2 * i];
+      if (2 * i + 1 < nprev) {
+        float4 b0 = cmn[2 * i + 1], b1 = cmx[2 * i + 1];
+        a0 = make_float4(fminf(a0.x, b0.x), fminf(a0.y, b0.y), fminf(a0.z, b0.z), 0.f);
+        a1 = make_float4(fmaxf(a1.x, b1.x), fmaxf(a1.y, b1.y), fmaxf(a1.z, b1.z), 0.f);
+      }
+      pmn[i] = a0;
+      pmx[i] = a1;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ bool box_overlap(float4 amn, float4 amx, float4 bmn, float4 bmx) {  // bvh.rs:58
+  return amn.x <= bmx.x && amx.x >= bmn.x && amn.y <= bmx.y && amx.y >= bmn.y && amn.z <= bmx.z && amx.z >= bmn.z;
+}
+
+// Traversal for leaf i: visits subtrees holding leaves > i whose boxes overlap.
+// mode 0 counts, mode 1 writes at the scanned offset.
+template <int MODE>
+__device__ void self_traverse(const SelfContactDev& S, const SelfInst& I, uint32_t i, uint32_t* count_out,
+                              uint2* out, uint32_t cap) {
+  const float4* mn = S.box_min + I.box_base;
+  const float4* mx = S.box_max + I.box_base;
+  float4 qmn = mn[i], qmx = mx[i];
+  uint32_t stack[64];
+  int sp = 0;
+  stack[sp++] = ((I.nlevels - 1) << 26) | 0u;  // (level, index) packed; index < 2^26
+  uint32_t found = 0;
+  uint32_t base = MODE == 1 ? *count_out : 0;
+  while (sp > 0) {
+    uint32_t code = stack[--sp];
+    uint32_t l = code >> 26, k = code & ((1u << 26) - 1);
+    uint64_t hi = (uint64_t(k) + 1) << l;  // one past the last leaf of the node
+    if (hi <= uint64_t(i) + 1) continue;
+    uint32_t o = I.lvl_off[l] + k;
+    if (!box_overlap(qmn, qmx, mn[o], mx[o])) continue;
+    if (l == 0) {
+      if (MODE == 1) {
+        uint32_t slot = base + found;
+        if (slot < cap) out[slot] = make_uint2(I.tbase + i, I.tbase + k);
+      }
+      ++found;
+      continue;
+    }
+    // children (l-1, 2k) and (l-1, 2k+1); the right child may not exist.
+    // The stack never holds more than two entries per level (< 64).
+    if (2 * k + 1 < I.lvl_cnt[l - 1]) stack[sp++] = ((l - 1) << 26) | (2 * k + 1);
+    stack[sp++] = ((l - 1) << 26) | (2 * k);
+  }
+  if (MODE == 0) *count_out = found;
+}
+
+__global__ void __launch_bounds__(256) k_self_count(BatchDev B, SelfContactDev S) {
+  int4 ch = B.tri_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) { S.cnt[ch.y + threadIdx.x] = 0; return; }
+  const SelfInst I = S.inst[ch.x];
+  uint32_t t = uint32_t(ch.y) + threadIdx.x;
+  uint32_t c = 0;
+  self_traverse<0>(S, I, t - I.tbase, &c, nullptr, 0);
+  S.cnt[t] = c;
+}
+
+// Exclusive scan of the per-triangle counts (three phases).
+__global__ void __launch_bounds__(kScanBlock) k_scan_local(uint32_t* v, uint32_t n, uint32_t* block_sums) {
+  __shared__ uint32_t sh[kScanBlock];
+  uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+  uint32_t x = i < n ? v[i] : 0u;
+  sh[threadIdx.x] = x;
+  __syncthreads();
+  for (int o = 1; o < kScanBlock; o <<= 1) {
+    uint32_t y = threadIdx.x >= uint32_t(o) ? sh[threadIdx.x - o] : 0u;
+    __syncthreads();
+    sh[threadIdx.x] += y;
+    __syncthreads();
+  }
+  if (i < n) v[i] = sh[threadIdx.x] - x;
+  if (threadIdx.x == kScanBlock - 1) block_sums[blockIdx.x] = sh[threadIdx.x];
+}
+__global__ void __launch_bounds__(kScanBlock) k_scan_sums(uint32_t* block_sums, uint32_t nb, uint32_t* total) {
+  __shared__ uint32_t sh[kScanBlock];
+  uint32_t carry = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += kScanBlock) {
+    uint32_t i = b0 + threadIdx.x;
+    uint32_t x = i < nb ? block_sums[i] : 0u;
+    sh[threadIdx.x] = x;
+    __syncthreads();
+    for (int o = 1; o < kScanBlock; o <<= 1) {
+      uint32_t y = threadIdx.x >= uint32_t(o) ? sh[threadIdx.x - o] : 0u;
+      __syncthreads();
+      sh[threadIdx.x] += y;
+      __syncthreads();
+    }
+    if (i < nb) block_sums[i] = carry + sh[threadIdx.x] - x;
+    uint32_t last = sh[kScanBlock - 1];
+    __syncthreads();
+    carry += last;
+  }
+  if (threadIdx.x == 0) total[0] = carry;
+}
+__global__ void __launch_bounds__(kScanBlock) k_scan_add(uint32_t* v, uint32_t n, const uint32_t* block_sums) {
+  uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+  if (i < n) v[i] += block_sums[blockIdx.x];
+}
+
+__global__ void __launch_bounds__(256) k_self_write(BatchDev B, SelfContactDev S) {
+  int4 ch = B.tri_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  const SelfInst I = S.inst[ch.x];
+  uint32_t t = uint32_t(ch.y) + threadIdx.x;
+  uint32_t off = S.cnt[t];
+  self_traverse<1>(S, I, t - I.tbase, &off, S.pairs, uint32_t(S.pair_cap));
+  if (threadIdx.x == 0 && S.npairs[0] > S.pair_cap) {
+    S.npairs[1] = 1;
+    atomicOr(B.status, 2u);  // candidate pairs exceeded the buffer
+  }
+}
+
+// ------------------------------------------------- distance primitives
+// crates/vistio-contact/src/distance_primitives.rs (FP32 like the reference).
+template <class R> struct V3d { R x, y, z; };
+template <class R> __device__ __forceinline__ V3d<R> mk(R a, R b, R c) { return {a, b, c}; }
+template <class R> __device__ __forceinline__ V3d<R> vsub(V3d<R> a, V3d<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class R> __device__ __forceinline__ V3d<R> vadd(V3d<R> a, V3d<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class R> __device__ __forceinline__ V3d<R> vmul(V3d<R> a, R s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class R> __device__ __forceinline__ R vdot(V3d<R> a, V3d<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R> __device__ __forceinline__ V3d<R> vcross(V3d<R> a, V3d<R> b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class R> __device__ __forceinline__ R rclampd(R v, R lo, R hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ V3d<float> ld3(const float4* p, uint32_t i) { float4 a = p[i]; return {a.x, a.y, a.z}; }
+
+__device__ float pt_seg_d2(V3d<float> p, V3d<float> a, V3d<float> b) {  // :308-318
+  V3d<float> ab = vsub(b, a), ap = vsub(p, a);
+  float ab2 = vdot(ab, ab);
+  if (ab2 < 1e-20f) return vdot(ap, ap);
+  float t = rclampd(vdot(ap, ab) / ab2, 0.f, 1.f);
+  V3d<float> c = vadd(a, vmul(ab, t));
+  V3d<float> d = vsub(p, c);
+  return vdot(d, d);
+}
+
+__device__ float pt_d2(V3d<float> p, V3d<float> a, V3d<float> b, V3d<float> c) {  // :36-116
+  V3d<float> ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a), bp = vsub(p, b), cp = vsub(p, c);
+  V3d<float> nrm = vcross(ab, ac);
+  if (vdot(nrm, nrm) < 1e-20f) {
+    float dab = pt_seg_d2(p, a, b), dbc = pt_seg_d2(p, b, c), dca = pt_seg_d2(p, c, a);
+    if (dab <= dbc && dab <= dca) return dab;
+    if (dbc <= dca) return dbc;
+    return dca;
+  }
+  float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+  if (d1 <= 0.f && d2 <= 0.f) return vdot(ap, ap);
+  float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+  if (d3 >= 0.f && d4 <= d3) return vdot(bp, bp);
+  float d5 = vdot(ab, cp), d6 = vdot(ac, cp);
+  if (d6 >= 0.f && d5 <= d6) return vdot(cp, cp);
+  float vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+    float v = d1 / (d1 - d3);
+    V3d<float> q = vsub(p, vadd(a, vmul(ab, v)));
+    return vdot(q, q);
+  }
+  float va = d3 * d6 - d5 * d4;
+  if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
+    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    V3d<float> q = vsub(p, vadd(b, vmul(vsub(c, b), w)));
+    return vdot(q, q);
+  }
+  float vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+    float w = d2 / (d2 - d6);
+    V3d<float> q = vsub(p, vadd(a, vmul(ac, w)));
+    return vdot(q, q);
+  }
+  float den = 1.f / (va + vb + vc);
+  float v = vb * den, w = vc * den;
+  V3d<float> q = vsub(p, vadd(vadd(a, vmul(ab, v)), vmul(ac, w)));
+  return vdot(q, q);
+}
+
+__device__ void pt_grad(V3d<float> p, V3d<float> a, V3d<float> b, V3d<float> c, V3d<float> g[4]) {  // :124-177
+  for (int k = 0; k < 4; ++k) g[k] = {0.f, 0.f, 0.f};
+  V3d<float> ab = vsub(b, a), ac = vsub(c, a), nrm = vcross(ab, ac);
+  float a2 = vdot(nrm, nrm);
+  if (a2 < 1e-20f) return;
+  V3d<float> n = vmul(nrm, 1.f / sqrtf(a2));
+  float sd = vdot(vsub(p, a), n);
+  V3d<float> pr = vsub(p, vmul(n, sd));
+  V3d<float> v2 = vsub(pr, a);
+  float d00 = vdot(ab, ab), d01 = vdot(ab, ac), d11 = vdot(ac, ac), d20 = vdot(v2, ab), d21 = vdot(v2, ac);
+  float den = d00 * d11 - d01 * d01;
+  if (fabsf(den) < 1e-20f) return;
+  float inv = 1.f / den;
+  float v = (d11 * d20 - d01 * d21) * inv, w = (d00 * d21 - d01 * d20) * inv, u = 1.f - v - w;
+  V3d<float> cl = vadd(vadd(vmul(a, u), vmul(b, v)), vmul(c, w));
+  V3d<float> d = vsub(p, cl);
+  g[0] = vmul(d, 2.f);
+  g[1] = vmul(d, -2.f * u);
+  g[2] = vmul(d, -2.f * v);
+  g[3] = vmul(d, -2.f * w);
+}
+
+__device__ void ee_params(V3d<float> d1, V3d<float> d2, V3d<float> r, bool grad_form, float* s_out, float* t_out,
+                          bool* degen_both) {
+  float a = vdot(d1, d1), e = vdot(d2, d2), f = vdot(d2, r);
+  const float eps = 1e-10f;
+  *degen_both = false;
+  float s, t;
+  if (grad_form) {  // edge_edge_distance_gradient (:251-303)
+    if (a < eps || e < eps) { s = 0.f; t = 0.f; }
+    else {
+      float c = vdot(d1, r), b = vdot(d1, d2), den = a * e - b * b;
+      s = fabsf(den) > eps ? rclampd((b * f - c * e) / den, 0.f, 1.f) : 0.f;
+      t = (b * s + f) / e;
+      if (t < 0.f) { t = 0.f; s = rclampd(-c / a, 0.f, 1.f); }
+      else if (t > 1.f) { t = 1.f; s = rclampd((b - c) / a, 0.f, 1.f); }
+    }
+  } else {  // edge_edge_distance_squared (:185-246)
+    if (a < eps && e < eps) { *degen_both = true; s = 0.f; t = 0.f; }
+    else if (a < eps) { t = rclampd(f / e, 0.f, 1.f); s = 0.f; }
+    else {
+      float c = vdot(d1, r);
+      if (e < eps) { s = rclampd(-c / a, 0.f, 1.f); t = 0.f; }
+      else {
+        float b = vdot(d1, d2), den = a * e - b * b;
+        s = fabsf(den) > eps ? rclampd((b * f - c * e) / den, 0.f, 1.f) : 0.f;
+        t = (b * s + f) / e;
+        if (t < 0.f) { t = 0.f; s = rclampd(-c / a, 0.f, 1.f); }
+        else if (t > 1.f) { t = 1.f; s = rclampd((b - c) / a, 0.f, 1.f); }
+      }
+    }
+  }
+  *s_out = s;
+  *t_out = t;
+}
+
+__device__ float ee_d2(V3d<float> a0, V3d<float> a1, V3d<float> b0, V3d<float> b1) {
+  V3d<float> d1 = vsub(a1, a0), d2 = vsub(b1, b0), r = vsub(a0, b0);
+  float s, t;
+  bool dg;
+  ee_params(d1, d2, r, false, &s, &t, &dg);
+  if (dg) return vdot(r, r);
+  V3d<float> q = vsub(vadd(a0, vmul(d1, s)), vadd(b0, vmul(d2, t)));
+  return vdot(q, q);
+}
+
+__device__ void ee_grad(V3d<float> a0, V3d<float> a1, V3d<float> b0, V3d<float> b1, V3d<float> g[4]) {
+  V3d<float> d1 = vsub(a1, a0), d2 = vsub(b1, b0), r = vsub(a0, b0);
+  float s, t;
+  bool dg;
+  ee_params(d1, d2, r, true, &s, &t, &dg);
+  V3d<float> q = vsub(vadd(a0, vmul(d1, s)), vadd(b0, vmul(d2, t)));
+  g[0] = vmul(q, 2.f * (1.f - s));
+  g[1] = vmul(q, 2.f * s);
+  g[2] = vmul(q, -2.f * (1.f - t));
+  g[3] = vmul(q, -2.f * t);
+}
+
+// barrier_gradient_with_thickness (barrier.rs:138-162)
+__device__ __forceinline__ float scaled_barrier_grad_thick(float d, float d_hat, float kappa, float th) {
+  float tsq = th * th, de = d - tsq;
+  float raw = de <= 0.f ? barrier_grad_dev(1e-12f, d_hat) : barrier_grad_dev(de, d_hat);
+  float r = kappa * raw;
+  if (isfinite(r)) return r;
+  return signbit(r) ? -1e6f : 1e6f;
+}
+
+__device__ __forceinline__ bool excluded(const SelfContactDev& S, uint32_t i, uint32_t j) {
+  for (uint32_t p = S.adj_ptr[i], e = S.adj_ptr[i + 1]; p < e; ++p) {
+    uint32_t a = S.adj[p];
+    if (a == j) return true;
+    if (a > j) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void add_grad(float4* G, uint32_t v, V3d<float> g, float bg) {
+  float* p = reinterpret_cast<float*>(G + v);
+  atomicAdd(p + 0, bg * g.x);
+  atomicAdd(p + 1, bg * g.y);
+  atomicAdd(p + 2, bg * g.z);
+}
+
+// SelfCollisionSystem::detect_ipc_contacts (self_collision.rs:199-276) and
+// IpcContactSet::compute_barrier_gradient (ipc_response.rs:170-219), per
+// candidate pair: 3+3 vertex-triangle and 9 edge-edge tests.
+__global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactDev S, int mode) {
+  const StepParams& P = *B.prm;
+  uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
+  float4* G = mode == 0 ? B.grad : B.grad_up;
+  const float dh = P.d_hat, kap = P.kappa, th = P.thickness;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+    uint2 pr = S.pairs[k];
+    uint32_t inst = S.tri_inst[pr.x];
+    InstRed& R = B.red[inst];
+    if (R.al_done) continue;
+    uint4 A = B.tri_idx[pr.x], Bt = B.tri_idx[pr.y];
+    uint32_t av[3] = {A.x, A.y, A.z}, bv[3] = {Bt.x, Bt.y, Bt.z};
+    uint32_t nact = 0;
+    bool viol = false;
+    for (int side = 0; side < 2; ++side) {
+      const uint32_t* X = side == 0 ? av : bv;
+      const uint32_t* Yt = side == 0 ? bv : av;
+      V3d<float> ta = ld3(B.pos, Yt[0]), tb = ld3(B.pos, Yt[1]), tc = ld3(B.pos, Yt[2]);
+      for (int q = 0; q < 3; ++q) {
+        uint32_t v = X[q];
+        if (v == Yt[0] || v == Yt[1] || v == Yt[2]) continue;
+        if (excluded(S, v, Yt[0]) || excluded(S, v, Yt[1]) || excluded(S, v, Yt[2])) continue;
+        V3d<float> p = ld3(B.pos, v);
+        float d = pt_d2(p, ta, tb, tc);
+        if (!(d < dh && d > 0.f)) continue;
+        ++nact;
+        if (d <= 1e-12f) viol = true;
+        float bg = th > 0.f ? scaled_barrier_grad_thick(d, dh, kap, th) : scaled_barrier_grad_dev(d, dh, kap);
+        V3d<float> g[4];
+        pt_grad(p, ta, tb, tc, g);
+        add_grad(G, v, g[0], bg); add_grad(G, Yt[0], g[1], bg); add_grad(G, Yt[1], g[2], bg); add_grad(G, Yt[2], g[3], bg);
+      }
+    }
+    uint32_t ae[3][2] = {{av[0], av[1]}, {av[1], av[2]}, {av[2], av[0]}};
+    uint32_t be[3][2] = {{bv[0], bv[1]}, {bv[1], bv[2]}, {bv[2], bv[0]}};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        uint32_t a0 = ae[i][0], a1 = ae[i][1], b0 = be[j][0], b1 = be[j][1];
+        if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) continue;
+        if (excluded(S, a0, b0) && excluded(S, a0, b1) && excluded(S, a1, b0) && excluded(S, a1, b1)) continue;
+        V3d<float> p0 = ld3(B.pos, a0), p1 = ld3(B.pos, a1), q0 = ld3(B.pos, b0), q1 = ld3(B.pos, b1);
+        float d = ee_d2(p0, p1, q0, q1);
+        if (!(d < dh && d > 0.f)) continue;
+        ++nact;
+        if (d <= 1e-12f) viol = true;
+        float bg = th > 0.f ? scaled_barrier_grad_thick(d, dh, kap, th) : scaled_barrier_grad_dev(d, dh, kap);
+        V3d<float> g[4];
+        ee_grad(p0, p1, q0, q1, g);
+        add_grad(G, a0, g[0], bg); add_grad(G, a1, g[1], bg); add_grad(G, b0, g[2], bg); add_grad(G, b1, g[3], bg);
+      }
+    if (mode == 1 && nact) {
+      atomicAdd(&R.active, nact);
+      if (viol) atomicMax(&R.maxviol_bits, __float_as_uint(1e-3f));
+    }
+  }
+}
+
+// ------------------------------------------------------------------ CCD
+// solve_cubic_roots / solve_quadratic_roots (crates/vistio-contact/src/ccd.rs:299-377)
+template <class R> __device__ int quad_roots(R a, R b, R c, R* out) {
+  const R eps = R(1e-8f);
+  if (fabs(a) < eps) {
+    if (fabs(b) < eps) return 0;
+    out[0] = -c / b;
+    return 1;
+  }
+  R disc = b * b - R(4) * a * c;
+  if (disc < -eps) return 0;
+  if (fabs(disc) <= eps) { out[0] = -b / (R(2) * a); return 1; }
+  R sd = sqrt(disc);
+  out[0] = (-b + sd) / (R(2) * a);
+  out[1] = (-b - sd) / (R(2) * a);
+  return 2;
+}
+template <class R> __device__ int cubic_roots(R a, R b, R c, R d, R* out) {
+  const R eps = R(1e-8f);
+  if (fabs(a) < eps) return quad_roots(b, c, d, out);
+  R p = b / a, q = c / a, r = d / a;
+  R ad = q - p * p / R(3);
+  R bd = r - p * q / R(3) + R(2) * p * p * p / R(27);
+  R disc = bd * bd / R(4) + ad * ad * ad / R(27);
+  R shift = -p / R(3);
+  if (disc > eps) {
+    R sd = sqrt(disc);
+    out[0] = cbrt(-bd / R(2) + sd) + cbrt(-bd / R(2) - sd) + shift;
+    return 1;
+  } else if (fabs(disc) <= eps) {
+    if (fabs(bd) < eps) { out[0] = shift; return 1; }
+    R u = cbrt(bd / R(2));
+    out[0] = R(-2) * u + shift;
+    out[1] = u + shift;
+    return 2;
+  }
+  R rv = sqrt(-ad * ad * ad / R(27));
+  if (fabs(rv) < R(1e-12f)) { out[0] = shift; return 1; }
+  R cv = rclampd(-bd / (R(2) * rv), R(-1), R(1));
+  R th = acos(cv);
+  R m = R(2) * cbrt(rv);
+  const R pi = R(3.14159265358979323846);
+  out[0] = m * cos(th / R(3)) + shift;
+  out[1] = m * cos((th + R(2) * pi) / R(3)) + shift;
+  out[2] = m * cos((th + R(4) * pi) / R(3)) + shift;
+  return 3;
+}
+
+// vertex_triangle_ccd (ccd.rs:32-129): returns the safe TOI or a value > 1 for no hit.
+template <class R>
+__device__ R vt_ccd(V3d<R> p0, V3d<R> p1, V3d<R> a0, V3d<R> a1, V3d<R> b0, V3d<R> b1, V3d<R> c0, V3d<R> c1) {
+  const R margin = R(0.9f), min_toi = R(1e-6f);
+  V3d<R> dp = vsub(p1, p0);
+  V3d<R> ar = vsub(a0, p0), br = vsub(b0, p0), cr = vsub(c0, p0);
+  V3d<R> av = vsub(vsub(a1, a0), dp), bvv = vsub(vsub(b1, b0), dp), cv = vsub(vsub(c1, c0), dp);
+  V3d<R> bvxcv = vcross(bvv, cv), brxcv = vcross(br, cv), bvxcr = vcross(bvv, cr), brxcr = vcross(br, cr);
+  R ca = vdot(av, bvxcv);
+  R cb = vdot(ar, bvxcv) + vdot(av, vadd(brxcv, bvxcr));
+  R cc = vdot(ar, vadd(brxcv, bvxcr)) + vdot(av, brxcr);
+  R cd = vdot(ar, brxcr);
+  R roots[3];
+  int nr = cubic_roots<R>(ca, cb, cc, cd, roots);
+  R best = R(2);
+  for (int i = 0; i < nr; ++i) {
+    R t = roots[i];
+    if (t < -min_toi || t > R(1) + min_toi) continue;
+    t = rclampd(t, R(0), R(1));
+    V3d<R> pa = vadd(ar, vmul(av, t)), pb = vadd(br, vmul(bvv, t)), pc = vadd(cr, vmul(cv, t));
+    V3d<R> v0 = vsub(pb, pa), v1 = vsub(pc, pa);
+    V3d<R> n = vcross(v0, v1);
+    if (vdot(n, n) < R(1e-20f)) continue;
+    V3d<R> v2 = vmul(pa, R(-1));
+    R d00 = vdot(v0, v0), d01 = vdot(v0, v1), d11 = vdot(v1, v1), d20 = vdot(v2, v0), d21 = vdot(v2, v1);
+    R den = d00 * d11 - d01 * d01;
+    if (fabs(den) < R(1e-20f)) continue;
+    R inv = R(1) / den;
+    R u = (d11 * d20 - d01 * d21) * inv, w = (d00 * d21 - d01 * d20) * inv, v = R(1) - u - w;
+    const R tol = R(0.01f);
+    if (v >= -tol && u >= -tol && w >= -tol) {
+      R safe = fmax(t * margin, min_toi);
+      best = fmin(best, safe);
+    }
+  }
+  return best;
+}
+
+// compute_max_step_size over the last detect's pairs (ccd.rs:238-292).
+__global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactDev S) {
+  uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+    uint2 pr = S.pairs[k];
+    uint32_t inst = S.tri_inst[pr.x];
+    InstRed& R = B.red[inst];
+    if (R.al_done) continue;
+    const InstDev I = B.inst[inst];
+    uint4 A = B.tri_idx[pr.x], Bt = B.tri_idx[pr.y];
+    uint32_t av[3] = {A.x, A.y, A.z}, bv[3] = {Bt.x, Bt.y, Bt.z};
+    auto P0 = [&](uint32_t v) { return ld3(B.pos, v); };
+    auto P1 = [&](uint32_t v) {
+      float4 x = B.pos[v], d = B.Y[I.vbase + B.perm_local[v]];
+      return mk<float>(x.x + d.x, x.y + d.y, x.z + d.z);
+    };
+    float best = 2.f;
+    for (int side = 0; side < 2; ++side) {
+      const uint32_t* X = side == 0 ? av : bv;
+      const uint32_t* Yt = side == 0 ? bv : av;
+      for (int q = 0; q < 3; ++q) {
+        uint32_t v = X[q];
+        if (v == Yt[0] || v == Yt[1] || v == Yt[2]) continue;
+        best = fminf(best, vt_ccd<float>(P0(v), P1(v), P0(Yt[0]), P1(Yt[0]), P0(Yt[1]), P1(Yt[1]), P0(Yt[2]), P1(Yt[2])));
+      }
+    }
+    if (best <= 1.f) atomicMin(&R.toi_bits, __float_as_uint(best));
+  }
+}
+
+// ---------------------------------------------------------------- host side
+inline uint32_t self_detect_launches() { return 7; }
+inline uint32_t self_ccd_launches() { return 1; }
+
+inline void launch_self_detect(const BatchDev& d, const SelfContactDev& S, uint32_t n_vtx_chunks,
+                               uint32_t n_tri_chunks, int mode, cudaStream_t st) {
+  k_clear_grad<<<n_vtx_chunks, 256, 0, st>>>(d, mode);
+  // the margin lives in StepParams (thickness); read on device via a copy below
+  k_self_boxes<<<S.ninst, 1024, 0, st>>>(d, S, -1.f);
+  k_self_count<<<n_tri_chunks, 256, 0, st>>>(d, S);
+  k_scan_local<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);
+  k_scan_sums<<<1, kScanBlock, 0, st>>>(S.block_sums, S.scan_blocks, S.npairs);
+  k_scan_add<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);
+  k_self_write<<<n_tri_chunks, 256, 0, st>>>(d, S);
+  k_self_grad<<<4 * 148, 256, 0, st>>>(d, S, mode);
+}
+
+inline void launch_self_ccd(const BatchDev& d, const SelfContactDev& S, cudaStream_t st) {
+  k_self_ccd<<<4 * 148, 256, 0, st>>>(d, S);
+}
+
+vistio_status ensure_self_contact(const BatchDev& d, SelfContactDev& S, const std::vector<vistio_solver*>& solvers,
+                                  const std::vector<uint32_t>& vbase, uint64_t T, cudaStream_t st, std::string* err);
+
+vistio_status broadphase_pairs_impl(cudaStream_t st, std::string* err, uint32_t nv, const float* px, const float* py,
+                                    const float* pz, uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs,
+                                    uint64_t cap, uint64_t* count);
+vistio_status ccd_hits_impl(cudaStream_t st, std::string* err, uint32_t nv, const float* p0, const float* p1,
+                            uint32_t nt, const uint32_t* tris, uint64_t npairs, const uint32_t* pairs, uint32_t* hits,
+                            uint64_t cap, uint64_t* nhits, float* min_toi);
+
+}  // namespace vistio

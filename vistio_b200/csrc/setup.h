@@ -1,0 +1,95 @@
+// Host-side set-up for one drape instance: rest-state element data, hinge
+// (bending) data, lumped masses, the constant PD system matrix and its
+// supernodal FP64 Cholesky factor laid out for the GPU triangular sweeps.
+//
+// This is the part of ProjectiveDynamicsSolver::init* that runs once per
+// (topology, material, dt) in the reference (crates/vistio-solver/src/
+// pd_solver.rs:106-257); it stays on the host and produces the flat arrays
+// the batch packer uploads to HBM.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace vistio {
+
+enum ModelKind : int32_t { MODEL_ARAP = 0, MODEL_COROT = 1, MODEL_ORTHO = 2, MODEL_ANISO = 3, MODEL_ISO_LINEAR = 4 };
+enum BendKind : int32_t { BEND_NONE = 0, BEND_DIHEDRAL = 1, BEND_DS = 2, BEND_DS_ANISO = 3 };
+
+struct SetupParams {
+  int32_t model = MODEL_ARAP;
+  int32_t bending = BEND_DIHEDRAL;
+  float stiffness = 1000.f;       // element weight = stiffness * rest area
+  float bend_stiffness = 1e-4f;   // hinge weight = bend_stiffness * edge length
+  float density_gsm = 200.f;
+  float warp = 0.f, weft = 0.f;   // membrane model warp/weft
+  float bend_warp = 0.f, bend_weft = 0.f;
+  float matrix_dt = 1.0f / 60.0f; // dt used in A (the reference always assembles with 1/60)
+};
+
+// Supernodal factor of P A P^T = L L^T in the layout the GPU sweeps read.
+// Columns are in the permuted (elimination) order.
+struct Supernode {
+  uint32_t first;     // first column
+  uint32_t ncols;     // s
+  uint32_t nrows;     // |R|: rows strictly below the diagonal block
+  uint32_t rows_off;  // offset of R (sorted row indices) in Factor::rows
+  uint64_t panel_off; // offset of the |R| x s row-major panel in Factor::vals
+  uint64_t diag_off;  // offset of inv(L_kk), s x s column-major, in Factor::vals
+  uint32_t parent;    // parent supernode, or UINT32_MAX for a root
+  uint32_t level;     // height in the supernodal elimination tree (leaves = 0)
+};
+
+struct Factor {
+  uint32_t n = 0;
+  std::vector<uint32_t> perm;   // perm[new] = old vertex
+  std::vector<uint32_t> iperm;  // iperm[old] = new
+  std::vector<Supernode> sn;
+  std::vector<uint32_t> rows;   // below-diagonal row structures
+  std::vector<double> vals;     // panels and inverted diagonal blocks (FP64)
+  std::vector<uint32_t> row_sn; // supernode owning each column
+  // Level schedule: supernodes grouped by level; rows of those supernodes.
+  uint32_t nlevels = 0;
+  std::vector<uint32_t> level_ptr;  // nlevels+1 offsets into level_rows
+  std::vector<uint32_t> level_rows; // rows (columns) of the level's supernodes, grouped by supernode
+  // Forward-sweep pull lists: for each row r, the (supernode, panel row) pairs
+  // of the descendants whose panels hold row r.
+  std::vector<uint32_t> fwd_ptr;    // n+1
+  std::vector<uint32_t> fwd_sn;     // supernode id
+  std::vector<uint32_t> fwd_pos;    // row position inside that supernode's panel
+  uint64_t nnz_L = 0;               // nonzeros of the simplicial factor (incl. diagonal)
+  uint64_t nnz_stored = 0;          // entries stored in panels + diagonal blocks
+};
+
+struct InstanceSetup {
+  uint32_t nv = 0, nt = 0, nh = 0;
+  SetupParams prm;
+  std::vector<float> rest;          // 3*nv rest positions
+  std::vector<uint32_t> tris;       // 3*nt
+  std::vector<float> dm_inv;        // 4*nt (column-major Dm^-1)
+  std::vector<float> area;          // nt
+  std::vector<float> tri_w;         // nt
+  std::vector<uint32_t> hinge_v;    // 4*nh (v0, v1, wing_a, wing_b)
+  std::vector<float> hinge_st;      // 4*nh stencil
+  std::vector<float> hinge_w;       // nh
+  std::vector<float> hinge_rest;    // nh rest dihedral angle
+  std::vector<float> mass;          // solver lumped masses (pinned = 1e8)
+  std::vector<uint8_t> pinned;
+  // Constant system matrix A (CSR, f64 sums of the f32 triplets).
+  std::vector<uint32_t> A_ptr, A_col;
+  std::vector<double> A_val;
+  Factor factor;
+};
+
+// Builds everything; returns an empty string on success or an error text.
+// `status` receives the status code (0 ok, 1 invalid mesh, 3 invalid config, 11 not SPD).
+std::string build_instance(uint32_t nv, const float* px, const float* py, const float* pz,
+                           uint32_t nt, const uint32_t* tris, const uint8_t* pinned,
+                           const SetupParams& prm, InstanceSetup& out, int* status);
+
+// Factorizes a general SPD matrix (CSR, either triangle or both) into the GPU layout.
+// coords (3*n) steer the nested dissection; may be null (a BFS-based split is used).
+std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
+                          const double* vals, const float* coords, Factor& f, int* status);
+
+}  // namespace vistio

@@ -1,0 +1,1136 @@
+// C ABI of the B200 drape solver (include/vistio_cuda.h).
+//
+// Ownership: a vistio_solver owns the host-side set-up of one garment (the
+// reference's ProjectiveDynamicsSolver after init) and, once stepped, a
+// device batch holding just that garment. A vistio_batch packs any number of
+// solvers into one set of ragged SoA buffers in HBM and advances them with a
+// single CUDA graph per step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vistio_cuda.h"
+#include "contact_kernels.cuh"
+#include "self_contact.cuh"
+#include "setup.h"
+
+using namespace vistio;
+
+struct vistio_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+};
+
+struct vistio_solver {
+  vistio_ctx* ctx = nullptr;
+  vistio_solver_config cfg{};
+  InstanceSetup setup;
+  std::vector<float> host_pos, host_vel;  // SimulationState before the first device step
+  int32_t has_ground = 0;
+  float ground_h = 0.f;
+  vistio_batch* own = nullptr;            // batch of one, created on the first step
+};
+
+namespace {
+
+constexpr int kElemThreads = 256;
+constexpr int kSolveThreads = 256;
+
+thread_local std::string g_tls_error;
+
+vistio_status fail(vistio_ctx* ctx, vistio_status s, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  g_tls_error = msg;
+  return s;
+}
+
+#define CU(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? VISTIO_ERR_OOM : VISTIO_ERR_GPU, \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));             \
+    }                                                                              \
+  } while (0)
+
+template <class T> struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t alloc(size_t count) {
+    n = count;
+    if (count == 0) count = 1;
+    return cudaMalloc(&p, count * sizeof(T));
+  }
+  cudaError_t upload(const std::vector<T>& h, cudaStream_t s) {
+    cudaError_t e = alloc(h.size());
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+}  // namespace
+
+struct vistio_batch {
+  vistio_ctx* ctx = nullptr;
+  std::vector<vistio_solver*> solvers;
+  uint32_t ninst = 0;
+  uint64_t V = 0, T = 0, H = 0, NSN = 0;
+  std::vector<uint32_t> vbase;
+  vistio_solver_config cfg{};
+  // device buffers
+  DevBuf<InstDev> inst;
+  DevBuf<int4> tri_chunks, hinge_chunks, vtx_chunks;
+  DevBuf<float4> pos, vel, prev, pred, Y, Tm, hinge_out, grad, grad_up, lam, fin_n;
+  DevBuf<float> mass, tri_w, tri_out, vals;
+  DevBuf<uint8_t> pinned, in_contact, in_contact_up, ever;
+  DevBuf<uint4> tri_idx, hinge_idx;
+  DevBuf<float4> tri_dm, hinge_st;
+  DevBuf<float2> hinge_wr;
+  DevBuf<uint32_t> vtri_ptr, vtri, vhinge_ptr, vhinge, perm_local, rows, level_ptr, level_rows, row_sn, fwd_ptr, status;
+  DevBuf<SnDev> sn;
+  DevBuf<uint2> fwd;
+  DevBuf<InstRed> red;
+  DevBuf<StepParams> prm;
+  SelfContactDev self;       // self-contact buffers (allocated on first use)
+  uint32_t n_tri_chunks = 0, n_hinge_chunks = 0, n_vtx_chunks = 0;
+  uint64_t factor_bytes = 0, device_bytes = 0;
+  BatchDev dev{};
+  cudaGraphExec_t graph_plain = nullptr, graph_ipc = nullptr;
+  int graph_ipc_self = -1;
+  uint32_t launches_plain = 0, launches_ipc = 0;
+  ~vistio_batch() {
+    if (graph_plain) cudaGraphExecDestroy(graph_plain);
+    if (graph_ipc) cudaGraphExecDestroy(graph_ipc);
+  }
+};
+
+struct vistio_factor {
+  vistio_ctx* ctx = nullptr;
+  uint32_t n = 0;
+  std::vector<uint32_t> A_ptr, A_col;
+  std::vector<double> A_val;
+  Factor f;
+  vistio_batch* b = nullptr;  // solve-only device layout
+};
+
+namespace {
+
+vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch* b);
+
+std::vector<int4> make_chunks(const std::vector<uint64_t>& base, const std::vector<uint64_t>& count) {
+  std::vector<int4> ch;
+  for (size_t k = 0; k < base.size(); ++k)
+    for (uint64_t s = 0; s < count[k]; s += kElemThreads)
+      ch.push_back(make_int4(int(k), int(base[k] + s), int(std::min<uint64_t>(kElemThreads, count[k] - s)), 0));
+  return ch;
+}
+
+vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch* b) {
+  cudaStream_t st = ctx->stream;
+  b->ctx = ctx;
+  b->solvers.assign(solvers, solvers + n);
+  b->ninst = n;
+  b->cfg = solvers[0]->cfg;
+  std::vector<InstDev> hi(n);
+  std::vector<uint64_t> vb(n), vc(n), tb(n), tc(n), hb(n), hc(n);
+  uint64_t V = 0, T = 0, H = 0, NSN = 0, NROWS = 0, NVALS = 0, NLVL = 0, NFWD = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    const InstanceSetup& I = solvers[k]->setup;
+    vb[k] = V; vc[k] = I.nv; tb[k] = T; tc[k] = I.nt; hb[k] = H; hc[k] = I.nh;
+    InstDev& d = hi[k];
+    d.vbase = uint32_t(V); d.nv = I.nv;
+    d.lvl_base = uint32_t(NLVL); d.nlvl = I.factor.nlevels;
+    d.model = I.prm.model; d.warp = I.prm.warp; d.weft = I.prm.weft;
+    d.inv_hmat2 = 1.f / (I.prm.matrix_dt * I.prm.matrix_dt);
+    d.has_ground = solvers[k]->has_ground; d.ground_h = solvers[k]->ground_h;
+    d.sn_base = uint32_t(NSN); d.nsn = uint32_t(I.factor.sn.size());
+    V += I.nv; T += I.nt; H += I.nh; NSN += I.factor.sn.size(); NROWS += I.factor.rows.size();
+    NVALS += I.factor.vals.size(); NLVL += I.factor.nlevels + 1; NFWD += I.factor.fwd_sn.size();
+  }
+  if (V >= (1ull << 31) || 3 * T >= (1ull << 30) || 4 * H >= (1ull << 30))
+    return fail(ctx, VISTIO_ERR_CAPACITY, "batch too large for 32-bit element indices");
+  b->V = V; b->T = T; b->H = H; b->NSN = NSN;
+  b->vbase.assign(vb.begin(), vb.end());
+  std::vector<float4> pos(V), vel(V);
+  std::vector<float> mass(V);
+  std::vector<uint8_t> pin(V);
+  std::vector<uint4> tri_idx(T);
+  std::vector<float4> tri_dm(T);
+  std::vector<float> tri_w(T);
+  std::vector<uint4> hinge_idx(H);
+  std::vector<float4> hinge_st(H);
+  std::vector<float2> hinge_wr(H);
+  std::vector<uint32_t> vtri_ptr(V + 1, 0), vhinge_ptr(V + 1, 0), perm_local(V), row_sn(V), fwd_ptr(V + 1, 0),
+      level_rows, level_ptr, rows;
+  std::vector<uint32_t> vtri(3 * T), vhinge(4 * H);
+  std::vector<SnDev> sn(NSN);
+  std::vector<float> vals(NVALS);
+  std::vector<uint2> fwd(NFWD);
+  level_rows.reserve(V);
+  rows.reserve(NROWS);
+  uint64_t snb = 0, rowsb = 0, valsb = 0, fwdb = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    vistio_solver* S = solvers[k];
+    const InstanceSetup& I = S->setup;
+    const Factor& F = I.factor;
+    uint64_t v0 = vb[k], t0 = tb[k], h0 = hb[k];
+    for (uint32_t i = 0; i < I.nv; ++i) {
+      pos[v0 + i] = make_float4(S->host_pos[3 * i], S->host_pos[3 * i + 1], S->host_pos[3 * i + 2], 0.f);
+      vel[v0 + i] = make_float4(S->host_vel[3 * i], S->host_vel[3 * i + 1], S->host_vel[3 * i + 2], 0.f);
+      mass[v0 + i] = I.mass[i];
+      pin[v0 + i] = I.pinned[i];
+      perm_local[v0 + i] = F.iperm[i];
+    }
+    for (uint32_t t = 0; t < I.nt; ++t) {
+      tri_idx[t0 + t] = make_uint4(uint32_t(v0 + I.tris[3 * t]), uint32_t(v0 + I.tris[3 * t + 1]),
+                                   uint32_t(v0 + I.tris[3 * t + 2]), 0u);
+      tri_dm[t0 + t] = make_float4(I.dm_inv[4 * t], I.dm_inv[4 * t + 1], I.dm_inv[4 * t + 2], I.dm_inv[4 * t + 3]);
+      tri_w[t0 + t] = I.tri_w[t];
+    }
+    for (uint32_t h = 0; h < I.nh; ++h) {
+      hinge_idx[h0 + h] = make_uint4(uint32_t(v0 + I.hinge_v[4 * h]), uint32_t(v0 + I.hinge_v[4 * h + 1]),
+                                     uint32_t(v0 + I.hinge_v[4 * h + 2]), uint32_t(v0 + I.hinge_v[4 * h + 3]));
+      hinge_st[h0 + h] = make_float4(I.hinge_st[4 * h], I.hinge_st[4 * h + 1], I.hinge_st[4 * h + 2], I.hinge_st[4 * h + 3]);
+      hinge_wr[h0 + h] = make_float2(I.hinge_w[h], I.hinge_rest[h]);
+    }
+    // factor
+    for (size_t s = 0; s < F.sn.size(); ++s) {
+      const Supernode& X = F.sn[s];
+      SnDev& d = sn[snb + s];
+      d.first = X.first; d.ncols = X.ncols; d.nrows = X.nrows;
+      d.rows_off = uint32_t(rowsb + X.rows_off);
+      d.panel_off = valsb + X.panel_off;
+      d.diag_off = valsb + X.diag_off;
+    }
+    rows.insert(rows.end(), F.rows.begin(), F.rows.end());
+    for (size_t q = 0; q < F.vals.size(); ++q) vals[valsb + q] = float(F.vals[q]);
+    {  // level_ptr entries are global offsets into level_rows
+      uint32_t base = uint32_t(level_rows.size());
+      for (uint32_t l = 0; l <= F.nlevels; ++l) level_ptr.push_back(base + F.level_ptr[l]);
+      level_rows.insert(level_rows.end(), F.level_rows.begin(), F.level_rows.end());
+    }
+    for (uint32_t r = 0; r < I.nv; ++r) {
+      row_sn[v0 + r] = uint32_t(snb + F.row_sn[r]);
+      fwd_ptr[v0 + r] = uint32_t(fwdb + F.fwd_ptr[r]);
+    }
+    for (size_t q = 0; q < F.fwd_sn.size(); ++q) fwd[fwdb + q] = make_uint2(uint32_t(snb + F.fwd_sn[q]), F.fwd_pos[q]);
+    snb += F.sn.size(); rowsb += F.rows.size(); valsb += F.vals.size(); fwdb += F.fwd_sn.size();
+  }
+  fwd_ptr[V] = uint32_t(fwdb);
+  // vertex incidence
+  for (uint64_t t = 0; t < T; ++t) { vtri_ptr[tri_idx[t].x + 1]++; vtri_ptr[tri_idx[t].y + 1]++; vtri_ptr[tri_idx[t].z + 1]++; }
+  for (uint64_t h = 0; h < H; ++h) {
+    vhinge_ptr[hinge_idx[h].x + 1]++; vhinge_ptr[hinge_idx[h].y + 1]++;
+    vhinge_ptr[hinge_idx[h].z + 1]++; vhinge_ptr[hinge_idx[h].w + 1]++;
+  }
+  for (uint64_t i = 0; i < V; ++i) { vtri_ptr[i + 1] += vtri_ptr[i]; vhinge_ptr[i + 1] += vhinge_ptr[i]; }
+  {
+    std::vector<uint32_t> c1(vtri_ptr.begin(), vtri_ptr.end() - 1), c2(vhinge_ptr.begin(), vhinge_ptr.end() - 1);
+    for (uint64_t t = 0; t < T; ++t) {
+      uint32_t ids[3] = {tri_idx[t].x, tri_idx[t].y, tri_idx[t].z};
+      for (uint32_t s = 0; s < 3; ++s) vtri[c1[ids[s]]++] = uint32_t(t << 2) | s;
+    }
+    for (uint64_t h = 0; h < H; ++h) {
+      uint32_t ids[4] = {hinge_idx[h].x, hinge_idx[h].y, hinge_idx[h].z, hinge_idx[h].w};
+      for (uint32_t s = 0; s < 4; ++s) vhinge[c2[ids[s]]++] = uint32_t(h << 2) | s;
+    }
+  }
+  auto tch = make_chunks(tb, tc), hch = make_chunks(hb, hc), vch = make_chunks(vb, vc);
+  b->n_tri_chunks = uint32_t(tch.size()); b->n_hinge_chunks = uint32_t(hch.size()); b->n_vtx_chunks = uint32_t(vch.size());
+  CU(cudaSetDevice(ctx->device));
+  CU(b->inst.upload(hi, st));
+  CU(b->tri_chunks.upload(tch, st)); CU(b->hinge_chunks.upload(hch, st)); CU(b->vtx_chunks.upload(vch, st));
+  CU(b->pos.upload(pos, st)); CU(b->vel.upload(vel, st));
+  CU(b->prev.upload(pos, st)); CU(b->pred.upload(pos, st));
+  CU(b->mass.upload(mass, st)); CU(b->pinned.upload(pin, st));
+  CU(b->tri_idx.upload(tri_idx, st)); CU(b->tri_dm.upload(tri_dm, st)); CU(b->tri_w.upload(tri_w, st));
+  CU(b->tri_out.alloc(9 * T));
+  CU(b->hinge_idx.upload(hinge_idx, st)); CU(b->hinge_st.upload(hinge_st, st)); CU(b->hinge_wr.upload(hinge_wr, st));
+  CU(b->hinge_out.alloc(H));
+  CU(b->vtri_ptr.upload(vtri_ptr, st)); CU(b->vtri.upload(vtri, st));
+  CU(b->vhinge_ptr.upload(vhinge_ptr, st)); CU(b->vhinge.upload(vhinge, st));
+  CU(b->perm_local.upload(perm_local, st));
+  CU(b->Y.alloc(V)); CU(b->Tm.alloc(V));
+  CU(b->sn.upload(sn, st)); CU(b->rows.upload(rows, st)); CU(b->vals.upload(vals, st));
+  CU(b->level_ptr.upload(level_ptr, st)); CU(b->level_rows.upload(level_rows, st));
+  CU(b->row_sn.upload(row_sn, st)); CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
+  CU(b->grad.alloc(V)); CU(b->grad_up.alloc(V)); CU(b->lam.alloc(V)); CU(b->fin_n.alloc(V));
+  CU(cudaMemsetAsync(b->lam.p, 0, V * sizeof(float4), st));
+  CU(cudaMemsetAsync(b->grad.p, 0, V * sizeof(float4), st));
+  CU(cudaMemsetAsync(b->grad_up.p, 0, V * sizeof(float4), st));
+  CU(b->in_contact.alloc(V)); CU(b->in_contact_up.alloc(V)); CU(b->ever.alloc(V));
+  CU(b->red.alloc(n)); CU(cudaMemsetAsync(b->red.p, 0, n * sizeof(InstRed), st));
+  CU(b->prm.alloc(1));
+  CU(b->status.alloc(1)); CU(cudaMemsetAsync(b->status.p, 0, sizeof(uint32_t), st));
+  CU(cudaStreamSynchronize(st));
+  b->factor_bytes = vals.size() * sizeof(float) + sn.size() * sizeof(SnDev) + rows.size() * 4 + fwd.size() * 8 +
+                    fwd_ptr.size() * 4 + row_sn.size() * 4 + level_rows.size() * 4 + level_ptr.size() * 4;
+  b->device_bytes = b->factor_bytes + V * (16 * 10 + 4 + 3 + 4 * 3) + T * (16 + 16 + 4 + 36 + 12) +
+                    H * (16 + 16 + 8 + 16 + 16) + (V + 1) * 8;
+  BatchDev& d = b->dev;
+  d.inst = b->inst.p; d.tri_chunks = b->tri_chunks.p; d.hinge_chunks = b->hinge_chunks.p; d.vtx_chunks = b->vtx_chunks.p;
+  d.pos = b->pos.p; d.vel = b->vel.p; d.prev = b->prev.p; d.pred = b->pred.p; d.mass = b->mass.p; d.pinned = b->pinned.p;
+  d.tri_idx = b->tri_idx.p; d.tri_dm = b->tri_dm.p; d.tri_w = b->tri_w.p; d.tri_out = b->tri_out.p;
+  d.hinge_idx = b->hinge_idx.p; d.hinge_st = b->hinge_st.p; d.hinge_wr = b->hinge_wr.p; d.hinge_out = b->hinge_out.p;
+  d.vtri_ptr = b->vtri_ptr.p; d.vtri = b->vtri.p; d.vhinge_ptr = b->vhinge_ptr.p; d.vhinge = b->vhinge.p;
+  d.perm_local = b->perm_local.p; d.row_vertex = nullptr; d.Y = b->Y.p; d.T = b->Tm.p;
+  d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.level_ptr = b->level_ptr.p; d.level_rows = b->level_rows.p;
+  d.row_sn = b->row_sn.p; d.fwd_ptr = b->fwd_ptr.p; d.fwd = b->fwd.p;
+  d.grad = b->grad.p; d.grad_up = b->grad_up.p; d.lam = b->lam.p; d.fin_n = b->fin_n.p;
+  d.in_contact = b->in_contact.p; d.in_contact_up = b->in_contact_up.p; d.ever = b->ever.p;
+  d.red = b->red.p; d.prm = b->prm.p; d.status = b->status.p;
+  return VISTIO_OK;
+}
+
+StepParams make_params(const vistio_solver_config& c, float dt, const vistio_contact_desc* ct, float avg_mass) {
+  StepParams p{};
+  p.dt = dt;
+  p.inv_dt2 = 1.f / (dt * dt);
+  for (int k = 0; k < 3; ++k) p.gravity[k] = c.gravity[k];
+  p.damping = c.damping;
+  p.rayleigh = c.rayleigh_mass_damping;
+  p.al_tolerance = c.al_tolerance;
+  p.al_mu_growth = c.al_mu_growth;
+  p.al_mu_initial = c.al_mu_initial;
+  p.friction = c.friction_coefficient;
+  p.contact_damping = c.contact_damping;
+  p.contact_damping_max = c.contact_damping_max;
+  p.contact_vthresh = c.contact_velocity_threshold;
+  p.adaptive_damping = c.adaptive_contact_damping;
+  if (ct) {
+    p.ipc = 1;
+    float dh = c.compliant_contact ? c.barrier_d_hat * c.compliant_d_hat_scale : c.barrier_d_hat;
+    p.d_hat = dh;
+    p.max_vel = (0.5f * std::sqrt(dh)) / dt;  // pd_solver.rs:573-595
+    p.has_ground = ct->has_ground;
+    p.ground_h = ct->ground_height;
+    p.has_sphere = ct->has_sphere;
+    for (int k = 0; k < 3; ++k) p.sphere_c[k] = ct->sphere_center[k];
+    p.sphere_r = ct->sphere_radius;
+    p.self_collision = ct->self_collision;
+    p.thickness = ct->thickness;
+    float kap = ct->kappa;
+    if (!(kap > 0.f)) {
+      // estimate_initial_kappa (barrier.rs:97-116) with the runner's inputs:
+      // configured kappa, average vertex mass, |g_y|, configured d_hat.
+      float cfgk = c.barrier_kappa;
+      if (cfgk > 0.f) kap = cfgk;
+      else {
+        float dhat = c.barrier_d_hat, dmid = dhat * 0.5f;
+        float dcl = std::fmin(std::fmax(dmid, dhat * 1e-3f), dhat);
+        double d64 = dcl, dd = dhat, diff = d64 - dd;
+        float gm = float(-(diff) * (2.0 * std::log(d64 / dd) + diff / d64));
+        gm = std::fabs(gm);
+        if (gm < 1e-12f) kap = 1e4f;
+        else {
+          kap = avg_mass * std::fabs(c.gravity[1]) / (2.f * std::sqrt(dmid) * gm);
+          kap = std::fmin(std::fmax(kap, 1.f), 1e6f);
+        }
+      }
+    }
+    p.kappa = kap;
+  }
+  return p;
+}
+
+void launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update) {
+  if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev);
+  if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev);
+  k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+  k_solve<kSolveThreads><<<b->ninst, kSolveThreads, 0, st>>>(b->dev, do_update);
+}
+
+vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out, uint32_t* nlaunch) {
+  vistio_ctx* ctx = b->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaGraph_t g = nullptr;
+  uint32_t iters = b->cfg.max_iterations;
+  uint32_t per_iter = (b->n_tri_chunks ? 1 : 0) + (b->n_hinge_chunks ? 1 : 0) + 2;
+  uint32_t small_grid = (b->ninst + 127) / 128;
+  CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  k_predict<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+  uint32_t L = 2;
+  if (!ipc) {
+    for (uint32_t it = 0; it < iters; ++it) launch_plain_iteration(b, st, 1);
+    L += iters * per_iter;
+  } else {
+    for (uint32_t al = 0; al < b->cfg.al_max_iterations; ++al) {
+      k_al_begin<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
+      if (self) { launch_self_detect(b->dev, b->self, b->n_vtx_chunks, b->n_tri_chunks, 0, st); L += self_detect_launches(); }
+      k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 0);
+      for (uint32_t it = 0; it < iters; ++it) {
+        launch_plain_iteration(b, st, 0);
+        if (self) { launch_self_ccd(b->dev, b->self, st); L += self_ccd_launches(); }
+        k_ccd<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+        k_ipc_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+      }
+      if (self) { launch_self_detect(b->dev, b->self, b->n_vtx_chunks, b->n_tri_chunks, 1, st); L += self_detect_launches(); }
+      k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 1);
+      k_al_end<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+      k_al_finish<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
+      L += 5 + iters * (per_iter + 2);
+    }
+  }
+  k_finalize<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+  cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (e != cudaSuccess) return fail(ctx, VISTIO_ERR_GPU, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(ctx, VISTIO_ERR_GPU, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  *nlaunch = L;
+  return VISTIO_OK;
+}
+
+float batch_avg_mass(vistio_batch* b) {
+  // The runner passes scenario.vertex_mass; the library uses the first
+  // garment's mean free-vertex lumped mass.
+  const InstanceSetup& I = b->solvers[0]->setup;
+  double s = 0;
+  uint32_t c = 0;
+  for (uint32_t i = 0; i < I.nv; ++i) if (!I.pinned[i]) { s += I.mass[i]; ++c; }
+  return c ? float(s / c) : 1e-3f;
+}
+
+vistio_status batch_run(vistio_batch* b, float dt, uint32_t nsteps, const vistio_contact_desc* ct) {
+  vistio_ctx* ctx = b->ctx;
+  cudaStream_t st = ctx->stream;
+  if (!(dt > 0.f) || !std::isfinite(dt)) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "dt must be positive");
+  bool ipc = ct != nullptr;
+  bool self = ipc && ct->self_collision;
+  if (self) {
+    vistio_status s = ensure_self_contact(b->dev, b->self, b->solvers, b->vbase, b->T, st, &ctx->last_error);
+    if (s != VISTIO_OK) return s;
+  }
+  StepParams p = make_params(b->cfg, dt, ct, batch_avg_mass(b));
+  CU(cudaMemcpyAsync(b->prm.p, &p, sizeof(p), cudaMemcpyHostToDevice, st));
+  cudaGraphExec_t* ge = ipc ? &b->graph_ipc : &b->graph_plain;
+  if (ipc && *ge && b->graph_ipc_self != int(self)) { cudaGraphExecDestroy(*ge); *ge = nullptr; }
+  if (!*ge) {
+    vistio_status s = capture(b, ipc, self, ge, ipc ? &b->launches_ipc : &b->launches_plain);
+    if (s != VISTIO_OK) return s;
+    if (ipc) b->graph_ipc_self = int(self);
+  }
+  for (uint32_t k = 0; k < nsteps; ++k) CU(cudaGraphLaunch(*ge, st));
+  return VISTIO_OK;
+}
+
+vistio_status ensure_own(vistio_solver* s) {
+  if (s->own) return VISTIO_OK;
+  auto* b = new vistio_batch();
+  vistio_solver* arr[1] = {s};
+  vistio_status r = pack_batch(s->ctx, arr, 1, b);
+  if (r != VISTIO_OK) { delete b; return r; }
+  s->own = b;
+  return VISTIO_OK;
+}
+
+vistio_status read_result(vistio_batch* b, uint32_t k, vistio_step_result* res, bool ipc, double wall) {
+  vistio_ctx* ctx = b->ctx;
+  InstRed R;
+  uint32_t status = 0;
+  CU(cudaMemcpyAsync(&R, b->red.p + k, sizeof(R), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(&status, b->status.p, sizeof(status), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  double resid = R.norm_sq > 1e-12 ? std::sqrt(R.diff_sq / R.norm_sq) : std::sqrt(R.diff_sq);
+  if (res) {
+    std::memset(res, 0, sizeof(*res));
+    res->iterations = R.iters;
+    res->final_residual = resid;
+    res->converged = (ipc && R.al_done) || resid < b->cfg.tolerance;
+    res->wall_time = wall;
+    res->al_iterations = R.al_iters;
+    res->active_contacts = R.last_active;
+    res->last_alpha = ipc ? R.alpha : 1.f;
+    res->status = status ? VISTIO_ERR_SOLVER_DIVERGENCE : VISTIO_OK;
+  }
+  if (status) return fail(ctx, VISTIO_ERR_SOLVER_DIVERGENCE, "non-finite positions in the global solve");
+  return VISTIO_OK;
+}
+
+vistio_status init_common(vistio_ctx* ctx, const vistio_mesh_desc* mesh, const vistio_solver_config* cfg,
+                          const SetupParams& prm, const uint8_t* pinned, vistio_solver** out) {
+  if (!ctx || !mesh || !cfg || !out) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  if (!mesh->pos_x || !mesh->pos_y || !mesh->pos_z || !mesh->indices)
+    return fail(ctx, VISTIO_ERR_INVALID_MESH, "null mesh array");
+  if (cfg->max_iterations == 0) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "max_iterations must be > 0");
+  std::vector<uint8_t> pin(mesh->vertex_count, 0);
+  if (pinned) std::memcpy(pin.data(), pinned, mesh->vertex_count);
+  auto s = std::make_unique<vistio_solver>();
+  s->ctx = ctx;
+  s->cfg = *cfg;
+  int st = 0;
+  std::string err = build_instance(mesh->vertex_count, mesh->pos_x, mesh->pos_y, mesh->pos_z, mesh->triangle_count,
+                                   mesh->indices, pin.data(), prm, s->setup, &st);
+  if (!err.empty()) {
+    vistio_status code = st == 1 ? VISTIO_ERR_INVALID_MESH : st == 11 ? VISTIO_ERR_NOT_SPD : VISTIO_ERR_INVALID_CONFIG;
+    return fail(ctx, code, err);
+  }
+  s->host_pos = s->setup.rest;
+  s->host_vel.assign(s->host_pos.size(), 0.f);
+  *out = s.release();
+  return VISTIO_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* vistio_status_string(vistio_status s) {
+  switch (s) {
+    case VISTIO_OK: return "ok";
+    case VISTIO_ERR_INVALID_MESH: return "invalid mesh";
+    case VISTIO_ERR_INVALID_MATERIAL: return "invalid material parameter";
+    case VISTIO_ERR_INVALID_CONFIG: return "invalid configuration";
+    case VISTIO_ERR_IO: return "i/o error";
+    case VISTIO_ERR_SERIALIZATION: return "serialization error";
+    case VISTIO_ERR_GPU: return "gpu error";
+    case VISTIO_ERR_SOLVER_DIVERGENCE: return "solver divergence";
+    case VISTIO_ERR_INVARIANT: return "invariant violation";
+    case VISTIO_ERR_TIMEOUT: return "timeout";
+    case VISTIO_ERR_OOM: return "out of device memory";
+    case VISTIO_ERR_NOT_SPD: return "matrix not positive definite";
+    case VISTIO_ERR_CAPACITY: return "capacity exceeded";
+  }
+  return "unknown";
+}
+
+const char* vistio_last_error(const vistio_ctx* ctx) {
+  return ctx ? ctx->last_error.c_str() : g_tls_error.c_str();
+}
+
+vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
+  vistio_ctx* ctx = nullptr;
+  if (!out) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null out");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return fail(nullptr, VISTIO_ERR_GPU, "no CUDA device available");
+  if (device < 0 || device >= n) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "device index out of range");
+  auto c = std::make_unique<vistio_ctx>();
+  c->device = device;
+  ctx = c.get();
+  CU(cudaSetDevice(device));
+  CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  *out = c.release();
+  return VISTIO_OK;
+}
+
+vistio_status vistio_ctx_destroy(vistio_ctx* ctx) {
+  if (!ctx) return VISTIO_OK;
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_sync(vistio_ctx* ctx) {
+  if (!ctx) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null context");
+  CU(cudaStreamSynchronize(ctx->stream));
+  return VISTIO_OK;
+}
+
+vistio_status vistio_solver_init(vistio_ctx* ctx, const vistio_mesh_desc* mesh, const vistio_solver_config* cfg,
+                                 const uint8_t* pinned, vistio_solver** out) {
+  if (!cfg) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null config");
+  SetupParams p;  // pd_solver.rs:228-246
+  p.model = MODEL_ARAP;
+  p.bending = BEND_DIHEDRAL;
+  p.stiffness = cfg->stretch_weight * 1000.0f;
+  p.bend_stiffness = cfg->bending_weight * 100.0f;
+  p.density_gsm = 200.0f;
+  p.matrix_dt = 1.0f / 60.0f;
+  return init_common(ctx, mesh, cfg, p, pinned, out);
+}
+
+vistio_status vistio_solver_init_with_material(vistio_ctx* ctx, const vistio_mesh_desc* mesh,
+                                               const vistio_solver_config* cfg, const vistio_material_desc* m,
+                                               const vistio_model_desc* model, int32_t bending_kind,
+                                               const uint8_t* pinned, vistio_solver** out) {
+  if (!m || !model) return fail(ctx, VISTIO_ERR_INVALID_MATERIAL, "null material or model");
+  if (!(m->density > 0.f) || !std::isfinite(m->density))
+    return fail(ctx, VISTIO_ERR_INVALID_MATERIAL, "density must be positive");
+  if (model->kind < 0 || model->kind > 4) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "unknown model kind");
+  if (bending_kind < 0 || bending_kind > 3) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "unknown bending kind");
+  SetupParams p;  // pd_solver.rs:115-132, element.rs:106, bending.rs:160, discrete_shells.rs:206
+  p.model = model->kind;
+  p.bending = bending_kind;
+  p.stiffness = ((m->stretch_stiffness_warp + m->stretch_stiffness_weft) / 2.0f) * 10.0f;
+  p.bend_stiffness = ((m->bending_stiffness_warp + m->bending_stiffness_weft) / 2.0f) * 100.0f;
+  p.density_gsm = m->density;
+  p.warp = model->warp_stiffness;
+  p.weft = model->weft_stiffness;
+  p.bend_warp = m->bending_stiffness_warp;
+  p.bend_weft = m->bending_stiffness_weft;
+  p.matrix_dt = 1.0f / 60.0f;
+  return init_common(ctx, mesh, cfg, p, pinned, out);
+}
+
+vistio_status vistio_solver_init_explicit(vistio_ctx* ctx, const vistio_mesh_desc* mesh, const vistio_solver_config* cfg,
+                                          const vistio_setup_desc* sd, const uint8_t* pinned, vistio_solver** out) {
+  if (!sd) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null setup");
+  if (sd->model < 0 || sd->model > 4 || sd->bending < 0 || sd->bending > 3)
+    return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "unknown model or bending kind");
+  if (!(sd->density_gsm > 0.f)) return fail(ctx, VISTIO_ERR_INVALID_MATERIAL, "density must be positive");
+  SetupParams p;
+  p.model = sd->model; p.bending = sd->bending; p.stiffness = sd->stiffness; p.bend_stiffness = sd->bend_stiffness;
+  p.density_gsm = sd->density_gsm; p.warp = sd->warp_stiffness; p.weft = sd->weft_stiffness;
+  p.bend_warp = sd->bend_warp; p.bend_weft = sd->bend_weft; p.matrix_dt = sd->matrix_dt;
+  return init_common(ctx, mesh, cfg, p, pinned, out);
+}
+
+vistio_status vistio_solver_destroy(vistio_solver* s) {
+  if (!s) return VISTIO_OK;
+  delete s->own;
+  delete s;
+  return VISTIO_OK;
+}
+
+const char* vistio_solver_name(const vistio_solver*) { return "ProjectiveDynamics"; }
+
+vistio_status vistio_solver_info(const vistio_solver* s, uint32_t* nv, uint32_t* nt, uint32_t* nh, uint64_t* nnz_a,
+                                 uint64_t* nnz_l, uint32_t* nsn, uint32_t* nlv) {
+  if (!s) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null solver");
+  if (nv) *nv = s->setup.nv;
+  if (nt) *nt = s->setup.nt;
+  if (nh) *nh = s->setup.nh;
+  if (nnz_a) *nnz_a = s->setup.A_col.size();
+  if (nnz_l) *nnz_l = s->setup.factor.nnz_L;
+  if (nsn) *nsn = uint32_t(s->setup.factor.sn.size());
+  if (nlv) *nlv = s->setup.factor.nlevels;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_solver_lumped_masses(const vistio_solver* s, float* out) {
+  if (!s || !out) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  std::memcpy(out, s->setup.mass.data(), s->setup.nv * sizeof(float));
+  return VISTIO_OK;
+}
+
+vistio_status vistio_solver_set_ground(vistio_solver* s, int32_t has, float h) {
+  if (!s) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null solver");
+  vistio_ctx* ctx = s->ctx;
+  s->has_ground = has;
+  s->ground_h = h;
+  if (s->own) {
+    InstDev d;
+    CU(cudaStreamSynchronize(ctx->stream));
+    CU(cudaMemcpy(&d, s->own->inst.p, sizeof(d), cudaMemcpyDeviceToHost));
+    d.has_ground = has;
+    d.ground_h = h;
+    CU(cudaMemcpy(s->own->inst.p, &d, sizeof(d), cudaMemcpyHostToDevice));
+  }
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_set_state(vistio_batch* b, uint32_t k, const float* px, const float* py, const float* pz,
+                                     const float* vx, const float* vy, const float* vz) {
+  if (!b || k >= b->ninst) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "bad batch index");
+  vistio_ctx* ctx = b->ctx;
+  uint32_t nv = b->solvers[k]->setup.nv;
+  std::vector<float4> p(nv), v(nv);
+  CU(cudaStreamSynchronize(ctx->stream));
+  CU(cudaMemcpy(p.data(), b->pos.p + b->vbase[k], nv * sizeof(float4), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(v.data(), b->vel.p + b->vbase[k], nv * sizeof(float4), cudaMemcpyDeviceToHost));
+  for (uint32_t i = 0; i < nv; ++i) {
+    if (px) p[i].x = px[i];
+    if (py) p[i].y = py[i];
+    if (pz) p[i].z = pz[i];
+    if (vx) v[i].x = vx[i];
+    if (vy) v[i].y = vy[i];
+    if (vz) v[i].z = vz[i];
+  }
+  CU(cudaMemcpyAsync(b->pos.p + b->vbase[k], p.data(), nv * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(b->vel.p + b->vbase[k], v.data(), nv * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_get_state(vistio_batch* b, uint32_t k, float* px, float* py, float* pz, float* vx,
+                                     float* vy, float* vz) {
+  if (!b || k >= b->ninst) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "bad batch index");
+  vistio_ctx* ctx = b->ctx;
+  uint32_t nv = b->solvers[k]->setup.nv;
+  std::vector<float4> p(nv), v(nv);
+  CU(cudaMemcpyAsync(p.data(), b->pos.p + b->vbase[k], nv * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(v.data(), b->vel.p + b->vbase[k], nv * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  uint32_t status = 0;
+  CU(cudaMemcpy(&status, b->status.p, sizeof(status), cudaMemcpyDeviceToHost));
+  for (uint32_t i = 0; i < nv; ++i) {
+    if (px) px[i] = p[i].x;
+    if (py) py[i] = p[i].y;
+    if (pz) pz[i] = p[i].z;
+    if (vx) vx[i] = v[i].x;
+    if (vy) vy[i] = v[i].y;
+    if (vz) vz[i] = v[i].z;
+  }
+  if (status) return fail(ctx, VISTIO_ERR_SOLVER_DIVERGENCE, "non-finite positions in the global solve");
+  return VISTIO_OK;
+}
+
+vistio_status vistio_solver_set_state(vistio_solver* s, const float* px, const float* py, const float* pz,
+                                      const float* vx, const float* vy, const float* vz) {
+  if (!s) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null solver");
+  for (uint32_t i = 0; i < s->setup.nv; ++i) {
+    if (px) s->host_pos[3 * i] = px[i];
+    if (py) s->host_pos[3 * i + 1] = py[i];
+    if (pz) s->host_pos[3 * i + 2] = pz[i];
+    if (vx) s->host_vel[3 * i] = vx[i];
+    if (vy) s->host_vel[3 * i + 1] = vy[i];
+    if (vz) s->host_vel[3 * i + 2] = vz[i];
+  }
+  if (s->own) return vistio_batch_set_state(s->own, 0, px, py, pz, vx, vy, vz);
+  return VISTIO_OK;
+}
+
+vistio_status vistio_solver_get_state(vistio_solver* s, float* px, float* py, float* pz, float* vx, float* vy,
+                                      float* vz) {
+  if (!s) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null solver");
+  if (s->own) return vistio_batch_get_state(s->own, 0, px, py, pz, vx, vy, vz);
+  for (uint32_t i = 0; i < s->setup.nv; ++i) {
+    if (px) px[i] = s->host_pos[3 * i];
+    if (py) py[i] = s->host_pos[3 * i + 1];
+    if (pz) pz[i] = s->host_pos[3 * i + 2];
+    if (vx) vx[i] = s->host_vel[3 * i];
+    if (vy) vy[i] = s->host_vel[3 * i + 1];
+    if (vz) vz[i] = s->host_vel[3 * i + 2];
+  }
+  return VISTIO_OK;
+}
+
+vistio_status vistio_step(vistio_solver* s, float dt, vistio_step_result* res) {
+  if (!s) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "Solver not initialized. Call init() first.");
+  auto t0 = std::chrono::steady_clock::now();
+  vistio_status r = ensure_own(s);
+  if (r != VISTIO_OK) return r;
+  r = batch_run(s->own, dt, 1, nullptr);
+  if (r != VISTIO_OK) return r;
+  r = read_result(s->own, 0, res, false, 0.0);
+  if (res) res->wall_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return r;
+}
+
+vistio_status vistio_step_with_ipc(vistio_solver* s, float dt, const vistio_contact_desc* contact,
+                                   vistio_step_result* res) {
+  if (!s) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "Solver not initialized. Call init() first.");
+  if (!contact) return fail(s->ctx, VISTIO_ERR_INVALID_CONFIG, "null contact description");
+  auto t0 = std::chrono::steady_clock::now();
+  vistio_status r = ensure_own(s);
+  if (r != VISTIO_OK) return r;
+  r = batch_run(s->own, dt, 1, contact);
+  if (r != VISTIO_OK) return r;
+  r = read_result(s->own, 0, res, true, 0.0);
+  if (res) res->wall_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return r;
+}
+
+vistio_status vistio_batch_create(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch** out) {
+  if (!ctx || !solvers || n == 0 || !out) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "empty batch");
+  for (uint32_t k = 0; k < n; ++k)
+    if (!solvers[k]) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null solver in batch");
+  for (uint32_t k = 1; k < n; ++k)
+    if (solvers[k]->cfg.max_iterations != solvers[0]->cfg.max_iterations ||
+        solvers[k]->cfg.al_max_iterations != solvers[0]->cfg.al_max_iterations)
+      return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "instances of a batch must share iteration counts");
+  auto* b = new vistio_batch();
+  vistio_status r = pack_batch(ctx, solvers, n, b);
+  if (r != VISTIO_OK) { delete b; return r; }
+  *out = b;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_destroy(vistio_batch* b) {
+  if (!b) return VISTIO_OK;
+  cudaStreamSynchronize(b->ctx->stream);
+  delete b;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_step(vistio_batch* b, float dt, uint32_t nsteps, const vistio_contact_desc* contact) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  return batch_run(b, dt, nsteps, contact);
+}
+
+vistio_status vistio_batch_upload_positions(vistio_batch* b, const float* xyz) {
+  if (!b || !xyz) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  vistio_ctx* ctx = b->ctx;
+  CU(cudaMemcpy2DAsync(b->pos.p, sizeof(float4), xyz, 3 * sizeof(float), 3 * sizeof(float), b->V,
+                       cudaMemcpyHostToDevice, ctx->stream));
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_download_positions(vistio_batch* b, float* xyz) {
+  if (!b || !xyz) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  vistio_ctx* ctx = b->ctx;
+  CU(cudaMemcpy2DAsync(xyz, 3 * sizeof(float), b->pos.p, sizeof(float4), 3 * sizeof(float), b->V,
+                       cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* ni, uint64_t* tv, uint64_t* tt, uint64_t* th,
+                                uint64_t* fb, uint64_t* db) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  if (ni) *ni = b->ninst;
+  if (tv) *tv = b->V;
+  if (tt) *tt = b->T;
+  if (th) *th = b->H;
+  if (fb) *fb = b->factor_bytes;
+  if (db) *db = b->device_bytes;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* launches) {
+  if (!b || !launches) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  *launches = b->graph_ipc ? b->launches_ipc : b->launches_plain;
+  return VISTIO_OK;
+}
+
+void* vistio_batch_stream(vistio_batch* b) { return b ? (void*)b->ctx->stream : nullptr; }
+
+// ---- SparseSolver mirror (sparse.rs:110-120, faer_solver.rs:67-129) ----
+vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
+                                      const float* values, vistio_factor** out) {
+  if (!ctx || !row_ptr || !col_idx || !values || !out) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  if (n == 0) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "Cannot factorize empty matrix");
+  auto f = std::make_unique<vistio_factor>();
+  f->ctx = ctx;
+  f->n = n;
+  // CSR f32 with possible duplicates -> summed f64 (faer's triplet semantics).
+  std::vector<std::pair<uint64_t, double>> tr;
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p) {
+      if (col_idx[p] >= n) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "column index out of range");
+      tr.push_back({(uint64_t(i) << 32) | col_idx[p], double(values[p])});
+    }
+  std::stable_sort(tr.begin(), tr.end(), [](auto& a, auto& b) { return a.first < b.first; });
+  f->A_ptr.assign(n + 1, 0);
+  for (size_t k = 0; k < tr.size();) {
+    size_t j = k;
+    double s = 0;
+    while (j < tr.size() && tr[j].first == tr[k].first) s += tr[j++].second;
+    uint32_t r = uint32_t(tr[k].first >> 32);
+    f->A_col.push_back(uint32_t(tr[k].first & 0xffffffffu));
+    f->A_val.push_back(s);
+    f->A_ptr[r + 1]++;
+    k = j;
+  }
+  for (uint32_t i = 0; i < n; ++i) f->A_ptr[i + 1] += f->A_ptr[i];
+  // faer reads the upper triangle (Side::Upper): mirror A's upper part.
+  std::vector<uint32_t> up_ptr(n + 1, 0), up_col;
+  std::vector<double> up_val;
+  for (uint32_t i = 0; i < n; ++i) {
+    for (uint32_t p = f->A_ptr[i]; p < f->A_ptr[i + 1]; ++p)
+      if (f->A_col[p] >= i) { up_col.push_back(f->A_col[p]); up_val.push_back(f->A_val[p]); }
+    up_ptr[i + 1] = uint32_t(up_col.size());
+  }
+  int st = 0;
+  std::string err = factorize_csr(n, up_ptr.data(), up_col.data(), up_val.data(), nullptr, f->f, &st);
+  if (!err.empty()) return fail(ctx, st == 11 ? VISTIO_ERR_NOT_SPD : VISTIO_ERR_INVALID_CONFIG, err);
+  // Device layout: a one-instance batch with no elements.
+  auto* s = new vistio_solver();
+  s->ctx = ctx;
+  s->cfg.max_iterations = 1;
+  s->setup.nv = n;
+  s->setup.factor = f->f;
+  s->setup.mass.assign(n, 0.f);
+  s->setup.pinned.assign(n, 0);
+  s->setup.prm.matrix_dt = 1.f;
+  s->host_pos.assign(3 * size_t(n), 0.f);
+  s->host_vel.assign(3 * size_t(n), 0.f);
+  f->b = new vistio_batch();
+  vistio_solver* arr[1] = {s};
+  vistio_status r = pack_batch(ctx, arr, 1, f->b);
+  if (r != VISTIO_OK) { delete f->b; f->b = nullptr; delete s; return r; }
+  StepParams p{};
+  p.dt = 1.f;
+  CU(cudaMemcpy(f->b->prm.p, &p, sizeof(p), cudaMemcpyHostToDevice));
+  *out = f.release();
+  return VISTIO_OK;
+}
+
+vistio_status vistio_sparse_solve(vistio_factor* f, const float* rhs, float* solution) {
+  if (!f) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "Solver not factorized. Call factorize() first.");
+  if (!rhs || !solution) return fail(f->ctx, VISTIO_ERR_INVALID_CONFIG, "null vector");
+  vistio_ctx* ctx = f->ctx;
+  uint32_t n = f->n;
+  vistio_batch* b = f->b;
+  // f32 rhs -> device sweeps in FP32 -> two FP64 iterative-refinement passes
+  // with the residual b - A x formed on the host in f64.
+  std::vector<double> x(n, 0.0), r(n);
+  for (uint32_t i = 0; i < n; ++i) r[i] = double(rhs[i]);
+  std::vector<float4> y(n);
+  for (int pass = 0; pass < 3; ++pass) {
+    for (uint32_t i = 0; i < n; ++i) y[f->f.iperm[i]] = make_float4(float(r[i]), 0.f, 0.f, 0.f);
+    CU(cudaMemcpyAsync(b->Y.p, y.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+    k_solve<kSolveThreads><<<1, kSolveThreads, 0, ctx->stream>>>(b->dev, 0);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(y.data(), b->Y.p, n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (uint32_t i = 0; i < n; ++i) x[i] += double(y[f->f.iperm[i]].x);
+    for (uint32_t i = 0; i < n; ++i) {
+      double s = double(rhs[i]);
+      for (uint32_t p = f->A_ptr[i]; p < f->A_ptr[i + 1]; ++p) s -= f->A_val[p] * x[f->A_col[p]];
+      r[i] = s;
+    }
+  }
+  for (uint32_t i = 0; i < n; ++i) solution[i] = float(x[i]);
+  return VISTIO_OK;
+}
+
+vistio_status vistio_sparse_destroy(vistio_factor* f) {
+  if (!f) return VISTIO_OK;
+  if (f->b) {
+    vistio_solver* s = f->b->solvers.empty() ? nullptr : f->b->solvers[0];
+    delete f->b;
+    delete s;
+  }
+  delete f;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_broadphase_pairs(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py, const float* pz,
+                                      uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs, uint64_t cap,
+                                      uint64_t* count) {
+  return broadphase_pairs_impl(ctx ? ctx->stream : nullptr, ctx ? &ctx->last_error : nullptr, nv, px, py, pz, nt, tris,
+                               margin, pairs, cap, count);
+}
+
+vistio_status vistio_ccd_hits(vistio_ctx* ctx, uint32_t nv, const float* p0, const float* p1, uint32_t nt,
+                              const uint32_t* tris, uint64_t npairs, const uint32_t* pairs, uint32_t* hits,
+                              uint64_t cap, uint64_t* nhits, float* min_toi) {
+  return ccd_hits_impl(ctx ? ctx->stream : nullptr, ctx ? &ctx->last_error : nullptr, nv, p0, p1, nt, tris, npairs,
+                       pairs, hits, cap, nhits, min_toi);
+}
+
+}  // extern "C"
+
+// ======================================================= self-contact host
+namespace vistio {
+
+namespace {
+// Builds the per-garment tree layout and the exclusion lists.
+vistio_status self_build(SelfContactDev& S, const std::vector<std::pair<const uint32_t*, uint32_t>>& tris,
+                         const std::vector<uint32_t>& nverts, const std::vector<uint32_t>& vbase, uint64_t T,
+                         cudaStream_t st, std::string* err) {
+  auto bad = [&](cudaError_t e, const char* what) {
+    if (err) *err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? VISTIO_ERR_OOM : VISTIO_ERR_GPU;
+  };
+  uint32_t n = uint32_t(tris.size());
+  std::vector<SelfInst> si(n);
+  std::vector<uint32_t> tri_inst(T);
+  uint64_t tb = 0, boxes = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    uint32_t nt = tris[k].second;
+    if (nt >= (1u << 26)) { if (err) *err = "too many triangles for self contact"; return VISTIO_ERR_CAPACITY; }
+    SelfInst& I = si[k];
+    std::memset(&I, 0, sizeof(I));
+    I.tbase = uint32_t(tb);
+    I.nt = nt;
+    I.box_base = uint32_t(boxes);
+    uint32_t cnt = nt, off = 0, l = 0;
+    while (true) {
+      I.lvl_off[l] = off;
+      I.lvl_cnt[l] = cnt;
+      off += cnt;
+      ++l;
+      if (cnt <= 1) break;
+      cnt = (cnt + 1) / 2;
+    }
+    I.nlevels = l;
+    boxes += off;
+    for (uint32_t t = 0; t < nt; ++t) tri_inst[tb + t] = k;
+    tb += nt;
+  }
+  // exclusion lists: 1-ring plus the vertex (exclusion.rs:27-58, depth 1), global ids
+  uint64_t V = 0;
+  for (uint32_t k = 0; k < n; ++k) V = std::max<uint64_t>(V, uint64_t(vbase[k]) + nverts[k]);
+  std::vector<std::vector<uint32_t>> ring(V);
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t* t = tris[k].first;
+    for (uint32_t i = 0; i < tris[k].second; ++i) {
+      uint32_t v[3] = {vbase[k] + t[3 * i], vbase[k] + t[3 * i + 1], vbase[k] + t[3 * i + 2]};
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) ring[v[a]].push_back(v[b]);
+    }
+  }
+  std::vector<uint32_t> aptr(V + 1, 0), adj;
+  for (uint64_t v = 0; v < V; ++v) {
+    auto& r = ring[v];
+    r.push_back(uint32_t(v));
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+    adj.insert(adj.end(), r.begin(), r.end());
+    aptr[v + 1] = uint32_t(adj.size());
+  }
+  S.release();
+  S.ninst = n;
+  S.T = T;
+  S.pair_cap = std::max<uint64_t>(1024, 48 * T);
+  S.scan_blocks = uint32_t((T + kScanBlock - 1) / kScanBlock);
+  if (S.scan_blocks == 0) S.scan_blocks = 1;
+  cudaError_t e;
+#define SA(ptr, bytes) if ((e = cudaMalloc(&ptr, bytes)) != cudaSuccess) return bad(e, "cudaMalloc")
+  SA(S.inst, n * sizeof(SelfInst));
+  SA(S.tri_inst, std::max<uint64_t>(T, 1) * 4);
+  SA(S.box_min, std::max<uint64_t>(boxes, 1) * sizeof(float4));
+  SA(S.box_max, std::max<uint64_t>(boxes, 1) * sizeof(float4));
+  SA(S.cnt, std::max<uint64_t>(T, 1) * 4);
+  SA(S.block_sums, S.scan_blocks * 4ull);
+  SA(S.pairs, S.pair_cap * sizeof(uint2));
+  SA(S.npairs, 8);
+  SA(S.adj_ptr, (V + 1) * 4);
+  SA(S.adj, std::max<size_t>(adj.size(), 1) * 4);
+#undef SA
+  if ((e = cudaMemcpyAsync(S.inst, si.data(), n * sizeof(SelfInst), cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
+  if (T && (e = cudaMemcpyAsync(S.tri_inst, tri_inst.data(), T * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
+  if ((e = cudaMemcpyAsync(S.adj_ptr, aptr.data(), (V + 1) * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
+  if (!adj.empty() && (e = cudaMemcpyAsync(S.adj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
+  if ((e = cudaMemsetAsync(S.npairs, 0, 8, st)) != cudaSuccess) return bad(e, "memset");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return bad(e, "sync");
+  S.ready = true;
+  return VISTIO_OK;
+}
+}  // namespace
+
+vistio_status ensure_self_contact(const BatchDev&, SelfContactDev& S, const std::vector<vistio_solver*>& solvers,
+                                  const std::vector<uint32_t>& vbase, uint64_t T, cudaStream_t st, std::string* err) {
+  if (S.ready) return VISTIO_OK;
+  std::vector<std::pair<const uint32_t*, uint32_t>> tris;
+  std::vector<uint32_t> nverts;
+  for (auto* s : solvers) {
+    tris.push_back({s->setup.tris.data(), s->setup.nt});
+    nverts.push_back(s->setup.nv);
+  }
+  return self_build(S, tris, nverts, vbase, T, st, err);
+}
+
+vistio_status broadphase_pairs_impl(cudaStream_t st, std::string* err, uint32_t nv, const float* px, const float* py,
+                                    const float* pz, uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs,
+                                    uint64_t cap, uint64_t* count) {
+  if (!px || !py || !pz || !tris || !count) { if (err) *err = "null argument"; return VISTIO_ERR_INVALID_CONFIG; }
+  if (nt == 0) { *count = 0; return VISTIO_OK; }
+  for (uint64_t k = 0; k < 3ull * nt; ++k)
+    if (tris[k] >= nv) { if (err) *err = "triangle index out of range"; return VISTIO_ERR_INVALID_MESH; }
+  vistio_ctx* ctx = nullptr;
+  std::vector<float4> pos(nv);
+  for (uint32_t i = 0; i < nv; ++i) pos[i] = make_float4(px[i], py[i], pz[i], 0.f);
+  std::vector<uint4> ti(nt);
+  for (uint32_t t = 0; t < nt; ++t) ti[t] = make_uint4(tris[3 * t], tris[3 * t + 1], tris[3 * t + 2], 0u);
+  std::vector<uint64_t> b0{0}, c0{nt};
+  auto ch = make_chunks(b0, c0);
+  DevBuf<float4> dpos; DevBuf<uint4> dti; DevBuf<int4> dch; DevBuf<InstRed> dred; DevBuf<StepParams> dprm;
+  DevBuf<uint32_t> dstatus;
+  CU(dpos.upload(pos, st)); CU(dti.upload(ti, st)); CU(dch.upload(ch, st));
+  CU(dred.alloc(1)); CU(cudaMemsetAsync(dred.p, 0, sizeof(InstRed), st));
+  StepParams p{};
+  std::vector<StepParams> pv{p};
+  CU(dprm.upload(pv, st));
+  CU(dstatus.alloc(1)); CU(cudaMemsetAsync(dstatus.p, 0, 4, st));
+  BatchDev d{};
+  d.pos = dpos.p; d.tri_idx = dti.p; d.tri_chunks = dch.p; d.red = dred.p; d.prm = dprm.p; d.status = dstatus.p;
+  SelfContactDev S;
+  std::vector<std::pair<const uint32_t*, uint32_t>> tl{{tris, nt}};
+  std::vector<uint32_t> nvs{nv}, vb{0};
+  vistio_status r = self_build(S, tl, nvs, vb, nt, st, err);
+  if (r != VISTIO_OK) return r;
+  k_self_boxes<<<1, 1024, 0, st>>>(d, S, margin);
+  k_self_count<<<uint32_t(ch.size()), 256, 0, st>>>(d, S);
+  k_scan_local<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, nt, S.block_sums);
+  k_scan_sums<<<1, kScanBlock, 0, st>>>(S.block_sums, S.scan_blocks, S.npairs);
+  k_scan_add<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, nt, S.block_sums);
+  uint32_t total = 0;
+  CU(cudaMemcpyAsync(&total, S.npairs, 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  if (total > S.pair_cap) {  // grow and recount
+    cudaFree(S.pairs);
+    S.pair_cap = total;
+    CU(cudaMalloc(&S.pairs, uint64_t(total) * sizeof(uint2)));
+  }
+  k_self_write<<<uint32_t(ch.size()), 256, 0, st>>>(d, S);
+  CU(cudaGetLastError());
+  std::vector<uint2> hp(total);
+  if (total) CU(cudaMemcpyAsync(hp.data(), S.pairs, uint64_t(total) * sizeof(uint2), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  std::sort(hp.begin(), hp.end(), [](uint2 a, uint2 b) { return a.x != b.x ? a.x < b.x : a.y < b.y; });
+  *count = total;
+  if (pairs)
+    for (uint64_t k = 0; k < total && k < cap; ++k) { pairs[2 * k] = hp[k].x; pairs[2 * k + 1] = hp[k].y; }
+  if (pairs && total > cap) { if (err) *err = "pair buffer too small"; return VISTIO_ERR_CAPACITY; }
+  return VISTIO_OK;
+}
+
+// FP64 vertex-triangle CCD per candidate pair for the hit-set boundary test.
+__global__ void k_ccd_hits(const float* p0, const float* p1, const uint32_t* tris, const uint32_t* pairs,
+                           uint64_t npairs, uint2* hits, double* tois) {
+  uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= npairs) return;
+  uint32_t ta = pairs[2 * k], tb = pairs[2 * k + 1];
+  uint32_t A[3] = {tris[3 * ta], tris[3 * ta + 1], tris[3 * ta + 2]};
+  uint32_t Bv[3] = {tris[3 * tb], tris[3 * tb + 1], tris[3 * tb + 2]};
+  auto L0 = [&](uint32_t v) { return mk<double>(p0[3 * v], p0[3 * v + 1], p0[3 * v + 2]); };
+  auto L1 = [&](uint32_t v) { return mk<double>(p1[3 * v], p1[3 * v + 1], p1[3 * v + 2]); };
+  for (int side = 0; side < 2; ++side) {
+    const uint32_t* X = side == 0 ? A : Bv;
+    const uint32_t* Y = side == 0 ? Bv : A;
+    uint32_t ty = side == 0 ? tb : ta;
+    for (int q = 0; q < 3; ++q) {
+      uint32_t v = X[q];
+      uint64_t slot = 6 * k + 3 * side + q;
+      hits[slot] = make_uint2(0xffffffffu, 0xffffffffu);
+      tois[slot] = 2.0;
+      if (v == Y[0] || v == Y[1] || v == Y[2]) continue;
+      double t = vt_ccd<double>(L0(v), L1(v), L0(Y[0]), L1(Y[0]), L0(Y[1]), L1(Y[1]), L0(Y[2]), L1(Y[2]));
+      if (t <= 1.0) { hits[slot] = make_uint2(v, ty); tois[slot] = t; }
+    }
+  }
+}
+
+vistio_status ccd_hits_impl(cudaStream_t st, std::string* err, uint32_t nv, const float* p0, const float* p1,
+                            uint32_t nt, const uint32_t* tris, uint64_t npairs, const uint32_t* pairs, uint32_t* hits,
+                            uint64_t cap, uint64_t* nhits, float* min_toi) {
+  if (!p0 || !p1 || !tris || (!pairs && npairs) || !nhits) { if (err) *err = "null argument"; return VISTIO_ERR_INVALID_CONFIG; }
+  for (uint64_t k = 0; k < 2 * npairs; ++k)
+    if (pairs[k] >= nt) { if (err) *err = "pair index out of range"; return VISTIO_ERR_INVALID_CONFIG; }
+  for (uint64_t k = 0; k < 3ull * nt; ++k)
+    if (tris[k] >= nv) { if (err) *err = "triangle index out of range"; return VISTIO_ERR_INVALID_MESH; }
+  vistio_ctx* ctx = nullptr;
+  std::vector<float> a(p0, p0 + 3ull * nv), b(p1, p1 + 3ull * nv);
+  std::vector<uint32_t> tv(tris, tris + 3ull * nt), pv(pairs, pairs + 2 * npairs);
+  DevBuf<float> d0, d1; DevBuf<uint32_t> dt, dp; DevBuf<uint2> dh; DevBuf<double> dtoi;
+  CU(d0.upload(a, st)); CU(d1.upload(b, st)); CU(dt.upload(tv, st)); CU(dp.upload(pv, st));
+  CU(dh.alloc(6 * std::max<uint64_t>(npairs, 1))); CU(dtoi.alloc(6 * std::max<uint64_t>(npairs, 1)));
+  if (npairs) k_ccd_hits<<<uint32_t((npairs + 127) / 128), 128, 0, st>>>(d0.p, d1.p, dt.p, dp.p, npairs, dh.p, dtoi.p);
+  CU(cudaGetLastError());
+  std::vector<uint2> hh(6 * npairs);
+  std::vector<double> tt(6 * npairs);
+  if (npairs) {
+    CU(cudaMemcpyAsync(hh.data(), dh.p, hh.size() * sizeof(uint2), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(tt.data(), dtoi.p, tt.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CU(cudaStreamSynchronize(st));
+  std::vector<std::pair<uint32_t, uint32_t>> out;
+  double mt = 1.0;
+  for (size_t k = 0; k < hh.size(); ++k)
+    if (hh[k].x != 0xffffffffu) { out.push_back({hh[k].x, hh[k].y}); mt = std::min(mt, tt[k]); }
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+  *nhits = out.size();
+  if (min_toi) *min_toi = float(std::max(mt, 1e-6));
+  if (hits)
+    for (size_t k = 0; k < out.size() && k < cap; ++k) { hits[2 * k] = out[k].first; hits[2 * k + 1] = out[k].second; }
+  if (hits && out.size() > cap) { if (err) *err = "hit buffer too small"; return VISTIO_ERR_CAPACITY; }
+  return VISTIO_OK;
+}
+
+}  // namespace vistio
