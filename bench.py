@@ -1,0 +1,380 @@
+"""Benchmark: batched drape steps/s on B200 (the batched-sheets workload).
+
+Workload: 512 hanging sheets of uneven size (grid side 8 distinct values drawn
+uniformly from 16..128 and assigned round-robin, side length U[0.5, 2] m,
+stretch log-U[2e2, 5e3] N/m, bending log-U[1e-5, 1e-3] N m, density
+U[0.08, 0.30] kg/m^2), plain PD step with 10 local-global iterations,
+dt = 1/60 s, seeded synthetic inputs. One step advances every instance once;
+the metric is instance-steps per second over the whole job.
+
+Arms:
+  default            the CUDA batch (one CUDA graph per step over ragged SoA);
+  --impl reference   the reference CPU path (the oracle's FP32 restatement,
+                     since the Rust reference cannot be built here) on all
+                     host threads, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched drape steps/sec vs plain GPU PD at <=1e-4 m err; p50/p99 latency"
+UNIT = "instance-steps/s"
+DT = 1.0 / 60.0
+ITERS = 10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--no-baselines", action="store_true", help="skip the CPU and plain-GPU side measurements")
+    return ap.parse_args()
+
+
+def workload(n_instances, rank=0):
+    from vistio_b200 import scenarios
+    return scenarios.batched_specs(n_instances=n_instances, seed=scenarios.SEED + rank)
+
+
+def config_block(n, gpus):
+    return {"workload": f"batched hanging sheets: {n} instances/GPU, grid side 16-128 (8 topologies), "
+                        f"{ITERS} PD iterations, dt=1/60 s",
+            "instances_per_gpu": n, "iterations": ITERS, "dt": DT, "parallelism": f"instances sharded, {gpus} GPU",
+            "l2": "inputs larger than L2 (factor panels alone exceed 126 MB)"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path) if l.strip()]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- oracle CPU
+def oracle_sample(specs_sample, steps, threads):
+    """Times the oracle's FP32 restatement of the reference step (the
+    reference CPU path) on the given instances; returns (seconds, instance-steps)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    from vistio_b200 import scenarios
+    sims = []
+    for s in specs_sample:
+        m = scenarios.hanging_sheet(s.side, s.length)
+        p = O.init_params(stiffness=s.stretch, bend_stiffness=s.bending, density_gsm=s.density_gsm)
+        sims.append(O.OracleSim(m, p, O.default_config(max_iterations=ITERS), precision=0))
+
+    def run(sim):
+        for _ in range(steps):
+            sim.step(DT)
+
+    t0 = time.perf_counter()
+    if threads <= 1:
+        for sm in sims:
+            run(sm)
+    else:
+        with cf.ThreadPoolExecutor(threads) as ex:
+            list(ex.map(run, sims))
+    return time.perf_counter() - t0, len(sims) * steps
+
+
+def cpu_sample_specs(specs):
+    """One instance of each topology (each topology is 1/8 of the instances)."""
+    seen, out = set(), []
+    for s in specs:
+        if s.side not in seen:
+            seen.add(s.side)
+            out.append(s)
+    return out
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    specs = workload(args.instances)
+    sample = cpu_sample_specs(specs)
+    threads = os.cpu_count() or 1
+    # every step is one step of a bounded sample: each topology x (threads // 8 + 1) copies
+    copies = max(1, threads // len(sample))
+    batch = [s for s in sample for _ in range(copies)]
+    for _ in range(args.warmup):
+        oracle_sample(batch[: len(sample)], 1, threads)
+    secs, units = oracle_sample(batch, args.steps, threads)
+    v = units / secs
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 Cholesky)", "data": "synthetic",
+            "config": config_block(args.instances, args.gpus),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{len(batch)} instances ({copies} of each of the {len(sample)} topologies) "
+                                       f"per step, one instance per host thread"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference is Rust (no toolchain here): its CPU path is timed through the oracle restatement"}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- our arm
+def build_batch(specs, threads):
+    from vistio_b200 import api, scenarios
+    cfg = api.drape_config(max_iterations=ITERS)
+    ctx = api.default_context()
+
+    def make(s):
+        m = scenarios.hanging_sheet(s.side, s.length)
+        setup = api.SetupDesc(stiffness=s.stretch, bend_stiffness=s.bending, density_gsm=s.density_gsm)
+        return api.ProjectiveDynamicsSolver(ctx).init_explicit(m, cfg, setup, pinned=m.pinned)
+
+    order = sorted(range(len(specs)), key=lambda k: -specs[k].side)  # big garments first in the grid
+    with cf.ThreadPoolExecutor(threads) as ex:
+        solvers = list(ex.map(make, [specs[k] for k in order]))
+    return api.Batch(solvers), solvers
+
+
+def oracle_nnz_by_side(specs):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    from vistio_b200 import scenarios
+    out = {}
+    for s in cpu_sample_specs(specs):
+        m = scenarios.hanging_sheet(s.side, 1.0)
+        out[s.side] = O.OracleSim(m, O.init_params(), O.default_config()).factor_nnz()
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from vistio_b200 import api
+    api._default_ctx = api.Context(local)
+
+    threads = max(1, (os.cpu_count() or 1) // max(1, world))
+    specs = workload(args.instances, rank)
+    t0 = time.time()
+    batch, solvers = build_batch(specs, threads)
+    setup_s = time.time() - t0
+    info = batch.info()
+    V = info["vertices"]
+    stream = torch.cuda.ExternalStream(batch.stream())
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        batch.step(DT, 1)
+    torch.cuda.synchronize()
+    launches_per_step = batch.launches_per_step()
+
+    # ---- device-timed region: K steps, per-step events on the batch stream
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            evs[0].record(stream)
+            for k in range(args.steps):
+                batch.step(DT, 1)
+                evs[k + 1].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    total_ms = max_over_ranks(evs[0].elapsed_time(evs[-1]))
+    value = len(specs) * world * args.steps / (total_ms / 1e3)
+    clocks = clk.summary()
+
+    # ---- end to end: positions from pinned host memory in, positions back out, each step
+    host_in = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
+    host_out = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
+    batch.download_positions(host_in.numpy())
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            batch.upload_positions(host_in.numpy())
+            batch.step(DT, 1)
+            batch.download_positions(host_out.numpy())
+            host_in.copy_(host_out)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = len(specs) * world * e2e_steps / (e2e_ms / 1e3)
+
+    # ---- per-kernel timing of one plain iteration's phases (live, CUDA events)
+    phases = ["membrane", "bending", "gather", "solve"]
+    reps = 5
+    kern_ms = {}
+    with torch.cuda.stream(stream):
+        for ph in phases:
+            tot = 0.0
+            for _ in range(reps):
+                if ph == "solve":
+                    batch.launch_phase("gather")  # a fresh residual for the sweep
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                batch.launch_phase(ph)
+                b.record(stream)
+                b.synchronize()
+                tot += a.elapsed_time(b)
+            kern_ms[ph] = tot / reps
+    torch.cuda.synchronize()
+    dom = max(kern_ms, key=kern_ms.get)
+
+    # algorithmic bytes per launch (per-unit figures x units)
+    nnz_ref = oracle_nnz_by_side(specs)
+    nnz_total = sum(nnz_ref[s.side] for s in specs)
+    T, H = info["triangles"], info["hinges"]
+    alg = {"solve": 2 * (8 * nnz_total + 12 * V), "membrane": 32 * T + 12 * V + 36 * T,
+           "bending": 40 * H + 12 * H, "gather": 12 * V * 3 + 36 * T + 12 * H}
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    achieved = alg[dom] / (kern_ms[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": {"solve": "k_solve", "membrane": "k_tri", "bending": "k_hinge",
+                                          "gather": "k_gather"}[dom],
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": "measured" if peaks else "fallback",
+                "traffic": None, "kernel_ms": kern_ms[dom],
+                "phase_ms": kern_ms, "algorithmic_bytes": alg[dom],
+                "kernel_declared_bytes": batch.phase_bytes(dom)}
+    prof = os.path.join(ROOT, "profiles", "k_solve_traffic.json")
+    if os.path.exists(prof):
+        try:
+            tr = json.load(open(prof))
+            if dom == "solve" and tr.get("bytes_per_vertex"):
+                roofline["traffic"] = tr["bytes_per_vertex"] * V
+                roofline["traffic_source"] = tr.get("source")
+        except Exception:
+            pass
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 factorization)", "data": "synthetic",
+           "config": config_block(len(specs), world),
+           "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
+           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 12 * V * world,
+                   "d2h_bytes_per_step": 12 * V * world, "steps": e2e_steps},
+           "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
+           "clocks": clocks, "roofline": roofline,
+           "batch": {"vertices": V, "triangles": T, "hinges": H, "factor_bytes": info["factor_bytes"],
+                     "setup_s": setup_s}}
+
+    if rank == 0 and not args.no_baselines:
+        # plain one-instance-per-launch GPU PD on one instance of each topology
+        from vistio_b200 import api, scenarios
+        sample = cpu_sample_specs(specs)
+        cfg = api.drape_config(max_iterations=ITERS)
+        plain = []
+        for s in sample:
+            m = scenarios.hanging_sheet(s.side, s.length)
+            setup = api.SetupDesc(stiffness=s.stretch, bend_stiffness=s.bending, density_gsm=s.density_gsm)
+            plain.append(api.ProjectiveDynamicsSolver().init_explicit(m, cfg, setup, pinned=m.pinned))
+        for p in plain:
+            p.step(DT)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        psteps = 5
+        for _ in range(psteps):
+            for p in plain:
+                p.step(DT)
+        torch.cuda.synchronize()
+        plain_v = len(plain) * psteps / (time.perf_counter() - t0)
+        out["plain_gpu"] = {"value": plain_v, "unit": UNIT,
+                            "how": "each instance stepped alone (one graph launch per instance-step, result read "
+                                   "back each step), one instance of each topology",
+                            "batched_over_plain": value / world / plain_v}
+        # CPU baseline: the oracle's FP32 restatement, single thread, one instance per topology
+        secs, units = oracle_sample(sample, 2, 1)
+        out["cpu_baseline"] = {"value": units / secs, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": f"one instance of each of the {len(sample)} topologies x 2 steps "
+                                         f"({secs:.1f} s); each topology is 1/8 of the workload"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

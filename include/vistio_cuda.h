@@ -217,6 +217,15 @@ vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, ui
 vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* launches);
 /* The stream the batch runs on (cudaStream_t as void*), for event timing. */
 void* vistio_batch_stream(vistio_batch* b);
+/* Launches one kernel phase of a plain PD iteration on the batch stream, for
+ * per-kernel timing: 0 predict, 1 local membrane, 2 local bending, 3 residual
+ * gather, 4 forward + back substitution (no position update), 5 finalize.
+ * Uses the step constants of the last vistio_batch_step call. Asynchronous. */
+vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase);
+/* Algorithmic bytes of one launch of a phase over the whole batch (see
+ * vistio_batch_launch_phase), from the batch's element counts and factor sizes:
+ * stored factor entries are counted at 4 bytes each. */
+vistio_status vistio_batch_phase_bytes(const vistio_batch* b, int32_t phase, uint64_t* bytes);
 
 /* ---- SparseSolver mirror ---- */
 vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,

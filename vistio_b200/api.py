@@ -367,6 +367,16 @@ class Batch:
     def stream(self) -> int:
         return L.lib().vistio_batch_stream(self.h) or 0
 
+    PHASES = {"predict": 0, "membrane": 1, "bending": 2, "gather": 3, "solve": 4, "finalize": 5}
+
+    def launch_phase(self, phase: str):
+        L.check(L.lib().vistio_batch_launch_phase(self.h, self.PHASES[phase]), self.ctx.h)
+
+    def phase_bytes(self, phase: str) -> int:
+        v = C.c_uint64()
+        L.check(L.lib().vistio_batch_phase_bytes(self.h, self.PHASES[phase], C.byref(v)), self.ctx.h)
+        return v.value
+
 
 class SparseSolver:
     """SparseSolver / FaerSolver mirror (crates/vistio-math/src/sparse.rs:110-120)."""

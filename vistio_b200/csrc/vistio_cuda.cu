@@ -797,6 +797,43 @@ vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* la
 
 void* vistio_batch_stream(vistio_batch* b) { return b ? (void*)b->ctx->stream : nullptr; }
 
+vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  vistio_ctx* ctx = b->ctx;
+  cudaStream_t st = ctx->stream;
+  switch (phase) {
+    case 0: k_predict<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
+    case 1: if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev); break;
+    case 2: if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); break;
+    case 3: k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
+    case 4: k_solve<kSolveThreads><<<b->ninst, kSolveThreads, 0, st>>>(b->dev, 0); break;
+    case 5: k_finalize<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
+    default: return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "unknown phase");
+  }
+  CU(cudaGetLastError());
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_phase_bytes(const vistio_batch* b, int32_t phase, uint64_t* bytes) {
+  if (!b || !bytes) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  uint64_t V = b->V, T = b->T, H = b->H, stored = 0, fwd = 0, rows = 0;
+  for (auto* s : b->solvers) {
+    stored += s->setup.factor.nnz_stored;
+    fwd += s->setup.factor.fwd_sn.size();
+    rows += s->setup.factor.rows.size();
+  }
+  switch (phase) {
+    case 0: *bytes = V * (16 * 4 + 16 + 1); break;            // read x, v; write prev, pred, x
+    case 1: *bytes = T * (16 + 16 + 4 + 36) + 3 * T * 16; break; // indices, Dm^-1, w, 3 contributions; 3 gathered x
+    case 2: *bytes = H * (16 + 16 + 8 + 16) + 4 * H * 16; break; // indices, stencil, (w, theta0), out; 4 gathered x
+    case 3: *bytes = V * (4 + 16 + 16 + 16) + (V + 1) * 8 + 3 * T * (4 + 12) + 4 * H * (4 + 16 + 4); break;
+    case 4: *bytes = 2 * 4 * stored + fwd * 8 + rows * 4 + V * (4 * 16 + 2 * 16) + V * 8; break;
+    case 5: *bytes = V * (16 * 3 + 1 + 16); break;
+    default: return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "unknown phase");
+  }
+  return VISTIO_OK;
+}
+
 // ---- SparseSolver mirror (sparse.rs:110-120, faer_solver.rs:67-129) ----
 vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
                                       const float* values, vistio_factor** out) {
