@@ -17,48 +17,53 @@ using namespace vistio;
 
 template <class T>
 static void sweep(const Factor& F, const std::vector<T>& vals, std::vector<T>& Y) {
+  // Replays k_solve: forward pulls the pushed updates U, applies inv(L_kk) and
+  // pushes U = P y per supernode of each level; backward per level forms
+  // t = y - P^T x and applies inv(L_kk)^T.
   uint32_t n = F.n;
-  std::vector<T> Tm(n);
+  std::vector<T> Tm(n), U(F.rows.size());
   for (uint32_t l = 0; l < F.nlevels; ++l) {
     for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
       uint32_t r = F.level_rows[i];
       T t = Y[r];
-      for (uint32_t q = F.fwd_ptr[r]; q < F.fwd_ptr[r + 1]; ++q) {
-        const Supernode& S = F.sn[F.fwd_sn[q]];
-        const T* pr = vals.data() + S.panel_off + uint64_t(F.fwd_pos[q]) * S.ncols;
-        for (uint32_t c = 0; c < S.ncols; ++c) t -= pr[c] * Y[S.first + c];
-      }
+      for (uint32_t q = F.fwd_ptr[r]; q < F.fwd_ptr[r + 1]; ++q)
+        t -= U[F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]];
       Tm[r] = t;
     }
-    for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
-      uint32_t r = F.level_rows[i];
-      const Supernode& S = F.sn[F.row_sn[r]];
-      uint32_t c = r - S.first, s = S.ncols;
-      const T* D = vals.data() + S.diag_off;
-      T y = 0;
-      for (uint32_t c2 = 0; c2 <= c; ++c2) y += D[uint64_t(c2) * s + c] * Tm[S.first + c2];
-      Y[r] = y;
+    for (uint32_t q = F.level_sn_ptr[l]; q < F.level_sn_ptr[l + 1]; ++q) {
+      const Supernode& S = F.sn[F.level_sn[q]];
+      uint32_t s = S.ncols;
+      const T* D = vals.data() + S.diag_off;  // column-major inverse
+      for (uint32_t c = 0; c < s; ++c) {
+        T y = 0;
+        for (uint32_t c2 = 0; c2 <= c; ++c2) y += D[uint64_t(c2) * s + c] * Tm[S.first + c2];
+        Y[S.first + c] = y;
+      }
+      const T* Pn = vals.data() + S.panel_off;  // row-major m x s
+      for (uint32_t j = 0; j < S.nrows; ++j) {
+        T u = 0;
+        for (uint32_t c = 0; c < s; ++c) u += Pn[uint64_t(j) * s + c] * Y[S.first + c];
+        U[S.rows_off + j] = u;
+      }
     }
   }
   for (int l = int(F.nlevels) - 1; l >= 0; --l) {
-    for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
-      uint32_t r = F.level_rows[i];
-      const Supernode& S = F.sn[F.row_sn[r]];
-      uint32_t c = r - S.first, s = S.ncols;
-      T t = Y[r];
-      const T* pc = vals.data() + S.panel_off + c;
+    for (uint32_t q = F.level_sn_ptr[l]; q < F.level_sn_ptr[l + 1]; ++q) {
+      const Supernode& S = F.sn[F.level_sn[q]];
+      uint32_t s = S.ncols;
+      const T* Pn = vals.data() + S.panel_off;
       const uint32_t* rr = F.rows.data() + S.rows_off;
-      for (uint32_t j = 0; j < S.nrows; ++j) t -= pc[uint64_t(j) * s] * Y[rr[j]];
-      Tm[r] = t;
-    }
-    for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
-      uint32_t r = F.level_rows[i];
-      const Supernode& S = F.sn[F.row_sn[r]];
-      uint32_t c = r - S.first, s = S.ncols;
-      const T* D = vals.data() + S.diag_off + uint64_t(c) * s;
-      T x = 0;
-      for (uint32_t c2 = c; c2 < s; ++c2) x += D[c2] * Tm[S.first + c2];
-      Y[r] = x;
+      for (uint32_t c = 0; c < s; ++c) {
+        T t = 0;
+        for (uint32_t j = 0; j < S.nrows; ++j) t += Pn[uint64_t(j) * s + c] * Y[rr[j]];
+        Tm[S.first + c] = Y[S.first + c] - t;
+      }
+      const T* D = vals.data() + S.diag_off;
+      for (uint32_t c = 0; c < s; ++c) {
+        T x = 0;
+        for (uint32_t c2 = c; c2 < s; ++c2) x += D[uint64_t(c) * s + c2] * Tm[S.first + c2];
+        Y[S.first + c] = x;
+      }
     }
   }
 }

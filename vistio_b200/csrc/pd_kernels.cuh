@@ -21,7 +21,7 @@ namespace vistio {
 
 struct InstDev {
   uint32_t vbase, nv;
-  uint32_t lvl_base, nlvl;
+  uint32_t lvl_base, nlvl;     // offsets into level_ptr / level_sn_ptr
   int32_t model;
   float warp, weft;
   float inv_hmat2;   // 1 / matrix_dt^2
@@ -30,13 +30,18 @@ struct InstDev {
   uint32_t sn_base, nsn;
 };
 
+// One supernode in HBM: an s x s inverted diagonal block and the m x s
+// panel below it, each stored twice so both sweeps read them coalesced:
+//   pt  panel, column-major (PT[c][j] at c*m + j)   forward  u = P y
+//   p   panel, row-major    (P[j][c]  at j*s + c)   backward t -= P^T x
+//   dc  inv(L_kk), column-major (Linv[c][c2] at c2*s + c)  forward
+//   dr  inv(L_kk), row-major    (Linv[c2][c] at c2*s + c)  backward
 struct SnDev {
   uint32_t first;    // first column (instance-local permuted row)
-  uint32_t ncols;
-  uint32_t nrows;
-  uint32_t rows_off; // into rows pool (instance-local rows)
-  uint64_t panel_off;
-  uint64_t diag_off;
+  uint32_t ncols;    // s
+  uint32_t nrows;    // m
+  uint32_t rows_off; // first of the m entries of this supernode in rows / U (global)
+  uint64_t pt_off, p_off, dc_off, dr_off;
 };
 
 // Per-step constants read from device memory so a captured graph stays valid
@@ -111,13 +116,15 @@ struct BatchDev {
   float4* Y;               // rhs / y / delta, indexed by vbase + row
   float4* T;               // scratch of the sweeps
   const SnDev* sn;
-  const uint32_t* rows;
+  const uint32_t* rows;        // below-diagonal rows of every supernode (instance-local)
   const float* vals;
-  const uint32_t* level_ptr;
-  const uint32_t* level_rows;
-  const uint32_t* row_sn;      // global row -> global supernode
-  const uint32_t* fwd_ptr;     // global row -> offsets
-  const uint2* fwd;            // (global supernode, panel row)
+  const uint32_t* level_ptr;   // per instance nlvl+1 offsets into level_rows
+  const uint32_t* level_rows;  // rows of each level (instance-local)
+  const uint32_t* level_sn_ptr;// per instance nlvl+1 offsets into level_sn
+  const uint32_t* level_sn;    // supernodes of each level (global ids), largest first
+  const uint32_t* fwd_ptr;     // global row -> offsets into fwd
+  const uint32_t* fwd;         // U slots summed into the row by the forward sweep
+  float4* U;                   // forward updates, one per (supernode, panel row)
   // contact / IPC
   float4* grad;            // barrier gradient of the detect at the start of the AL pass
   float4* grad_up;         // gradient of the re-detect
@@ -338,90 +345,176 @@ __global__ void __launch_bounds__(256) k_gather(BatchDev B) {
   B.Y[I.vbase + B.perm_local[g]] = make_float4(r.x, r.y, r.z, 0.f);
 }
 
-__device__ __forceinline__ void f4_fms(float4& t, float a, float4 y) {
-  t.x -= a * y.x; t.y -= a * y.y; t.z -= a * y.z;
+__device__ __forceinline__ void f4_fma(float4& t, float a, float4 y) {
+  t.x += a * y.x; t.y += a * y.y; t.z += a * y.z;
+}
+__device__ __forceinline__ float4 f4_sub(float4 a, float4 b) {
+  return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, 0.f);
+}
+
+// y[f..f+s) = inv(L_kk) t  (lanes / threads over c; coalesced dc reads)
+__device__ __forceinline__ void diag_fwd(const SnDev& S, const float* vals, const float4* T, float4* Y,
+                                         uint32_t c0, uint32_t stride) {
+  const float* D = vals + S.dc_off;
+  const uint32_t s = S.ncols, f = S.first;
+  for (uint32_t c = c0; c < s; c += stride) {
+    float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, D[uint64_t(c2) * s + c], T[f + c2]);
+    Y[f + c] = y;
+  }
+}
+// U[j] = P[j,:] . y_k  (lanes / threads over j; coalesced pt reads)
+__device__ __forceinline__ void push_fwd(const SnDev& S, const float* vals, const float4* Y, float4* U,
+                                         uint32_t j0, uint32_t stride) {
+  const float* PT = vals + S.pt_off;
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  for (uint32_t j = j0; j < m; j += stride) {
+    float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (uint32_t c = 0; c < s; ++c) f4_fma(u, PT[uint64_t(c) * m + j], Y[f + c]);
+    U[S.rows_off + j] = u;
+  }
+}
+// x[f..f+s) = inv(L_kk)^T t  (lanes / threads over c; coalesced dr reads)
+__device__ __forceinline__ void diag_bwd(const SnDev& S, const float* vals, const float4* T, float4* Y,
+                                         uint32_t c0, uint32_t stride) {
+  const float* D = vals + S.dr_off;
+  const uint32_t s = S.ncols, f = S.first;
+  for (uint32_t c = c0; c < s; c += stride) {
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, D[uint64_t(c2) * s + c], T[f + c2]);
+    Y[f + c] = x;
+  }
+}
+// Warp-cooperative t[c] = y[c] - sum_j P[j][c] x[R_j]; small panels use
+// (row group, column) lanes and a shuffle reduction over the row groups.
+__device__ __forceinline__ void panel_bwd_warp(const SnDev& S, const float* vals, const uint32_t* rows,
+                                               const float4* Y, float4* T, uint32_t lane) {
+  const float* P = vals + S.p_off;
+  const uint32_t* R = rows + S.rows_off;
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  if (s >= 16) {
+    for (uint32_t c = lane; c < s; c += 32) {
+      float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+      for (uint32_t j = 0; j < m; ++j) f4_fma(t, P[uint64_t(j) * s + c], Y[R[j]]);
+      T[f + c] = f4_sub(Y[f + c], t);
+    }
+  } else {
+    uint32_t sp = s <= 1 ? 1 : s <= 2 ? 2 : s <= 4 ? 4 : s <= 8 ? 8 : 16;
+    uint32_t cc = lane & (sp - 1), jj = lane / sp, G = 32 / sp;
+    float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (cc < s)
+      for (uint32_t j = jj; j < m; j += G) f4_fma(t, P[uint64_t(j) * s + cc], Y[R[j]]);
+    for (uint32_t o = sp; o < 32; o <<= 1) {
+      t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+      t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+      t.z += __shfl_xor_sync(0xffffffffu, t.z, o);
+    }
+    if (jj == 0 && cc < s) T[f + cc] = f4_sub(Y[f + cc], t);
+  }
 }
 
 // Supernodal forward + back substitution for one instance per block, on
-// P A P^T = L L^T with inv(L_kk) stored per supernode; then (plain step) the
-// position update, pin reset, ground clamp and residual sums.
-// Levels of the supernodal elimination tree are separated by __syncthreads.
+// P A P^T = L L^T. Forward: per level, each row pulls the updates U its
+// descendants pushed, the supernode applies inv(L_kk), then pushes its own
+// updates U = P y for its ancestors; backward: per level (top down), each
+// supernode forms t = y - P^T x from its ancestors and applies inv(L_kk)^T.
+// Levels with at least one supernode per warp run a supernode per warp;
+// narrower levels run each supernode with the whole block. Afterwards (plain
+// step) the position update, pin reset, ground clamp and residual sums.
 template <int NT>
 __global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
+  constexpr uint32_t NW = NT / 32;
   const uint32_t inst = blockIdx.x;
   const InstDev I = B.inst[inst];
   const StepParams& P = *B.prm;
   InstRed& R = B.red[inst];
   if (P.ipc && R.al_done) return;
-  const uint32_t vb = I.vbase;
+  const uint32_t vb = I.vbase, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float4* Y = B.Y + vb;
   float4* T = B.T + vb;
   const uint32_t* lp = B.level_ptr + I.lvl_base;
-  // forward: y = L^-1 r
+  const uint32_t* lsp = B.level_sn_ptr + I.lvl_base;
+  __shared__ float4 s_part[NT];
+  // ---- forward: y = L^-1 r
   for (uint32_t l = 0; l < I.nlvl; ++l) {
-    uint32_t b = lp[l], e = lp[l + 1];
-    for (uint32_t i = b + threadIdx.x; i < e; i += NT) {
+    for (uint32_t i = lp[l] + tid, e = lp[l + 1]; i < e; i += NT) {
       uint32_t r = B.level_rows[i];
-      uint32_t g = vb + r;
       float4 t = Y[r];
-      for (uint32_t q = B.fwd_ptr[g], qe = B.fwd_ptr[g + 1]; q < qe; ++q) {
-        uint2 f = B.fwd[q];
-        SnDev S = B.sn[f.x];
-        const float* pr = B.vals + S.panel_off + uint64_t(f.y) * S.ncols;
-        const float4* yy = Y + S.first;
-        for (uint32_t c = 0; c < S.ncols; ++c) f4_fms(t, pr[c], yy[c]);
-      }
+      uint32_t q = B.fwd_ptr[vb + r], qe = B.fwd_ptr[vb + r + 1];
+#pragma unroll 4
+      for (; q < qe; ++q) t = f4_sub(t, B.U[B.fwd[q]]);
       T[r] = t;
     }
     __syncthreads();
-    for (uint32_t i = b + threadIdx.x; i < e; i += NT) {
-      uint32_t r = B.level_rows[i];
-      SnDev S = B.sn[B.row_sn[vb + r]];
-      uint32_t c = r - S.first, s = S.ncols;
-      const float* D = B.vals + S.diag_off;
-      float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (uint32_t c2 = 0; c2 <= c; ++c2) {
-        float a = D[uint64_t(c2) * s + c];
-        float4 tt = T[S.first + c2];
-        y.x += a * tt.x; y.y += a * tt.y; y.z += a * tt.z;
+    uint32_t sb = lsp[l], se = lsp[l + 1];
+    if (se - sb >= NW) {
+      for (uint32_t k = sb + warp; k < se; k += NW) {
+        SnDev S = B.sn[B.level_sn[k]];
+        diag_fwd(S, B.vals, T, Y, lane, 32);
+        __syncwarp();
+        push_fwd(S, B.vals, Y, B.U, lane, 32);
       }
-      Y[r] = y;
+    } else {
+      for (uint32_t k = sb; k < se; ++k) {
+        SnDev S = B.sn[B.level_sn[k]];
+        diag_fwd(S, B.vals, T, Y, tid, NT);
+        __syncthreads();
+        push_fwd(S, B.vals, Y, B.U, tid, NT);
+      }
     }
     __syncthreads();
   }
-  // backward: d = L^-T y
+  // ---- backward: d = L^-T y
   for (int l = int(I.nlvl) - 1; l >= 0; --l) {
-    uint32_t b = lp[l], e = lp[l + 1];
-    for (uint32_t i = b + threadIdx.x; i < e; i += NT) {
-      uint32_t r = B.level_rows[i];
-      SnDev S = B.sn[B.row_sn[vb + r]];
-      uint32_t c = r - S.first, s = S.ncols;
-      float4 t = Y[r];
-      const float* pc = B.vals + S.panel_off + c;
-      const uint32_t* rr = B.rows + S.rows_off;
-      for (uint32_t j = 0; j < S.nrows; ++j) f4_fms(t, pc[uint64_t(j) * s], Y[rr[j]]);
-      T[r] = t;
-    }
-    __syncthreads();
-    for (uint32_t i = b + threadIdx.x; i < e; i += NT) {
-      uint32_t r = B.level_rows[i];
-      SnDev S = B.sn[B.row_sn[vb + r]];
-      uint32_t c = r - S.first, s = S.ncols;
-      const float* D = B.vals + S.diag_off + uint64_t(c) * s;
-      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (uint32_t c2 = c; c2 < s; ++c2) {
-        float a = D[c2];
-        float4 tt = T[S.first + c2];
-        x.x += a * tt.x; x.y += a * tt.y; x.z += a * tt.z;
+    uint32_t sb = lsp[l], se = lsp[l + 1];
+    if (se - sb >= NW) {
+      for (uint32_t k = sb + warp; k < se; k += NW) {
+        SnDev S = B.sn[B.level_sn[k]];
+        panel_bwd_warp(S, B.vals, B.rows, Y, T, lane);
+        __syncwarp();
+        diag_bwd(S, B.vals, T, Y, lane, 32);
       }
-      Y[r] = x;
+    } else {
+      for (uint32_t k = sb; k < se; ++k) {
+        SnDev S = B.sn[B.level_sn[k]];
+        const float* Pm = B.vals + S.p_off;
+        const uint32_t* Rr = B.rows + S.rows_off;
+        const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+        // columns x row-slices: thread (c, part) sums rows j = part (mod np)
+        uint32_t sr = (s + 31) & ~31u;
+        for (uint32_t cb = 0; cb < sr; cb += NT) {
+          uint32_t width = min(sr - cb, (uint32_t)NT);
+          uint32_t np = NT / width;
+          uint32_t c = cb + tid % width, part = tid / width;
+          float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (part < np && c < s)
+            for (uint32_t j = part; j < m; j += np) f4_fma(t, Pm[uint64_t(j) * s + c], Y[Rr[j]]);
+          s_part[tid] = t;
+          __syncthreads();
+          if (tid < width && cb + tid < s) {
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (uint32_t q = 0; q < np; ++q) {
+              float4 v = s_part[q * width + tid];
+              a.x += v.x; a.y += v.y; a.z += v.z;
+            }
+            T[f + cb + tid] = f4_sub(Y[f + cb + tid], a);
+          }
+          __syncthreads();
+        }
+        diag_bwd(S, B.vals, T, Y, tid, NT);
+        __syncthreads();
+      }
     }
     __syncthreads();
   }
   // residual sums (pd_solver.rs:403-421) and, for the plain step, the update.
   double dsq = 0.0, nsq = 0.0;
   bool bad = false;
-  for (uint32_t v = threadIdx.x; v < I.nv; v += NT) {
+  for (uint32_t v = tid; v < I.nv; v += NT) {
     uint32_t g = vb + v;
     float4 d = Y[B.perm_local[g]];
     float4 x = B.pos[g];
@@ -438,17 +531,17 @@ __global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
       B.pos[g] = nx;
     }
   }
-  __shared__ double s_a[NT / 32], s_b[NT / 32];
+  __shared__ double s_a[NW], s_b[NW];
   for (int o = 16; o > 0; o >>= 1) {
     dsq += __shfl_down_sync(0xffffffffu, dsq, o);
     nsq += __shfl_down_sync(0xffffffffu, nsq, o);
   }
-  if ((threadIdx.x & 31) == 0) { s_a[threadIdx.x >> 5] = dsq; s_b[threadIdx.x >> 5] = nsq; }
+  if (lane == 0) { s_a[warp] = dsq; s_b[warp] = nsq; }
   if (bad) atomicOr(B.status, 1u);
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     double a = 0.0, bb = 0.0;
-    for (int k = 0; k < NT / 32; ++k) { a += s_a[k]; bb += s_b[k]; }
+    for (uint32_t k = 0; k < NW; ++k) { a += s_a[k]; bb += s_b[k]; }
     R.diff_sq = a;
     R.norm_sq = bb;
     R.iters += 1;

@@ -468,10 +468,19 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
   f.level_ptr.assign(nl + 1, 0);
   std::vector<std::vector<uint32_t>> bylvl(nl);
   for (uint32_t k = 0; k < nsn; ++k) bylvl[f.sn[k].level].push_back(k);
+  f.level_sn_ptr.assign(nl + 1, 0);
   for (uint32_t l = 0; l < nl; ++l) {
-    for (uint32_t k : bylvl[l])
+    std::stable_sort(bylvl[l].begin(), bylvl[l].end(), [&](uint32_t a, uint32_t b) {
+      uint64_t wa = uint64_t(f.sn[a].ncols) * (f.sn[a].ncols + f.sn[a].nrows);
+      uint64_t wb = uint64_t(f.sn[b].ncols) * (f.sn[b].ncols + f.sn[b].nrows);
+      return wa > wb;
+    });
+    for (uint32_t k : bylvl[l]) {
+      f.level_sn.push_back(k);
       for (uint32_t c = 0; c < f.sn[k].ncols; ++c) f.level_rows.push_back(f.sn[k].first + c);
+    }
     f.level_ptr[l + 1] = uint32_t(f.level_rows.size());
+    f.level_sn_ptr[l + 1] = uint32_t(f.level_sn.size());
   }
   // Forward pull lists.
   f.fwd_ptr.assign(n + 1, 0);

@@ -52,6 +52,8 @@ struct Factor {
   uint32_t nlevels = 0;
   std::vector<uint32_t> level_ptr;  // nlevels+1 offsets into level_rows
   std::vector<uint32_t> level_rows; // rows (columns) of the level's supernodes, grouped by supernode
+  std::vector<uint32_t> level_sn_ptr; // nlevels+1 offsets into level_sn
+  std::vector<uint32_t> level_sn;     // supernodes of each level, largest first
   // Forward-sweep pull lists: for each row r, the (supernode, panel row) pairs
   // of the descendants whose panels hold row r.
   std::vector<uint32_t> fwd_ptr;    // n+1

@@ -95,9 +95,10 @@ struct vistio_batch {
   DevBuf<uint4> tri_idx, hinge_idx;
   DevBuf<float4> tri_dm, hinge_st;
   DevBuf<float2> hinge_wr;
-  DevBuf<uint32_t> vtri_ptr, vtri, vhinge_ptr, vhinge, perm_local, rows, level_ptr, level_rows, row_sn, fwd_ptr, status;
+  DevBuf<uint32_t> vtri_ptr, vtri, vhinge_ptr, vhinge, perm_local, rows, level_ptr, level_rows, level_sn_ptr,
+      level_sn, fwd_ptr, fwd, status;
   DevBuf<SnDev> sn;
-  DevBuf<uint2> fwd;
+  DevBuf<float4> U;
   DevBuf<InstRed> red;
   DevBuf<StepParams> prm;
   SelfContactDev self;       // self-contact buffers (allocated on first use)
@@ -125,6 +126,8 @@ struct vistio_factor {
 namespace {
 
 vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch* b);
+
+inline uint64_t pad4(uint64_t n) { return (n + 3) & ~3ull; }
 
 std::vector<int4> make_chunks(const std::vector<uint64_t>& base, const std::vector<uint64_t>& count) {
   std::vector<int4> ch;
@@ -154,7 +157,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     d.has_ground = solvers[k]->has_ground; d.ground_h = solvers[k]->ground_h;
     d.sn_base = uint32_t(NSN); d.nsn = uint32_t(I.factor.sn.size());
     V += I.nv; T += I.nt; H += I.nh; NSN += I.factor.sn.size(); NROWS += I.factor.rows.size();
-    NVALS += I.factor.vals.size(); NLVL += I.factor.nlevels + 1; NFWD += I.factor.fwd_sn.size();
+    for (const Supernode& X : I.factor.sn) NVALS += 2 * pad4(uint64_t(X.nrows) * X.ncols) + 2 * pad4(uint64_t(X.ncols) * X.ncols);
+    NLVL += I.factor.nlevels + 1; NFWD += I.factor.fwd_sn.size();
   }
   if (V >= (1ull << 31) || 3 * T >= (1ull << 30) || 4 * H >= (1ull << 30))
     return fail(ctx, VISTIO_ERR_CAPACITY, "batch too large for 32-bit element indices");
@@ -169,12 +173,12 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   std::vector<uint4> hinge_idx(H);
   std::vector<float4> hinge_st(H);
   std::vector<float2> hinge_wr(H);
-  std::vector<uint32_t> vtri_ptr(V + 1, 0), vhinge_ptr(V + 1, 0), perm_local(V), row_sn(V), fwd_ptr(V + 1, 0),
-      level_rows, level_ptr, rows;
+  std::vector<uint32_t> vtri_ptr(V + 1, 0), vhinge_ptr(V + 1, 0), perm_local(V), fwd_ptr(V + 1, 0),
+      level_rows, level_ptr, level_sn_ptr, level_sn, rows;
   std::vector<uint32_t> vtri(3 * T), vhinge(4 * H);
   std::vector<SnDev> sn(NSN);
-  std::vector<float> vals(NVALS);
-  std::vector<uint2> fwd(NFWD);
+  std::vector<float> vals(NVALS, 0.f);
+  std::vector<uint32_t> fwd(NFWD);
   level_rows.reserve(V);
   rows.reserve(NROWS);
   uint64_t snb = 0, rowsb = 0, valsb = 0, fwdb = 0;
@@ -202,28 +206,46 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       hinge_st[h0 + h] = make_float4(I.hinge_st[4 * h], I.hinge_st[4 * h + 1], I.hinge_st[4 * h + 2], I.hinge_st[4 * h + 3]);
       hinge_wr[h0 + h] = make_float2(I.hinge_w[h], I.hinge_rest[h]);
     }
-    // factor
-    for (size_t s = 0; s < F.sn.size(); ++s) {
-      const Supernode& X = F.sn[s];
-      SnDev& d = sn[snb + s];
-      d.first = X.first; d.ncols = X.ncols; d.nrows = X.nrows;
+    // factor: each panel and inverted diagonal block twice (see SnDev)
+    for (size_t q = 0; q < F.sn.size(); ++q) {
+      const Supernode& X = F.sn[q];
+      SnDev& d = sn[snb + q];
+      const uint32_t sc = X.ncols, m = X.nrows;
+      d.first = X.first; d.ncols = sc; d.nrows = m;
       d.rows_off = uint32_t(rowsb + X.rows_off);
-      d.panel_off = valsb + X.panel_off;
-      d.diag_off = valsb + X.diag_off;
+      d.pt_off = valsb; valsb += pad4(uint64_t(m) * sc);
+      d.p_off = valsb; valsb += pad4(uint64_t(m) * sc);
+      d.dc_off = valsb; valsb += pad4(uint64_t(sc) * sc);
+      d.dr_off = valsb; valsb += pad4(uint64_t(sc) * sc);
+      const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
+      const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
+      for (uint32_t j = 0; j < m; ++j)
+        for (uint32_t c = 0; c < sc; ++c) {
+          float v = float(Pn[uint64_t(j) * sc + c]);
+          vals[d.p_off + uint64_t(j) * sc + c] = v;
+          vals[d.pt_off + uint64_t(c) * m + j] = v;
+        }
+      for (uint32_t c = 0; c < sc; ++c)
+        for (uint32_t i = 0; i < sc; ++i) {
+          float v = float(Dn[uint64_t(c) * sc + i]);  // row i, column c
+          vals[d.dc_off + uint64_t(c) * sc + i] = v;
+          vals[d.dr_off + uint64_t(i) * sc + c] = v;
+        }
     }
     rows.insert(rows.end(), F.rows.begin(), F.rows.end());
-    for (size_t q = 0; q < F.vals.size(); ++q) vals[valsb + q] = float(F.vals[q]);
-    {  // level_ptr entries are global offsets into level_rows
-      uint32_t base = uint32_t(level_rows.size());
-      for (uint32_t l = 0; l <= F.nlevels; ++l) level_ptr.push_back(base + F.level_ptr[l]);
+    {  // level_ptr / level_sn_ptr entries are global offsets
+      uint32_t base = uint32_t(level_rows.size()), sbase = uint32_t(level_sn.size());
+      for (uint32_t l = 0; l <= F.nlevels; ++l) {
+        level_ptr.push_back(base + F.level_ptr[l]);
+        level_sn_ptr.push_back(sbase + F.level_sn_ptr[l]);
+      }
       level_rows.insert(level_rows.end(), F.level_rows.begin(), F.level_rows.end());
+      for (uint32_t k : F.level_sn) level_sn.push_back(uint32_t(snb + k));
     }
-    for (uint32_t r = 0; r < I.nv; ++r) {
-      row_sn[v0 + r] = uint32_t(snb + F.row_sn[r]);
-      fwd_ptr[v0 + r] = uint32_t(fwdb + F.fwd_ptr[r]);
-    }
-    for (size_t q = 0; q < F.fwd_sn.size(); ++q) fwd[fwdb + q] = make_uint2(uint32_t(snb + F.fwd_sn[q]), F.fwd_pos[q]);
-    snb += F.sn.size(); rowsb += F.rows.size(); valsb += F.vals.size(); fwdb += F.fwd_sn.size();
+    for (uint32_t r = 0; r < I.nv; ++r) fwd_ptr[v0 + r] = uint32_t(fwdb + F.fwd_ptr[r]);
+    for (size_t q = 0; q < F.fwd_sn.size(); ++q)
+      fwd[fwdb + q] = uint32_t(rowsb + F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]);
+    snb += F.sn.size(); rowsb += F.rows.size(); fwdb += F.fwd_sn.size();
   }
   fwd_ptr[V] = uint32_t(fwdb);
   // vertex incidence
@@ -262,7 +284,9 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->Y.alloc(V)); CU(b->Tm.alloc(V));
   CU(b->sn.upload(sn, st)); CU(b->rows.upload(rows, st)); CU(b->vals.upload(vals, st));
   CU(b->level_ptr.upload(level_ptr, st)); CU(b->level_rows.upload(level_rows, st));
-  CU(b->row_sn.upload(row_sn, st)); CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
+  CU(b->level_sn_ptr.upload(level_sn_ptr, st)); CU(b->level_sn.upload(level_sn, st));
+  CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
+  CU(b->U.alloc(rows.size()));
   CU(b->grad.alloc(V)); CU(b->grad_up.alloc(V)); CU(b->lam.alloc(V)); CU(b->fin_n.alloc(V));
   CU(cudaMemsetAsync(b->lam.p, 0, V * sizeof(float4), st));
   CU(cudaMemsetAsync(b->grad.p, 0, V * sizeof(float4), st));
@@ -272,8 +296,9 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->prm.alloc(1));
   CU(b->status.alloc(1)); CU(cudaMemsetAsync(b->status.p, 0, sizeof(uint32_t), st));
   CU(cudaStreamSynchronize(st));
-  b->factor_bytes = vals.size() * sizeof(float) + sn.size() * sizeof(SnDev) + rows.size() * 4 + fwd.size() * 8 +
-                    fwd_ptr.size() * 4 + row_sn.size() * 4 + level_rows.size() * 4 + level_ptr.size() * 4;
+  b->factor_bytes = vals.size() * sizeof(float) + sn.size() * sizeof(SnDev) + rows.size() * 4 + fwd.size() * 4 +
+                    fwd_ptr.size() * 4 + level_rows.size() * 4 + level_ptr.size() * 4 + level_sn.size() * 4 +
+                    level_sn_ptr.size() * 4 + rows.size() * 16;
   b->device_bytes = b->factor_bytes + V * (16 * 10 + 4 + 3 + 4 * 3) + T * (16 + 16 + 4 + 36 + 12) +
                     H * (16 + 16 + 8 + 16 + 16) + (V + 1) * 8;
   BatchDev& d = b->dev;
@@ -284,7 +309,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   d.vtri_ptr = b->vtri_ptr.p; d.vtri = b->vtri.p; d.vhinge_ptr = b->vhinge_ptr.p; d.vhinge = b->vhinge.p;
   d.perm_local = b->perm_local.p; d.row_vertex = nullptr; d.Y = b->Y.p; d.T = b->Tm.p;
   d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.level_ptr = b->level_ptr.p; d.level_rows = b->level_rows.p;
-  d.row_sn = b->row_sn.p; d.fwd_ptr = b->fwd_ptr.p; d.fwd = b->fwd.p;
+  d.level_sn_ptr = b->level_sn_ptr.p; d.level_sn = b->level_sn.p;
+  d.fwd_ptr = b->fwd_ptr.p; d.fwd = b->fwd.p; d.U = b->U.p;
   d.grad = b->grad.p; d.grad_up = b->grad_up.p; d.lam = b->lam.p; d.fin_n = b->fin_n.p;
   d.in_contact = b->in_contact.p; d.in_contact_up = b->in_contact_up.p; d.ever = b->ever.p;
   d.red = b->red.p; d.prm = b->prm.p; d.status = b->status.p;
@@ -827,7 +853,7 @@ vistio_status vistio_batch_phase_bytes(const vistio_batch* b, int32_t phase, uin
     case 1: *bytes = T * (16 + 16 + 4 + 36) + 3 * T * 16; break; // indices, Dm^-1, w, 3 contributions; 3 gathered x
     case 2: *bytes = H * (16 + 16 + 8 + 16) + 4 * H * 16; break; // indices, stencil, (w, theta0), out; 4 gathered x
     case 3: *bytes = V * (4 + 16 + 16 + 16) + (V + 1) * 8 + 3 * T * (4 + 12) + 4 * H * (4 + 16 + 4); break;
-    case 4: *bytes = 2 * 4 * stored + fwd * 8 + rows * 4 + V * (4 * 16 + 2 * 16) + V * 8; break;
+    case 4: *bytes = 2 * 4 * stored + fwd * 4 + rows * (4 + 2 * 16) + V * (4 * 16 + 2 * 16) + V * 8; break;
     case 5: *bytes = V * (16 * 3 + 1 + 16); break;
     default: return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "unknown phase");
   }
