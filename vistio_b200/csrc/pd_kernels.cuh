@@ -30,18 +30,17 @@ struct InstDev {
   uint32_t sn_base, nsn;
 };
 
-// One supernode in HBM: an s x s inverted diagonal block and the m x s
-// panel below it, each stored twice so both sweeps read them coalesced:
-//   pt  panel, column-major (PT[c][j] at c*m + j)   forward  u = P y
-//   p   panel, row-major    (P[j][c]  at j*s + c)   backward t -= P^T x
-//   dc  inv(L_kk), column-major (Linv[c][c2] at c2*s + c)  forward
-//   dr  inv(L_kk), row-major    (Linv[c2][c] at c2*s + c)  backward
+// One supernode in HBM: one contiguous, 16-byte aligned region holding
+//   D  inv(L_kk), s x s column-major (Linv[c][c2] at c2*s + c), then
+//   P  the m x s panel below the diagonal block, row-major (P[j][c] at j*s + c).
+// Both sweeps stage it through shared memory in row chunks.
 struct SnDev {
   uint32_t first;    // first column (instance-local permuted row)
   uint32_t ncols;    // s
   uint32_t nrows;    // m
   uint32_t rows_off; // first of the m entries of this supernode in rows / U (global)
-  uint64_t pt_off, p_off, dc_off, dr_off;
+  uint64_t d_off;    // D (float offset, multiple of 4)
+  uint64_t p_off;    // P (float offset)
 };
 
 // Per-step constants read from device memory so a captured graph stays valid
@@ -351,83 +350,162 @@ __device__ __forceinline__ void f4_fma(float4& t, float a, float4 y) {
 __device__ __forceinline__ float4 f4_sub(float4 a, float4 b) {
   return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, 0.f);
 }
+__device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, 0.f);
+}
 
-// y[f..f+s) = inv(L_kk) t  (lanes / threads over c; coalesced dc reads)
-__device__ __forceinline__ void diag_fwd(const SnDev& S, const float* vals, const float4* T, float4* Y,
-                                         uint32_t c0, uint32_t stride) {
-  const float* D = vals + S.dc_off;
-  const uint32_t s = S.ncols, f = S.first;
-  for (uint32_t c = c0; c < s; c += stride) {
-    float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+// Shared-memory sizing of k_solve: each warp owns a staging buffer of
+// kWarpFloats floats and kWarpVec float4 vector slots; a narrow level uses
+// all of them as one block-wide buffer.
+constexpr uint32_t kSolveWarps = 8;
+constexpr uint32_t kWarpFloats = 1792;
+constexpr uint32_t kWarpVec = 48;
+constexpr uint32_t kSolveSmem = kSolveWarps * (kWarpFloats * 4 + 3 * kWarpVec * 16);
+constexpr uint32_t kMaxSupernode = 256;  // enforced by the host set-up
+
+// A team is either one warp (a supernode per warp) or the whole block.
+struct Team {
+  uint32_t rank, size;
+  float* buf;      // staging buffer
+  uint32_t cap;    // floats in buf
+  float4* v0;      // vector slots (s entries each) ...
+  float4* v1;
+  float4* xg;      // gathered ancestor values, xcap entries
+  uint32_t vcap, xcap;
+  bool block;
+  __device__ __forceinline__ void sync() const {
+    if (block) __syncthreads();
+    else __syncwarp();
+  }
+};
+
+// Copies n floats into shared memory with independent, coalesced loads.
+__device__ __forceinline__ void stage(const Team& tm, float* dst, const float* __restrict__ src, uint32_t n) {
+  uint32_t i = tm.rank;
 #pragma unroll 4
-    for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, D[uint64_t(c2) * s + c], T[f + c2]);
+  for (; i < n; i += tm.size) dst[i] = __ldg(src + i);
+}
+
+// Forward step of one supernode: t = r - (pulled updates); y = inv(L_kk) t;
+// push U[j] = P[j,:] . y for every panel row.
+__device__ __forceinline__ void sn_forward(const BatchDev& B, const Team& tm, const SnDev& S, float4* Y,
+                                           uint32_t vb) {
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  const float* D = B.vals + S.d_off;
+  const float* Pp = B.vals + S.p_off;
+  for (uint32_t c = tm.rank; c < s; c += tm.size) {
+    float4 t = Y[f + c];
+    uint32_t q = B.fwd_ptr[vb + f + c], qe = B.fwd_ptr[vb + f + c + 1];
+#pragma unroll 4
+    for (; q < qe; ++q) t = f4_sub(t, B.U[B.fwd[q]]);
+    tm.v0[c] = t;
+  }
+  const bool dfit = s * s <= tm.cap;
+  if (dfit) stage(tm, tm.buf, D, s * s);
+  tm.sync();
+  for (uint32_t c = tm.rank; c < s; c += tm.size) {
+    float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (dfit) {
+      for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, tm.buf[c2 * s + c], tm.v0[c2]);
+    } else {
+#pragma unroll 4
+      for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, __ldg(D + uint64_t(c2) * s + c), tm.v0[c2]);
+    }
+    tm.v1[c] = y;
     Y[f + c] = y;
   }
-}
-// U[j] = P[j,:] . y_k  (lanes / threads over j; coalesced pt reads)
-__device__ __forceinline__ void push_fwd(const SnDev& S, const float* vals, const float4* Y, float4* U,
-                                         uint32_t j0, uint32_t stride) {
-  const float* PT = vals + S.pt_off;
-  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
-  for (uint32_t j = j0; j < m; j += stride) {
-    float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 4
-    for (uint32_t c = 0; c < s; ++c) f4_fma(u, PT[uint64_t(c) * m + j], Y[f + c]);
-    U[S.rows_off + j] = u;
+  tm.sync();
+  if (m == 0) return;
+  const uint32_t rc = max(1u, tm.cap / s);
+  for (uint32_t j0 = 0; j0 < m; j0 += rc) {
+    uint32_t nr = min(rc, m - j0);
+    stage(tm, tm.buf, Pp + uint64_t(j0) * s, nr * s);
+    tm.sync();
+    for (uint32_t j = tm.rank; j < nr; j += tm.size) {
+      float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float* row = tm.buf + j * s;
+      for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], tm.v1[c]);
+      B.U[S.rows_off + j0 + j] = u;
+    }
+    tm.sync();
   }
 }
-// x[f..f+s) = inv(L_kk)^T t  (lanes / threads over c; coalesced dr reads)
-__device__ __forceinline__ void diag_bwd(const SnDev& S, const float* vals, const float4* T, float4* Y,
-                                         uint32_t c0, uint32_t stride) {
-  const float* D = vals + S.dr_off;
-  const uint32_t s = S.ncols, f = S.first;
-  for (uint32_t c = c0; c < s; c += stride) {
+
+// Backward step of one supernode: t = y - P^T x[R]; x = inv(L_kk)^T t.
+// Team members split columns (width) x row slices (parts).
+__device__ __forceinline__ void sn_backward(const BatchDev& B, const Team& tm, const SnDev& S, float4* Y) {
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  const float* D = B.vals + S.d_off;
+  const float* Pp = B.vals + S.p_off;
+  const uint32_t* Rr = B.rows + S.rows_off;
+  for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
+  uint32_t width = 1;
+  while (width < s && width < tm.size) width <<= 1;
+  const uint32_t parts = tm.size / width;
+  const uint32_t cl = tm.rank % width, part = tm.rank / width;
+  const uint32_t rc = max(1u, min(tm.cap / s, tm.xcap));
+  for (uint32_t cb = 0; cb < s; cb += width) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t c = cb + cl;
+    for (uint32_t j0 = 0; j0 < m; j0 += rc) {
+      uint32_t nr = min(rc, m - j0);
+      stage(tm, tm.buf, Pp + uint64_t(j0) * s, nr * s);
+      for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = Y[Rr[j0 + j]];
+      tm.sync();
+      if (c < s && part < parts)
+        for (uint32_t j = part; j < nr; j += parts) f4_fma(acc, tm.buf[j * s + c], tm.xg[j]);
+      tm.sync();
+    }
+    // reduce the row slices (parts) of every column
+    if (!tm.block) {
+      for (uint32_t o = width; o < 32; o <<= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
+      }
+      if (part == 0 && c < s) tm.v0[c] = f4_sub(tm.v1[c], acc);
+    } else {
+      float4* red = tm.xg;  // xcap >= block size
+      red[tm.rank] = acc;
+      tm.sync();
+      if (tm.rank < width && cb + tm.rank < s) {
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t q = 0; q < parts; ++q) a = f4_add(a, red[q * width + tm.rank]);
+        tm.v0[cb + tm.rank] = f4_sub(tm.v1[cb + tm.rank], a);
+      }
+    }
+    tm.sync();
+  }
+  const bool dfit = s * s <= tm.cap;
+  if (dfit) {
+    stage(tm, tm.buf, D, s * s);
+    tm.sync();
+  }
+  for (uint32_t c = tm.rank; c < s; c += tm.size) {
     float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (dfit) {
+      for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, tm.buf[c * s + c2], tm.v0[c2]);
+    } else {
 #pragma unroll 4
-    for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, D[uint64_t(c2) * s + c], T[f + c2]);
+      for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, __ldg(D + uint64_t(c) * s + c2), tm.v0[c2]);
+    }
     Y[f + c] = x;
   }
-}
-// Warp-cooperative t[c] = y[c] - sum_j P[j][c] x[R_j]; small panels use
-// (row group, column) lanes and a shuffle reduction over the row groups.
-__device__ __forceinline__ void panel_bwd_warp(const SnDev& S, const float* vals, const uint32_t* rows,
-                                               const float4* Y, float4* T, uint32_t lane) {
-  const float* P = vals + S.p_off;
-  const uint32_t* R = rows + S.rows_off;
-  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
-  if (s >= 16) {
-    for (uint32_t c = lane; c < s; c += 32) {
-      float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 4
-      for (uint32_t j = 0; j < m; ++j) f4_fma(t, P[uint64_t(j) * s + c], Y[R[j]]);
-      T[f + c] = f4_sub(Y[f + c], t);
-    }
-  } else {
-    uint32_t sp = s <= 1 ? 1 : s <= 2 ? 2 : s <= 4 ? 4 : s <= 8 ? 8 : 16;
-    uint32_t cc = lane & (sp - 1), jj = lane / sp, G = 32 / sp;
-    float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (cc < s)
-      for (uint32_t j = jj; j < m; j += G) f4_fma(t, P[uint64_t(j) * s + cc], Y[R[j]]);
-    for (uint32_t o = sp; o < 32; o <<= 1) {
-      t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
-      t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
-      t.z += __shfl_xor_sync(0xffffffffu, t.z, o);
-    }
-    if (jj == 0 && cc < s) T[f + cc] = f4_sub(Y[f + cc], t);
-  }
+  tm.sync();
 }
 
 // Supernodal forward + back substitution for one instance per block, on
-// P A P^T = L L^T. Forward: per level, each row pulls the updates U its
-// descendants pushed, the supernode applies inv(L_kk), then pushes its own
-// updates U = P y for its ancestors; backward: per level (top down), each
-// supernode forms t = y - P^T x from its ancestors and applies inv(L_kk)^T.
-// Levels with at least one supernode per warp run a supernode per warp;
-// narrower levels run each supernode with the whole block. Afterwards (plain
-// step) the position update, pin reset, ground clamp and residual sums.
+// P A P^T = L L^T. Per level of the supernodal elimination tree: supernodes
+// too large for a warp's staging buffer run one at a time with the whole
+// block, the rest run one per warp. Forward rows pull the updates U their
+// descendants pushed; backward rows read their ancestors' solutions.
+// Afterwards (plain step) the position update, pin reset, ground clamp and
+// residual sums.
 template <int NT>
 __global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
-  constexpr uint32_t NW = NT / 32;
+  static_assert(NT == 32 * kSolveWarps, "k_solve block size");
+  constexpr uint32_t NW = kSolveWarps;
+  extern __shared__ float4 smem4[];
   const uint32_t inst = blockIdx.x;
   const InstDev I = B.inst[inst];
   const StepParams& P = *B.prm;
@@ -435,80 +513,39 @@ __global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
   if (P.ipc && R.al_done) return;
   const uint32_t vb = I.vbase, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float4* Y = B.Y + vb;
-  float4* T = B.T + vb;
-  const uint32_t* lp = B.level_ptr + I.lvl_base;
   const uint32_t* lsp = B.level_sn_ptr + I.lvl_base;
-  __shared__ float4 s_part[NT];
-  // ---- forward: y = L^-1 r
+  float* fbuf = reinterpret_cast<float*>(smem4);
+  float4* vbuf = smem4 + NW * kWarpFloats / 4;
+  Team wt{lane, 32, fbuf + warp * kWarpFloats, kWarpFloats, vbuf + warp * 3 * kWarpVec,
+          vbuf + warp * 3 * kWarpVec + kWarpVec, vbuf + warp * 3 * kWarpVec + 2 * kWarpVec, kWarpVec, kWarpVec, false};
+  // block team: all warps' buffers; the 1152 vector slots split 448 / 448 / 256
+  // (supernodes have at most kMaxSupernode <= 448 columns; xg doubles as the
+  // NT-entry reduction buffer).
+  static_assert(3 * kWarpVec * kSolveWarps >= 448 + 448 + NT, "block-team vector slots");
+  Team bt{tid, NT, fbuf, NW * kWarpFloats, vbuf, vbuf + 448, vbuf + 896, 448, NT, true};
+  auto fits_warp = [&](const SnDev& S) { return S.ncols <= kWarpVec && S.ncols * S.ncols <= kWarpFloats; };
+  // ---- forward
   for (uint32_t l = 0; l < I.nlvl; ++l) {
-    for (uint32_t i = lp[l] + tid, e = lp[l + 1]; i < e; i += NT) {
-      uint32_t r = B.level_rows[i];
-      float4 t = Y[r];
-      uint32_t q = B.fwd_ptr[vb + r], qe = B.fwd_ptr[vb + r + 1];
-#pragma unroll 4
-      for (; q < qe; ++q) t = f4_sub(t, B.U[B.fwd[q]]);
-      T[r] = t;
-    }
-    __syncthreads();
     uint32_t sb = lsp[l], se = lsp[l + 1];
-    if (se - sb >= NW) {
-      for (uint32_t k = sb + warp; k < se; k += NW) {
-        SnDev S = B.sn[B.level_sn[k]];
-        diag_fwd(S, B.vals, T, Y, lane, 32);
-        __syncwarp();
-        push_fwd(S, B.vals, Y, B.U, lane, 32);
-      }
-    } else {
-      for (uint32_t k = sb; k < se; ++k) {
-        SnDev S = B.sn[B.level_sn[k]];
-        diag_fwd(S, B.vals, T, Y, tid, NT);
-        __syncthreads();
-        push_fwd(S, B.vals, Y, B.U, tid, NT);
-      }
+    uint32_t k = sb;
+    for (; k < se; ++k) {  // largest first: the block handles the ones a warp cannot
+      SnDev S = B.sn[B.level_sn[k]];
+      if (fits_warp(S) && se - k >= 2) break;
+      sn_forward(B, bt, S, Y, vb);
     }
+    for (uint32_t q = k + warp; q < se; q += NW) sn_forward(B, wt, B.sn[B.level_sn[q]], Y, vb);
     __syncthreads();
   }
-  // ---- backward: d = L^-T y
+  // ---- backward
   for (int l = int(I.nlvl) - 1; l >= 0; --l) {
     uint32_t sb = lsp[l], se = lsp[l + 1];
-    if (se - sb >= NW) {
-      for (uint32_t k = sb + warp; k < se; k += NW) {
-        SnDev S = B.sn[B.level_sn[k]];
-        panel_bwd_warp(S, B.vals, B.rows, Y, T, lane);
-        __syncwarp();
-        diag_bwd(S, B.vals, T, Y, lane, 32);
-      }
-    } else {
-      for (uint32_t k = sb; k < se; ++k) {
-        SnDev S = B.sn[B.level_sn[k]];
-        const float* Pm = B.vals + S.p_off;
-        const uint32_t* Rr = B.rows + S.rows_off;
-        const uint32_t s = S.ncols, m = S.nrows, f = S.first;
-        // columns x row-slices: thread (c, part) sums rows j = part (mod np)
-        uint32_t sr = (s + 31) & ~31u;
-        for (uint32_t cb = 0; cb < sr; cb += NT) {
-          uint32_t width = min(sr - cb, (uint32_t)NT);
-          uint32_t np = NT / width;
-          uint32_t c = cb + tid % width, part = tid / width;
-          float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (part < np && c < s)
-            for (uint32_t j = part; j < m; j += np) f4_fma(t, Pm[uint64_t(j) * s + c], Y[Rr[j]]);
-          s_part[tid] = t;
-          __syncthreads();
-          if (tid < width && cb + tid < s) {
-            float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (uint32_t q = 0; q < np; ++q) {
-              float4 v = s_part[q * width + tid];
-              a.x += v.x; a.y += v.y; a.z += v.z;
-            }
-            T[f + cb + tid] = f4_sub(Y[f + cb + tid], a);
-          }
-          __syncthreads();
-        }
-        diag_bwd(S, B.vals, T, Y, tid, NT);
-        __syncthreads();
-      }
+    uint32_t k = sb;
+    for (; k < se; ++k) {
+      SnDev S = B.sn[B.level_sn[k]];
+      if (fits_warp(S) && se - k >= 2) break;
+      sn_backward(B, bt, S, Y);
     }
+    for (uint32_t q = k + warp; q < se; q += NW) sn_backward(B, wt, B.sn[B.level_sn[q]], Y);
     __syncthreads();
   }
   // residual sums (pd_solver.rs:403-421) and, for the plain step, the update.

@@ -352,7 +352,8 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
     std::vector<uint32_t> nkids(n, 0);
     for (uint32_t j = 0; j < n; ++j) if (parent[j] >= 0) nkids[parent[j]]++;
     for (uint32_t j = 0; j < n; ++j) {
-      bool cont = j > 0 && parent[j - 1] == int(j) && nkids[j] == 1 && cnt[j - 1] == cnt[j] + 1;
+      bool cont = j > 0 && parent[j - 1] == int(j) && nkids[j] == 1 && cnt[j - 1] == cnt[j] + 1 &&
+                  j - sfirst.back() < kMaxSupernodeCols;
       if (!cont) sfirst.push_back(j);
     }
   }
@@ -389,7 +390,8 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
           actual += cnt[j];
         }
         uint64_t zeros = dense - actual;
-        bool ok = (s_new <= 8) || (s_new <= 32 && zeros * 5 <= dense) || (s_new <= 256 && zeros * 20 <= dense);
+        bool ok = (s_new <= 8) || (s_new <= 32 && zeros * 5 <= dense) ||
+                  (s_new <= kMaxSupernodeCols && zeros * 20 <= dense);
         if (!ok) break;
         SN m;
         m.f = cur_sn.f;

@@ -27,6 +27,9 @@ struct SetupParams {
   float matrix_dt = 1.0f / 60.0f; // dt used in A (the reference always assembles with 1/60)
 };
 
+// Largest supernode (columns); the GPU sweeps size their shared-memory vectors for it.
+constexpr uint32_t kMaxSupernodeCols = 256;
+
 // Supernodal factor of P A P^T = L L^T in the layout the GPU sweeps read.
 // Columns are in the permuted (elimination) order.
 struct Supernode {

@@ -42,7 +42,7 @@ struct vistio_solver {
 namespace {
 
 constexpr int kElemThreads = 256;
-constexpr int kSolveThreads = 256;
+constexpr int kSolveThreads = 32 * kSolveWarps;
 
 thread_local std::string g_tls_error;
 
@@ -157,7 +157,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     d.has_ground = solvers[k]->has_ground; d.ground_h = solvers[k]->ground_h;
     d.sn_base = uint32_t(NSN); d.nsn = uint32_t(I.factor.sn.size());
     V += I.nv; T += I.nt; H += I.nh; NSN += I.factor.sn.size(); NROWS += I.factor.rows.size();
-    for (const Supernode& X : I.factor.sn) NVALS += 2 * pad4(uint64_t(X.nrows) * X.ncols) + 2 * pad4(uint64_t(X.ncols) * X.ncols);
+    for (const Supernode& X : I.factor.sn) NVALS += pad4(uint64_t(X.ncols) * X.ncols) + pad4(uint64_t(X.nrows) * X.ncols);
     NLVL += I.factor.nlevels + 1; NFWD += I.factor.fwd_sn.size();
   }
   if (V >= (1ull << 31) || 3 * T >= (1ull << 30) || 4 * H >= (1ull << 30))
@@ -206,31 +206,19 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       hinge_st[h0 + h] = make_float4(I.hinge_st[4 * h], I.hinge_st[4 * h + 1], I.hinge_st[4 * h + 2], I.hinge_st[4 * h + 3]);
       hinge_wr[h0 + h] = make_float2(I.hinge_w[h], I.hinge_rest[h]);
     }
-    // factor: each panel and inverted diagonal block twice (see SnDev)
+    // factor: per supernode one 16-byte aligned region [D | P] (see SnDev)
     for (size_t q = 0; q < F.sn.size(); ++q) {
       const Supernode& X = F.sn[q];
       SnDev& d = sn[snb + q];
       const uint32_t sc = X.ncols, m = X.nrows;
       d.first = X.first; d.ncols = sc; d.nrows = m;
       d.rows_off = uint32_t(rowsb + X.rows_off);
-      d.pt_off = valsb; valsb += pad4(uint64_t(m) * sc);
+      d.d_off = valsb; valsb += pad4(uint64_t(sc) * sc);
       d.p_off = valsb; valsb += pad4(uint64_t(m) * sc);
-      d.dc_off = valsb; valsb += pad4(uint64_t(sc) * sc);
-      d.dr_off = valsb; valsb += pad4(uint64_t(sc) * sc);
       const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
       const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
-      for (uint32_t j = 0; j < m; ++j)
-        for (uint32_t c = 0; c < sc; ++c) {
-          float v = float(Pn[uint64_t(j) * sc + c]);
-          vals[d.p_off + uint64_t(j) * sc + c] = v;
-          vals[d.pt_off + uint64_t(c) * m + j] = v;
-        }
-      for (uint32_t c = 0; c < sc; ++c)
-        for (uint32_t i = 0; i < sc; ++i) {
-          float v = float(Dn[uint64_t(c) * sc + i]);  // row i, column c
-          vals[d.dc_off + uint64_t(c) * sc + i] = v;
-          vals[d.dr_off + uint64_t(i) * sc + c] = v;
-        }
+      for (uint64_t e = 0; e < uint64_t(m) * sc; ++e) vals[d.p_off + e] = float(Pn[e]);
+      for (uint64_t e = 0; e < uint64_t(sc) * sc; ++e) vals[d.d_off + e] = float(Dn[e]);
     }
     rows.insert(rows.end(), F.rows.begin(), F.rows.end());
     {  // level_ptr / level_sn_ptr entries are global offsets
@@ -372,7 +360,7 @@ void launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update) {
   if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev);
   if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev);
   k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
-  k_solve<kSolveThreads><<<b->ninst, kSolveThreads, 0, st>>>(b->dev, do_update);
+  k_solve<kSolveThreads><<<b->ninst, kSolveThreads, kSolveSmem, st>>>(b->dev, do_update);
 }
 
 vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out, uint32_t* nlaunch) {
@@ -546,6 +534,7 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   ctx = c.get();
   CU(cudaSetDevice(device));
   CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CU(cudaFuncSetAttribute(k_solve<kSolveThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   *out = c.release();
   return VISTIO_OK;
 }
@@ -832,7 +821,7 @@ vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase) {
     case 1: if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev); break;
     case 2: if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); break;
     case 3: k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
-    case 4: k_solve<kSolveThreads><<<b->ninst, kSolveThreads, 0, st>>>(b->dev, 0); break;
+    case 4: k_solve<kSolveThreads><<<b->ninst, kSolveThreads, kSolveSmem, st>>>(b->dev, 0); break;
     case 5: k_finalize<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
     default: return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "unknown phase");
   }
@@ -853,7 +842,7 @@ vistio_status vistio_batch_phase_bytes(const vistio_batch* b, int32_t phase, uin
     case 1: *bytes = T * (16 + 16 + 4 + 36) + 3 * T * 16; break; // indices, Dm^-1, w, 3 contributions; 3 gathered x
     case 2: *bytes = H * (16 + 16 + 8 + 16) + 4 * H * 16; break; // indices, stencil, (w, theta0), out; 4 gathered x
     case 3: *bytes = V * (4 + 16 + 16 + 16) + (V + 1) * 8 + 3 * T * (4 + 12) + 4 * H * (4 + 16 + 4); break;
-    case 4: *bytes = 2 * 4 * stored + fwd * 4 + rows * (4 + 2 * 16) + V * (4 * 16 + 2 * 16) + V * 8; break;
+    case 4: *bytes = 2 * 4 * stored + fwd * 4 + rows * (4 + 2 * 16) + V * (2 * 16 + 2 * 16) + V * 8; break;
     case 5: *bytes = V * (16 * 3 + 1 + 16); break;
     default: return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "unknown phase");
   }
@@ -935,7 +924,7 @@ vistio_status vistio_sparse_solve(vistio_factor* f, const float* rhs, float* sol
   for (int pass = 0; pass < 3; ++pass) {
     for (uint32_t i = 0; i < n; ++i) y[f->f.iperm[i]] = make_float4(float(r[i]), 0.f, 0.f, 0.f);
     CU(cudaMemcpyAsync(b->Y.p, y.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
-    k_solve<kSolveThreads><<<1, kSolveThreads, 0, ctx->stream>>>(b->dev, 0);
+    k_solve<kSolveThreads><<<1, kSolveThreads, kSolveSmem, ctx->stream>>>(b->dev, 0);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(y.data(), b->Y.p, n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
