@@ -363,32 +363,89 @@ constexpr uint32_t kWarpVec = 48;
 constexpr uint32_t kSolveSmem = kSolveWarps * (kWarpFloats * 4 + 3 * kWarpVec * 16);
 constexpr uint32_t kMaxSupernode = 256;  // enforced by the host set-up
 
+// ------------------------------------------------ TMA bulk staging
+// A contiguous global range is brought into shared memory with one
+// cp.async.bulk (TMA) whose completion is tracked by an mbarrier
+// transaction count. Waits are bounded: after kWaitLimit polls the team
+// records VISTIO timeout status bit 2 and stops using the data.
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// One thread: expect `bytes` on the barrier and start the bulk copy.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t b = smem_u32(bar);
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(b), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // A team is either one warp (a supernode per warp) or the whole block.
 struct Team {
   uint32_t rank, size;
-  float* buf;      // staging buffer
+  float* buf;      // staging buffer (16-byte aligned)
   uint32_t cap;    // floats in buf
   float4* v0;      // vector slots (s entries each) ...
   float4* v1;
   float4* xg;      // gathered ancestor values, xcap entries
   uint32_t vcap, xcap;
   bool block;
+  uint64_t* bar;   // mbarrier of this team's staging buffer
+  uint32_t parity; // phase of the next completion
+  uint32_t* abort; // shared flag: a bounded wait gave up
   __device__ __forceinline__ void sync() const {
     if (block) __syncthreads();
     else __syncwarp();
   }
 };
 
-// Copies n floats into shared memory with independent, coalesced loads.
-__device__ __forceinline__ void stage(const Team& tm, float* dst, const float* __restrict__ src, uint32_t n) {
-  uint32_t i = tm.rank;
-#pragma unroll 4
-  for (; i < n; i += tm.size) dst[i] = __ldg(src + i);
+// Brings floats [src, src + n) into the team buffer with one bulk copy of the
+// enclosing 16-byte aligned window (the vals pool is padded so the window
+// never leaves the allocation); returns where src[0] landed. Ends with the
+// team synchronised and the data visible.
+__device__ __forceinline__ const float* stage(Team& tm, const float* __restrict__ src, uint32_t n,
+                                              uint32_t* status) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uintptr_t lo = a & ~uintptr_t(15);
+  const uintptr_t hi = (a + uintptr_t(n) * 4 + 15) & ~uintptr_t(15);
+  tm.sync();  // previous readers of the buffer are done
+  if (tm.rank == 0) bulk_g2s(tm.buf, reinterpret_cast<const void*>(lo), uint32_t(hi - lo), tm.bar);
+  bool ok = mbar_wait(tm.bar, tm.parity);
+  tm.parity ^= 1u;
+  if (!ok) {
+    atomicOr(status, 4u);
+    *tm.abort = 1u;
+  }
+  return tm.buf + (a - lo) / 4;
 }
 
 // Forward step of one supernode: t = r - (pulled updates); y = inv(L_kk) t;
 // push U[j] = P[j,:] . y for every panel row.
-__device__ __forceinline__ void sn_forward(const BatchDev& B, const Team& tm, const SnDev& S, float4* Y,
+__device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const SnDev& S, float4* Y,
                                            uint32_t vb) {
   const uint32_t s = S.ncols, m = S.nrows, f = S.first;
   const float* D = B.vals + S.d_off;
@@ -400,13 +457,13 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, const Team& tm, co
     for (; q < qe; ++q) t = f4_sub(t, B.U[B.fwd[q]]);
     tm.v0[c] = t;
   }
-  const bool dfit = s * s <= tm.cap;
-  if (dfit) stage(tm, tm.buf, D, s * s);
+  const bool dfit = s * s + 8 <= tm.cap;
+  const float* Ds = dfit ? stage(tm, D, s * s, B.status) : nullptr;
   tm.sync();
   for (uint32_t c = tm.rank; c < s; c += tm.size) {
     float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
     if (dfit) {
-      for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, tm.buf[c2 * s + c], tm.v0[c2]);
+      for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, Ds[c2 * s + c], tm.v0[c2]);
     } else {
 #pragma unroll 4
       for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, __ldg(D + uint64_t(c2) * s + c), tm.v0[c2]);
@@ -416,14 +473,13 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, const Team& tm, co
   }
   tm.sync();
   if (m == 0) return;
-  const uint32_t rc = max(1u, tm.cap / s);
+  const uint32_t rc = max(1u, (tm.cap - 8) / s);
   for (uint32_t j0 = 0; j0 < m; j0 += rc) {
     uint32_t nr = min(rc, m - j0);
-    stage(tm, tm.buf, Pp + uint64_t(j0) * s, nr * s);
-    tm.sync();
+    const float* Ps = stage(tm, Pp + uint64_t(j0) * s, nr * s, B.status);
     for (uint32_t j = tm.rank; j < nr; j += tm.size) {
       float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-      const float* row = tm.buf + j * s;
+      const float* row = Ps + j * s;
       for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], tm.v1[c]);
       B.U[S.rows_off + j0 + j] = u;
     }
@@ -433,7 +489,7 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, const Team& tm, co
 
 // Backward step of one supernode: t = y - P^T x[R]; x = inv(L_kk)^T t.
 // Team members split columns (width) x row slices (parts).
-__device__ __forceinline__ void sn_backward(const BatchDev& B, const Team& tm, const SnDev& S, float4* Y) {
+__device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const SnDev& S, float4* Y) {
   const uint32_t s = S.ncols, m = S.nrows, f = S.first;
   const float* D = B.vals + S.d_off;
   const float* Pp = B.vals + S.p_off;
@@ -443,19 +499,20 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, const Team& tm, c
   while (width < s && width < tm.size) width <<= 1;
   const uint32_t parts = tm.size / width;
   const uint32_t cl = tm.rank % width, part = tm.rank / width;
-  const uint32_t rc = max(1u, min(tm.cap / s, tm.xcap));
+  const uint32_t rc = max(1u, min((tm.cap - 8) / s, tm.xcap));
   for (uint32_t cb = 0; cb < s; cb += width) {
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t c = cb + cl;
     for (uint32_t j0 = 0; j0 < m; j0 += rc) {
       uint32_t nr = min(rc, m - j0);
-      stage(tm, tm.buf, Pp + uint64_t(j0) * s, nr * s);
+      tm.sync();  // previous readers of xg are done
       for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = Y[Rr[j0 + j]];
+      const float* Ps = stage(tm, Pp + uint64_t(j0) * s, nr * s, B.status);
       tm.sync();
       if (c < s && part < parts)
-        for (uint32_t j = part; j < nr; j += parts) f4_fma(acc, tm.buf[j * s + c], tm.xg[j]);
-      tm.sync();
+        for (uint32_t j = part; j < nr; j += parts) f4_fma(acc, Ps[j * s + c], tm.xg[j]);
     }
+    tm.sync();
     // reduce the row slices (parts) of every column
     if (!tm.block) {
       for (uint32_t o = width; o < 32; o <<= 1) {
@@ -476,15 +533,13 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, const Team& tm, c
     }
     tm.sync();
   }
-  const bool dfit = s * s <= tm.cap;
-  if (dfit) {
-    stage(tm, tm.buf, D, s * s);
-    tm.sync();
-  }
+  const bool dfit = s * s + 8 <= tm.cap;
+  const float* Ds = dfit ? stage(tm, D, s * s, B.status) : nullptr;
+  tm.sync();
   for (uint32_t c = tm.rank; c < s; c += tm.size) {
     float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
     if (dfit) {
-      for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, tm.buf[c * s + c2], tm.v0[c2]);
+      for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Ds[c * s + c2], tm.v0[c2]);
     } else {
 #pragma unroll 4
       for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, __ldg(D + uint64_t(c) * s + c2), tm.v0[c2]);
@@ -516,16 +571,23 @@ __global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
   const uint32_t* lsp = B.level_sn_ptr + I.lvl_base;
   float* fbuf = reinterpret_cast<float*>(smem4);
   float4* vbuf = smem4 + NW * kWarpFloats / 4;
+  __shared__ uint64_t s_bar[NW + 1];
+  __shared__ uint32_t s_abort;
+  if (tid <= NW) mbar_init(&s_bar[tid]);
+  if (tid == 0) s_abort = 0u;
+  mbar_fence_init();
+  __syncthreads();
   Team wt{lane, 32, fbuf + warp * kWarpFloats, kWarpFloats, vbuf + warp * 3 * kWarpVec,
-          vbuf + warp * 3 * kWarpVec + kWarpVec, vbuf + warp * 3 * kWarpVec + 2 * kWarpVec, kWarpVec, kWarpVec, false};
+          vbuf + warp * 3 * kWarpVec + kWarpVec, vbuf + warp * 3 * kWarpVec + 2 * kWarpVec, kWarpVec, kWarpVec, false,
+          &s_bar[warp], 0u, &s_abort};
   // block team: all warps' buffers; the 1152 vector slots split 448 / 448 / 256
   // (supernodes have at most kMaxSupernode <= 448 columns; xg doubles as the
   // NT-entry reduction buffer).
   static_assert(3 * kWarpVec * kSolveWarps >= 448 + 448 + NT, "block-team vector slots");
-  Team bt{tid, NT, fbuf, NW * kWarpFloats, vbuf, vbuf + 448, vbuf + 896, 448, NT, true};
+  Team bt{tid, NT, fbuf, NW * kWarpFloats, vbuf, vbuf + 448, vbuf + 896, 448, NT, true, &s_bar[NW], 0u, &s_abort};
   auto fits_warp = [&](const SnDev& S) { return S.ncols <= kWarpVec && S.ncols * S.ncols <= kWarpFloats; };
   // ---- forward
-  for (uint32_t l = 0; l < I.nlvl; ++l) {
+  for (uint32_t l = 0; l < I.nlvl && !s_abort; ++l) {
     uint32_t sb = lsp[l], se = lsp[l + 1];
     uint32_t k = sb;
     for (; k < se; ++k) {  // largest first: the block handles the ones a warp cannot
@@ -537,7 +599,7 @@ __global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
     __syncthreads();
   }
   // ---- backward
-  for (int l = int(I.nlvl) - 1; l >= 0; --l) {
+  for (int l = int(I.nlvl) - 1; l >= 0 && !s_abort; --l) {
     uint32_t sb = lsp[l], se = lsp[l + 1];
     uint32_t k = sb;
     for (; k < se; ++k) {

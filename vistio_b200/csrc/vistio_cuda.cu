@@ -177,7 +177,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       level_rows, level_ptr, level_sn_ptr, level_sn, rows;
   std::vector<uint32_t> vtri(3 * T), vhinge(4 * H);
   std::vector<SnDev> sn(NSN);
-  std::vector<float> vals(NVALS, 0.f);
+  std::vector<float> vals(NVALS + 4, 0.f);  // +16 bytes: staging windows round up to 16 bytes
   std::vector<uint32_t> fwd(NFWD);
   level_rows.reserve(V);
   rows.reserve(NROWS);
@@ -464,8 +464,11 @@ vistio_status read_result(vistio_batch* b, uint32_t k, vistio_step_result* res, 
     res->al_iterations = R.al_iters;
     res->active_contacts = R.last_active;
     res->last_alpha = ipc ? R.alpha : 1.f;
-    res->status = status ? VISTIO_ERR_SOLVER_DIVERGENCE : VISTIO_OK;
+    res->status = (status & 4u) ? VISTIO_ERR_TIMEOUT : (status & 2u) ? VISTIO_ERR_CAPACITY
+                : status ? VISTIO_ERR_SOLVER_DIVERGENCE : VISTIO_OK;
   }
+  if (status & 4u) return fail(ctx, VISTIO_ERR_TIMEOUT, "a bounded device wait gave up");
+  if (status & 2u) return fail(ctx, VISTIO_ERR_CAPACITY, "self-contact candidate pairs exceeded the buffer");
   if (status) return fail(ctx, VISTIO_ERR_SOLVER_DIVERGENCE, "non-finite positions in the global solve");
   return VISTIO_OK;
 }
