@@ -21,7 +21,8 @@ namespace vistio {
 
 struct InstDev {
   uint32_t vbase, nv;
-  uint32_t lvl_base, nlvl;     // offsets into level_ptr / level_sn_ptr
+  uint32_t nlvl;               // levels of the supernodal elimination tree
+  uint32_t pad0;
   int32_t model;
   float warp, weft;
   float inv_hmat2;   // 1 / matrix_dt^2
@@ -41,6 +42,8 @@ struct SnDev {
   uint32_t rows_off; // first of the m entries of this supernode in rows / U (global)
   uint64_t d_off;    // D (float offset, multiple of 4)
   uint64_t p_off;    // P (float offset)
+  uint32_t vbase;    // first vertex (row) of the owning instance
+  uint32_t inst;     // owning instance
 };
 
 // Per-step constants read from device memory so a captured graph stays valid
@@ -117,13 +120,10 @@ struct BatchDev {
   const SnDev* sn;
   const uint32_t* rows;        // below-diagonal rows of every supernode (instance-local)
   const float* vals;
-  const uint32_t* level_ptr;   // per instance nlvl+1 offsets into level_rows
-  const uint32_t* level_rows;  // rows of each level (instance-local)
-  const uint32_t* level_sn_ptr;// per instance nlvl+1 offsets into level_sn
-  const uint32_t* level_sn;    // supernodes of each level (global ids), largest first
   const uint32_t* fwd_ptr;     // global row -> offsets into fwd
   const uint32_t* fwd;         // U slots summed into the row by the forward sweep
   float4* U;                   // forward updates, one per (supernode, panel row)
+  const uint32_t* lvl_items;   // supernodes of each batch level (block items first)
   // contact / IPC
   float4* grad;            // barrier gradient of the detect at the start of the AL pass
   float4* grad_up;         // gradient of the re-detect
@@ -354,7 +354,7 @@ __device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
   return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, 0.f);
 }
 
-// Shared-memory sizing of k_solve: each warp owns a staging buffer of
+// Shared-memory sizing of the sweep kernels: each warp owns a staging buffer of
 // kWarpFloats floats and kWarpVec float4 vector slots; a narrow level uses
 // all of them as one block-wide buffer.
 constexpr uint32_t kSolveWarps = 8;
@@ -362,6 +362,11 @@ constexpr uint32_t kWarpFloats = 1792;
 constexpr uint32_t kWarpVec = 48;
 constexpr uint32_t kSolveSmem = kSolveWarps * (kWarpFloats * 4 + 3 * kWarpVec * 16);
 constexpr uint32_t kMaxSupernode = 256;  // enforced by the host set-up
+// A supernode is a warp item when its vectors and diagonal block fit a warp's
+// slots and its block is small; larger ones get a whole block.
+__host__ __device__ constexpr bool warp_item(uint32_t s, uint32_t m) {
+  return s <= 42 && uint64_t(s) * (s + m) <= 6144;
+}
 
 // ------------------------------------------------ TMA bulk staging
 // A contiguous global range is brought into shared memory with one
@@ -549,77 +554,88 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
   tm.sync();
 }
 
-// Supernodal forward + back substitution for one instance per block, on
-// P A P^T = L L^T. Per level of the supernodal elimination tree: supernodes
-// too large for a warp's staging buffer run one at a time with the whole
-// block, the rest run one per warp. Forward rows pull the updates U their
-// descendants pushed; backward rows read their ancestors' solutions.
-// Afterwards (plain step) the position update, pin reset, ground clamp and
-// residual sums.
-template <int NT>
-__global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
-  static_assert(NT == 32 * kSolveWarps, "k_solve block size");
-  constexpr uint32_t NW = kSolveWarps;
-  extern __shared__ float4 smem4[];
-  const uint32_t inst = blockIdx.x;
-  const InstDev I = B.inst[inst];
-  const StepParams& P = *B.prm;
-  InstRed& R = B.red[inst];
-  if (P.ipc && R.al_done) return;
-  const uint32_t vb = I.vbase, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float4* Y = B.Y + vb;
-  const uint32_t* lsp = B.level_sn_ptr + I.lvl_base;
+// Shared-memory teams of one sweep kernel block: eight warp teams and, over
+// the same memory, one block team.
+struct SweepTeams {
+  Team wt, bt;
+};
+__device__ __forceinline__ SweepTeams make_teams(float4* smem4, uint64_t* s_bar, uint32_t* s_abort) {
+  constexpr uint32_t NW = kSolveWarps, NT = 32 * kSolveWarps;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float* fbuf = reinterpret_cast<float*>(smem4);
   float4* vbuf = smem4 + NW * kWarpFloats / 4;
-  __shared__ uint64_t s_bar[NW + 1];
-  __shared__ uint32_t s_abort;
   if (tid <= NW) mbar_init(&s_bar[tid]);
-  if (tid == 0) s_abort = 0u;
+  if (tid == 0) *s_abort = 0u;
   mbar_fence_init();
   __syncthreads();
-  Team wt{lane, 32, fbuf + warp * kWarpFloats, kWarpFloats, vbuf + warp * 3 * kWarpVec,
-          vbuf + warp * 3 * kWarpVec + kWarpVec, vbuf + warp * 3 * kWarpVec + 2 * kWarpVec, kWarpVec, kWarpVec, false,
-          &s_bar[warp], 0u, &s_abort};
+  SweepTeams t;
+  t.wt = Team{lane, 32, fbuf + warp * kWarpFloats, kWarpFloats, vbuf + warp * 3 * kWarpVec,
+              vbuf + warp * 3 * kWarpVec + kWarpVec, vbuf + warp * 3 * kWarpVec + 2 * kWarpVec, kWarpVec, kWarpVec,
+              false, &s_bar[warp], 0u, s_abort};
   // block team: all warps' buffers; the 1152 vector slots split 448 / 448 / 256
   // (supernodes have at most kMaxSupernode <= 448 columns; xg doubles as the
   // NT-entry reduction buffer).
   static_assert(3 * kWarpVec * kSolveWarps >= 448 + 448 + NT, "block-team vector slots");
-  Team bt{tid, NT, fbuf, NW * kWarpFloats, vbuf, vbuf + 448, vbuf + 896, 448, NT, true, &s_bar[NW], 0u, &s_abort};
-  auto fits_warp = [&](const SnDev& S) { return S.ncols <= kWarpVec && S.ncols * S.ncols <= kWarpFloats; };
-  // ---- forward
-  for (uint32_t l = 0; l < I.nlvl && !s_abort; ++l) {
-    uint32_t sb = lsp[l], se = lsp[l + 1];
-    uint32_t k = sb;
-    for (; k < se; ++k) {  // largest first: the block handles the ones a warp cannot
-      SnDev S = B.sn[B.level_sn[k]];
-      if (fits_warp(S) && se - k >= 2) break;
-      sn_forward(B, bt, S, Y, vb);
-    }
-    for (uint32_t q = k + warp; q < se; q += NW) sn_forward(B, wt, B.sn[B.level_sn[q]], Y, vb);
-    __syncthreads();
+  t.bt = Team{tid, NT, fbuf, NW * kWarpFloats, vbuf, vbuf + 448, vbuf + 896, 448, NT, true, &s_bar[NW], 0u, s_abort};
+  return t;
+}
+
+// One level of the forward (DIR = 0) or backward (DIR = 1) sweep over every
+// instance of the batch. The level's supernodes (across instances) are listed
+// with those too large for a warp first: blocks [0, nblock) take one of those
+// each with the whole block; the remaining blocks take eight of the rest, one
+// per warp. Supernodes of a level are independent; levels are ordered by
+// kernel boundaries.
+template <int DIR>
+__global__ void __launch_bounds__(32 * kSolveWarps) k_level(BatchDev B, uint32_t off, uint32_t nblock, uint32_t nwarp) {
+  extern __shared__ float4 smem4[];
+  __shared__ uint64_t s_bar[kSolveWarps + 1];
+  __shared__ uint32_t s_abort;
+  SweepTeams t = make_teams(smem4, s_bar, &s_abort);
+  const bool ipc = B.prm->ipc != 0;
+  if (blockIdx.x < nblock) {
+    SnDev S = B.sn[B.lvl_items[off + blockIdx.x]];
+    if (ipc && B.red[S.inst].al_done) return;
+    if (DIR == 0) sn_forward(B, t.bt, S, B.Y + S.vbase, S.vbase);
+    else sn_backward(B, t.bt, S, B.Y + S.vbase);
+  } else {
+    uint32_t q = (blockIdx.x - nblock) * kSolveWarps + (threadIdx.x >> 5);
+    if (q >= nwarp) return;
+    SnDev S = B.sn[B.lvl_items[off + nblock + q]];
+    if (ipc && B.red[S.inst].al_done) return;
+    if (DIR == 0) sn_forward(B, t.wt, S, B.Y + S.vbase, S.vbase);
+    else sn_backward(B, t.wt, S, B.Y + S.vbase);
   }
-  // ---- backward
-  for (int l = int(I.nlvl) - 1; l >= 0 && !s_abort; --l) {
-    uint32_t sb = lsp[l], se = lsp[l + 1];
-    uint32_t k = sb;
-    for (; k < se; ++k) {
-      SnDev S = B.sn[B.level_sn[k]];
-      if (fits_warp(S) && se - k >= 2) break;
-      sn_backward(B, bt, S, Y);
-    }
-    for (uint32_t q = k + warp; q < se; q += NW) sn_backward(B, wt, B.sn[B.level_sn[q]], Y);
-    __syncthreads();
-  }
-  // residual sums (pd_solver.rs:403-421) and, for the plain step, the update.
+}
+
+// Clears the per-instance residual sums before a sweep.
+__global__ void k_red_reset(BatchDev B, uint32_t ninst) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ninst) return;
+  InstRed& R = B.red[k];
+  if (B.prm->ipc && R.al_done) return;
+  R.diff_sq = 0.0;
+  R.norm_sq = 0.0;
+  R.toi_bits = __float_as_uint(1.0f);
+  R.gdd = 0.0;
+}
+
+// After the sweeps: residual sums (pd_solver.rs:403-421) and, for the plain
+// step, x <- x + d, the pin reset (:429-435) and the ground clamp (:438).
+__global__ void __launch_bounds__(256) k_update(BatchDev B, int do_update) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  const InstDev I = B.inst[ch.x];
+  InstRed& R = B.red[ch.x];
+  if (B.prm->ipc && R.al_done) return;
   double dsq = 0.0, nsq = 0.0;
   bool bad = false;
-  for (uint32_t v = tid; v < I.nv; v += NT) {
-    uint32_t g = vb + v;
-    float4 d = Y[B.perm_local[g]];
+  if ((int)threadIdx.x < ch.z) {
+    uint32_t g = uint32_t(ch.y) + threadIdx.x;
+    float4 d = B.Y[I.vbase + B.perm_local[g]];
     float4 x = B.pos[g];
-    dsq += double(d.x) * d.x + double(d.y) * d.y + double(d.z) * d.z;
-    nsq += double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z;
-    if (!(isfinite(d.x) && isfinite(d.y) && isfinite(d.z))) bad = true;
+    dsq = double(d.x) * d.x + double(d.y) * d.y + double(d.z) * d.z;
+    nsq = double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z;
+    bad = !(isfinite(d.x) && isfinite(d.y) && isfinite(d.z));
     if (do_update) {
       float4 nx;
       if (B.pinned[g]) nx = B.prev[g];
@@ -630,24 +646,16 @@ __global__ void __launch_bounds__(NT) k_solve(BatchDev B, int do_update) {
       B.pos[g] = nx;
     }
   }
-  __shared__ double s_a[NW], s_b[NW];
   for (int o = 16; o > 0; o >>= 1) {
     dsq += __shfl_down_sync(0xffffffffu, dsq, o);
     nsq += __shfl_down_sync(0xffffffffu, nsq, o);
   }
-  if (lane == 0) { s_a[warp] = dsq; s_b[warp] = nsq; }
   if (bad) atomicOr(B.status, 1u);
-  __syncthreads();
-  if (tid == 0) {
-    double a = 0.0, bb = 0.0;
-    for (uint32_t k = 0; k < NW; ++k) { a += s_a[k]; bb += s_b[k]; }
-    R.diff_sq = a;
-    R.norm_sq = bb;
-    R.iters += 1;
-    // reset the per-iteration reductions of the IPC line search
-    R.toi_bits = __float_as_uint(1.0f);
-    R.gdd = 0.0;
+  if ((threadIdx.x & 31) == 0 && (dsq != 0.0 || nsq != 0.0)) {
+    atomicAdd(&R.diff_sq, dsq);
+    atomicAdd(&R.norm_sq, nsq);
   }
+  if (threadIdx.x == 0 && ch.y == int(I.vbase)) R.iters += 1;
 }
 
 // save_previous + (IPC) velocity clamp + predict + x <- pred (state.rs:145-169,

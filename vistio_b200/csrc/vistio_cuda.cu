@@ -95,8 +95,9 @@ struct vistio_batch {
   DevBuf<uint4> tri_idx, hinge_idx;
   DevBuf<float4> tri_dm, hinge_st;
   DevBuf<float2> hinge_wr;
-  DevBuf<uint32_t> vtri_ptr, vtri, vhinge_ptr, vhinge, perm_local, rows, level_ptr, level_rows, level_sn_ptr,
-      level_sn, fwd_ptr, fwd, status;
+  DevBuf<uint32_t> vtri_ptr, vtri, vhinge_ptr, vhinge, perm_local, rows, lvl_items, fwd_ptr, fwd, status;
+  // batch levels of the sweeps: offset into lvl_items, block items, warp items
+  std::vector<uint32_t> lvl_off, lvl_nb, lvl_nw;
   DevBuf<SnDev> sn;
   DevBuf<float4> U;
   DevBuf<InstRed> red;
@@ -151,7 +152,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     vb[k] = V; vc[k] = I.nv; tb[k] = T; tc[k] = I.nt; hb[k] = H; hc[k] = I.nh;
     InstDev& d = hi[k];
     d.vbase = uint32_t(V); d.nv = I.nv;
-    d.lvl_base = uint32_t(NLVL); d.nlvl = I.factor.nlevels;
+    d.nlvl = I.factor.nlevels;
     d.model = I.prm.model; d.warp = I.prm.warp; d.weft = I.prm.weft;
     d.inv_hmat2 = 1.f / (I.prm.matrix_dt * I.prm.matrix_dt);
     d.has_ground = solvers[k]->has_ground; d.ground_h = solvers[k]->ground_h;
@@ -174,13 +175,15 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   std::vector<float4> hinge_st(H);
   std::vector<float2> hinge_wr(H);
   std::vector<uint32_t> vtri_ptr(V + 1, 0), vhinge_ptr(V + 1, 0), perm_local(V), fwd_ptr(V + 1, 0),
-      level_rows, level_ptr, level_sn_ptr, level_sn, rows;
+      rows;
   std::vector<uint32_t> vtri(3 * T), vhinge(4 * H);
   std::vector<SnDev> sn(NSN);
   std::vector<float> vals(NVALS + 4, 0.f);  // +16 bytes: staging windows round up to 16 bytes
   std::vector<uint32_t> fwd(NFWD);
-  level_rows.reserve(V);
   rows.reserve(NROWS);
+  uint32_t LMAX = 0;
+  for (uint32_t k = 0; k < n; ++k) LMAX = std::max(LMAX, solvers[k]->setup.factor.nlevels);
+  std::vector<std::vector<uint32_t>> lvl_block(LMAX), lvl_warp(LMAX);
   uint64_t snb = 0, rowsb = 0, valsb = 0, fwdb = 0;
   for (uint32_t k = 0; k < n; ++k) {
     vistio_solver* S = solvers[k];
@@ -215,27 +218,33 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       d.rows_off = uint32_t(rowsb + X.rows_off);
       d.d_off = valsb; valsb += pad4(uint64_t(sc) * sc);
       d.p_off = valsb; valsb += pad4(uint64_t(m) * sc);
+      d.vbase = uint32_t(v0);
+      d.inst = k;
+      (warp_item(sc, m) ? lvl_warp : lvl_block)[X.level].push_back(uint32_t(snb + q));
       const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
       const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
       for (uint64_t e = 0; e < uint64_t(m) * sc; ++e) vals[d.p_off + e] = float(Pn[e]);
       for (uint64_t e = 0; e < uint64_t(sc) * sc; ++e) vals[d.d_off + e] = float(Dn[e]);
     }
     rows.insert(rows.end(), F.rows.begin(), F.rows.end());
-    {  // level_ptr / level_sn_ptr entries are global offsets
-      uint32_t base = uint32_t(level_rows.size()), sbase = uint32_t(level_sn.size());
-      for (uint32_t l = 0; l <= F.nlevels; ++l) {
-        level_ptr.push_back(base + F.level_ptr[l]);
-        level_sn_ptr.push_back(sbase + F.level_sn_ptr[l]);
-      }
-      level_rows.insert(level_rows.end(), F.level_rows.begin(), F.level_rows.end());
-      for (uint32_t k : F.level_sn) level_sn.push_back(uint32_t(snb + k));
-    }
     for (uint32_t r = 0; r < I.nv; ++r) fwd_ptr[v0 + r] = uint32_t(fwdb + F.fwd_ptr[r]);
     for (size_t q = 0; q < F.fwd_sn.size(); ++q)
       fwd[fwdb + q] = uint32_t(rowsb + F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]);
     snb += F.sn.size(); rowsb += F.rows.size(); fwdb += F.fwd_sn.size();
   }
   fwd_ptr[V] = uint32_t(fwdb);
+  // batch levels: block items (heaviest first), then warp items
+  std::vector<uint32_t> items;
+  for (uint32_t l = 0; l < LMAX; ++l) {
+    auto weight = [&](uint32_t q) { return uint64_t(sn[q].ncols) * (sn[q].ncols + sn[q].nrows); };
+    std::stable_sort(lvl_block[l].begin(), lvl_block[l].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
+    std::stable_sort(lvl_warp[l].begin(), lvl_warp[l].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
+    b->lvl_off.push_back(uint32_t(items.size()));
+    b->lvl_nb.push_back(uint32_t(lvl_block[l].size()));
+    b->lvl_nw.push_back(uint32_t(lvl_warp[l].size()));
+    items.insert(items.end(), lvl_block[l].begin(), lvl_block[l].end());
+    items.insert(items.end(), lvl_warp[l].begin(), lvl_warp[l].end());
+  }
   // vertex incidence
   for (uint64_t t = 0; t < T; ++t) { vtri_ptr[tri_idx[t].x + 1]++; vtri_ptr[tri_idx[t].y + 1]++; vtri_ptr[tri_idx[t].z + 1]++; }
   for (uint64_t h = 0; h < H; ++h) {
@@ -271,8 +280,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->perm_local.upload(perm_local, st));
   CU(b->Y.alloc(V)); CU(b->Tm.alloc(V));
   CU(b->sn.upload(sn, st)); CU(b->rows.upload(rows, st)); CU(b->vals.upload(vals, st));
-  CU(b->level_ptr.upload(level_ptr, st)); CU(b->level_rows.upload(level_rows, st));
-  CU(b->level_sn_ptr.upload(level_sn_ptr, st)); CU(b->level_sn.upload(level_sn, st));
+  CU(b->lvl_items.upload(items, st));
   CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
   CU(b->U.alloc(rows.size()));
   CU(b->grad.alloc(V)); CU(b->grad_up.alloc(V)); CU(b->lam.alloc(V)); CU(b->fin_n.alloc(V));
@@ -285,8 +293,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->status.alloc(1)); CU(cudaMemsetAsync(b->status.p, 0, sizeof(uint32_t), st));
   CU(cudaStreamSynchronize(st));
   b->factor_bytes = vals.size() * sizeof(float) + sn.size() * sizeof(SnDev) + rows.size() * 4 + fwd.size() * 4 +
-                    fwd_ptr.size() * 4 + level_rows.size() * 4 + level_ptr.size() * 4 + level_sn.size() * 4 +
-                    level_sn_ptr.size() * 4 + rows.size() * 16;
+                    fwd_ptr.size() * 4 + items.size() * 4 + rows.size() * 16;
   b->device_bytes = b->factor_bytes + V * (16 * 10 + 4 + 3 + 4 * 3) + T * (16 + 16 + 4 + 36 + 12) +
                     H * (16 + 16 + 8 + 16 + 16) + (V + 1) * 8;
   BatchDev& d = b->dev;
@@ -296,8 +303,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   d.hinge_idx = b->hinge_idx.p; d.hinge_st = b->hinge_st.p; d.hinge_wr = b->hinge_wr.p; d.hinge_out = b->hinge_out.p;
   d.vtri_ptr = b->vtri_ptr.p; d.vtri = b->vtri.p; d.vhinge_ptr = b->vhinge_ptr.p; d.vhinge = b->vhinge.p;
   d.perm_local = b->perm_local.p; d.row_vertex = nullptr; d.Y = b->Y.p; d.T = b->Tm.p;
-  d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.level_ptr = b->level_ptr.p; d.level_rows = b->level_rows.p;
-  d.level_sn_ptr = b->level_sn_ptr.p; d.level_sn = b->level_sn.p;
+  d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.lvl_items = b->lvl_items.p;
   d.fwd_ptr = b->fwd_ptr.p; d.fwd = b->fwd.p; d.U = b->U.p;
   d.grad = b->grad.p; d.grad_up = b->grad_up.p; d.lam = b->lam.p; d.fin_n = b->fin_n.p;
   d.in_contact = b->in_contact.p; d.in_contact_up = b->in_contact_up.p; d.ever = b->ever.p;
@@ -356,11 +362,29 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
   return p;
 }
 
-void launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update) {
-  if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev);
-  if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev);
+// The global solve: both sweeps level by level over the whole batch, then the
+// residual sums and (plain step) the position update.
+uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update) {
+  uint32_t L = uint32_t(b->lvl_off.size()), n = 2;
+  k_red_reset<<<(b->ninst + 127) / 128, 128, 0, st>>>(b->dev, b->ninst);
+  for (uint32_t l = 0; l < L; ++l) {
+    uint32_t grid = b->lvl_nb[l] + (b->lvl_nw[l] + kSolveWarps - 1) / kSolveWarps;
+    if (grid) { k_level<0><<<grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
+  }
+  for (int l = int(L) - 1; l >= 0; --l) {
+    uint32_t grid = b->lvl_nb[l] + (b->lvl_nw[l] + kSolveWarps - 1) / kSolveWarps;
+    if (grid) { k_level<1><<<grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
+  }
+  k_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, do_update);
+  return n;
+}
+
+uint32_t launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update) {
+  uint32_t n = 1;
+  if (b->n_tri_chunks) { k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
+  if (b->n_hinge_chunks) { k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
   k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
-  k_solve<kSolveThreads><<<b->ninst, kSolveThreads, kSolveSmem, st>>>(b->dev, do_update);
+  return n + launch_solve(b, st, do_update);
 }
 
 vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out, uint32_t* nlaunch) {
@@ -368,21 +392,19 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
   cudaStream_t st = ctx->stream;
   cudaGraph_t g = nullptr;
   uint32_t iters = b->cfg.max_iterations;
-  uint32_t per_iter = (b->n_tri_chunks ? 1 : 0) + (b->n_hinge_chunks ? 1 : 0) + 2;
   uint32_t small_grid = (b->ninst + 127) / 128;
   CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   k_predict<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
   uint32_t L = 2;
   if (!ipc) {
-    for (uint32_t it = 0; it < iters; ++it) launch_plain_iteration(b, st, 1);
-    L += iters * per_iter;
+    for (uint32_t it = 0; it < iters; ++it) L += launch_plain_iteration(b, st, 1);
   } else {
     for (uint32_t al = 0; al < b->cfg.al_max_iterations; ++al) {
       k_al_begin<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
       if (self) { launch_self_detect(b->dev, b->self, b->n_vtx_chunks, b->n_tri_chunks, 0, st); L += self_detect_launches(); }
       k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 0);
       for (uint32_t it = 0; it < iters; ++it) {
-        launch_plain_iteration(b, st, 0);
+        L += launch_plain_iteration(b, st, 0) + 2;
         if (self) { launch_self_ccd(b->dev, b->self, st); L += self_ccd_launches(); }
         k_ccd<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
         k_ipc_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
@@ -391,7 +413,7 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
       k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 1);
       k_al_end<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
       k_al_finish<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
-      L += 5 + iters * (per_iter + 2);
+      L += 5;
     }
   }
   k_finalize<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
@@ -537,7 +559,8 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   ctx = c.get();
   CU(cudaSetDevice(device));
   CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-  CU(cudaFuncSetAttribute(k_solve<kSolveThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_level<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_level<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   *out = c.release();
   return VISTIO_OK;
 }
@@ -824,7 +847,7 @@ vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase) {
     case 1: if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev); break;
     case 2: if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); break;
     case 3: k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
-    case 4: k_solve<kSolveThreads><<<b->ninst, kSolveThreads, kSolveSmem, st>>>(b->dev, 0); break;
+    case 4: launch_solve(b, st, 0); break;
     case 5: k_finalize<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
     default: return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "unknown phase");
   }
@@ -927,7 +950,7 @@ vistio_status vistio_sparse_solve(vistio_factor* f, const float* rhs, float* sol
   for (int pass = 0; pass < 3; ++pass) {
     for (uint32_t i = 0; i < n; ++i) y[f->f.iperm[i]] = make_float4(float(r[i]), 0.f, 0.f, 0.f);
     CU(cudaMemcpyAsync(b->Y.p, y.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
-    k_solve<kSolveThreads><<<1, kSolveThreads, kSolveSmem, ctx->stream>>>(b->dev, 0);
+    launch_solve(b, ctx->stream, 0);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(y.data(), b->Y.p, n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
