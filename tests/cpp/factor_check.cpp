@@ -16,56 +16,63 @@
 using namespace vistio;
 
 template <class T>
+static void fwd_sn(const Factor& F, const std::vector<T>& vals, std::vector<T>& Y, std::vector<T>& Tm,
+                   std::vector<T>& U, uint32_t k) {
+  const Supernode& S = F.sn[k];
+  uint32_t s = S.ncols;
+  for (uint32_t c = 0; c < s; ++c) {
+    uint32_t r = S.first + c;
+    T t = Y[r];
+    for (uint32_t q = F.fwd_ptr[r]; q < F.fwd_ptr[r + 1]; ++q) t -= U[F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]];
+    Tm[r] = t;
+  }
+  const T* D = vals.data() + S.diag_off;  // column-major inverse
+  for (uint32_t c = 0; c < s; ++c) {
+    T y = 0;
+    for (uint32_t c2 = 0; c2 <= c; ++c2) y += D[uint64_t(c2) * s + c] * Tm[S.first + c2];
+    Y[S.first + c] = y;
+  }
+  const T* Pn = vals.data() + S.panel_off;  // row-major m x s
+  for (uint32_t j = 0; j < S.nrows; ++j) {
+    T u = 0;
+    for (uint32_t c = 0; c < s; ++c) u += Pn[uint64_t(j) * s + c] * Y[S.first + c];
+    U[S.rows_off + j] = u;
+  }
+}
+
+template <class T>
+static void bwd_sn(const Factor& F, const std::vector<T>& vals, std::vector<T>& Y, std::vector<T>& Tm, uint32_t k) {
+  const Supernode& S = F.sn[k];
+  uint32_t s = S.ncols;
+  const T* Pn = vals.data() + S.panel_off;
+  const uint32_t* rr = F.rows.data() + S.rows_off;
+  for (uint32_t c = 0; c < s; ++c) {
+    T t = 0;
+    for (uint32_t j = 0; j < S.nrows; ++j) t += Pn[uint64_t(j) * s + c] * Y[rr[j]];
+    Tm[S.first + c] = Y[S.first + c] - t;
+  }
+  const T* D = vals.data() + S.diag_off;
+  for (uint32_t c = 0; c < s; ++c) {
+    T x = 0;
+    for (uint32_t c2 = c; c2 < s; ++c2) x += D[uint64_t(c) * s + c2] * Tm[S.first + c2];
+    Y[S.first + c] = x;
+  }
+}
+
+// Replays the GPU schedule: forward = bottom subtrees (postorder), then the
+// top levels ascending; backward = top levels descending, then the bottom
+// subtrees in reverse postorder.
+template <class T>
 static void sweep(const Factor& F, const std::vector<T>& vals, std::vector<T>& Y) {
-  // Replays k_solve: forward pulls the pushed updates U, applies inv(L_kk) and
-  // pushes U = P y per supernode of each level; backward per level forms
-  // t = y - P^T x and applies inv(L_kk)^T.
-  uint32_t n = F.n;
-  std::vector<T> Tm(n), U(F.rows.size());
-  for (uint32_t l = 0; l < F.nlevels; ++l) {
-    for (uint32_t i = F.level_ptr[l]; i < F.level_ptr[l + 1]; ++i) {
-      uint32_t r = F.level_rows[i];
-      T t = Y[r];
-      for (uint32_t q = F.fwd_ptr[r]; q < F.fwd_ptr[r + 1]; ++q)
-        t -= U[F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]];
-      Tm[r] = t;
-    }
-    for (uint32_t q = F.level_sn_ptr[l]; q < F.level_sn_ptr[l + 1]; ++q) {
-      const Supernode& S = F.sn[F.level_sn[q]];
-      uint32_t s = S.ncols;
-      const T* D = vals.data() + S.diag_off;  // column-major inverse
-      for (uint32_t c = 0; c < s; ++c) {
-        T y = 0;
-        for (uint32_t c2 = 0; c2 <= c; ++c2) y += D[uint64_t(c2) * s + c] * Tm[S.first + c2];
-        Y[S.first + c] = y;
-      }
-      const T* Pn = vals.data() + S.panel_off;  // row-major m x s
-      for (uint32_t j = 0; j < S.nrows; ++j) {
-        T u = 0;
-        for (uint32_t c = 0; c < s; ++c) u += Pn[uint64_t(j) * s + c] * Y[S.first + c];
-        U[S.rows_off + j] = u;
-      }
-    }
-  }
-  for (int l = int(F.nlevels) - 1; l >= 0; --l) {
-    for (uint32_t q = F.level_sn_ptr[l]; q < F.level_sn_ptr[l + 1]; ++q) {
-      const Supernode& S = F.sn[F.level_sn[q]];
-      uint32_t s = S.ncols;
-      const T* Pn = vals.data() + S.panel_off;
-      const uint32_t* rr = F.rows.data() + S.rows_off;
-      for (uint32_t c = 0; c < s; ++c) {
-        T t = 0;
-        for (uint32_t j = 0; j < S.nrows; ++j) t += Pn[uint64_t(j) * s + c] * Y[rr[j]];
-        Tm[S.first + c] = Y[S.first + c] - t;
-      }
-      const T* D = vals.data() + S.diag_off;
-      for (uint32_t c = 0; c < s; ++c) {
-        T x = 0;
-        for (uint32_t c2 = c; c2 < s; ++c2) x += D[uint64_t(c) * s + c2] * Tm[S.first + c2];
-        Y[S.first + c] = x;
-      }
-    }
-  }
+  std::vector<T> Tm(F.n), U(F.rows.size());
+  for (size_t q = 0; q < F.sub_first.size(); ++q)
+    for (uint32_t k = F.sub_first[q]; k <= F.sub_last[q]; ++k) fwd_sn(F, vals, Y, Tm, U, k);
+  for (uint32_t l = 0; l < F.nlevels; ++l)
+    for (uint32_t q = F.level_sn_ptr[l]; q < F.level_sn_ptr[l + 1]; ++q) fwd_sn(F, vals, Y, Tm, U, F.level_sn[q]);
+  for (int l = int(F.nlevels) - 1; l >= 0; --l)
+    for (uint32_t q = F.level_sn_ptr[l]; q < F.level_sn_ptr[l + 1]; ++q) bwd_sn(F, vals, Y, Tm, F.level_sn[q]);
+  for (size_t q = 0; q < F.sub_first.size(); ++q)
+    for (int k = int(F.sub_last[q]); k >= int(F.sub_first[q]); --k) bwd_sn(F, vals, Y, Tm, uint32_t(k));
 }
 
 int main(int argc, char** argv) {
@@ -129,8 +136,8 @@ int main(int argc, char** argv) {
   uint32_t maxs = 0;
   for (auto& S : F.sn) maxs = std::max(maxs, S.ncols);
   printf("{\"nv\": %u, \"nh\": %u, \"nnz_a\": %zu, \"nnz_l\": %llu, \"stored\": %llu, \"supernodes\": %zu, "
-         "\"levels\": %u, \"max_snode\": %u, \"fwd_entries\": %zu, \"resid64\": %.3e, \"resid32\": %.3e}\n",
+         "\"levels\": %u, \"subtrees\": %zu, \"max_snode\": %u, \"fwd_entries\": %zu, \"resid64\": %.3e, \"resid32\": %.3e}\n",
          nv, I.nh, I.A_col.size(), (unsigned long long)F.nnz_L, (unsigned long long)F.nnz_stored, F.sn.size(),
-         F.nlevels, maxs, F.fwd_sn.size(), resid(yd), resid(yf));
+         F.nlevels, F.sub_first.size(), maxs, F.fwd_sn.size(), resid(yd), resid(yf));
   return 0;
 }

@@ -171,9 +171,9 @@ class Context:
         self.h = h
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and L is not None and L._lib is not None:
             L.lib().vistio_ctx_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -259,9 +259,9 @@ class ProjectiveDynamicsSolver:
         return self
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and L is not None and L._lib is not None:
             L.lib().vistio_solver_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -319,9 +319,9 @@ class Batch:
         self.nverts = [s.nv for s in solvers]
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and L is not None and L._lib is not None:
             L.lib().vistio_batch_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -411,9 +411,9 @@ class SparseSolver:
         return x
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and L is not None and L._lib is not None:
             L.lib().vistio_sparse_destroy(self.h)
-            self.h = None
+        self.h = None
 
 
 def broadphase_pairs(pos: np.ndarray, tris: np.ndarray, margin: float, ctx: Optional[Context] = None) -> np.ndarray:

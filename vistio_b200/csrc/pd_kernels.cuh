@@ -124,6 +124,7 @@ struct BatchDev {
   const uint32_t* fwd;         // U slots summed into the row by the forward sweep
   float4* U;                   // forward updates, one per (supernode, panel row)
   const uint32_t* lvl_items;   // supernodes of each batch level (block items first)
+  const uint2* sub_items;      // bottom subtrees: (first, last) supernode of each
   // contact / IPC
   float4* grad;            // barrier gradient of the detect at the start of the AL pass
   float4* grad_up;         // gradient of the re-detect
@@ -448,13 +449,10 @@ __device__ __forceinline__ const float* stage(Team& tm, const float* __restrict_
   return tm.buf + (a - lo) / 4;
 }
 
-// Forward step of one supernode: t = r - (pulled updates); y = inv(L_kk) t;
-// push U[j] = P[j,:] . y for every panel row.
-__device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const SnDev& S, float4* Y,
-                                           uint32_t vb) {
-  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
-  const float* D = B.vals + S.d_off;
-  const float* Pp = B.vals + S.p_off;
+// Pull for the rows of supernode S: t = r - sum of the updates U that its
+// descendants pushed (lanes / threads over columns).
+__device__ __forceinline__ void sn_pull(const BatchDev& B, const Team& tm, const SnDev& S, const float4* Y) {
+  const uint32_t s = S.ncols, f = S.first, vb = S.vbase;
   for (uint32_t c = tm.rank; c < s; c += tm.size) {
     float4 t = Y[f + c];
     uint32_t q = B.fwd_ptr[vb + f + c], qe = B.fwd_ptr[vb + f + c + 1];
@@ -462,19 +460,60 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const Sn
     for (; q < qe; ++q) t = f4_sub(t, B.U[B.fwd[q]]);
     tm.v0[c] = t;
   }
-  const bool dfit = s * s + 8 <= tm.cap;
-  const float* Ds = dfit ? stage(tm, D, s * s, B.status) : nullptr;
-  tm.sync();
+}
+
+// y = inv(L_kk) t with the whole diagonal block in shared memory (Ds, column-major).
+__device__ __forceinline__ void sn_diag_fwd_smem(const Team& tm, const SnDev& S, const float* Ds, float4* Y) {
+  const uint32_t s = S.ncols, f = S.first;
   for (uint32_t c = tm.rank; c < s; c += tm.size) {
     float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (dfit) {
-      for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, Ds[c2 * s + c], tm.v0[c2]);
-    } else {
-#pragma unroll 4
-      for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, __ldg(D + uint64_t(c2) * s + c), tm.v0[c2]);
-    }
+    for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, Ds[c2 * s + c], tm.v0[c2]);
     tm.v1[c] = y;
     Y[f + c] = y;
+  }
+}
+
+// U[j] = P[j,:] . y for nr rows staged at Ps (row-major, s columns).
+__device__ __forceinline__ void sn_push_rows(const BatchDev& B, const Team& tm, const SnDev& S, const float* Ps,
+                                             uint32_t j0, uint32_t nr) {
+  const uint32_t s = S.ncols;
+  for (uint32_t j = tm.rank; j < nr; j += tm.size) {
+    float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float* row = Ps + j * s;
+    for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], tm.v1[c]);
+    B.U[S.rows_off + j0 + j] = u;
+  }
+}
+
+// Forward step of one supernode: pull, y = inv(L_kk) t, push U = P y. The
+// diagonal block and the panel are staged through the team buffer (the
+// block in column chunks when it does not fit, the panel in row chunks).
+__device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const SnDev& S) {
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  float4* Y = B.Y + S.vbase;
+  const float* D = B.vals + S.d_off;
+  const float* Pp = B.vals + S.p_off;
+  sn_pull(B, tm, S, Y);
+  if (s * s + 8 <= tm.cap) {
+    const float* Ds = stage(tm, D, s * s, B.status);
+    tm.sync();
+    sn_diag_fwd_smem(tm, S, Ds, Y);
+  } else {
+    // column chunks [c0, c1) of D; y accumulates in v1
+    for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t cw = max(1u, (tm.cap - 8) / s);
+    for (uint32_t c0 = 0; c0 < s; c0 += cw) {
+      uint32_t c1 = min(s, c0 + cw);
+      const float* Dc = stage(tm, D + uint64_t(c0) * s, (c1 - c0) * s, B.status);
+      for (uint32_t c = c0 + tm.rank; c < s; c += tm.size) {
+        float4 y = tm.v1[c];
+        uint32_t ce = min(c1, c + 1);
+        for (uint32_t c2 = c0; c2 < ce; ++c2) f4_fma(y, Dc[(c2 - c0) * s + c], tm.v0[c2]);
+        tm.v1[c] = y;
+      }
+    }
+    tm.sync();
+    for (uint32_t c = tm.rank; c < s; c += tm.size) Y[f + c] = tm.v1[c];
   }
   tm.sync();
   if (m == 0) return;
@@ -482,26 +521,63 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const Sn
   for (uint32_t j0 = 0; j0 < m; j0 += rc) {
     uint32_t nr = min(rc, m - j0);
     const float* Ps = stage(tm, Pp + uint64_t(j0) * s, nr * s, B.status);
-    for (uint32_t j = tm.rank; j < nr; j += tm.size) {
-      float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-      const float* row = Ps + j * s;
-      for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], tm.v1[c]);
-      B.U[S.rows_off + j0 + j] = u;
+    sn_push_rows(B, tm, S, Ps, j0, nr);
+  }
+  tm.sync();
+}
+
+// Team-wide sums over row slices: thread (cl, part) of a (width x parts)
+// split holds acc for column cb + cl; column sums land in out[cb + cl].
+__device__ __forceinline__ void team_column_sum(const Team& tm, float4 acc, uint32_t width, uint32_t parts,
+                                                uint32_t cb, uint32_t s, const float4* base, float4* out,
+                                                bool subtract) {
+  const uint32_t cl = tm.rank % width, part = tm.rank / width;
+  if (!tm.block) {
+    for (uint32_t o = width; o < 32; o <<= 1) {
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+      acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
     }
+    if (part == 0 && cb + cl < s) out[cb + cl] = subtract ? f4_sub(base[cb + cl], acc) : acc;
+  } else {
+    float4* red = tm.xg;  // xcap >= block size
     tm.sync();
+    red[tm.rank] = acc;
+    tm.sync();
+    if (tm.rank < width && cb + tm.rank < s) {
+      float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (uint32_t q = 0; q < parts; ++q) a = f4_add(a, red[q * width + tm.rank]);
+      out[cb + tm.rank] = subtract ? f4_sub(base[cb + tm.rank], a) : a;
+    }
+  }
+  tm.sync();
+}
+
+__device__ __forceinline__ uint32_t team_width(const Team& tm, uint32_t s) {
+  uint32_t width = 1;
+  while (width < s && width < tm.size) width <<= 1;
+  return width;
+}
+
+// x = inv(L_kk)^T t with the whole diagonal block in shared memory (Ds).
+__device__ __forceinline__ void sn_diag_bwd_smem(const Team& tm, const SnDev& S, const float* Ds, float4* Y) {
+  const uint32_t s = S.ncols, f = S.first;
+  for (uint32_t c = tm.rank; c < s; c += tm.size) {
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Ds[c * s + c2], tm.v0[c2]);
+    Y[f + c] = x;
   }
 }
 
 // Backward step of one supernode: t = y - P^T x[R]; x = inv(L_kk)^T t.
-// Team members split columns (width) x row slices (parts).
-__device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const SnDev& S, float4* Y) {
+__device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const SnDev& S) {
   const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  float4* Y = B.Y + S.vbase;
   const float* D = B.vals + S.d_off;
   const float* Pp = B.vals + S.p_off;
   const uint32_t* Rr = B.rows + S.rows_off;
   for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
-  uint32_t width = 1;
-  while (width < s && width < tm.size) width <<= 1;
+  const uint32_t width = team_width(tm, s);
   const uint32_t parts = tm.size / width;
   const uint32_t cl = tm.rank % width, part = tm.rank / width;
   const uint32_t rc = max(1u, min((tm.cap - 8) / s, tm.xcap));
@@ -518,40 +594,74 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
         for (uint32_t j = part; j < nr; j += parts) f4_fma(acc, Ps[j * s + c], tm.xg[j]);
     }
     tm.sync();
-    // reduce the row slices (parts) of every column
-    if (!tm.block) {
-      for (uint32_t o = width; o < 32; o <<= 1) {
-        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
-        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
-        acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
-      }
-      if (part == 0 && c < s) tm.v0[c] = f4_sub(tm.v1[c], acc);
-    } else {
-      float4* red = tm.xg;  // xcap >= block size
-      red[tm.rank] = acc;
-      tm.sync();
-      if (tm.rank < width && cb + tm.rank < s) {
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (uint32_t q = 0; q < parts; ++q) a = f4_add(a, red[q * width + tm.rank]);
-        tm.v0[cb + tm.rank] = f4_sub(tm.v1[cb + tm.rank], a);
-      }
-    }
+    team_column_sum(tm, acc, width, parts, cb, s, tm.v1, tm.v0, true);
+  }
+  if (s * s + 8 <= tm.cap) {
+    const float* Ds = stage(tm, D, s * s, B.status);
     tm.sync();
-  }
-  const bool dfit = s * s + 8 <= tm.cap;
-  const float* Ds = dfit ? stage(tm, D, s * s, B.status) : nullptr;
-  tm.sync();
-  for (uint32_t c = tm.rank; c < s; c += tm.size) {
-    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (dfit) {
-      for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Ds[c * s + c2], tm.v0[c2]);
-    } else {
-#pragma unroll 4
-      for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, __ldg(D + uint64_t(c) * s + c2), tm.v0[c2]);
+    sn_diag_bwd_smem(tm, S, Ds, Y);
+  } else {
+    // column chunks of D: x_c needs column c (rows c..s-1)
+    const uint32_t cw = max(1u, (tm.cap - 8) / s);
+    for (uint32_t c0 = 0; c0 < s; c0 += cw) {
+      uint32_t c1 = min(s, c0 + cw);
+      const float* Dc = stage(tm, D + uint64_t(c0) * s, (c1 - c0) * s, B.status);
+      const uint32_t w = team_width(tm, c1 - c0), np = tm.size / w;
+      const uint32_t ccl = tm.rank % w, pp = tm.rank / w, cc = c0 + ccl;
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (cc < c1 && pp < np)
+        for (uint32_t r = cc + pp; r < s; r += np) f4_fma(acc, Dc[(cc - c0) * s + r], tm.v0[r]);
+      team_column_sum(tm, acc, w, np, c0, c1, nullptr, Y + f, false);
     }
-    Y[f + c] = x;
   }
   tm.sync();
+}
+
+// The supernodes [first, last] of one bottom subtree, staged with one bulk
+// copy, swept in postorder (forward) or reverse postorder (backward) from
+// shared memory by one warp.
+template <int DIR>
+__device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint32_t first, uint32_t last) {
+  const SnDev F = B.sn[first], Lz = B.sn[last];
+  const uint64_t end = Lz.p_off + ((uint64_t(Lz.nrows) * Lz.ncols + 3) & ~3ull);
+  const float* base = stage(tm, B.vals + F.d_off, uint32_t(end - F.d_off), B.status);
+  for (uint32_t i = 0; i <= last - first; ++i) {
+    const uint32_t k = DIR == 0 ? first + i : last - i;
+    const SnDev S = B.sn[k];
+    const float* Ds = base + (S.d_off - F.d_off);
+    const float* Ps = base + (S.p_off - F.d_off);
+    float4* Y = B.Y + S.vbase;
+    const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+    if (DIR == 0) {
+      sn_pull(B, tm, S, Y);
+      tm.sync();
+      sn_diag_fwd_smem(tm, S, Ds, Y);
+      tm.sync();
+      sn_push_rows(B, tm, S, Ps, 0, m);
+      tm.sync();
+    } else {
+      const uint32_t* Rr = B.rows + S.rows_off;
+      for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
+      const uint32_t width = team_width(tm, s), parts = tm.size / width;
+      const uint32_t cl = tm.rank % width, part = tm.rank / width;
+      for (uint32_t cb = 0; cb < s; cb += width) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        const uint32_t c = cb + cl;
+        for (uint32_t j0 = 0; j0 < m; j0 += tm.xcap) {
+          uint32_t nr = min(tm.xcap, m - j0);
+          tm.sync();
+          for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = Y[Rr[j0 + j]];
+          tm.sync();
+          if (c < s && part < parts)
+            for (uint32_t j = part; j < nr; j += parts) f4_fma(acc, Ps[(j0 + j) * s + c], tm.xg[j]);
+        }
+        tm.sync();
+        team_column_sum(tm, acc, width, parts, cb, s, tm.v1, tm.v0, true);
+      }
+      sn_diag_bwd_smem(tm, S, Ds, Y);
+      tm.sync();
+    }
+  }
 }
 
 // Shared-memory teams of one sweep kernel block: eight warp teams and, over
@@ -596,16 +706,30 @@ __global__ void __launch_bounds__(32 * kSolveWarps) k_level(BatchDev B, uint32_t
   if (blockIdx.x < nblock) {
     SnDev S = B.sn[B.lvl_items[off + blockIdx.x]];
     if (ipc && B.red[S.inst].al_done) return;
-    if (DIR == 0) sn_forward(B, t.bt, S, B.Y + S.vbase, S.vbase);
-    else sn_backward(B, t.bt, S, B.Y + S.vbase);
+    if (DIR == 0) sn_forward(B, t.bt, S);
+    else sn_backward(B, t.bt, S);
   } else {
     uint32_t q = (blockIdx.x - nblock) * kSolveWarps + (threadIdx.x >> 5);
     if (q >= nwarp) return;
     SnDev S = B.sn[B.lvl_items[off + nblock + q]];
     if (ipc && B.red[S.inst].al_done) return;
-    if (DIR == 0) sn_forward(B, t.wt, S, B.Y + S.vbase, S.vbase);
-    else sn_backward(B, t.wt, S, B.Y + S.vbase);
+    if (DIR == 0) sn_forward(B, t.wt, S);
+    else sn_backward(B, t.wt, S);
   }
+}
+
+// Bottom subtrees of every instance, one per warp.
+template <int DIR>
+__global__ void __launch_bounds__(32 * kSolveWarps) k_subtree(BatchDev B, uint32_t nitems) {
+  extern __shared__ float4 smem4[];
+  __shared__ uint64_t s_bar[kSolveWarps + 1];
+  __shared__ uint32_t s_abort;
+  SweepTeams t = make_teams(smem4, s_bar, &s_abort);
+  uint32_t q = blockIdx.x * kSolveWarps + (threadIdx.x >> 5);
+  if (q >= nitems) return;
+  uint2 it = B.sub_items[q];
+  if (B.prm->ipc && B.red[B.sn[it.x].inst].al_done) return;
+  subtree_sweep<DIR>(B, t.wt, it.x, it.y);
 }
 
 // Clears the per-instance residual sums before a sweep.

@@ -425,9 +425,40 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
     S.parent = S.nrows ? f.row_sn[sns[k].below[0]] : UINT32_MAX;
     S.level = 0;
   }
-  for (uint32_t k = 0; k < nsn; ++k)  // children precede parents (postorder)
-    if (f.sn[k].parent != UINT32_MAX)
-      f.sn[f.sn[k].parent].level = std::max(f.sn[f.sn[k].parent].level, f.sn[k].level + 1);
+  // Bottom subtrees whose packed data fits kSubtreeFloats are swept whole by
+  // one warp; the supernodes above them are swept level by level, a top
+  // supernode's level being one more than its highest top child (children
+  // that are bottom subtrees count as below level 0).
+  {
+    std::vector<uint64_t> sub(nsn, 0);
+    std::vector<uint32_t> cnt_sub(nsn, 1);
+    for (uint32_t k = 0; k < nsn; ++k) {  // children precede parents (postorder)
+      sub[k] += sn_floats(f.sn[k].ncols, f.sn[k].nrows);
+      uint32_t p = f.sn[k].parent;
+      if (p != UINT32_MAX) { sub[p] += sub[k]; cnt_sub[p] += cnt_sub[k]; }
+    }
+    std::vector<char> bottom(nsn, 0);
+    for (int k = int(nsn) - 1; k >= 0; --k) {  // parents first
+      uint32_t p = f.sn[k].parent;
+      bool fits = sub[k] <= kSubtreeFloats;
+      if (p != UINT32_MAX && bottom[p]) bottom[k] = 1;
+      else if (fits) {
+        bottom[k] = 1;
+        f.sub_first.push_back(uint32_t(k) + 1 - cnt_sub[k]);
+        f.sub_last.push_back(uint32_t(k));
+      }
+    }
+    std::reverse(f.sub_first.begin(), f.sub_first.end());
+    std::reverse(f.sub_last.begin(), f.sub_last.end());
+    std::vector<int> top_lvl(nsn, -1);
+    for (uint32_t k = 0; k < nsn; ++k) {
+      if (bottom[k]) { f.sn[k].level = kBottomLevel; continue; }
+      if (top_lvl[k] < 0) top_lvl[k] = 0;
+      f.sn[k].level = uint32_t(top_lvl[k]);
+      uint32_t p = f.sn[k].parent;
+      if (p != UINT32_MAX) top_lvl[p] = std::max(top_lvl[p], top_lvl[k] + 1);
+    }
+  }
   f.vals.assign(off, 0.0);
   f.nnz_stored = off;
   // Scatter the simplicial columns into panels and diagonal blocks.
@@ -463,13 +494,13 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
       }
     }
   }
-  // Level schedule.
+  // Level schedule of the top supernodes.
   uint32_t nl = 0;
-  for (auto& S : f.sn) nl = std::max(nl, S.level + 1);
+  for (auto& S : f.sn) if (S.level != kBottomLevel) nl = std::max(nl, S.level + 1);
   f.nlevels = nl;
   f.level_ptr.assign(nl + 1, 0);
   std::vector<std::vector<uint32_t>> bylvl(nl);
-  for (uint32_t k = 0; k < nsn; ++k) bylvl[f.sn[k].level].push_back(k);
+  for (uint32_t k = 0; k < nsn; ++k) if (f.sn[k].level != kBottomLevel) bylvl[f.sn[k].level].push_back(k);
   f.level_sn_ptr.assign(nl + 1, 0);
   for (uint32_t l = 0; l < nl; ++l) {
     std::stable_sort(bylvl[l].begin(), bylvl[l].end(), [&](uint32_t a, uint32_t b) {

@@ -29,6 +29,14 @@ struct SetupParams {
 
 // Largest supernode (columns); the GPU sweeps size their shared-memory vectors for it.
 constexpr uint32_t kMaxSupernodeCols = 256;
+// Bottom subtrees of the supernodal elimination tree whose factor data (in
+// floats, as packed for the GPU: pad4(s*s) + pad4(m*s) per supernode) fits
+// this budget are swept as one unit by one warp.
+constexpr uint32_t kSubtreeFloats = 1792;
+constexpr uint32_t kBottomLevel = 0xffffffffu;
+inline uint64_t sn_floats(uint32_t s, uint32_t m) {
+  return ((uint64_t(s) * s + 3) & ~3ull) + ((uint64_t(m) * s + 3) & ~3ull);
+}
 
 // Supernodal factor of P A P^T = L L^T in the layout the GPU sweeps read.
 // Columns are in the permuted (elimination) order.
@@ -40,7 +48,7 @@ struct Supernode {
   uint64_t panel_off; // offset of the |R| x s row-major panel in Factor::vals
   uint64_t diag_off;  // offset of inv(L_kk), s x s column-major, in Factor::vals
   uint32_t parent;    // parent supernode, or UINT32_MAX for a root
-  uint32_t level;     // height in the supernodal elimination tree (leaves = 0)
+  uint32_t level;     // sweep level above the bottom subtrees (kBottomLevel inside one)
 };
 
 struct Factor {
@@ -57,6 +65,8 @@ struct Factor {
   std::vector<uint32_t> level_rows; // rows (columns) of the level's supernodes, grouped by supernode
   std::vector<uint32_t> level_sn_ptr; // nlevels+1 offsets into level_sn
   std::vector<uint32_t> level_sn;     // supernodes of each level, largest first
+  // Bottom subtrees: supernode ranges [first, last] in postorder (last = root).
+  std::vector<uint32_t> sub_first, sub_last;
   // Forward-sweep pull lists: for each row r, the (supernode, panel row) pairs
   // of the descendants whose panels hold row r.
   std::vector<uint32_t> fwd_ptr;    // n+1

@@ -22,6 +22,7 @@
 #include "setup.h"
 
 using namespace vistio;
+static_assert(kSubtreeFloats <= kWarpFloats, "a bottom subtree must fit one warp buffer");
 
 struct vistio_ctx {
   int device = 0;
@@ -96,6 +97,8 @@ struct vistio_batch {
   DevBuf<float4> tri_dm, hinge_st;
   DevBuf<float2> hinge_wr;
   DevBuf<uint32_t> vtri_ptr, vtri, vhinge_ptr, vhinge, perm_local, rows, lvl_items, fwd_ptr, fwd, status;
+  DevBuf<uint2> sub_items;
+  uint32_t n_sub = 0;
   // batch levels of the sweeps: offset into lvl_items, block items, warp items
   std::vector<uint32_t> lvl_off, lvl_nb, lvl_nw;
   DevBuf<SnDev> sn;
@@ -184,6 +187,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   uint32_t LMAX = 0;
   for (uint32_t k = 0; k < n; ++k) LMAX = std::max(LMAX, solvers[k]->setup.factor.nlevels);
   std::vector<std::vector<uint32_t>> lvl_block(LMAX), lvl_warp(LMAX);
+  std::vector<uint2> subs;
   uint64_t snb = 0, rowsb = 0, valsb = 0, fwdb = 0;
   for (uint32_t k = 0; k < n; ++k) {
     vistio_solver* S = solvers[k];
@@ -220,13 +224,15 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       d.p_off = valsb; valsb += pad4(uint64_t(m) * sc);
       d.vbase = uint32_t(v0);
       d.inst = k;
-      (warp_item(sc, m) ? lvl_warp : lvl_block)[X.level].push_back(uint32_t(snb + q));
+      if (X.level != kBottomLevel) (warp_item(sc, m) ? lvl_warp : lvl_block)[X.level].push_back(uint32_t(snb + q));
       const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
       const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
       for (uint64_t e = 0; e < uint64_t(m) * sc; ++e) vals[d.p_off + e] = float(Pn[e]);
       for (uint64_t e = 0; e < uint64_t(sc) * sc; ++e) vals[d.d_off + e] = float(Dn[e]);
     }
     rows.insert(rows.end(), F.rows.begin(), F.rows.end());
+    for (size_t q = 0; q < F.sub_first.size(); ++q)
+      subs.push_back(make_uint2(uint32_t(snb + F.sub_first[q]), uint32_t(snb + F.sub_last[q])));
     for (uint32_t r = 0; r < I.nv; ++r) fwd_ptr[v0 + r] = uint32_t(fwdb + F.fwd_ptr[r]);
     for (size_t q = 0; q < F.fwd_sn.size(); ++q)
       fwd[fwdb + q] = uint32_t(rowsb + F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]);
@@ -281,6 +287,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->Y.alloc(V)); CU(b->Tm.alloc(V));
   CU(b->sn.upload(sn, st)); CU(b->rows.upload(rows, st)); CU(b->vals.upload(vals, st));
   CU(b->lvl_items.upload(items, st));
+  CU(b->sub_items.upload(subs, st));
+  b->n_sub = uint32_t(subs.size());
   CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
   CU(b->U.alloc(rows.size()));
   CU(b->grad.alloc(V)); CU(b->grad_up.alloc(V)); CU(b->lam.alloc(V)); CU(b->fin_n.alloc(V));
@@ -303,7 +311,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   d.hinge_idx = b->hinge_idx.p; d.hinge_st = b->hinge_st.p; d.hinge_wr = b->hinge_wr.p; d.hinge_out = b->hinge_out.p;
   d.vtri_ptr = b->vtri_ptr.p; d.vtri = b->vtri.p; d.vhinge_ptr = b->vhinge_ptr.p; d.vhinge = b->vhinge.p;
   d.perm_local = b->perm_local.p; d.row_vertex = nullptr; d.Y = b->Y.p; d.T = b->Tm.p;
-  d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.lvl_items = b->lvl_items.p;
+  d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.lvl_items = b->lvl_items.p; d.sub_items = b->sub_items.p;
   d.fwd_ptr = b->fwd_ptr.p; d.fwd = b->fwd.p; d.U = b->U.p;
   d.grad = b->grad.p; d.grad_up = b->grad_up.p; d.lam = b->lam.p; d.fin_n = b->fin_n.p;
   d.in_contact = b->in_contact.p; d.in_contact_up = b->in_contact_up.p; d.ever = b->ever.p;
@@ -366,7 +374,9 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
 // residual sums and (plain step) the position update.
 uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update) {
   uint32_t L = uint32_t(b->lvl_off.size()), n = 2;
+  const uint32_t sub_grid = (b->n_sub + kSolveWarps - 1) / kSolveWarps;
   k_red_reset<<<(b->ninst + 127) / 128, 128, 0, st>>>(b->dev, b->ninst);
+  if (sub_grid) { k_subtree<0><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->n_sub); ++n; }
   for (uint32_t l = 0; l < L; ++l) {
     uint32_t grid = b->lvl_nb[l] + (b->lvl_nw[l] + kSolveWarps - 1) / kSolveWarps;
     if (grid) { k_level<0><<<grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
@@ -375,6 +385,7 @@ uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update) {
     uint32_t grid = b->lvl_nb[l] + (b->lvl_nw[l] + kSolveWarps - 1) / kSolveWarps;
     if (grid) { k_level<1><<<grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
   }
+  if (sub_grid) { k_subtree<1><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->n_sub); ++n; }
   k_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, do_update);
   return n;
 }
@@ -561,6 +572,8 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CU(cudaFuncSetAttribute(k_level<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_level<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_subtree<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_subtree<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   *out = c.release();
   return VISTIO_OK;
 }
