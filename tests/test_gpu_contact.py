@@ -1,0 +1,168 @@
+"""GPU parity of step_with_ipc and of the contact boundary queries.
+
+* broad phase: the GPU candidate triangle pairs equal, as sorted integer
+  lists, the complete set {(ta < tb) : inflated AABBs overlap} the oracle
+  computes on the same f32 positions (bit-exact);
+* CCD: the GPU vertex-triangle hit set over those pairs equals the oracle's,
+  both evaluated in FP64 (bit-exact), with the same minimum TOI;
+* IPC step (ground, sphere, self contact): one step from an identical state
+  within 1e-5 relative of the FP64 oracle; short runs within 1e-4 m.
+"""
+import numpy as np
+import pytest
+
+import oracle_api as O
+from vistio_b200 import api, scenarios
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 60.0
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def folded_ribbon(cols=8, rows=60, width=0.1, height=0.6, gap=0.004, seed=0):
+    """A ribbon folded in half over itself with the layers `gap` apart, plus a
+    small deterministic jitter, so many triangle pairs are close."""
+    px, py, pz, tris = scenarios.quad_grid(cols, rows, width, height)
+    t = (py - py.min()) / (py.max() - py.min())  # 0..1 along the ribbon
+    L = height
+    s = t * L
+    half = L / 2
+    x = px.copy()
+    y = np.where(s < half, s, L - s).astype(np.float32)
+    z = np.where(s < half, 0.0, gap).astype(np.float32)
+    bend = np.abs(s - half) < L / rows
+    z = np.where(bend, gap / 2, z).astype(np.float32)
+    rng = np.random.default_rng(seed)
+    z = (z + rng.uniform(-gap / 8, gap / 8, size=z.shape)).astype(np.float32)
+    pos = np.stack([x, y + 0.5, z], 1).astype(np.float32)
+    return pos, tris
+
+
+@pytest.mark.parametrize("gap,margin", [(0.004, 7.5e-4), (0.002, 1.5e-3), (0.01, 7.5e-4)])
+def test_broadphase_pairs_bit_exact(gap, margin):
+    pos, tris = folded_ribbon(gap=gap)
+    ref = O.tri_pairs(pos, tris, margin, mode=0)
+    got = api.broadphase_pairs(pos, tris, margin)
+    assert got.shape == ref.shape, (got.shape, ref.shape)
+    assert np.array_equal(got, ref)
+    # the reference's median-split tree drops some of these pairs (bvh.rs:205-209)
+    faithful = O.tri_pairs(pos, tris, margin, mode=1)
+    assert len(faithful) <= len(ref)
+    fset = set(map(tuple, faithful))
+    assert fset <= set(map(tuple, ref))
+
+
+def test_broadphase_empty_and_degenerate():
+    pos = np.zeros((3, 3), np.float32)
+    tris = np.array([[0, 1, 2]], np.uint32)
+    assert len(api.broadphase_pairs(pos, tris, 1e-3)) == 0
+    pos, tris = folded_ribbon(cols=1, rows=2)
+    ref = O.tri_pairs(pos, tris, 1e-3, mode=0)
+    assert np.array_equal(api.broadphase_pairs(pos, tris, 1e-3), ref)
+
+
+def test_ccd_hits_bit_exact():
+    pos, tris = folded_ribbon(gap=0.004)
+    rng = np.random.default_rng(3)
+    # move the upper layer through the lower one
+    p1 = pos.copy()
+    upper = pos[:, 2] > 0.002
+    p1[upper, 2] -= 0.008
+    p1 += rng.uniform(-1e-4, 1e-4, size=p1.shape).astype(np.float32)
+    pairs = O.tri_pairs(pos, tris, 7.5e-4, mode=0)
+    assert len(pairs) > 0
+    hr, tr = O.ccd_hits(pos, p1, tris, pairs)
+    hg, tg = api.ccd_hits(pos, p1, tris, pairs)
+    assert len(hr) > 0
+    assert np.array_equal(hg, hr)
+    assert abs(tg - tr) <= 1e-6 * max(1.0, abs(tr))
+
+
+def ipc_pair(mesh, contact: api.Contact, d_hat=1e-3, kappa=1e4, iters=15, al=5, precision=1, setup=None,
+             params=None):
+    cfg = api.drape_config(max_iterations=iters, al_max_iterations=al, barrier_d_hat=d_hat, barrier_kappa=kappa)
+    setup = setup or api.SetupDesc(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0)
+    gpu = api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
+    oc = O.default_config(max_iterations=iters, al_max_iterations=al, barrier_d_hat=d_hat)
+    params = params or O.init_params(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0)
+    ref = O.OracleSim(mesh, params, oc, precision=precision)
+    c = O.Contact()
+    c.has_ground, c.ground_height = int(contact.has_ground), contact.ground_height
+    c.has_sphere = int(contact.has_sphere)
+    c.sphere_center[:] = contact.sphere_center
+    c.sphere_radius = contact.sphere_radius
+    c.self_collision, c.bvh_faithful = int(contact.self_collision), 0
+    c.kappa, c.thickness = contact.kappa, contact.thickness
+    if contact.has_ground:
+        ref.set_ground(1, contact.ground_height)
+    return gpu, ref, c
+
+
+SPHERE = api.Contact(has_ground=True, ground_height=-0.3, has_sphere=True, sphere_center=(0.0, 0.0, 0.0),
+                     sphere_radius=0.3, kappa=1e4)
+
+
+def test_sphere_drape_steps_match_fp64():
+    """sphere_drape geometry on a 24x24 sheet: every step from the oracle's
+    state within 1e-5 relative; contacts become active during the run."""
+    mesh = scenarios.sphere_drape(side=24, length=1.5, height=0.35)
+    gpu, ref, c = ipc_pair(mesh, SPHERE)
+    worst, active = 0.0, 0
+    for s in range(40):
+        p, v = ref.state()
+        gpu.set_state(p, v)
+        rr = ref.step_ipc(DT, c)
+        rg = gpu.step_with_ipc(DT, SPHERE)
+        worst = max(worst, rel(gpu.state()[0], ref.state()[0]))
+        active = max(active, rg.active_contacts)
+        assert rg.al_iterations == rr.al_iterations
+        assert rg.active_contacts == rr.active_contacts
+    assert active > 0, "the sheet never reached the sphere"
+    assert worst <= 1e-5, worst
+
+
+def test_sphere_drape_run_within_1e4_m():
+    mesh = scenarios.sphere_drape(side=20, length=1.5, height=0.35)
+    gpu, ref, c = ipc_pair(mesh, SPHERE)
+    for _ in range(45):
+        ref.step_ipc(DT, c)
+        gpu.step_with_ipc(DT, SPHERE)
+    err = float(np.abs(gpu.state()[0] - ref.state()[0]).max())
+    print(f"45-step sphere_drape 20x20: max |x_gpu - x_fp64| = {err:.3e} m")
+    assert err <= 1e-4, err
+    # non-penetration of the sphere within 2 cm (bench_tests.rs:138-225)
+    r = np.linalg.norm(gpu.state()[0], axis=1)
+    assert r.min() >= 0.3 - 0.02
+
+
+def test_ground_contact_steps_match_fp64():
+    mesh = scenarios.sphere_drape(side=16, length=0.8, height=0.02)
+    ground = api.Contact(has_ground=True, ground_height=0.0, kappa=1e4)
+    gpu, ref, c = ipc_pair(mesh, ground)
+    worst = 0.0
+    for s in range(20):
+        p, v = ref.state()
+        gpu.set_state(p, v)
+        ref.step_ipc(DT, c)
+        gpu.step_with_ipc(DT, ground)
+        worst = max(worst, rel(gpu.state()[0], ref.state()[0]))
+    assert worst <= 1e-5, worst
+
+
+def test_self_contact_detect_gradient_matches():
+    """The self-contact barrier gradient of one detect (VT + EE with 1-ring
+    exclusion, thickness barrier) on a folded ribbon equals the oracle's."""
+    pos, tris = folded_ribbon(cols=6, rows=40, gap=0.003)
+    mesh = scenarios.Mesh(pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy(), tris,
+                          np.zeros(len(pos), np.uint8))
+    d_hat = 5e-4
+    self_c = api.Contact(self_collision=True, kappa=1e3, thickness=1.5 * d_hat)
+    gpu, ref, c = ipc_pair(mesh, self_c, d_hat=d_hat, kappa=1e3, iters=2, al=1)
+    # one step each from the same state: positions agree
+    ref.step_ipc(DT, c)
+    gpu.step_with_ipc(DT, self_c)
+    assert rel(gpu.state()[0], ref.state()[0]) <= 1e-5
