@@ -21,6 +21,7 @@
 #include "../../include/vistio_cuda.h"
 
 struct vistio_solver;
+struct vistio_ctx;
 
 namespace vistio {
 
@@ -32,22 +33,31 @@ struct SelfInst {
   uint32_t lvl_cnt[28];    // boxes on each level
 };
 
-struct SelfContactDev {
+// Device view of the self-contact buffers: plain pointers, passed to kernels by value.
+struct SelfContactView {
+  uint32_t ninst;
+  uint64_t T;
+  uint64_t pair_cap;
+  SelfInst* inst;      // per garment
+  uint32_t* tri_inst;  // triangle -> garment
+  float4* box_min;     // all tree levels
+  float4* box_max;
+  uint32_t* cnt;       // per triangle pair counts, then exclusive offsets
+  uint32_t* block_sums;
+  uint2* pairs;        // global (ta, tb)
+  uint32_t* npairs;    // [0] pair count, [1] overflow flag
+  uint32_t* adj_ptr;   // 1-ring exclusion lists (sorted, include the vertex itself)
+  uint32_t* adj;
+  uint32_t scan_blocks;
+};
+
+// Host-side owner of those buffers (never passed to a kernel).
+struct SelfContactDev : SelfContactView {
   bool ready = false;
-  uint32_t ninst = 0;
-  uint64_t T = 0;
-  uint64_t pair_cap = 0;
-  SelfInst* inst = nullptr;      // per garment
-  uint32_t* tri_inst = nullptr;  // triangle -> garment
-  float4* box_min = nullptr;     // all tree levels
-  float4* box_max = nullptr;
-  uint32_t* cnt = nullptr;       // per triangle pair counts, then exclusive offsets
-  uint32_t* block_sums = nullptr;
-  uint2* pairs = nullptr;        // global (ta, tb)
-  uint32_t* npairs = nullptr;    // [0] pair count, [1] overflow flag
-  uint32_t* adj_ptr = nullptr;   // 1-ring exclusion lists (sorted, include the vertex itself)
-  uint32_t* adj = nullptr;
-  uint32_t scan_blocks = 0;
+  SelfContactDev() : SelfContactView{} {}
+  SelfContactDev(const SelfContactDev&) = delete;
+  SelfContactDev& operator=(const SelfContactDev&) = delete;
+  SelfContactView view() const { return static_cast<const SelfContactView&>(*this); }
   void release() {
     cudaFree(inst); cudaFree(tri_inst); cudaFree(box_min); cudaFree(box_max); cudaFree(cnt);
     cudaFree(block_sums); cudaFree(pairs); cudaFree(npairs); cudaFree(adj_ptr); cudaFree(adj);
@@ -62,7 +72,7 @@ constexpr int kScanBlock = 1024;
 // ---------------------------------------------------------------- trees
 // Leaf boxes (bvh.rs:29-43, inflated by the margin) and the level-by-level
 // refit, one block per garment.
-__global__ void __launch_bounds__(1024) k_self_boxes(BatchDev B, SelfContactDev S, float margin_arg) {
+__global__ void __launch_bounds__(1024) k_self_boxes(BatchDev B, SelfContactView S, float margin_arg) {
   const SelfInst I = S.inst[blockIdx.x];
   if (B.prm->ipc && B.red[blockIdx.x].al_done) return;
   const float margin = margin_arg >= 0.f ? margin_arg : B.prm->thickness;
@@ -104,7 +114,7 @@ __device__ __forceinline__ bool box_overlap(float4 amn, float4 amx, float4 bmn, 
 // Traversal for leaf i: visits subtrees holding leaves > i whose boxes overlap.
 // mode 0 counts, mode 1 writes at the scanned offset.
 template <int MODE>
-__device__ void self_traverse(const SelfContactDev& S, const SelfInst& I, uint32_t i, uint32_t* count_out,
+__device__ void self_traverse(const SelfContactView& S, const SelfInst& I, uint32_t i, uint32_t* count_out,
                               uint2* out, uint32_t cap) {
   const float4* mn = S.box_min + I.box_base;
   const float4* mx = S.box_max + I.box_base;
@@ -137,7 +147,7 @@ __device__ void self_traverse(const SelfContactDev& S, const SelfInst& I, uint32
   if (MODE == 0) *count_out = found;
 }
 
-__global__ void __launch_bounds__(256) k_self_count(BatchDev B, SelfContactDev S) {
+__global__ void __launch_bounds__(256) k_self_count(BatchDev B, SelfContactView S) {
   int4 ch = B.tri_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) { S.cnt[ch.y + threadIdx.x] = 0; return; }
@@ -190,7 +200,7 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_add(uint32_t* v, uint32_t n
   if (i < n) v[i] += block_sums[blockIdx.x];
 }
 
-__global__ void __launch_bounds__(256) k_self_write(BatchDev B, SelfContactDev S) {
+__global__ void __launch_bounds__(256) k_self_write(BatchDev B, SelfContactView S) {
   int4 ch = B.tri_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) return;
@@ -355,7 +365,7 @@ __device__ __forceinline__ float scaled_barrier_grad_thick(float d, float d_hat,
   return signbit(r) ? -1e6f : 1e6f;
 }
 
-__device__ __forceinline__ bool excluded(const SelfContactDev& S, uint32_t i, uint32_t j) {
+__device__ __forceinline__ bool excluded(const SelfContactView& S, uint32_t i, uint32_t j) {
   for (uint32_t p = S.adj_ptr[i], e = S.adj_ptr[i + 1]; p < e; ++p) {
     uint32_t a = S.adj[p];
     if (a == j) return true;
@@ -374,7 +384,7 @@ __device__ __forceinline__ void add_grad(float4* G, uint32_t v, V3d<float> g, fl
 // SelfCollisionSystem::detect_ipc_contacts (self_collision.rs:199-276) and
 // IpcContactSet::compute_barrier_gradient (ipc_response.rs:170-219), per
 // candidate pair: 3+3 vertex-triangle and 9 edge-edge tests.
-__global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactDev S, int mode) {
+__global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactView S, int mode) {
   const StepParams& P = *B.prm;
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   float4* G = mode == 0 ? B.grad : B.grad_up;
@@ -518,7 +528,7 @@ __device__ R vt_ccd(V3d<R> p0, V3d<R> p1, V3d<R> a0, V3d<R> a1, V3d<R> b0, V3d<R
 }
 
 // compute_max_step_size over the last detect's pairs (ccd.rs:238-292).
-__global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactDev S) {
+__global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactView S) {
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
     uint2 pr = S.pairs[k];
@@ -551,11 +561,10 @@ __global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactDev S) 
 inline uint32_t self_detect_launches() { return 7; }
 inline uint32_t self_ccd_launches() { return 1; }
 
-inline void launch_self_detect(const BatchDev& d, const SelfContactDev& S, uint32_t n_vtx_chunks,
+inline void launch_self_detect(const BatchDev& d, const SelfContactView& S, uint32_t n_vtx_chunks,
                                uint32_t n_tri_chunks, int mode, cudaStream_t st) {
   k_clear_grad<<<n_vtx_chunks, 256, 0, st>>>(d, mode);
-  // the margin lives in StepParams (thickness); read on device via a copy below
-  k_self_boxes<<<S.ninst, 1024, 0, st>>>(d, S, -1.f);
+  k_self_boxes<<<S.ninst, 1024, 0, st>>>(d, S, -1.f);  // margin: StepParams::thickness
   k_self_count<<<n_tri_chunks, 256, 0, st>>>(d, S);
   k_scan_local<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);
   k_scan_sums<<<1, kScanBlock, 0, st>>>(S.block_sums, S.scan_blocks, S.npairs);
@@ -564,17 +573,17 @@ inline void launch_self_detect(const BatchDev& d, const SelfContactDev& S, uint3
   k_self_grad<<<4 * 148, 256, 0, st>>>(d, S, mode);
 }
 
-inline void launch_self_ccd(const BatchDev& d, const SelfContactDev& S, cudaStream_t st) {
+inline void launch_self_ccd(const BatchDev& d, const SelfContactView& S, cudaStream_t st) {
   k_self_ccd<<<4 * 148, 256, 0, st>>>(d, S);
 }
 
 vistio_status ensure_self_contact(const BatchDev& d, SelfContactDev& S, const std::vector<vistio_solver*>& solvers,
                                   const std::vector<uint32_t>& vbase, uint64_t T, cudaStream_t st, std::string* err);
 
-vistio_status broadphase_pairs_impl(cudaStream_t st, std::string* err, uint32_t nv, const float* px, const float* py,
+vistio_status broadphase_pairs_impl(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py,
                                     const float* pz, uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs,
                                     uint64_t cap, uint64_t* count);
-vistio_status ccd_hits_impl(cudaStream_t st, std::string* err, uint32_t nv, const float* p0, const float* p1,
+vistio_status ccd_hits_impl(vistio_ctx* ctx, uint32_t nv, const float* p0, const float* p1,
                             uint32_t nt, const uint32_t* tris, uint64_t npairs, const uint32_t* pairs, uint32_t* hits,
                             uint64_t cap, uint64_t* nhits, float* min_toi);
 

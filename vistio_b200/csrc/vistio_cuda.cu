@@ -412,15 +412,15 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
   } else {
     for (uint32_t al = 0; al < b->cfg.al_max_iterations; ++al) {
       k_al_begin<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
-      if (self) { launch_self_detect(b->dev, b->self, b->n_vtx_chunks, b->n_tri_chunks, 0, st); L += self_detect_launches(); }
+      if (self) { launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 0, st); L += self_detect_launches(); }
       k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 0);
       for (uint32_t it = 0; it < iters; ++it) {
         L += launch_plain_iteration(b, st, 0) + 2;
-        if (self) { launch_self_ccd(b->dev, b->self, st); L += self_ccd_launches(); }
+        if (self) { launch_self_ccd(b->dev, b->self.view(), st); L += self_ccd_launches(); }
         k_ccd<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
         k_ipc_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
       }
-      if (self) { launch_self_detect(b->dev, b->self, b->n_vtx_chunks, b->n_tri_chunks, 1, st); L += self_detect_launches(); }
+      if (self) { launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 1, st); L += self_detect_launches(); }
       k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 1);
       k_al_end<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
       k_al_finish<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
@@ -992,15 +992,13 @@ vistio_status vistio_sparse_destroy(vistio_factor* f) {
 vistio_status vistio_broadphase_pairs(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py, const float* pz,
                                       uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs, uint64_t cap,
                                       uint64_t* count) {
-  return broadphase_pairs_impl(ctx ? ctx->stream : nullptr, ctx ? &ctx->last_error : nullptr, nv, px, py, pz, nt, tris,
-                               margin, pairs, cap, count);
+  return broadphase_pairs_impl(ctx, nv, px, py, pz, nt, tris, margin, pairs, cap, count);
 }
 
 vistio_status vistio_ccd_hits(vistio_ctx* ctx, uint32_t nv, const float* p0, const float* p1, uint32_t nt,
                               const uint32_t* tris, uint64_t npairs, const uint32_t* pairs, uint32_t* hits,
                               uint64_t cap, uint64_t* nhits, float* min_toi) {
-  return ccd_hits_impl(ctx ? ctx->stream : nullptr, ctx ? &ctx->last_error : nullptr, nv, p0, p1, nt, tris, npairs,
-                       pairs, hits, cap, nhits, min_toi);
+  return ccd_hits_impl(ctx, nv, p0, p1, nt, tris, npairs, pairs, hits, cap, nhits, min_toi);
 }
 
 }  // extern "C"
@@ -1106,14 +1104,16 @@ vistio_status ensure_self_contact(const BatchDev&, SelfContactDev& S, const std:
   return self_build(S, tris, nverts, vbase, T, st, err);
 }
 
-vistio_status broadphase_pairs_impl(cudaStream_t st, std::string* err, uint32_t nv, const float* px, const float* py,
+vistio_status broadphase_pairs_impl(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py,
                                     const float* pz, uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs,
                                     uint64_t cap, uint64_t* count) {
-  if (!px || !py || !pz || !tris || !count) { if (err) *err = "null argument"; return VISTIO_ERR_INVALID_CONFIG; }
+  if (!ctx) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null context");
+  cudaStream_t st = ctx->stream;
+  std::string* err = &ctx->last_error;
+  if (!px || !py || !pz || !tris || !count) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null argument");
   if (nt == 0) { *count = 0; return VISTIO_OK; }
   for (uint64_t k = 0; k < 3ull * nt; ++k)
-    if (tris[k] >= nv) { if (err) *err = "triangle index out of range"; return VISTIO_ERR_INVALID_MESH; }
-  vistio_ctx* ctx = nullptr;
+    if (tris[k] >= nv) return fail(ctx, VISTIO_ERR_INVALID_MESH, "triangle index out of range");
   std::vector<float4> pos(nv);
   for (uint32_t i = 0; i < nv; ++i) pos[i] = make_float4(px[i], py[i], pz[i], 0.f);
   std::vector<uint4> ti(nt);
@@ -1135,8 +1135,8 @@ vistio_status broadphase_pairs_impl(cudaStream_t st, std::string* err, uint32_t 
   std::vector<uint32_t> nvs{nv}, vb{0};
   vistio_status r = self_build(S, tl, nvs, vb, nt, st, err);
   if (r != VISTIO_OK) return r;
-  k_self_boxes<<<1, 1024, 0, st>>>(d, S, margin);
-  k_self_count<<<uint32_t(ch.size()), 256, 0, st>>>(d, S);
+  k_self_boxes<<<1, 1024, 0, st>>>(d, S.view(), margin);
+  k_self_count<<<uint32_t(ch.size()), 256, 0, st>>>(d, S.view());
   k_scan_local<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, nt, S.block_sums);
   k_scan_sums<<<1, kScanBlock, 0, st>>>(S.block_sums, S.scan_blocks, S.npairs);
   k_scan_add<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, nt, S.block_sums);
@@ -1148,7 +1148,7 @@ vistio_status broadphase_pairs_impl(cudaStream_t st, std::string* err, uint32_t 
     S.pair_cap = total;
     CU(cudaMalloc(&S.pairs, uint64_t(total) * sizeof(uint2)));
   }
-  k_self_write<<<uint32_t(ch.size()), 256, 0, st>>>(d, S);
+  k_self_write<<<uint32_t(ch.size()), 256, 0, st>>>(d, S.view());
   CU(cudaGetLastError());
   std::vector<uint2> hp(total);
   if (total) CU(cudaMemcpyAsync(hp.data(), S.pairs, uint64_t(total) * sizeof(uint2), cudaMemcpyDeviceToHost, st));
@@ -1157,7 +1157,7 @@ vistio_status broadphase_pairs_impl(cudaStream_t st, std::string* err, uint32_t 
   *count = total;
   if (pairs)
     for (uint64_t k = 0; k < total && k < cap; ++k) { pairs[2 * k] = hp[k].x; pairs[2 * k + 1] = hp[k].y; }
-  if (pairs && total > cap) { if (err) *err = "pair buffer too small"; return VISTIO_ERR_CAPACITY; }
+  if (pairs && total > cap) return fail(ctx, VISTIO_ERR_CAPACITY, "pair buffer too small");
   return VISTIO_OK;
 }
 
@@ -1187,15 +1187,16 @@ __global__ void k_ccd_hits(const float* p0, const float* p1, const uint32_t* tri
   }
 }
 
-vistio_status ccd_hits_impl(cudaStream_t st, std::string* err, uint32_t nv, const float* p0, const float* p1,
+vistio_status ccd_hits_impl(vistio_ctx* ctx, uint32_t nv, const float* p0, const float* p1,
                             uint32_t nt, const uint32_t* tris, uint64_t npairs, const uint32_t* pairs, uint32_t* hits,
                             uint64_t cap, uint64_t* nhits, float* min_toi) {
-  if (!p0 || !p1 || !tris || (!pairs && npairs) || !nhits) { if (err) *err = "null argument"; return VISTIO_ERR_INVALID_CONFIG; }
+  if (!ctx) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null context");
+  cudaStream_t st = ctx->stream;
+  if (!p0 || !p1 || !tris || (!pairs && npairs) || !nhits) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null argument");
   for (uint64_t k = 0; k < 2 * npairs; ++k)
-    if (pairs[k] >= nt) { if (err) *err = "pair index out of range"; return VISTIO_ERR_INVALID_CONFIG; }
+    if (pairs[k] >= nt) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "pair index out of range");
   for (uint64_t k = 0; k < 3ull * nt; ++k)
-    if (tris[k] >= nv) { if (err) *err = "triangle index out of range"; return VISTIO_ERR_INVALID_MESH; }
-  vistio_ctx* ctx = nullptr;
+    if (tris[k] >= nv) return fail(ctx, VISTIO_ERR_INVALID_MESH, "triangle index out of range");
   std::vector<float> a(p0, p0 + 3ull * nv), b(p1, p1 + 3ull * nv);
   std::vector<uint32_t> tv(tris, tris + 3ull * nt), pv(pairs, pairs + 2 * npairs);
   DevBuf<float> d0, d1; DevBuf<uint32_t> dt, dp; DevBuf<uint2> dh; DevBuf<double> dtoi;
@@ -1220,7 +1221,7 @@ vistio_status ccd_hits_impl(cudaStream_t st, std::string* err, uint32_t nv, cons
   if (min_toi) *min_toi = float(std::max(mt, 1e-6));
   if (hits)
     for (size_t k = 0; k < out.size() && k < cap; ++k) { hits[2 * k] = out[k].first; hits[2 * k + 1] = out[k].second; }
-  if (hits && out.size() > cap) { if (err) *err = "hit buffer too small"; return VISTIO_ERR_CAPACITY; }
+  if (hits && out.size() > cap) return fail(ctx, VISTIO_ERR_CAPACITY, "hit buffer too small");
   return VISTIO_OK;
 }
 
