@@ -235,7 +235,8 @@ vistio_status vistio_sparse_destroy(vistio_factor* f);
 
 /* ---- contact boundary queries ---- */
 /* Candidate triangle pairs (ta < tb) whose AABBs inflated by `margin` overlap,
- * computed on the GPU (LBVH). Writes up to `cap` pairs sorted; *count = total. */
+ * computed on the GPU (balanced tree over mesh-order triangles, count / scan /
+ * write). Writes up to `cap` pairs sorted; *count = total. */
 vistio_status vistio_broadphase_pairs(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py, const float* pz,
                                       uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs, uint64_t cap,
                                       uint64_t* count);
