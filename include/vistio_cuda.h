@@ -240,6 +240,30 @@ vistio_status vistio_sparse_destroy(vistio_factor* f);
 vistio_status vistio_broadphase_pairs(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py, const float* pz,
                                       uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs, uint64_t cap,
                                       uint64_t* count);
+/* Allocation-free variant of vistio_broadphase_pairs (no counterpart in the
+ * reference). Same inputs and the same sorted pair list, but the call allocates
+ * and frees no device memory: every buffer it uses lives in one fixed region
+ * (about 16 MB) built into the library. For callers that cannot allocate on
+ * the call: a server whose device memory is fully committed to resident
+ * garments (a cudaMalloc could fail there), or a per-frame collision query on
+ * a latency-critical thread, where cudaFree would synchronise the whole device.
+ * Limits: at most VISTIO_NOALLOC_MAX_TRIANGLES triangles and
+ * VISTIO_NOALLOC_MAX_VERTICES vertices (else VISTIO_ERR_CAPACITY before any
+ * device work), and at most VISTIO_NOALLOC_MAX_PAIRS candidate pairs (else
+ * VISTIO_ERR_CAPACITY with *count set). pairs == NULL queries the count;
+ * cap < *count returns VISTIO_ERR_CAPACITY and writes nothing.
+ * The context's device must be current on the calling thread. The first call
+ * on each device looks up the region's address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture. The region is shared by every
+ * call on the device: calls on one device must not overlap (two threads or two
+ * contexts with calls in flight at once race on it). Each call clears the
+ * counters it needs; nothing has to be zeroed by the caller. */
+#define VISTIO_NOALLOC_MAX_TRIANGLES 65536u
+#define VISTIO_NOALLOC_MAX_VERTICES 65536u
+#define VISTIO_NOALLOC_MAX_PAIRS 1048576u
+vistio_status vistio_broadphase_pairs_noalloc(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py,
+                                              const float* pz, uint32_t nt, const uint32_t* tris, float margin,
+                                              uint32_t* pairs, uint64_t cap, uint64_t* count);
 /* Vertex-triangle CCD over candidate pairs on the GPU: sorted unique
  * (vertex, triangle) hits and the minimum safe TOI. */
 vistio_status vistio_ccd_hits(vistio_ctx* ctx, uint32_t nv, const float* p0, const float* p1, uint32_t nt,

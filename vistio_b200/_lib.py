@@ -110,6 +110,8 @@ SIGNATURES = {
                                           C.c_uint64, _u64p]),
     "vistio_ccd_hits": (C.c_int, [_vp, C.c_uint32, _fp, _fp, C.c_uint32, _u32p, C.c_uint64, _u32p, _u32p,
                                   C.c_uint64, _u64p, _fp]),
+    "vistio_broadphase_pairs_noalloc": (C.c_int, [_vp, C.c_uint32, _fp, _fp, _fp, C.c_uint32, _u32p, C.c_float,
+                                                  _u32p, C.c_uint64, _u64p]),
 }
 
 _lib = None

@@ -1226,3 +1226,208 @@ vistio_status ccd_hits_impl(vistio_ctx* ctx, uint32_t nv, const float* p0, const
 }
 
 }  // namespace vistio
+
+// ================================================ allocation-free broad phase
+// vistio_broadphase_pairs_noalloc runs the kernels of vistio_broadphase_pairs
+// with every device buffer carved out of one fixed region that is part of the
+// library image, so the call itself allocates and frees no device memory.
+// It is meant for callers that cannot allocate on the call: a server whose
+// HBM is fully committed to resident garments and factors (a cudaMalloc there
+// can fail, or push out memory it has promised elsewhere), and per-frame
+// collision queries on a latency-critical thread, where cudaFree's implicit
+// device-wide synchronisation would stall all other work on the GPU.
+//
+// The region is sized for meshes of up to kNaMaxTris triangles and kNaMaxVerts
+// vertices and for up to kNaMaxPairs candidate pairs (about 16 MB); larger
+// inputs are rejected with VISTIO_ERR_CAPACITY before any device work. There
+// is one region per device, so calls on the same device must not overlap:
+// two of them in flight at once (two threads, or two contexts' streams)
+// race on it.
+namespace vistio_na {
+constexpr uint32_t kNaMaxTris = 65536;
+constexpr uint32_t kNaMaxVerts = 65536;
+constexpr uint32_t kNaMaxPairs = 1u << 20;
+constexpr uint32_t kNaMaxBoxes = 2 * kNaMaxTris + 32;  // every tree level of kNaMaxTris leaves
+constexpr uint32_t kNaChunks = (kNaMaxTris + kElemThreads - 1) / kElemThreads;
+constexpr uint32_t kNaScanBlocks = (kNaMaxTris + vistio::kScanBlock - 1) / vistio::kScanBlock;
+constexpr int kNaMaxDevices = 64;
+
+constexpr uint64_t na_up(uint64_t x) { return (x + 255) & ~uint64_t(255); }
+
+// Byte offsets of the buffers inside the region, each 256-byte aligned.
+struct NaLayout {
+  static constexpr uint64_t raw_x = 0;  // caller's SoA positions, as given
+  static constexpr uint64_t raw_y = raw_x + na_up(4ull * kNaMaxVerts);
+  static constexpr uint64_t raw_z = raw_y + na_up(4ull * kNaMaxVerts);
+  static constexpr uint64_t raw_tri = raw_z + na_up(4ull * kNaMaxVerts);
+  static constexpr uint64_t pos = raw_tri + na_up(12ull * kNaMaxTris);  // float4 per vertex
+  static constexpr uint64_t tri = pos + na_up(16ull * kNaMaxVerts);     // uint4 per triangle
+  static constexpr uint64_t chunks = tri + na_up(16ull * kNaMaxTris);
+  // red, prm and status must start at zero on every call (cleared together).
+  static constexpr uint64_t red = chunks + na_up(16ull * kNaChunks);
+  static constexpr uint64_t prm = red + na_up(sizeof(vistio::InstRed));
+  static constexpr uint64_t status = prm + na_up(sizeof(vistio::StepParams));
+  static constexpr uint64_t zero_end = status + na_up(4);
+  static constexpr uint64_t inst = zero_end;
+  static constexpr uint64_t tri_inst = inst + na_up(sizeof(vistio::SelfInst));
+  static constexpr uint64_t box_min = tri_inst + na_up(4ull * kNaMaxTris);
+  static constexpr uint64_t box_max = box_min + na_up(16ull * kNaMaxBoxes);
+  static constexpr uint64_t cnt = box_max + na_up(16ull * kNaMaxBoxes);
+  static constexpr uint64_t block_sums = cnt + na_up(4ull * kNaMaxTris);
+  static constexpr uint64_t npairs = block_sums + na_up(4ull * kNaScanBlocks);  // [count, overflow]: zeroed
+  static constexpr uint64_t pairs = npairs + na_up(8);
+  static constexpr uint64_t bytes = pairs + na_up(8ull * kNaMaxPairs);
+};
+}  // namespace vistio_na
+
+using namespace vistio_na;
+static __device__ __align__(256) unsigned char g_na_scratch[NaLayout::bytes];
+
+namespace vistio_na {
+std::mutex g_na_mu;
+unsigned char* g_na_base[kNaMaxDevices] = {};
+
+// Device address of the region on the context's device, looked up once per
+// device (the first call on each device does it, with that device current).
+vistio_status na_region(vistio_ctx* ctx, unsigned char** out) {
+  int cur = -1;
+  CU(cudaGetDevice(&cur));
+  if (cur != ctx->device)
+    return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "the context's device must be current on the calling thread");
+  if (cur < 0 || cur >= kNaMaxDevices) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  if (!g_na_base[cur]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(ctx, VISTIO_ERR_GPU, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_na_base[cur] = static_cast<unsigned char*>(p);
+  }
+  *out = g_na_base[cur];
+  return VISTIO_OK;
+}
+
+// SoA positions and index triples -> the float4 / uint4 rows the broad-phase
+// kernels read; one chunk per 256 triangles, all of garment 0.
+__global__ void k_na_pack(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                          uint32_t nv, const uint32_t* __restrict__ t, uint32_t nt, float4* pos, uint4* tri,
+                          uint32_t* tri_inst, int4* chunks, uint32_t nchunks) {
+  const uint32_t n = nv > nt ? nv : nt;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (i < nv) pos[i] = make_float4(x[i], y[i], z[i], 0.f);
+    if (i < nt) {
+      tri[i] = make_uint4(t[3 * i], t[3 * i + 1], t[3 * i + 2], 0u);
+      tri_inst[i] = 0u;
+    }
+    if (i < nchunks) {
+      const uint32_t b = i * kElemThreads;
+      chunks[i] = make_int4(0, int(b), int(min(uint32_t(kElemThreads), nt - b)), 0);
+    }
+  }
+}
+
+struct NaPair { uint32_t a, b; };
+static_assert(sizeof(NaPair) == 8, "pairs are two packed u32");
+
+vistio_status broadphase_pairs_noalloc_impl(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py,
+                                            const float* pz, uint32_t nt, const uint32_t* tris, float margin,
+                                            uint32_t* pairs, uint64_t cap, uint64_t* count) {
+  if (!ctx) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null context");
+  if (!px || !py || !pz || !tris || !count) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  if (nt == 0) { *count = 0; return VISTIO_OK; }
+  if (nt > kNaMaxTris || nv > kNaMaxVerts)
+    return fail(ctx, VISTIO_ERR_CAPACITY,
+                "mesh too large for the allocation-free broad phase (at most 65536 triangles and 65536 vertices); "
+                "use vistio_broadphase_pairs");
+  for (uint64_t k = 0; k < 3ull * nt; ++k)
+    if (tris[k] >= nv) return fail(ctx, VISTIO_ERR_INVALID_MESH, "triangle index out of range");
+  unsigned char* base = nullptr;
+  vistio_status r = na_region(ctx, &base);
+  if (r != VISTIO_OK) return r;
+  cudaStream_t st = ctx->stream;
+  auto at = [&](uint64_t off) { return base + off; };
+
+  // Tree layout of one garment (host, on the stack).
+  SelfInst I;
+  std::memset(&I, 0, sizeof(I));
+  I.nt = nt;
+  for (uint32_t cntl = nt, off = 0, l = 0;; cntl = (cntl + 1) / 2) {
+    I.lvl_off[l] = off;
+    I.lvl_cnt[l] = cntl;
+    off += cntl;
+    I.nlevels = ++l;
+    if (cntl <= 1) break;
+  }
+  const uint32_t nchunks = (nt + kElemThreads - 1) / kElemThreads;
+  const uint32_t scan_blocks = (nt + kScanBlock - 1) / kScanBlock;
+
+  CU(cudaMemcpyAsync(at(NaLayout::raw_x), px, 4ull * nv, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(at(NaLayout::raw_y), py, 4ull * nv, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(at(NaLayout::raw_z), pz, 4ull * nv, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(at(NaLayout::raw_tri), tris, 12ull * nt, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(at(NaLayout::inst), &I, sizeof(I), cudaMemcpyHostToDevice, st));
+  CU(cudaMemsetAsync(at(NaLayout::red), 0, NaLayout::zero_end - NaLayout::red, st));
+  CU(cudaMemsetAsync(at(NaLayout::npairs), 0, 8, st));
+
+  BatchDev d{};
+  d.pos = reinterpret_cast<float4*>(at(NaLayout::pos));
+  d.tri_idx = reinterpret_cast<const uint4*>(at(NaLayout::tri));
+  d.tri_chunks = reinterpret_cast<const int4*>(at(NaLayout::chunks));
+  d.red = reinterpret_cast<InstRed*>(at(NaLayout::red));
+  d.prm = reinterpret_cast<const StepParams*>(at(NaLayout::prm));
+  d.status = reinterpret_cast<uint32_t*>(at(NaLayout::status));
+  SelfContactView S{};
+  S.ninst = 1;
+  S.T = nt;
+  S.pair_cap = kNaMaxPairs;
+  S.inst = reinterpret_cast<SelfInst*>(at(NaLayout::inst));
+  S.tri_inst = reinterpret_cast<uint32_t*>(at(NaLayout::tri_inst));
+  S.box_min = reinterpret_cast<float4*>(at(NaLayout::box_min));
+  S.box_max = reinterpret_cast<float4*>(at(NaLayout::box_max));
+  S.cnt = reinterpret_cast<uint32_t*>(at(NaLayout::cnt));
+  S.block_sums = reinterpret_cast<uint32_t*>(at(NaLayout::block_sums));
+  S.pairs = reinterpret_cast<uint2*>(at(NaLayout::pairs));
+  S.npairs = reinterpret_cast<uint32_t*>(at(NaLayout::npairs));
+  S.scan_blocks = scan_blocks;
+
+  const uint32_t pack_blocks = std::min<uint32_t>((std::max(nv, nt) + 255) / 256, 148 * 8);
+  k_na_pack<<<pack_blocks, 256, 0, st>>>(reinterpret_cast<const float*>(at(NaLayout::raw_x)),
+                                         reinterpret_cast<const float*>(at(NaLayout::raw_y)),
+                                         reinterpret_cast<const float*>(at(NaLayout::raw_z)), nv,
+                                         reinterpret_cast<const uint32_t*>(at(NaLayout::raw_tri)), nt,
+                                         d.pos, reinterpret_cast<uint4*>(at(NaLayout::tri)), S.tri_inst,
+                                         reinterpret_cast<int4*>(at(NaLayout::chunks)), nchunks);
+  k_self_boxes<<<1, 1024, 0, st>>>(d, S, margin);
+  k_self_count<<<nchunks, kElemThreads, 0, st>>>(d, S);
+  k_scan_local<<<scan_blocks, kScanBlock, 0, st>>>(S.cnt, nt, S.block_sums);
+  k_scan_sums<<<1, kScanBlock, 0, st>>>(S.block_sums, scan_blocks, S.npairs);
+  k_scan_add<<<scan_blocks, kScanBlock, 0, st>>>(S.cnt, nt, S.block_sums);
+  CU(cudaGetLastError());
+  uint32_t total = 0;
+  CU(cudaMemcpyAsync(&total, S.npairs, 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  *count = total;
+  if (total > kNaMaxPairs)
+    return fail(ctx, VISTIO_ERR_CAPACITY,
+                "more than 1048576 candidate pairs: beyond the allocation-free broad phase; use vistio_broadphase_pairs");
+  if (!pairs) return VISTIO_OK;  // size query
+  if (total > cap) return fail(ctx, VISTIO_ERR_CAPACITY, "pair buffer too small");
+  k_self_write<<<nchunks, kElemThreads, 0, st>>>(d, S);
+  CU(cudaGetLastError());
+  uint32_t status = 0;
+  if (total) CU(cudaMemcpyAsync(pairs, S.pairs, 8ull * total, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(&status, d.status, 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  if (status & 2u) return fail(ctx, VISTIO_ERR_CAPACITY, "candidate pairs exceeded the scratch");
+  NaPair* P = reinterpret_cast<NaPair*>(pairs);
+  std::sort(P, P + total, [](const NaPair& u, const NaPair& v) { return u.a != v.a ? u.a < v.a : u.b < v.b; });
+  return VISTIO_OK;
+}
+}  // namespace vistio_na
+
+extern "C" vistio_status vistio_broadphase_pairs_noalloc(vistio_ctx* ctx, uint32_t nv, const float* px,
+                                                         const float* py, const float* pz, uint32_t nt,
+                                                         const uint32_t* tris, float margin, uint32_t* pairs,
+                                                         uint64_t cap, uint64_t* count) {
+  return broadphase_pairs_noalloc_impl(ctx, nv, px, py, pz, nt, tris, margin, pairs, cap, count);
+}
