@@ -93,6 +93,13 @@ typedef struct vistio_solver_config {
   float contact_velocity_threshold;
   int32_t compliant_contact;
   int32_t adaptive_contact_damping;
+  /* FP64 iterative refinement of the global solve (no counterpart in the
+   * reference, whose solve runs in FP64): after the FP32 sweeps, the residual
+   * b - A d is formed in FP64 from the factored matrix and the sweeps solve for
+   * the correction, this many times (0, 1 or 2). step_with_ipc refines every
+   * solve; the plain step refines its last iteration's solve (each earlier
+   * iteration's error is corrected by the next iteration's residual). */
+  uint32_t refinement_sweeps;
 } vistio_solver_config;
 
 /* FabricProperties (crates/vistio-material/src/properties.rs:23-58). */

@@ -123,6 +123,19 @@ int main(int argc, char** argv) {
   std::vector<float> valsf(F.vals.begin(), F.vals.end());
   sweep<double>(F, F.vals, yd);
   sweep<float>(F, valsf, yf);
+  // one FP64 refinement as the GPU does it: W = b - A y with the permuted f64
+  // matrix, an FP32 sweep on W, y += W
+  std::vector<uint32_t> ap{0}, ac;
+  std::vector<double> av;
+  append_permuted_matrix(I, 0, ap, ac, av);
+  std::vector<float> yr(yf), w(nv);
+  for (uint32_t r = 0; r < nv; ++r) {
+    double acc = 0;
+    for (uint32_t q = ap[r]; q < ap[r + 1]; ++q) acc += av[q] * double(yf[ac[q]]);
+    w[r] = float(b[F.perm[r]] - acc);
+  }
+  sweep<float>(F, valsf, w);
+  for (uint32_t r = 0; r < nv; ++r) yr[r] = yf[r] + w[r];
   auto resid = [&](auto& y) {
     double rn = 0, bn = 0;
     for (uint32_t i = 0; i < nv; ++i) {
@@ -133,11 +146,17 @@ int main(int argc, char** argv) {
     }
     return std::sqrt(rn / bn);
   };
+  auto dist64 = [&](auto& y) {  // relative distance to the FP64 solution
+    double e = 0, n2 = 0;
+    for (uint32_t r = 0; r < nv; ++r) { double q = double(y[r]) - yd[r]; e += q * q; n2 += yd[r] * yd[r]; }
+    return std::sqrt(e / n2);
+  };
   uint32_t maxs = 0;
   for (auto& S : F.sn) maxs = std::max(maxs, S.ncols);
   printf("{\"nv\": %u, \"nh\": %u, \"nnz_a\": %zu, \"nnz_l\": %llu, \"stored\": %llu, \"supernodes\": %zu, "
-         "\"levels\": %u, \"subtrees\": %zu, \"max_snode\": %u, \"fwd_entries\": %zu, \"resid64\": %.3e, \"resid32\": %.3e}\n",
+         "\"levels\": %u, \"subtrees\": %zu, \"max_snode\": %u, \"fwd_entries\": %zu, \"resid64\": %.3e, \"resid32\": %.3e, "
+         "\"resid32_refined\": %.3e, \"err32\": %.3e, \"err32_refined\": %.3e}\n",
          nv, I.nh, I.A_col.size(), (unsigned long long)F.nnz_L, (unsigned long long)F.nnz_stored, F.sn.size(),
-         F.nlevels, F.sub_first.size(), maxs, F.fwd_sn.size(), resid(yd), resid(yf));
+         F.nlevels, F.sub_first.size(), maxs, F.fwd_sn.size(), resid(yd), resid(yf), resid(yr), dist64(yf), dist64(yr));
   return 0;
 }

@@ -5,14 +5,14 @@
   computes on the same f32 positions (bit-exact);
 * CCD: the GPU vertex-triangle hit set over those pairs equals the oracle's,
   both evaluated in FP64 (bit-exact), with the same minimum TOI;
-* IPC step (ground, sphere, self contact): one step from an identical state
-  within max(1e-5, 3 x e32) relative of the FP64 oracle, where e32 is the
-  error of the reference's own FP32 arithmetic (the oracle's ref32 mode) on
-  that same step. The reference's contact step has discontinuous decisions
-  (the backtracking test on grad . d, contact thresholds) and, with strong
-  barriers, amplifies rounding; its FP32 path departs from FP64 by up to
-  ~1e-4 on such steps, so the GPU is held to that bar there and to 1e-5
-  elsewhere. Short runs stay within 1e-4 m of FP64.
+* IPC step (ground, sphere): every step from an identical state within 1e-5
+  relative of the FP64 oracle, with the same AL pass count, active contacts
+  and step size. The reference's own FP32 arithmetic (the oracle's ref32 mode)
+  misses that bar on these steps (up to ~8e-4: the FP32 polar decomposition of
+  compressed triangles and the backtracking test amplify its rounding); the
+  GPU forms those parts in FP64 and is printed beside it.
+* self-contact step: within max(1e-5, e32) of FP64, e32 the ref32 error.
+  Short runs stay within 1e-4 m of FP64.
 """
 import numpy as np
 import pytest
@@ -102,7 +102,7 @@ def step_errors(gpu, ref64, ref32, c, contact, dt=DT):
 
 
 def within_reference_noise(e_gpu, e32):
-    return e_gpu <= max(1e-5, 3.0 * e32)
+    return e_gpu <= max(1e-5, e32)
 
 
 def ipc_pair(mesh, contact: api.Contact, d_hat=1e-3, kappa=1e4, iters=15, al=5, precision=1, setup=None,
@@ -131,22 +131,23 @@ SPHERE = api.Contact(has_ground=True, ground_height=-0.3, has_sphere=True, spher
 
 def test_sphere_drape_steps_match_fp64():
     """sphere_drape geometry on a 24x24 sheet: every step from the oracle's
-    state within the reference's own FP32 noise of FP64 (see module doc);
-    contacts become active during the run."""
+    state within 1e-5 relative of FP64 (see module doc); contacts become
+    active and the backtracking line search engages during the run."""
     mesh = scenarios.sphere_drape(side=24, length=1.5, height=0.35)
     gpu, ref, c = ipc_pair(mesh, SPHERE)
     _, ref32, _ = ipc_pair(mesh, SPHERE, precision=0)
-    active, tight = 0, 0
+    active, backtracked = 0, 0
     for s in range(40):
         e, e32, rg, r64, r32 = step_errors(gpu, ref, ref32, c, SPHERE)
         print(f"step {s}: gpu {e:.2e} ref32 {e32:.2e} alpha {rg.last_alpha} / {r64.last_alpha}")
-        assert within_reference_noise(e, e32), (s, e, e32)
-        tight += e <= 1e-5
-        active = max(active, rg.active_contacts)
+        assert e <= 1e-5, (s, e, e32)
         assert rg.al_iterations == r64.al_iterations
         assert rg.active_contacts == r64.active_contacts
+        assert rg.last_alpha == r64.last_alpha
+        active = max(active, rg.active_contacts)
+        backtracked += rg.last_alpha < 1.0
     assert active > 0, "the sheet never reached the sphere"
-    assert tight >= 30
+    assert backtracked > 0
 
 
 def test_sphere_drape_run_within_1e4_m():
@@ -170,7 +171,8 @@ def test_ground_contact_steps_match_fp64():
     _, ref32, _ = ipc_pair(mesh, ground, precision=0)
     for s in range(20):
         e, e32, rg, r64, r32 = step_errors(gpu, ref, ref32, c, ground)
-        assert within_reference_noise(e, e32), (s, e, e32)
+        assert e <= 1e-5, (s, e, e32)
+        assert rg.active_contacts == r64.active_contacts
 
 
 @pytest.mark.parametrize("iters,al", [(2, 1), (10, 3)])

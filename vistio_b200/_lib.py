@@ -31,7 +31,7 @@ class SolverConfigC(C.Structure):
                 ("al_tolerance", C.c_float), ("friction_coefficient", C.c_float), ("contact_damping", C.c_float),
                 ("compliant_d_hat_scale", C.c_float), ("contact_damping_max", C.c_float),
                 ("contact_velocity_threshold", C.c_float), ("compliant_contact", C.c_int32),
-                ("adaptive_contact_damping", C.c_int32)]
+                ("adaptive_contact_damping", C.c_int32), ("refinement_sweeps", C.c_uint32)]
 
 
 class MaterialDesc(C.Structure):

@@ -43,6 +43,9 @@ class SolverConfig:
     adaptive_contact_damping: bool = True
     contact_damping_max: float = 0.5
     contact_velocity_threshold: float = 0.1
+    # FP64 refinement sweeps of the global solve (this library only; the
+    # reference solves in FP64): 0, 1 or 2.
+    refinement_sweeps: int = 1
 
     def to_c(self) -> L.SolverConfigC:
         c = L.SolverConfigC()
@@ -56,6 +59,7 @@ class SolverConfig:
             setattr(c, f, float(getattr(self, f)))
         c.compliant_contact = int(bool(self.compliant_contact))
         c.adaptive_contact_damping = int(bool(self.adaptive_contact_damping))
+        c.refinement_sweeps = int(self.refinement_sweeps)
         return c
 
 
@@ -367,7 +371,7 @@ class Batch:
     def stream(self) -> int:
         return L.lib().vistio_batch_stream(self.h) or 0
 
-    PHASES = {"predict": 0, "membrane": 1, "bending": 2, "gather": 3, "solve": 4, "finalize": 5}
+    PHASES = {"predict": 0, "membrane": 1, "bending": 2, "gather": 3, "solve": 4, "finalize": 5, "refine": 6}
 
     def launch_phase(self, phase: str):
         L.check(L.lib().vistio_batch_launch_phase(self.h, self.PHASES[phase]), self.ctx.h)

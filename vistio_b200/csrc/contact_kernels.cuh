@@ -22,6 +22,19 @@ __device__ __forceinline__ float scaled_barrier_grad_dev(float d, float d_hat, f
   if (isfinite(r)) return r;
   return signbit(r) ? -1e6f : 1e6f;
 }
+// The same two functions with the squared distance itself in FP64 (the
+// reference's f32 clamp constants kept).
+__device__ __forceinline__ double barrier_grad64(double d, double d_hat) {
+  double dc = fmin(fmax(d, d_hat * double(1e-3f)), d_hat);
+  if (dc >= d_hat) return 0.0;
+  double diff = dc - d_hat;
+  return -diff * (2.0 * log(dc / d_hat) + diff / dc);
+}
+__device__ __forceinline__ double scaled_barrier_grad64(double d, double d_hat, double kappa) {
+  double r = kappa * barrier_grad64(d, d_hat);
+  if (isfinite(r)) return r;
+  return signbit(r) ? -1e6 : 1e6;
+}
 
 __device__ __forceinline__ void warp_sum_u32(uint32_t& v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -44,58 +57,67 @@ __global__ void __launch_bounds__(256) k_detect(BatchDev B, int mode) {
   if ((int)threadIdx.x < ch.z) {
     uint32_t g = uint32_t(ch.y) + threadIdx.x;
     float4 x = B.pos[g];
-    float3 gr = make_float3(0.f, 0.f, 0.f);
-    if (P.self_collision)  // self-contact gradients were accumulated by k_self_grad before this kernel
-      gr = f3(mode == 0 ? B.grad[g] : B.grad_up[g]);
-    float3 n = make_float3(0.f, 0.f, 0.f);
+    float3 gr, n;
     bool inc = false;
+    // The self-contact gradient was accumulated in FP64 by k_self_grad before
+    // this kernel; the collider barriers are added to it in FP64 too: near
+    // contact the sphere distance |p - c| - r cancels catastrophically and the
+    // log barrier magnifies the rounding, so distance, gradient and normal are
+    // formed in double and rounded once.
+    double gx = 0.0, gy = 0.0, gz = 0.0, nx = 0.0, ny = 0.0, nz = 0.0, vio = 0.0;
     if (P.self_collision) {
-      float gsq = dot3(gr, gr);
-      if (gsq > 1e-12f) { float gl = sqrtf(gsq); n = gr * (1.f / gl); inc = true; }
+      const double4 s = B.gacc[g];
+      gx = s.x; gy = s.y; gz = s.z;
+      const double gsq = gx * gx + gy * gy + gz * gz;
+      if (gsq > double(1e-12f)) { const double gl = sqrt(gsq); nx = gx / gl; ny = gy / gl; nz = gz / gl; inc = true; }
     }
-    const float dh = P.d_hat, kap = P.kappa;
+    const double dh = P.d_hat, kap = P.kappa;
     if (P.has_ground) {
-      float ds = x.y - P.ground_h;
-      if (ds <= 0.f) {
-        viol = fmaxf(viol, -ds);
-        float dc = fmaxf(-ds, 1e-6f);
+      const double ds = double(x.y) - double(P.ground_h);
+      if (ds <= 0.0) {
+        vio = fmax(vio, -ds);
+        const double dc = fmax(-ds, double(1e-6f));
         active++;
-        gr.y += scaled_barrier_grad_dev(dc * dc, dh, kap) * 2.f * dc;
+        gy += scaled_barrier_grad64(dc * dc, dh, kap) * 2.0 * dc;
       } else if (ds * ds < dh) {
         active++;
-        gr.y += scaled_barrier_grad_dev(ds * ds, dh, kap) * 2.f * ds;
+        gy += scaled_barrier_grad64(ds * ds, dh, kap) * 2.0 * ds;
       }
-      if (ds * ds < dh || ds <= 0.f) { n.y += 1.f; inc = true; }
+      if (ds * ds < dh || ds <= 0.0) { ny += 1.0; inc = true; }
     }
     if (P.has_sphere) {
-      float dx = x.x - P.sphere_c[0], dy = x.y - P.sphere_c[1], dz = x.z - P.sphere_c[2];
-      float r = sqrtf(dx * dx + dy * dy + dz * dz);
-      float ds = r - P.sphere_r;
-      if (ds <= 0.f) {
-        viol = fmaxf(viol, -ds);
-        float dc = fmaxf(-ds, 1e-6f);
+      const double dx = double(x.x) - double(P.sphere_c[0]), dy = double(x.y) - double(P.sphere_c[1]),
+                   dz = double(x.z) - double(P.sphere_c[2]);
+      const double r = sqrt(dx * dx + dy * dy + dz * dz);
+      const double ds = r - double(P.sphere_r);
+      if (ds <= 0.0) {
+        vio = fmax(vio, -ds);
+        const double dc = fmax(-ds, double(1e-6f));
         active++;
-        float bg = scaled_barrier_grad_dev(dc * dc, dh, kap);
-        if (r > 1e-6f) {
-          float f = bg * 2.f * dc;
-          gr.x += f * (dx / r); gr.y += f * (dy / r); gr.z += f * (dz / r);
+        const double bg = scaled_barrier_grad64(dc * dc, dh, kap);
+        if (r > double(1e-6f)) {
+          const double f = bg * 2.0 * dc;
+          gx += f * (dx / r); gy += f * (dy / r); gz += f * (dz / r);
         } else {
-          gr.y += bg * 2.f * dc;
+          gy += bg * 2.0 * dc;
         }
       } else if (ds * ds < dh) {
         active++;
-        float f = scaled_barrier_grad_dev(ds * ds, dh, kap) * 2.f * ds;
-        gr.x += f * (dx / r); gr.y += f * (dy / r); gr.z += f * (dz / r);
+        const double f = scaled_barrier_grad64(ds * ds, dh, kap) * 2.0 * ds;
+        gx += f * (dx / r); gy += f * (dy / r); gz += f * (dz / r);
       }
-      if (ds * ds < dh || ds <= 0.f) {
-        if (r > 1e-6f) { n.x += dx / r; n.y += dy / r; n.z += dz / r; }
+      if (ds * ds < dh || ds <= 0.0) {
+        if (r > double(1e-6f)) { nx += dx / r; ny += dy / r; nz += dz / r; }
         inc = true;
       }
     }
     if (inc) {
-      float ls = dot3(n, n);
-      if (ls > 1e-12f) n = n * (1.f / sqrtf(ls));
+      const double ls = nx * nx + ny * ny + nz * nz;
+      if (ls > double(1e-12f)) { const double il = 1.0 / sqrt(ls); nx *= il; ny *= il; nz *= il; }
     }
+    gr = make_float3(float(gx), float(gy), float(gz));
+    n = make_float3(float(nx), float(ny), float(nz));
+    viol = fmaxf(viol, float(vio));
     float4 g4 = make_float4(gr.x, gr.y, gr.z, 0.f);
     if (mode == 0) {
       B.grad[g] = g4;
@@ -239,13 +261,13 @@ __global__ void k_al_finish(BatchDev B, uint32_t ninst) {
   else R.mu *= P.al_mu_growth;
 }
 
-// Zeroes the gradient accumulators before a detect (self-contact adds into them).
-__global__ void __launch_bounds__(256) k_clear_grad(BatchDev B, int mode) {
+// Zeroes the FP64 self-contact gradient accumulator before a detect.
+__global__ void __launch_bounds__(256) k_clear_grad(BatchDev B) {
   int4 ch = B.vtx_chunks[blockIdx.x];
   if (B.red[ch.x].al_done) return;
   if ((int)threadIdx.x >= ch.z) return;
   uint32_t g = uint32_t(ch.y) + threadIdx.x;
-  (mode == 0 ? B.grad : B.grad_up)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+  B.gacc[g] = make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
 }  // namespace vistio

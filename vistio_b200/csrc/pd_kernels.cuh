@@ -125,9 +125,19 @@ struct BatchDev {
   float4* U;                   // forward updates, one per (supernode, panel row)
   const uint32_t* lvl_items;   // supernodes of each batch level (block items first)
   const uint2* sub_items;      // bottom subtrees: (first, last) supernode of each
+  // FP64 refinement: the factored matrix A (f64, rows and columns in each
+  // instance's solve order, global row ids), the right-hand side the first
+  // sweep solved (R0) and the correction vector the refinement sweeps solve in
+  // place (W).
+  const uint32_t* a_ptr;
+  const uint32_t* a_col;
+  const double* a_val;
+  float4* R0;
+  float4* W;
   // contact / IPC
   float4* grad;            // barrier gradient of the detect at the start of the AL pass
   float4* grad_up;         // gradient of the re-detect
+  double4* gacc;           // FP64 accumulator of the self-contact gradient of one detect
   float4* lam;             // AL multipliers
   float4* fin_n;           // final contact normal (ever in contact)
   uint8_t* in_contact;     // of the detect at the start of the AL pass
@@ -149,9 +159,17 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
 }
 __device__ __forceinline__ float len3(float3 a) { return sqrtf(dot3(a, a)); }
 
-struct M32 { float3 c0, c1; };
+// double3 arithmetic for the FP64 local projection.
+__device__ __forceinline__ double3 operator+(double3 a, double3 b) { return make_double3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ double3 operator-(double3 a, double3 b) { return make_double3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ double3 operator*(double3 a, double s) { return make_double3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ double dot3(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double3 d3(float4 a) { return make_double3(a.x, a.y, a.z); }
 
-__device__ __forceinline__ M32 mul2(const M32& f, float a, float b, float c, float d) {
+// 3x2 column-major matrix (mat3x2.rs:16) in FP64.
+struct M32 { double3 c0, c1; };
+
+__device__ __forceinline__ M32 mul2(const M32& f, double a, double b, double c, double d) {
   // f * [[a, c], [b, d]] (column-major [a, b, c, d], mat3x2.rs:62)
   M32 r;
   r.c0 = f.c0 * a + f.c1 * b;
@@ -159,43 +177,47 @@ __device__ __forceinline__ M32 mul2(const M32& f, float a, float b, float c, flo
   return r;
 }
 
-// polar_decomposition_3x2 (crates/vistio-math/src/decomposition.rs:76-138).
+// polar_decomposition_3x2 (crates/vistio-math/src/decomposition.rs:76-138),
+// through the eigen-decomposition of F^T F like the reference. It runs in
+// FP64: its rounding grows as 1 / sigma_min^2 in compressed triangles, and in
+// FP32 that error dominates a step's error wherever the sheet is pressed
+// together. The thresholds are the reference's f32 constants.
 struct PolarD {
   M32 rot;
-  float s0, s1;
-  float2 v0, v1;
+  double s0, s1;
+  double2 v0, v1;
 };
 __device__ __forceinline__ PolarD polar_dev(const M32& f) {
-  float a = dot3(f.c0, f.c0), b = dot3(f.c0, f.c1), d = dot3(f.c1, f.c1);
-  float ht = 0.5f * (a + d), hd = 0.5f * (a - d);
-  float disc = sqrtf(hd * hd + b * b);
-  float l0 = fmaxf(ht + disc, 0.f), l1 = fmaxf(ht - disc, 0.f);
-  float s0 = sqrtf(l0), s1 = sqrtf(l1);
-  const float eps = 1.0e-10f;
+  double a = dot3(f.c0, f.c0), b = dot3(f.c0, f.c1), d = dot3(f.c1, f.c1);
+  double ht = 0.5 * (a + d), hd = 0.5 * (a - d);
+  double disc = sqrt(hd * hd + b * b);
+  double l0 = fmax(ht + disc, 0.0), l1 = fmax(ht - disc, 0.0);
+  double s0 = sqrt(l0), s1 = sqrt(l1);
+  const double eps = double(1.0e-10f);
   PolarD p;
   if (s0 < eps) {
-    p.rot.c0 = make_float3(1.f, 0.f, 0.f);
-    p.rot.c1 = make_float3(0.f, 1.f, 0.f);
-    p.s0 = p.s1 = 0.f;
-    p.v0 = make_float2(1.f, 0.f);
-    p.v1 = make_float2(0.f, 1.f);
+    p.rot.c0 = make_double3(1.0, 0.0, 0.0);
+    p.rot.c1 = make_double3(0.0, 1.0, 0.0);
+    p.s0 = p.s1 = 0.0;
+    p.v0 = make_double2(1.0, 0.0);
+    p.v1 = make_double2(0.0, 1.0);
     return p;
   }
-  float2 v0, v1;
-  if (fabsf(b) > eps) {
-    float vx = l0 - d, vy = b;
-    float r = 1.f / sqrtf(vx * vx + vy * vy);
-    v0 = make_float2(vx * r, vy * r);
-    v1 = make_float2(-v0.y, v0.x);
+  double2 v0, v1;
+  if (fabs(b) > eps) {
+    double vx = l0 - d, vy = b;
+    double r = 1.0 / sqrt(vx * vx + vy * vy);
+    v0 = make_double2(vx * r, vy * r);
+    v1 = make_double2(-v0.y, v0.x);
   } else if (a >= d) {
-    v0 = make_float2(1.f, 0.f); v1 = make_float2(0.f, 1.f);
+    v0 = make_double2(1.0, 0.0); v1 = make_double2(0.0, 1.0);
   } else {
-    v0 = make_float2(0.f, 1.f); v1 = make_float2(1.f, 0.f);
+    v0 = make_double2(0.0, 1.0); v1 = make_double2(1.0, 0.0);
   }
-  float is0 = 1.f / s0, is1 = s1 > eps ? 1.f / s1 : 0.f;
-  float si00 = v0.x * v0.x * is0 + v1.x * v1.x * is1;
-  float si01 = v0.x * v0.y * is0 + v1.x * v1.y * is1;
-  float si11 = v0.y * v0.y * is0 + v1.y * v1.y * is1;
+  double is0 = 1.0 / s0, is1 = s1 > eps ? 1.0 / s1 : 0.0;
+  double si00 = v0.x * v0.x * is0 + v1.x * v1.x * is1;
+  double si01 = v0.x * v0.y * is0 + v1.x * v1.y * is1;
+  double si11 = v0.y * v0.y * is0 + v1.y * v1.y * is1;
   p.rot = mul2(f, si00, si01, si01, si11);
   p.s0 = s0; p.s1 = s1; p.v0 = v0; p.v1 = v1;
   return p;
@@ -203,30 +225,31 @@ __device__ __forceinline__ PolarD polar_dev(const M32& f) {
 
 // Target deformation gradient of the membrane model
 // (element.rs:127-174 and crates/vistio-material/src/*.rs).
-__device__ __forceinline__ M32 model_target(int model, const M32& F, float warp, float weft) {
+__device__ __forceinline__ M32 model_target(int model, const M32& F, float warp_f, float weft_f) {
   if (model == 4) {  // IsotropicLinearModel: identity (isotropic.rs:42-57)
-    M32 r; r.c0 = make_float3(1.f, 0.f, 0.f); r.c1 = make_float3(0.f, 1.f, 0.f); return r;
+    M32 r; r.c0 = make_double3(1.0, 0.0, 0.0); r.c1 = make_double3(0.0, 1.0, 0.0); return r;
   }
   PolarD p = polar_dev(F);
   if (model == 0) return p.rot;  // ARAP: R
-  float s0t, s1t;
+  const double warp = warp_f, weft = weft_f;
+  double s0t, s1t;
   if (model == 1) {  // co-rotational, tension field: min(sigma, 1) (decomposition.rs:50-66)
-    s0t = fminf(p.s0, 1.f); s1t = fminf(p.s1, 1.f);
+    s0t = fmin(p.s0, 1.0); s1t = fmin(p.s1, 1.0);
   } else if (model == 2) {  // orthotropic (orthotropic.rs:51-79)
-    float mk = fmaxf(fmaxf(warp, weft), 1e-6f);
-    float kw = warp / mk, kf = weft / mk;
-    s0t = p.s0 + (1.f - p.s0) * kw;
-    s1t = p.s1 + (1.f - p.s1) * kf;
+    double mk = fmax(fmax(warp, weft), double(1e-6f));
+    double kw = warp / mk, kf = weft / mk;
+    s0t = p.s0 + (1.0 - p.s0) * kw;
+    s1t = p.s1 + (1.0 - p.s1) * kf;
   } else {  // anisotropic co-rotational (anisotropic.rs:78-143)
-    float kw = fminf(fmaxf(warp, 0.f), 1.f), kf = fminf(fmaxf(weft, 0.f), 1.f);
-    float cos2 = p.v0.x * p.v0.x, sin2 = p.v0.y * p.v0.y;
-    float k0 = kw * cos2 + kf * sin2, k1 = kw * sin2 + kf * cos2;
-    s0t = p.s0 > 1.f ? 1.f + (p.s0 - 1.f) * (1.f - k0) : p.s0;
-    s1t = p.s1 > 1.f ? 1.f + (p.s1 - 1.f) * (1.f - k1) : p.s1;
+    double kw = fmin(fmax(warp, 0.0), 1.0), kf = fmin(fmax(weft, 0.0), 1.0);
+    double cos2 = p.v0.x * p.v0.x, sin2 = p.v0.y * p.v0.y;
+    double k0 = kw * cos2 + kf * sin2, k1 = kw * sin2 + kf * cos2;
+    s0t = p.s0 > 1.0 ? 1.0 + (p.s0 - 1.0) * (1.0 - k0) : p.s0;
+    s1t = p.s1 > 1.0 ? 1.0 + (p.s1 - 1.0) * (1.0 - k1) : p.s1;
   }
-  float t00 = p.v0.x * p.v0.x * s0t + p.v1.x * p.v1.x * s1t;
-  float t01 = p.v0.x * p.v0.y * s0t + p.v1.x * p.v1.y * s1t;
-  float t11 = p.v0.y * p.v0.y * s0t + p.v1.y * p.v1.y * s1t;
+  double t00 = p.v0.x * p.v0.x * s0t + p.v1.x * p.v1.x * s1t;
+  double t01 = p.v0.x * p.v0.y * s0t + p.v1.x * p.v1.y * s1t;
+  double t11 = p.v0.y * p.v0.y * s0t + p.v1.y * p.v1.y * s1t;
   return mul2(p.rot, t00, t01, t01, t11);
 }
 
@@ -241,25 +264,27 @@ __global__ void __launch_bounds__(256) k_tri(BatchDev B) {
   uint4 id = B.tri_idx[t];
   float4 dm = B.tri_dm[t];
   float w = B.tri_w[t];
-  float3 p0 = f3(B.pos[id.x]), p1 = f3(B.pos[id.y]), p2 = f3(B.pos[id.z]);
+  // FP64 from the FP32 positions on (the projection is the ill-conditioned
+  // part; the outputs are rounded once).
+  const double3 p0 = d3(B.pos[id.x]), p1 = d3(B.pos[id.y]), p2 = d3(B.pos[id.z]);
   M32 ds; ds.c0 = p1 - p0; ds.c1 = p2 - p0;
   M32 F = mul2(ds, dm.x, dm.y, dm.z, dm.w);
   float det = dm.x * dm.w - dm.y * dm.z;
-  float3 d0 = make_float3(0.f, 0.f, 0.f), d1 = d0;
+  double3 d0 = make_double3(0.0, 0.0, 0.0), d1 = d0;
   if (fabsf(det) > 1e-12f) {  // element.rs:192-202: degenerate rest shape keeps p
     M32 Ft = model_target(I.model, F, I.warp, I.weft);
-    d0 = (Ft.c0 - F.c0) * w;
-    d1 = (Ft.c1 - F.c1) * w;
+    d0 = (Ft.c0 - F.c0) * double(w);
+    d1 = (Ft.c1 - F.c1) * double(w);
   }
   // g = [[-(a+b), -(c+d)], [a, c], [b, d]] (assembly.rs:77-81)
-  float g00 = -(dm.x + dm.y), g01 = -(dm.z + dm.w);
-  float3 c0 = d0 * g00 + d1 * g01;
-  float3 c1 = d0 * dm.x + d1 * dm.z;
-  float3 c2 = d0 * dm.y + d1 * dm.w;
+  const double g00 = -(double(dm.x) + double(dm.y)), g01 = -(double(dm.z) + double(dm.w));
+  const double3 c0 = d0 * g00 + d1 * g01;
+  const double3 c1 = d0 * double(dm.x) + d1 * double(dm.z);
+  const double3 c2 = d0 * double(dm.y) + d1 * double(dm.w);
   float* o = B.tri_out + 9ull * t;
-  o[0] = c0.x; o[1] = c0.y; o[2] = c0.z;
-  o[3] = c1.x; o[4] = c1.y; o[5] = c1.z;
-  o[6] = c2.x; o[7] = c2.y; o[8] = c2.z;
+  o[0] = float(c0.x); o[1] = float(c0.y); o[2] = float(c0.z);
+  o[3] = float(c1.x); o[4] = float(c1.y); o[5] = float(c1.z);
+  o[6] = float(c2.x); o[7] = float(c2.y); o[8] = float(c2.z);
 }
 
 // Rotation of v = p - centre about `axis` by angle minus v itself:
@@ -312,7 +337,8 @@ __global__ void __launch_bounds__(256) k_hinge(BatchDev B) {
 
 // Residual gather: r_i = m_i (pred_i / dt^2 - x_i / h^2) + sum of element
 // terms [- (mu grad_i + lambda_i)], written in solve (permuted) order.
-__global__ void __launch_bounds__(256) k_gather(BatchDev B) {
+// keep_rhs also stores r in R0 for a refinement of this iteration's solve.
+__global__ void __launch_bounds__(256) k_gather(BatchDev B, int keep_rhs) {
   int4 ch = B.vtx_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   const InstDev I = B.inst[ch.x];
@@ -342,7 +368,9 @@ __global__ void __launch_bounds__(256) k_gather(BatchDev B) {
     float4 gr = B.grad[g], la = B.lam[g];
     r.x -= mu * gr.x + la.x; r.y -= mu * gr.y + la.y; r.z -= mu * gr.z + la.z;
   }
-  B.Y[I.vbase + B.perm_local[g]] = make_float4(r.x, r.y, r.z, 0.f);
+  const uint32_t row = I.vbase + B.perm_local[g];
+  B.Y[row] = make_float4(r.x, r.y, r.z, 0.f);
+  if (keep_rhs) B.R0[row] = make_float4(r.x, r.y, r.z, 0.f);
 }
 
 __device__ __forceinline__ void f4_fma(float4& t, float a, float4 y) {
@@ -744,9 +772,39 @@ __global__ void k_red_reset(BatchDev B, uint32_t ninst) {
   R.gdd = 0.0;
 }
 
+// Iterative refinement of the global solve: W = R0 - A d in FP64, with d the
+// sweeps' FP32 solution in Y and A the f64 matrix that was factored. Each
+// instance's rows are numbered like its vertices, so the vertex chunks cover
+// them. The sweeps then solve A e = W in place and d + e replaces d.
+__global__ void __launch_bounds__(256) k_refine(BatchDev B) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  const uint32_t p = uint32_t(ch.y) + threadIdx.x;
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  for (uint32_t q = B.a_ptr[p], qe = B.a_ptr[p + 1]; q < qe; ++q) {
+    const double a = B.a_val[q];
+    const float4 d = B.Y[B.a_col[q]];
+    ax += a * d.x; ay += a * d.y; az += a * d.z;
+  }
+  const float4 r = B.R0[p];
+  B.W[p] = make_float4(float(double(r.x) - ax), float(double(r.y) - ay), float(double(r.z) - az), 0.f);
+}
+
+// d <- d + e between two refinement sweeps.
+__global__ void __launch_bounds__(256) k_accum(BatchDev B) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  const uint32_t p = uint32_t(ch.y) + threadIdx.x;
+  B.Y[p] = f4_add(B.Y[p], B.W[p]);
+}
+
 // After the sweeps: residual sums (pd_solver.rs:403-421) and, for the plain
 // step, x <- x + d, the pin reset (:429-435) and the ground clamp (:438).
-__global__ void __launch_bounds__(256) k_update(BatchDev B, int do_update) {
+// add_w folds the last refinement correction into d (and into Y, where the
+// IPC kernels read d).
+__global__ void __launch_bounds__(256) k_update(BatchDev B, int do_update, int add_w) {
   int4 ch = B.vtx_chunks[blockIdx.x];
   const InstDev I = B.inst[ch.x];
   InstRed& R = B.red[ch.x];
@@ -755,7 +813,12 @@ __global__ void __launch_bounds__(256) k_update(BatchDev B, int do_update) {
   bool bad = false;
   if ((int)threadIdx.x < ch.z) {
     uint32_t g = uint32_t(ch.y) + threadIdx.x;
-    float4 d = B.Y[I.vbase + B.perm_local[g]];
+    const uint32_t row = I.vbase + B.perm_local[g];
+    float4 d = B.Y[row];
+    if (add_w) {
+      d = f4_add(d, B.W[row]);
+      B.Y[row] = d;
+    }
     float4 x = B.pos[g];
     dsq = double(d.x) * d.x + double(d.y) * d.y + double(d.z) * d.z;
     nsq = double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z;

@@ -229,104 +229,111 @@ template <class R> __device__ __forceinline__ R rclampd(R v, R lo, R hi) { retur
 
 __device__ __forceinline__ V3d<float> ld3(const float4* p, uint32_t i) { float4 a = p[i]; return {a.x, a.y, a.z}; }
 
-__device__ float pt_seg_d2(V3d<float> p, V3d<float> a, V3d<float> b) {  // :308-318
-  V3d<float> ab = vsub(b, a), ap = vsub(p, a);
-  float ab2 = vdot(ab, ab);
-  if (ab2 < 1e-20f) return vdot(ap, ap);
-  float t = rclampd(vdot(ap, ab) / ab2, 0.f, 1.f);
-  V3d<float> c = vadd(a, vmul(ab, t));
-  V3d<float> d = vsub(p, c);
+// The primitives are templated on the arithmetic type: FP32 screens every
+// candidate, FP64 evaluates those within 10 d_hat of contact (the log barrier
+// magnifies the cancellation in these distances there). The thresholds are the
+// reference's f32 constants.
+template <class R> __device__ __forceinline__ V3d<R> vdiv(V3d<R> a, R s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class R> __device__ __forceinline__ V3d<R> cvt(V3d<float> a) { return {R(a.x), R(a.y), R(a.z)}; }
+
+template <class R> __device__ R pt_seg_d2(V3d<R> p, V3d<R> a, V3d<R> b) {  // :308-318
+  V3d<R> ab = vsub(b, a), ap = vsub(p, a);
+  R ab2 = vdot(ab, ab);
+  if (ab2 < R(1e-20f)) return vdot(ap, ap);
+  R t = rclampd(vdot(ap, ab) / ab2, R(0), R(1));
+  V3d<R> c = vadd(a, vmul(ab, t));
+  V3d<R> d = vsub(p, c);
   return vdot(d, d);
 }
 
-__device__ float pt_d2(V3d<float> p, V3d<float> a, V3d<float> b, V3d<float> c) {  // :36-116
-  V3d<float> ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a), bp = vsub(p, b), cp = vsub(p, c);
-  V3d<float> nrm = vcross(ab, ac);
-  if (vdot(nrm, nrm) < 1e-20f) {
-    float dab = pt_seg_d2(p, a, b), dbc = pt_seg_d2(p, b, c), dca = pt_seg_d2(p, c, a);
+template <class R> __device__ R pt_d2(V3d<R> p, V3d<R> a, V3d<R> b, V3d<R> c) {  // :36-116
+  V3d<R> ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a), bp = vsub(p, b), cp = vsub(p, c);
+  V3d<R> nrm = vcross(ab, ac);
+  if (vdot(nrm, nrm) < R(1e-20f)) {
+    R dab = pt_seg_d2(p, a, b), dbc = pt_seg_d2(p, b, c), dca = pt_seg_d2(p, c, a);
     if (dab <= dbc && dab <= dca) return dab;
     if (dbc <= dca) return dbc;
     return dca;
   }
-  float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
-  if (d1 <= 0.f && d2 <= 0.f) return vdot(ap, ap);
-  float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
-  if (d3 >= 0.f && d4 <= d3) return vdot(bp, bp);
-  float d5 = vdot(ab, cp), d6 = vdot(ac, cp);
-  if (d6 >= 0.f && d5 <= d6) return vdot(cp, cp);
-  float vc = d1 * d4 - d3 * d2;
-  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
-    float v = d1 / (d1 - d3);
-    V3d<float> q = vsub(p, vadd(a, vmul(ab, v)));
+  R d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+  if (d1 <= R(0) && d2 <= R(0)) return vdot(ap, ap);
+  R d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+  if (d3 >= R(0) && d4 <= d3) return vdot(bp, bp);
+  R d5 = vdot(ab, cp), d6 = vdot(ac, cp);
+  if (d6 >= R(0) && d5 <= d6) return vdot(cp, cp);
+  R vc = d1 * d4 - d3 * d2;
+  if (vc <= R(0) && d1 >= R(0) && d3 <= R(0)) {
+    R v = d1 / (d1 - d3);
+    V3d<R> q = vsub(p, vadd(a, vmul(ab, v)));
     return vdot(q, q);
   }
-  float va = d3 * d6 - d5 * d4;
-  if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
-    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
-    V3d<float> q = vsub(p, vadd(b, vmul(vsub(c, b), w)));
+  R va = d3 * d6 - d5 * d4;
+  if (va <= R(0) && (d4 - d3) >= R(0) && (d5 - d6) >= R(0)) {
+    R w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    V3d<R> q = vsub(p, vadd(b, vmul(vsub(c, b), w)));
     return vdot(q, q);
   }
-  float vb = d5 * d2 - d1 * d6;
-  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
-    float w = d2 / (d2 - d6);
-    V3d<float> q = vsub(p, vadd(a, vmul(ac, w)));
+  R vb = d5 * d2 - d1 * d6;
+  if (vb <= R(0) && d2 >= R(0) && d6 <= R(0)) {
+    R w = d2 / (d2 - d6);
+    V3d<R> q = vsub(p, vadd(a, vmul(ac, w)));
     return vdot(q, q);
   }
-  float den = 1.f / (va + vb + vc);
-  float v = vb * den, w = vc * den;
-  V3d<float> q = vsub(p, vadd(vadd(a, vmul(ab, v)), vmul(ac, w)));
+  R den = R(1) / (va + vb + vc);
+  R v = vb * den, w = vc * den;
+  V3d<R> q = vsub(p, vadd(vadd(a, vmul(ab, v)), vmul(ac, w)));
   return vdot(q, q);
 }
 
-__device__ void pt_grad(V3d<float> p, V3d<float> a, V3d<float> b, V3d<float> c, V3d<float> g[4]) {  // :124-177
-  for (int k = 0; k < 4; ++k) g[k] = {0.f, 0.f, 0.f};
-  V3d<float> ab = vsub(b, a), ac = vsub(c, a), nrm = vcross(ab, ac);
-  float a2 = vdot(nrm, nrm);
-  if (a2 < 1e-20f) return;
-  V3d<float> n = vmul(nrm, 1.f / sqrtf(a2));
-  float sd = vdot(vsub(p, a), n);
-  V3d<float> pr = vsub(p, vmul(n, sd));
-  V3d<float> v2 = vsub(pr, a);
-  float d00 = vdot(ab, ab), d01 = vdot(ab, ac), d11 = vdot(ac, ac), d20 = vdot(v2, ab), d21 = vdot(v2, ac);
-  float den = d00 * d11 - d01 * d01;
-  if (fabsf(den) < 1e-20f) return;
-  float inv = 1.f / den;
-  float v = (d11 * d20 - d01 * d21) * inv, w = (d00 * d21 - d01 * d20) * inv, u = 1.f - v - w;
-  V3d<float> cl = vadd(vadd(vmul(a, u), vmul(b, v)), vmul(c, w));
-  V3d<float> d = vsub(p, cl);
-  g[0] = vmul(d, 2.f);
-  g[1] = vmul(d, -2.f * u);
-  g[2] = vmul(d, -2.f * v);
-  g[3] = vmul(d, -2.f * w);
+template <class R> __device__ void pt_grad(V3d<R> p, V3d<R> a, V3d<R> b, V3d<R> c, V3d<R> g[4]) {  // :124-177
+  for (int k = 0; k < 4; ++k) g[k] = {R(0), R(0), R(0)};
+  V3d<R> ab = vsub(b, a), ac = vsub(c, a), nrm = vcross(ab, ac);
+  R a2 = vdot(nrm, nrm);
+  if (a2 < R(1e-20f)) return;
+  V3d<R> n = vdiv(nrm, R(sqrt(a2)));
+  R sd = vdot(vsub(p, a), n);
+  V3d<R> pr = vsub(p, vmul(n, sd));
+  V3d<R> v2 = vsub(pr, a);
+  R d00 = vdot(ab, ab), d01 = vdot(ab, ac), d11 = vdot(ac, ac), d20 = vdot(v2, ab), d21 = vdot(v2, ac);
+  R den = d00 * d11 - d01 * d01;
+  if (fabs(den) < R(1e-20f)) return;
+  R inv = R(1) / den;
+  R v = (d11 * d20 - d01 * d21) * inv, w = (d00 * d21 - d01 * d20) * inv, u = R(1) - v - w;
+  V3d<R> cl = vadd(vadd(vmul(a, u), vmul(b, v)), vmul(c, w));
+  V3d<R> d = vsub(p, cl);
+  g[0] = vmul(d, R(2));
+  g[1] = vmul(d, R(-2) * u);
+  g[2] = vmul(d, R(-2) * v);
+  g[3] = vmul(d, R(-2) * w);
 }
 
-__device__ void ee_params(V3d<float> d1, V3d<float> d2, V3d<float> r, bool grad_form, float* s_out, float* t_out,
-                          bool* degen_both) {
-  float a = vdot(d1, d1), e = vdot(d2, d2), f = vdot(d2, r);
-  const float eps = 1e-10f;
+template <class R>
+__device__ void ee_params(V3d<R> d1, V3d<R> d2, V3d<R> r, bool grad_form, R* s_out, R* t_out, bool* degen_both) {
+  R a = vdot(d1, d1), e = vdot(d2, d2), f = vdot(d2, r);
+  const R eps = R(1e-10f);
   *degen_both = false;
-  float s, t;
+  R s, t;
   if (grad_form) {  // edge_edge_distance_gradient (:251-303)
-    if (a < eps || e < eps) { s = 0.f; t = 0.f; }
+    if (a < eps || e < eps) { s = R(0); t = R(0); }
     else {
-      float c = vdot(d1, r), b = vdot(d1, d2), den = a * e - b * b;
-      s = fabsf(den) > eps ? rclampd((b * f - c * e) / den, 0.f, 1.f) : 0.f;
+      R c = vdot(d1, r), b = vdot(d1, d2), den = a * e - b * b;
+      s = fabs(den) > eps ? rclampd((b * f - c * e) / den, R(0), R(1)) : R(0);
       t = (b * s + f) / e;
-      if (t < 0.f) { t = 0.f; s = rclampd(-c / a, 0.f, 1.f); }
-      else if (t > 1.f) { t = 1.f; s = rclampd((b - c) / a, 0.f, 1.f); }
+      if (t < R(0)) { t = R(0); s = rclampd(-c / a, R(0), R(1)); }
+      else if (t > R(1)) { t = R(1); s = rclampd((b - c) / a, R(0), R(1)); }
     }
   } else {  // edge_edge_distance_squared (:185-246)
-    if (a < eps && e < eps) { *degen_both = true; s = 0.f; t = 0.f; }
-    else if (a < eps) { t = rclampd(f / e, 0.f, 1.f); s = 0.f; }
+    if (a < eps && e < eps) { *degen_both = true; s = R(0); t = R(0); }
+    else if (a < eps) { t = rclampd(f / e, R(0), R(1)); s = R(0); }
     else {
-      float c = vdot(d1, r);
-      if (e < eps) { s = rclampd(-c / a, 0.f, 1.f); t = 0.f; }
+      R c = vdot(d1, r);
+      if (e < eps) { s = rclampd(-c / a, R(0), R(1)); t = R(0); }
       else {
-        float b = vdot(d1, d2), den = a * e - b * b;
-        s = fabsf(den) > eps ? rclampd((b * f - c * e) / den, 0.f, 1.f) : 0.f;
+        R b = vdot(d1, d2), den = a * e - b * b;
+        s = fabs(den) > eps ? rclampd((b * f - c * e) / den, R(0), R(1)) : R(0);
         t = (b * s + f) / e;
-        if (t < 0.f) { t = 0.f; s = rclampd(-c / a, 0.f, 1.f); }
-        else if (t > 1.f) { t = 1.f; s = rclampd((b - c) / a, 0.f, 1.f); }
+        if (t < R(0)) { t = R(0); s = rclampd(-c / a, R(0), R(1)); }
+        else if (t > R(1)) { t = R(1); s = rclampd((b - c) / a, R(0), R(1)); }
       }
     }
   }
@@ -334,35 +341,35 @@ __device__ void ee_params(V3d<float> d1, V3d<float> d2, V3d<float> r, bool grad_
   *t_out = t;
 }
 
-__device__ float ee_d2(V3d<float> a0, V3d<float> a1, V3d<float> b0, V3d<float> b1) {
-  V3d<float> d1 = vsub(a1, a0), d2 = vsub(b1, b0), r = vsub(a0, b0);
-  float s, t;
+template <class R> __device__ R ee_d2(V3d<R> a0, V3d<R> a1, V3d<R> b0, V3d<R> b1) {
+  V3d<R> d1 = vsub(a1, a0), d2 = vsub(b1, b0), r = vsub(a0, b0);
+  R s, t;
   bool dg;
   ee_params(d1, d2, r, false, &s, &t, &dg);
   if (dg) return vdot(r, r);
-  V3d<float> q = vsub(vadd(a0, vmul(d1, s)), vadd(b0, vmul(d2, t)));
+  V3d<R> q = vsub(vadd(a0, vmul(d1, s)), vadd(b0, vmul(d2, t)));
   return vdot(q, q);
 }
 
-__device__ void ee_grad(V3d<float> a0, V3d<float> a1, V3d<float> b0, V3d<float> b1, V3d<float> g[4]) {
-  V3d<float> d1 = vsub(a1, a0), d2 = vsub(b1, b0), r = vsub(a0, b0);
-  float s, t;
+template <class R> __device__ void ee_grad(V3d<R> a0, V3d<R> a1, V3d<R> b0, V3d<R> b1, V3d<R> g[4]) {
+  V3d<R> d1 = vsub(a1, a0), d2 = vsub(b1, b0), r = vsub(a0, b0);
+  R s, t;
   bool dg;
   ee_params(d1, d2, r, true, &s, &t, &dg);
-  V3d<float> q = vsub(vadd(a0, vmul(d1, s)), vadd(b0, vmul(d2, t)));
-  g[0] = vmul(q, 2.f * (1.f - s));
-  g[1] = vmul(q, 2.f * s);
-  g[2] = vmul(q, -2.f * (1.f - t));
-  g[3] = vmul(q, -2.f * t);
+  V3d<R> q = vsub(vadd(a0, vmul(d1, s)), vadd(b0, vmul(d2, t)));
+  g[0] = vmul(q, R(2) * (R(1) - s));
+  g[1] = vmul(q, R(2) * s);
+  g[2] = vmul(q, R(-2) * (R(1) - t));
+  g[3] = vmul(q, R(-2) * t);
 }
 
-// barrier_gradient_with_thickness (barrier.rs:138-162)
-__device__ __forceinline__ float scaled_barrier_grad_thick(float d, float d_hat, float kappa, float th) {
-  float tsq = th * th, de = d - tsq;
-  float raw = de <= 0.f ? barrier_grad_dev(1e-12f, d_hat) : barrier_grad_dev(de, d_hat);
-  float r = kappa * raw;
+// barrier_gradient_with_thickness (barrier.rs:138-162) in FP64.
+__device__ __forceinline__ double scaled_barrier_grad_thick64(double d, double d_hat, double kappa, double th) {
+  double tsq = th * th, de = d - tsq;
+  double raw = de <= 0.0 ? barrier_grad64(double(1e-12f), d_hat) : barrier_grad64(de, d_hat);
+  double r = kappa * raw;
   if (isfinite(r)) return r;
-  return signbit(r) ? -1e6f : 1e6f;
+  return signbit(r) ? -1e6 : 1e6;
 }
 
 __device__ __forceinline__ bool excluded(const SelfContactView& S, uint32_t i, uint32_t j) {
@@ -374,8 +381,10 @@ __device__ __forceinline__ bool excluded(const SelfContactView& S, uint32_t i, u
   return false;
 }
 
-__device__ __forceinline__ void add_grad(float4* G, uint32_t v, V3d<float> g, float bg) {
-  float* p = reinterpret_cast<float*>(G + v);
+// Contributions are summed in FP64: at a vertex between two layers they are
+// large and of opposite sign, and an FP32 sum would keep mostly rounding.
+__device__ __forceinline__ void add_grad(double4* G, uint32_t v, V3d<double> g, double bg) {
+  double* p = reinterpret_cast<double*>(G + v);
   atomicAdd(p + 0, bg * g.x);
   atomicAdd(p + 1, bg * g.y);
   atomicAdd(p + 2, bg * g.z);
@@ -383,12 +392,15 @@ __device__ __forceinline__ void add_grad(float4* G, uint32_t v, V3d<float> g, fl
 
 // SelfCollisionSystem::detect_ipc_contacts (self_collision.rs:199-276) and
 // IpcContactSet::compute_barrier_gradient (ipc_response.rs:170-219), per
-// candidate pair: 3+3 vertex-triangle and 9 edge-edge tests.
+// candidate pair: 3+3 vertex-triangle and 9 edge-edge tests. Each test is
+// screened in FP32; those with d^2 < 10 d_hat are decided and evaluated in
+// FP64 (distance, distance gradient, barrier) and rounded once.
 __global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactView S, int mode) {
   const StepParams& P = *B.prm;
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
-  float4* G = mode == 0 ? B.grad : B.grad_up;
-  const float dh = P.d_hat, kap = P.kappa, th = P.thickness;
+  double4* G = B.gacc;
+  const float screen = 10.f * P.d_hat;
+  const double dh = P.d_hat, kap = P.kappa, th = P.thickness;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
     uint2 pr = S.pairs[k];
     uint32_t inst = S.tri_inst[pr.x];
@@ -407,13 +419,15 @@ __global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactView S
         if (v == Yt[0] || v == Yt[1] || v == Yt[2]) continue;
         if (excluded(S, v, Yt[0]) || excluded(S, v, Yt[1]) || excluded(S, v, Yt[2])) continue;
         V3d<float> p = ld3(B.pos, v);
-        float d = pt_d2(p, ta, tb, tc);
-        if (!(d < dh && d > 0.f)) continue;
+        if (!(pt_d2<float>(p, ta, tb, tc) < screen)) continue;
+        const V3d<double> p8 = cvt<double>(p), a8 = cvt<double>(ta), b8 = cvt<double>(tb), c8 = cvt<double>(tc);
+        double d = pt_d2<double>(p8, a8, b8, c8);
+        if (!(d < dh && d > 0.0)) continue;
         ++nact;
-        if (d <= 1e-12f) viol = true;
-        float bg = th > 0.f ? scaled_barrier_grad_thick(d, dh, kap, th) : scaled_barrier_grad_dev(d, dh, kap);
-        V3d<float> g[4];
-        pt_grad(p, ta, tb, tc, g);
+        if (d <= double(1e-12f)) viol = true;
+        double bg = th > 0.0 ? scaled_barrier_grad_thick64(d, dh, kap, th) : scaled_barrier_grad64(d, dh, kap);
+        V3d<double> g[4];
+        pt_grad<double>(p8, a8, b8, c8, g);
         add_grad(G, v, g[0], bg); add_grad(G, Yt[0], g[1], bg); add_grad(G, Yt[1], g[2], bg); add_grad(G, Yt[2], g[3], bg);
       }
     }
@@ -425,13 +439,15 @@ __global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactView S
         if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) continue;
         if (excluded(S, a0, b0) && excluded(S, a0, b1) && excluded(S, a1, b0) && excluded(S, a1, b1)) continue;
         V3d<float> p0 = ld3(B.pos, a0), p1 = ld3(B.pos, a1), q0 = ld3(B.pos, b0), q1 = ld3(B.pos, b1);
-        float d = ee_d2(p0, p1, q0, q1);
-        if (!(d < dh && d > 0.f)) continue;
+        if (!(ee_d2<float>(p0, p1, q0, q1) < screen)) continue;
+        const V3d<double> P0 = cvt<double>(p0), P1 = cvt<double>(p1), Q0 = cvt<double>(q0), Q1 = cvt<double>(q1);
+        double d = ee_d2<double>(P0, P1, Q0, Q1);
+        if (!(d < dh && d > 0.0)) continue;
         ++nact;
-        if (d <= 1e-12f) viol = true;
-        float bg = th > 0.f ? scaled_barrier_grad_thick(d, dh, kap, th) : scaled_barrier_grad_dev(d, dh, kap);
-        V3d<float> g[4];
-        ee_grad(p0, p1, q0, q1, g);
+        if (d <= double(1e-12f)) viol = true;
+        double bg = th > 0.0 ? scaled_barrier_grad_thick64(d, dh, kap, th) : scaled_barrier_grad64(d, dh, kap);
+        V3d<double> g[4];
+        ee_grad<double>(P0, P1, Q0, Q1, g);
         add_grad(G, a0, g[0], bg); add_grad(G, a1, g[1], bg); add_grad(G, b0, g[2], bg); add_grad(G, b1, g[3], bg);
       }
     if (mode == 1 && nact) {
@@ -563,7 +579,7 @@ inline uint32_t self_ccd_launches() { return 1; }
 
 inline void launch_self_detect(const BatchDev& d, const SelfContactView& S, uint32_t n_vtx_chunks,
                                uint32_t n_tri_chunks, int mode, cudaStream_t st) {
-  k_clear_grad<<<n_vtx_chunks, 256, 0, st>>>(d, mode);
+  k_clear_grad<<<n_vtx_chunks, 256, 0, st>>>(d);
   k_self_boxes<<<S.ninst, 1024, 0, st>>>(d, S, -1.f);  // margin: StepParams::thickness
   k_self_count<<<n_tri_chunks, 256, 0, st>>>(d, S);
   k_scan_local<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);

@@ -698,4 +698,17 @@ std::string build_instance(uint32_t nv, const float* px, const float* py, const 
   return "";
 }
 
+void append_permuted_matrix(const InstanceSetup& I, uint32_t base, std::vector<uint32_t>& ptr,
+                            std::vector<uint32_t>& col, std::vector<double>& val) {
+  const Factor& F = I.factor;
+  for (uint32_t r = 0; r < I.nv; ++r) {
+    const uint32_t i = F.perm[r];
+    for (uint32_t q = I.A_ptr[i]; q < I.A_ptr[i + 1]; ++q) {
+      col.push_back(base + F.iperm[I.A_col[q]]);
+      val.push_back(I.A_val[q]);
+    }
+    ptr.push_back(uint32_t(col.size()));
+  }
+}
+
 }  // namespace vistio

@@ -102,6 +102,13 @@ std::string build_instance(uint32_t nv, const float* px, const float* py, const 
                            uint32_t nt, const uint32_t* tris, const uint8_t* pinned,
                            const SetupParams& prm, InstanceSetup& out, int* status);
 
+// Appends I's system matrix with rows and columns in solve (permuted) order:
+// for each permuted row r the end offset to ptr, and its entries (column
+// base + iperm[col], f64 value) to col / val. ptr starts as {0} (or the end of
+// the previous instance).
+void append_permuted_matrix(const InstanceSetup& I, uint32_t base, std::vector<uint32_t>& ptr,
+                            std::vector<uint32_t>& col, std::vector<double>& val);
+
 // Factorizes a general SPD matrix (CSR, either triangle or both) into the GPU layout.
 // coords (3*n) steer the nested dissection; may be null (a BFS-based split is used).
 std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,

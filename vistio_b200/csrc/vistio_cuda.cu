@@ -99,6 +99,12 @@ struct vistio_batch {
   DevBuf<uint32_t> vtri_ptr, vtri, vhinge_ptr, vhinge, perm_local, rows, lvl_items, fwd_ptr, fwd, status;
   DevBuf<uint2> sub_items;
   uint32_t n_sub = 0;
+  // FP64 refinement: permuted f64 CSR of A, kept right-hand side, correction
+  DevBuf<uint32_t> a_ptr, a_col;
+  DevBuf<double> a_val;
+  DevBuf<float4> R0, W;
+  uint32_t refine = 0;       // refinement sweeps per refined solve
+  BatchDev dev_w{};          // dev with Y = W: the sweeps of a refinement
   // batch levels of the sweeps: offset into lvl_items, block items, warp items
   std::vector<uint32_t> lvl_off, lvl_nb, lvl_nw;
   DevBuf<SnDev> sn;
@@ -106,6 +112,7 @@ struct vistio_batch {
   DevBuf<InstRed> red;
   DevBuf<StepParams> prm;
   SelfContactDev self;       // self-contact buffers (allocated on first use)
+  DevBuf<double4> gacc;      // FP64 self-contact gradient accumulator (first use)
   uint32_t n_tri_chunks = 0, n_hinge_chunks = 0, n_vtx_chunks = 0;
   uint64_t factor_bytes = 0, device_bytes = 0;
   BatchDev dev{};
@@ -239,6 +246,22 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     snb += F.sn.size(); rowsb += F.rows.size(); fwdb += F.fwd_sn.size();
   }
   fwd_ptr[V] = uint32_t(fwdb);
+  // f64 CSR of each instance's A with rows and columns in solve order (global ids)
+  std::vector<uint32_t> a_ptr, a_col;
+  std::vector<double> a_val;
+  bool have_a = b->cfg.refinement_sweeps > 0;
+  for (uint32_t k = 0; k < n && have_a; ++k) have_a = !solvers[k]->setup.A_ptr.empty();
+  if (have_a) {
+    uint64_t nnz = 0;
+    for (uint32_t k = 0; k < n; ++k) nnz += solvers[k]->setup.A_col.size();
+    if (nnz >= (1ull << 32)) return fail(ctx, VISTIO_ERR_CAPACITY, "batch too large for 32-bit matrix offsets");
+    a_ptr.reserve(V + 1);
+    a_ptr.push_back(0);
+    a_col.reserve(nnz);
+    a_val.reserve(nnz);
+    for (uint32_t k = 0; k < n; ++k) append_permuted_matrix(solvers[k]->setup, uint32_t(vb[k]), a_ptr, a_col, a_val);
+    b->refine = b->cfg.refinement_sweeps;
+  }
   // batch levels: block items (heaviest first), then warp items
   std::vector<uint32_t> items;
   for (uint32_t l = 0; l < LMAX; ++l) {
@@ -291,6 +314,10 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   b->n_sub = uint32_t(subs.size());
   CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
   CU(b->U.alloc(rows.size()));
+  if (b->refine) {
+    CU(b->a_ptr.upload(a_ptr, st)); CU(b->a_col.upload(a_col, st)); CU(b->a_val.upload(a_val, st));
+    CU(b->R0.alloc(V)); CU(b->W.alloc(V));
+  }
   CU(b->grad.alloc(V)); CU(b->grad_up.alloc(V)); CU(b->lam.alloc(V)); CU(b->fin_n.alloc(V));
   CU(cudaMemsetAsync(b->lam.p, 0, V * sizeof(float4), st));
   CU(cudaMemsetAsync(b->grad.p, 0, V * sizeof(float4), st));
@@ -304,6 +331,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
                     fwd_ptr.size() * 4 + items.size() * 4 + rows.size() * 16;
   b->device_bytes = b->factor_bytes + V * (16 * 10 + 4 + 3 + 4 * 3) + T * (16 + 16 + 4 + 36 + 12) +
                     H * (16 + 16 + 8 + 16 + 16) + (V + 1) * 8;
+  if (b->refine) b->device_bytes += (V + 1) * 4 + a_col.size() * 12 + V * 32;
   BatchDev& d = b->dev;
   d.inst = b->inst.p; d.tri_chunks = b->tri_chunks.p; d.hinge_chunks = b->hinge_chunks.p; d.vtx_chunks = b->vtx_chunks.p;
   d.pos = b->pos.p; d.vel = b->vel.p; d.prev = b->prev.p; d.pred = b->pred.p; d.mass = b->mass.p; d.pinned = b->pinned.p;
@@ -313,9 +341,12 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   d.perm_local = b->perm_local.p; d.row_vertex = nullptr; d.Y = b->Y.p; d.T = b->Tm.p;
   d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.lvl_items = b->lvl_items.p; d.sub_items = b->sub_items.p;
   d.fwd_ptr = b->fwd_ptr.p; d.fwd = b->fwd.p; d.U = b->U.p;
+  d.a_ptr = b->a_ptr.p; d.a_col = b->a_col.p; d.a_val = b->a_val.p; d.R0 = b->R0.p; d.W = b->W.p;
   d.grad = b->grad.p; d.grad_up = b->grad_up.p; d.lam = b->lam.p; d.fin_n = b->fin_n.p;
   d.in_contact = b->in_contact.p; d.in_contact_up = b->in_contact_up.p; d.ever = b->ever.p;
   d.red = b->red.p; d.prm = b->prm.p; d.status = b->status.p;
+  b->dev_w = d;
+  b->dev_w.Y = b->W.p;
   return VISTIO_OK;
 }
 
@@ -370,32 +401,50 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
   return p;
 }
 
-// The global solve: both sweeps level by level over the whole batch, then the
-// residual sums and (plain step) the position update.
-uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update) {
-  uint32_t L = uint32_t(b->lvl_off.size()), n = 2;
+// Forward then backward sweep, level by level over the whole batch, in place
+// on dv.Y (right-hand side in, solution out). Returns the launches.
+uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
+  uint32_t L = uint32_t(b->lvl_off.size()), n = 0;
   const uint32_t sub_grid = (b->n_sub + kSolveWarps - 1) / kSolveWarps;
-  k_red_reset<<<(b->ninst + 127) / 128, 128, 0, st>>>(b->dev, b->ninst);
-  if (sub_grid) { k_subtree<0><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->n_sub); ++n; }
+  if (sub_grid) { k_subtree<0><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_sub); ++n; }
   for (uint32_t l = 0; l < L; ++l) {
     uint32_t grid = b->lvl_nb[l] + (b->lvl_nw[l] + kSolveWarps - 1) / kSolveWarps;
-    if (grid) { k_level<0><<<grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
+    if (grid) { k_level<0><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
   }
   for (int l = int(L) - 1; l >= 0; --l) {
     uint32_t grid = b->lvl_nb[l] + (b->lvl_nw[l] + kSolveWarps - 1) / kSolveWarps;
-    if (grid) { k_level<1><<<grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
+    if (grid) { k_level<1><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
   }
-  if (sub_grid) { k_subtree<1><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(b->dev, b->n_sub); ++n; }
-  k_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, do_update);
+  if (sub_grid) { k_subtree<1><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_sub); ++n; }
   return n;
 }
 
-uint32_t launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update) {
+// One FP64 refinement: W = R0 - A d, then the sweeps solve A e = W in place.
+uint32_t launch_refinement(vistio_batch* b, cudaStream_t st) {
+  k_refine<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+  return 1 + launch_sweeps(b, b->dev_w, st);
+}
+
+// The global solve: the sweeps, `refine` FP64 refinement sweeps, then the
+// residual sums and (plain step) the position update.
+uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update, uint32_t refine) {
+  uint32_t n = 2;
+  k_red_reset<<<(b->ninst + 127) / 128, 128, 0, st>>>(b->dev, b->ninst);
+  n += launch_sweeps(b, b->dev, st);
+  for (uint32_t k = 0; k < refine; ++k) {
+    if (k) { k_accum<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
+    n += launch_refinement(b, st);
+  }
+  k_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, do_update, refine > 0);
+  return n;
+}
+
+uint32_t launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update, uint32_t refine) {
   uint32_t n = 1;
   if (b->n_tri_chunks) { k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
   if (b->n_hinge_chunks) { k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
-  k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
-  return n + launch_solve(b, st, do_update);
+  k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, refine > 0);
+  return n + launch_solve(b, st, do_update, refine);
 }
 
 vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out, uint32_t* nlaunch) {
@@ -408,14 +457,18 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
   k_predict<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
   uint32_t L = 2;
   if (!ipc) {
-    for (uint32_t it = 0; it < iters; ++it) L += launch_plain_iteration(b, st, 1);
+    // Each PD iteration recomputes its residual from x, so a sweep's error is
+    // corrected by the next iteration; only the last solve is refined.
+    for (uint32_t it = 0; it < iters; ++it) L += launch_plain_iteration(b, st, 1, it + 1 == iters ? b->refine : 0);
   } else {
     for (uint32_t al = 0; al < b->cfg.al_max_iterations; ++al) {
       k_al_begin<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
       if (self) { launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 0, st); L += self_detect_launches(); }
       k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 0);
       for (uint32_t it = 0; it < iters; ++it) {
-        L += launch_plain_iteration(b, st, 0) + 2;
+        // With backtracking (alpha < 1) part of each sweep's error stays in x:
+        // every solve is refined.
+        L += launch_plain_iteration(b, st, 0, b->refine) + 2;
         if (self) { launch_self_ccd(b->dev, b->self.view(), st); L += self_ccd_launches(); }
         k_ccd<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
         k_ipc_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
@@ -454,6 +507,10 @@ vistio_status batch_run(vistio_batch* b, float dt, uint32_t nsteps, const vistio
   bool ipc = ct != nullptr;
   bool self = ipc && ct->self_collision;
   if (self) {
+    if (!b->gacc.p) {
+      CU(b->gacc.alloc(b->V));
+      b->dev.gacc = b->dev_w.gacc = b->gacc.p;
+    }
     vistio_status s = ensure_self_contact(b->dev, b->self, b->solvers, b->vbase, b->T, st, &ctx->last_error);
     if (s != VISTIO_OK) return s;
   }
@@ -512,6 +569,7 @@ vistio_status init_common(vistio_ctx* ctx, const vistio_mesh_desc* mesh, const v
   if (!mesh->pos_x || !mesh->pos_y || !mesh->pos_z || !mesh->indices)
     return fail(ctx, VISTIO_ERR_INVALID_MESH, "null mesh array");
   if (cfg->max_iterations == 0) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "max_iterations must be > 0");
+  if (cfg->refinement_sweeps > 2) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "refinement_sweeps must be 0, 1 or 2");
   std::vector<uint8_t> pin(mesh->vertex_count, 0);
   if (pinned) std::memcpy(pin.data(), pinned, mesh->vertex_count);
   auto s = std::make_unique<vistio_solver>();
@@ -793,8 +851,9 @@ vistio_status vistio_batch_create(vistio_ctx* ctx, vistio_solver* const* solvers
     if (!solvers[k]) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null solver in batch");
   for (uint32_t k = 1; k < n; ++k)
     if (solvers[k]->cfg.max_iterations != solvers[0]->cfg.max_iterations ||
-        solvers[k]->cfg.al_max_iterations != solvers[0]->cfg.al_max_iterations)
-      return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "instances of a batch must share iteration counts");
+        solvers[k]->cfg.al_max_iterations != solvers[0]->cfg.al_max_iterations ||
+        solvers[k]->cfg.refinement_sweeps != solvers[0]->cfg.refinement_sweeps)
+      return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "instances of a batch must share iteration and refinement counts");
   auto* b = new vistio_batch();
   vistio_status r = pack_batch(ctx, solvers, n, b);
   if (r != VISTIO_OK) { delete b; return r; }
@@ -859,9 +918,13 @@ vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase) {
     case 0: k_predict<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
     case 1: if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev); break;
     case 2: if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); break;
-    case 3: k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
-    case 4: launch_solve(b, st, 0); break;
+    case 3: k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, b->refine > 0); break;
+    case 4: launch_solve(b, st, 0, 0); break;
     case 5: k_finalize<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
+    case 6:
+      if (!b->refine) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "the batch has no refinement sweeps");
+      launch_refinement(b, st);
+      break;
     default: return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "unknown phase");
   }
   CU(cudaGetLastError());
@@ -883,6 +946,13 @@ vistio_status vistio_batch_phase_bytes(const vistio_batch* b, int32_t phase, uin
     case 3: *bytes = V * (4 + 16 + 16 + 16) + (V + 1) * 8 + 3 * T * (4 + 12) + 4 * H * (4 + 16 + 4); break;
     case 4: *bytes = 2 * 4 * stored + fwd * 4 + rows * (4 + 2 * 16) + V * (2 * 16 + 2 * 16) + V * 8; break;
     case 5: *bytes = V * (16 * 3 + 1 + 16); break;
+    case 6: {  // refinement: A (f64 value + column), d gathered, R0, W; then one sweep pair
+      uint64_t nnz_a = 0;
+      for (auto* s : b->solvers) nnz_a += s->setup.A_col.size();
+      *bytes = nnz_a * 12 + (V + 1) * 4 + V * (16 + 16 + 16) +
+               2 * 4 * stored + fwd * 4 + rows * (4 + 2 * 16) + V * (2 * 16 + 2 * 16);
+      break;
+    }
     default: return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "unknown phase");
   }
   return VISTIO_OK;
@@ -963,7 +1033,7 @@ vistio_status vistio_sparse_solve(vistio_factor* f, const float* rhs, float* sol
   for (int pass = 0; pass < 3; ++pass) {
     for (uint32_t i = 0; i < n; ++i) y[f->f.iperm[i]] = make_float4(float(r[i]), 0.f, 0.f, 0.f);
     CU(cudaMemcpyAsync(b->Y.p, y.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
-    launch_solve(b, ctx->stream, 0);
+    launch_solve(b, ctx->stream, 0, 0);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(y.data(), b->Y.p, n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
