@@ -17,9 +17,9 @@ DT = 1.0 / 60.0
 
 
 def sheet_pair(side=20, length=1.0, stiffness=1e3, bend=1e-4, density=150.0, iters=10, model=0, bending=1,
-               warp=0.0, weft=0.0, bend_warp=0.0, bend_weft=0.0, precision=1):
+               warp=0.0, weft=0.0, bend_warp=0.0, bend_weft=0.0, precision=1, refine=0):
     mesh = scenarios.hanging_sheet(side, length)
-    cfg = api.drape_config(max_iterations=iters)
+    cfg = api.drape_config(max_iterations=iters, refinement_sweeps=refine)
     setup = api.SetupDesc(model=model, bending=bending, stiffness=stiffness, bend_stiffness=bend, density_gsm=density,
                           warp_stiffness=warp, weft_stiffness=weft, bend_warp=bend_warp, bend_weft=bend_weft)
     gpu = api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
@@ -75,17 +75,19 @@ def test_per_step_parity_along_a_trajectory():
     assert worst <= 1e-5, worst
 
 
-def test_full_hanging_sheet_run_within_1e4_m_of_fp64():
+@pytest.mark.parametrize("refine", [0, 1, 2])
+def test_full_hanging_sheet_run_within_1e4_m_of_fp64(refine):
     """hanging_sheet, 120 steps, 10 iterations: the GPU run stays within 1e-4 m
-    of the FP64 run; gravity lowers the centroid (solver_tests.rs:453-483)."""
-    mesh, gpu, ref = sheet_pair(precision=1)
+    of the FP64 run; gravity lowers the centroid (solver_tests.rs:453-483).
+    Also with 1 and 2 FP64 refinement sweeps of the last solve of each step."""
+    mesh, gpu, ref = sheet_pair(precision=1, refine=refine)
     for _ in range(120):
         gpu.step(DT)
         ref.step(DT)
     pg, _ = gpu.state()
     pr, _ = ref.state()
     err = float(np.abs(pg - pr).max())
-    print(f"120-step hanging_sheet: max |x_gpu - x_fp64| = {err:.3e} m")
+    print(f"120-step hanging_sheet, refinement {refine}: max |x_gpu - x_fp64| = {err:.3e} m")
     assert err <= 1e-4, err
     assert pg[:, 1].mean() < mesh.py.mean() - 0.1
 
@@ -125,6 +127,28 @@ def test_batch_equals_individual_solvers_bitwise():
         for _ in range(5):
             s.step(DT)
         assert np.array_equal(s.state()[0], batch.state(k)[0])
+
+
+def test_batch_whole_position_copies():
+    """download_positions returns every instance's positions in instance
+    order; upload_positions writes them back exactly (velocities untouched)."""
+    cfg = api.drape_config(max_iterations=4)
+    solvers = []
+    for side, length in [(7, 0.4), (13, 0.9), (4, 0.3)]:
+        mesh = scenarios.hanging_sheet(side, length)
+        solvers.append(api.ProjectiveDynamicsSolver().init(mesh, cfg, pinned=mesh.pinned))
+    batch = api.Batch(solvers)
+    batch.step(DT, 3)
+    allpos = batch.download_positions()
+    parts = [batch.state(k)[0] for k in range(3)]
+    assert np.array_equal(allpos, np.concatenate(parts))
+    vel_before = [batch.state(k)[1] for k in range(3)]
+    moved = (allpos + np.float32(0.25)).astype(np.float32)
+    batch.upload_positions(moved)
+    for k in range(3):
+        off = sum(len(p) for p in parts[:k])
+        assert np.array_equal(batch.state(k)[0], moved[off: off + len(parts[k])])
+        assert np.array_equal(batch.state(k)[1], vel_before[k])
 
 
 def test_sparse_solver_reference_cases():

@@ -845,6 +845,22 @@ __global__ void __launch_bounds__(256) k_update(BatchDev B, int do_update, int a
   if (threadIdx.x == 0 && ch.y == int(I.vbase)) R.iters += 1;
 }
 
+// Whole-batch positions between interleaved xyz (the host layout, one
+// contiguous copy) and the float4 state rows.
+__global__ void __launch_bounds__(256) k_unpack_pos(float4* pos, const float* __restrict__ xyz, uint64_t n) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    float4 p = pos[i];
+    p.x = xyz[3 * i]; p.y = xyz[3 * i + 1]; p.z = xyz[3 * i + 2];
+    pos[i] = p;
+  }
+}
+__global__ void __launch_bounds__(256) k_pack_pos(float* __restrict__ xyz, const float4* pos, uint64_t n) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    const float4 p = pos[i];
+    xyz[3 * i] = p.x; xyz[3 * i + 1] = p.y; xyz[3 * i + 2] = p.z;
+  }
+}
+
 // save_previous + (IPC) velocity clamp + predict + x <- pred (state.rs:145-169,
 // pd_solver.rs:273-283 and 566-603).
 __global__ void __launch_bounds__(256) k_predict(BatchDev B) {

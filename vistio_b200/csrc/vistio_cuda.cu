@@ -113,6 +113,7 @@ struct vistio_batch {
   DevBuf<StepParams> prm;
   SelfContactDev self;       // self-contact buffers (allocated on first use)
   DevBuf<double4> gacc;      // FP64 self-contact gradient accumulator (first use)
+  DevBuf<float> xyz_stage;   // interleaved positions for whole-batch copies (first use)
   uint32_t n_tri_chunks = 0, n_hinge_chunks = 0, n_vtx_chunks = 0;
   uint64_t factor_bytes = 0, device_bytes = 0;
   BatchDev dev{};
@@ -873,19 +874,28 @@ vistio_status vistio_batch_step(vistio_batch* b, float dt, uint32_t nsteps, cons
   return batch_run(b, dt, nsteps, contact);
 }
 
+// Whole-batch position copies: one contiguous copy of the interleaved xyz
+// through a device staging buffer, packed to / from the float4 rows by a
+// kernel (a strided 12-byte-row copy runs at a small fraction of the link).
 vistio_status vistio_batch_upload_positions(vistio_batch* b, const float* xyz) {
   if (!b || !xyz) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
   vistio_ctx* ctx = b->ctx;
-  CU(cudaMemcpy2DAsync(b->pos.p, sizeof(float4), xyz, 3 * sizeof(float), 3 * sizeof(float), b->V,
-                       cudaMemcpyHostToDevice, ctx->stream));
+  if (!b->xyz_stage.p) CU(b->xyz_stage.alloc(3 * b->V));
+  const uint32_t grid = uint32_t(std::min<uint64_t>((b->V + 255) / 256, 148 * 16));
+  CU(cudaMemcpyAsync(b->xyz_stage.p, xyz, 12 * b->V, cudaMemcpyHostToDevice, ctx->stream));
+  k_unpack_pos<<<grid, 256, 0, ctx->stream>>>(b->pos.p, b->xyz_stage.p, b->V);
+  CU(cudaGetLastError());
   return VISTIO_OK;
 }
 
 vistio_status vistio_batch_download_positions(vistio_batch* b, float* xyz) {
   if (!b || !xyz) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
   vistio_ctx* ctx = b->ctx;
-  CU(cudaMemcpy2DAsync(xyz, 3 * sizeof(float), b->pos.p, sizeof(float4), 3 * sizeof(float), b->V,
-                       cudaMemcpyDeviceToHost, ctx->stream));
+  if (!b->xyz_stage.p) CU(b->xyz_stage.alloc(3 * b->V));
+  const uint32_t grid = uint32_t(std::min<uint64_t>((b->V + 255) / 256, 148 * 16));
+  k_pack_pos<<<grid, 256, 0, ctx->stream>>>(b->xyz_stage.p, b->pos.p, b->V);
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(xyz, b->xyz_stage.p, 12 * b->V, cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
   return VISTIO_OK;
 }
