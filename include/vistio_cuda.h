@@ -234,6 +234,14 @@ vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase);
  * stored factor entries are counted at 4 bytes each. */
 vistio_status vistio_batch_phase_bytes(const vistio_batch* b, int32_t phase, uint64_t* bytes);
 
+/* ---- diagnostics (no counterpart in the reference) ---- */
+/* Runs the bounded barrier wait the sweep kernels use on a barrier nothing
+ * completes. The wait gives up after `polls` polls (1..2^22) and the call
+ * returns VISTIO_ERR_TIMEOUT, as a step whose staging copy never landed would;
+ * the context stays usable. Exercises the device-side failure path without a
+ * fault. */
+vistio_status vistio_diag_wait_timeout(vistio_ctx* ctx, uint32_t polls);
+
 /* ---- SparseSolver mirror ---- */
 vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
                                       const float* values, vistio_factor** out);

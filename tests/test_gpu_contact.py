@@ -192,3 +192,84 @@ def test_self_contact_step_matches(iters, al):
     print(f"self contact: gpu {e:.2e} ref32 {e32:.2e} active {rg.active_contacts} / {r64.active_contacts}")
     assert rg.active_contacts == r64.active_contacts
     assert e <= 1e-5, (e, e32)
+
+
+def steps_from_oracle(gpu, ref, c, contact, nsteps, dt=DT):
+    """nsteps GPU steps, each from the FP64 oracle's state; returns the worst
+    relative error and the last GPU step result."""
+    worst, rg = 0.0, None
+    for _ in range(nsteps):
+        p, v = ref.state()
+        gpu.set_state(p, v)
+        ref.step_ipc(dt, c)
+        rg = gpu.step_with_ipc(dt, contact)
+        worst = max(worst, rel(gpu.state()[0], ref.state()[0]))
+    return worst, rg
+
+
+def test_sphere_drape_64_configuration():
+    """The sphere-drape configuration at full size: 64x64 cells (4225
+    vertices), 1.5 m sheet at y = 0.5, sphere r = 0.3 at the origin, ground
+    -0.3, d_hat 1e-3, kappa 1e4, AL <= 5, 15 iterations. With these light
+    vertices (8e-5 kg) the barrier throws the sheet's centre back up within
+    the step in which it enters the contact zone (the reference's dynamics:
+    the oracle shows the same bounce). Steps 9-22, each from the FP64
+    oracle's state, cover two bounces and are each within 1e-5 of FP64."""
+    mesh = scenarios.sphere_drape(side=64, length=1.5, height=0.5)
+    assert mesh.nv == 4225 and mesh.nt == 8192
+    gpu, ref, c = ipc_pair(mesh, SPHERE)
+    centre = 32 * 65 + 32
+    for _ in range(9):
+        ref.step_ipc(DT, c)
+    worst, rose = 0.0, False
+    for _ in range(14):
+        p, v = ref.state()
+        gpu.set_state(p, v)
+        ref.step_ipc(DT, c)
+        gpu.step_with_ipc(DT, SPHERE)
+        pg = gpu.state()[0]
+        worst = max(worst, rel(pg, ref.state()[0]))
+        rose |= bool(pg[centre, 1] > p[centre, 1] + 0.01)  # only the barrier can lift the centre
+    print(f"sphere_drape 64x64: worst step error {worst:.2e}")
+    assert worst <= 1e-5, worst
+    assert rose, "the sheet never reached the sphere's barrier"
+
+
+def test_self_fold_configuration():
+    """The self-fold configuration at full size: a 0.2 m x 2.0 m ribbon of
+    40x400 cells (16441 vertices) rotated 45 degrees about x, orthotropic
+    membrane (warp 1e3, weft 6e2, element stiffness 1e3), self contact with
+    1-ring exclusion, ground y = 0, dt = 1/120, kappa from
+    estimate_initial_kappa with the mean vertex mass (runner.rs:190-195).
+    Two readings differ from the reference's literal wiring, because that
+    wiring makes the reference's own step diverge here (checked with the
+    oracle, FP64 and FP32 alike):
+    * the system matrix is assembled with the step's dt (1/120); with the
+      reference's fixed 1/60 the ribbon's height grows about 4x per step even
+      without contact;
+    * d_hat = 5e-4 m is a distance (barrier_d_hat = d_hat^2, thickness
+      1.5 d_hat); as a squared distance it puts every triangle pair within
+      3.2 cm of this 5 mm mesh in contact (1.4 M contacts).
+    The ribbon starts 1 mm above the ground so that contact begins at once;
+    each step is within 1e-5 of FP64."""
+    dt = 1.0 / 120.0
+    mesh = scenarios.self_fold(40, 400, 0.2, 2.0, lowest=0.001)
+    assert mesh.nv == 16441 and mesh.nt == 32000
+    d_hat = 5e-4
+    setup = api.SetupDesc(model=api.MODEL_ORTHOTROPIC, stiffness=1e3, warp_stiffness=1e3, weft_stiffness=6e2,
+                          bend_stiffness=1e-4, density_gsm=150.0, matrix_dt=dt)
+    params = O.init_params(model=O.MODEL_ORTHO, stiffness=1e3, warp=1e3, weft=6e2, bend_stiffness=1e-4,
+                           density_gsm=150.0, matrix_dt=dt)
+    probe = api.ProjectiveDynamicsSolver().init_explicit(mesh, api.drape_config(), setup, pinned=mesh.pinned)
+    kappa = float(O.lib().orc_estimate_kappa(0.0, float(probe.lumped_masses().mean()), 9.81, d_hat * d_hat))
+    # kappa <= 0 makes the library estimate it the same way
+    contact = api.Contact(has_ground=True, ground_height=0.0, self_collision=True, kappa=0.0, thickness=1.5 * d_hat)
+    gpu, ref, c = ipc_pair(mesh, contact, d_hat=d_hat * d_hat, kappa=0.0, iters=10, al=5, setup=setup, params=params)
+    c.kappa = kappa
+    worst, active = 0.0, 0
+    for _ in range(4):
+        w, rg = steps_from_oracle(gpu, ref, c, contact, 1, dt=dt)
+        worst, active = max(worst, w), max(active, rg.active_contacts)
+    print(f"self_fold 40x400: kappa {kappa:.4g}, worst step error {worst:.2e}, active contacts {active}")
+    assert worst <= 1e-5, worst
+    assert active > 0

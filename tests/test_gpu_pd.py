@@ -190,3 +190,18 @@ def test_not_spd_is_reported():
     with pytest.raises(api.L.VistioError) as e:
         s.factorize([0, 1, 2], [0, 1], [1.0, -1.0], 2)
     assert e.value.status == 11
+
+
+def test_bounded_device_wait_reports_timeout_and_context_survives():
+    """A device wait that nothing completes ends with VISTIO_ERR_TIMEOUT after
+    its poll limit (no hang, no fault), and the same context steps normally
+    afterwards."""
+    from vistio_b200 import _lib
+    ctx = api.default_context()
+    st = _lib.lib().vistio_diag_wait_timeout(ctx.h, 1 << 12)
+    assert st == 9, st  # VISTIO_ERR_TIMEOUT
+    assert b"gave up" in _lib.lib().vistio_last_error(ctx.h)
+    mesh, gpu, ref = sheet_pair(side=8, length=0.5)
+    gpu.step(DT)
+    ref.step(DT)
+    assert rel(gpu.state()[0], ref.state()[0]) <= 1e-5

@@ -103,6 +103,7 @@ SIGNATURES = {
     "vistio_batch_stream": (_vp, [_vp]),
     "vistio_batch_launch_phase": (C.c_int, [_vp, C.c_int32]),
     "vistio_batch_phase_bytes": (C.c_int, [_vp, C.c_int32, _u64p]),
+    "vistio_diag_wait_timeout": (C.c_int, [_vp, C.c_uint32]),
     "vistio_sparse_factorize": (C.c_int, [_vp, C.c_uint32, _u32p, _u32p, _fp, C.POINTER(_vp)]),
     "vistio_sparse_solve": (C.c_int, [_vp, _fp, _fp]),
     "vistio_sparse_destroy": (C.c_int, [_vp]),

@@ -424,9 +424,9 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kWaitLimit) {
   const uint32_t b = smem_u32(bar);
-  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -436,6 +436,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (done) return true;
   }
   return false;
+}
+
+// Diagnostic of the failure path: the sweeps' bounded wait on a barrier that
+// nothing completes gives up after `polls` polls and records the timeout
+// status bit, as a sweep whose staging copy never lands does.
+__global__ void k_diag_wait(uint32_t* status, uint32_t polls) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(&bar);
+  mbar_fence_init();
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, polls)) atomicOr(status, 4u);
 }
 
 // A team is either one warp (a supernode per warp) or the whole block.

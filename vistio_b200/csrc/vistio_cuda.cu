@@ -1069,6 +1069,22 @@ vistio_status vistio_sparse_destroy(vistio_factor* f) {
   return VISTIO_OK;
 }
 
+vistio_status vistio_diag_wait_timeout(vistio_ctx* ctx, uint32_t polls) {
+  if (!ctx) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null context");
+  if (polls == 0 || polls > kWaitLimit) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "polls must be in 1..2^22");
+  DevBuf<uint32_t> st;
+  uint32_t bits = 0;
+  CU(st.alloc(1));
+  CU(cudaMemsetAsync(st.p, 0, 4, ctx->stream));
+  k_diag_wait<<<1, 32, 0, ctx->stream>>>(st.p, polls);
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(&bits, st.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  if (bits & 4u)
+    return fail(ctx, VISTIO_ERR_TIMEOUT, "bounded device wait gave up after " + std::to_string(polls) + " polls");
+  return fail(ctx, VISTIO_ERR_INVARIANT, "the diagnostic wait completed although nothing signalled it");
+}
+
 vistio_status vistio_broadphase_pairs(vistio_ctx* ctx, uint32_t nv, const float* px, const float* py, const float* pz,
                                       uint32_t nt, const uint32_t* tris, float margin, uint32_t* pairs, uint64_t cap,
                                       uint64_t* count) {
