@@ -656,51 +656,99 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
   tm.sync();
 }
 
-// The supernodes [first, last] of one bottom subtree, staged with one bulk
-// copy, swept in postorder (forward) or reverse postorder (backward) from
-// shared memory by one warp.
+// The supernodes [first, last] of one bottom subtree, swept by one warp in
+// postorder (forward) or reverse postorder (backward). The subtree's columns
+// [c0, c1) are contiguous and every update to them comes from inside the
+// subtree, so its slice of the vector stays in shared memory (acc) for the
+// whole sweep: the forward sweep pulls nothing from global memory and pushes
+// only the updates bound for rows above the subtree (U slots that the top
+// levels pull); the backward sweep reads global memory only for the final
+// values of those rows. The factor data arrives with one bulk copy, issued
+// before the vector slice is loaded so that the two overlap.
 template <int DIR>
 __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint32_t first, uint32_t last) {
   const SnDev F = B.sn[first], Lz = B.sn[last];
   const uint64_t end = Lz.p_off + ((uint64_t(Lz.nrows) * Lz.ncols + 3) & ~3ull);
-  const float* base = stage(tm, B.vals + F.d_off, uint32_t(end - F.d_off), B.status);
+  const float* src = B.vals + F.d_off;  // 16-byte aligned: d_off is a multiple of 4
+  const uint32_t bytes = uint32_t(end - F.d_off) * 4u;
+  tm.sync();  // previous readers of the buffer are done
+  if (tm.rank == 0) bulk_g2s(tm.buf, src, bytes, tm.bar);
+  const uint32_t c0 = F.first, c1 = Lz.first + Lz.ncols, nc = c1 - c0;
+  float4* Yg = B.Y + F.vbase;
+  float4* acc = tm.v1;  // rows c0 .. c1 of this instance (nc <= vcap, enforced by the set-up)
+  for (uint32_t c = tm.rank; c < nc; c += tm.size) acc[c] = Yg[c0 + c];
+  const bool ok = mbar_wait(tm.bar, tm.parity);
+  tm.parity ^= 1u;
+  if (!ok) {
+    atomicOr(B.status, 4u);
+    *tm.abort = 1u;
+  }
+  tm.sync();
+  const float* base = tm.buf;
   for (uint32_t i = 0; i <= last - first; ++i) {
     const uint32_t k = DIR == 0 ? first + i : last - i;
     const SnDev S = B.sn[k];
     const float* Ds = base + (S.d_off - F.d_off);
     const float* Ps = base + (S.p_off - F.d_off);
-    float4* Y = B.Y + S.vbase;
-    const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+    const uint32_t* Rr = B.rows + S.rows_off;
+    const uint32_t s = S.ncols, m = S.nrows, f = S.first - c0;
     if (DIR == 0) {
-      sn_pull(B, tm, S, Y);
+      // t = acc (all descendant updates are in); y = inv(L_kk) t into acc
+      for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v0[c] = acc[f + c];
       tm.sync();
-      sn_diag_fwd_smem(tm, S, Ds, Y);
+      for (uint32_t c = tm.rank; c < s; c += tm.size) {
+        float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, Ds[c2 * s + c], tm.v0[c2]);
+        acc[f + c] = y;
+      }
       tm.sync();
-      sn_push_rows(B, tm, S, Ps, 0, m);
+      // u_j = P[j,:] . y: into acc for rows of the subtree (distinct rows per
+      // j, all below this supernode's block), else into the row's U slot
+      for (uint32_t j = tm.rank; j < m; j += tm.size) {
+        const uint32_t r = Rr[j];
+        float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float* row = Ps + j * s;
+        for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], acc[f + c]);
+        if (r < c1) acc[r - c0] = f4_sub(acc[r - c0], u);
+        else B.U[S.rows_off + j] = u;
+      }
       tm.sync();
     } else {
-      const uint32_t* Rr = B.rows + S.rows_off;
-      for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
+      // t = y - P^T x[R] (x of rows in the subtree from acc, above it from Y),
+      // the gathered x in chunks of xcap rows; s <= 64 needs at most two
+      // column rounds of width 32
       const uint32_t width = team_width(tm, s), parts = tm.size / width;
       const uint32_t cl = tm.rank % width, part = tm.rank / width;
-      for (uint32_t cb = 0; cb < s; cb += width) {
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        const uint32_t c = cb + cl;
-        for (uint32_t j0 = 0; j0 < m; j0 += tm.xcap) {
-          uint32_t nr = min(tm.xcap, m - j0);
-          tm.sync();
-          for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = Y[Rr[j0 + j]];
-          tm.sync();
-          if (c < s && part < parts)
-            for (uint32_t j = part; j < nr; j += parts) f4_fma(acc, Ps[(j0 + j) * s + c], tm.xg[j]);
+      float4 sum0 = make_float4(0.f, 0.f, 0.f, 0.f), sum1 = sum0;
+      for (uint32_t j0 = 0; j0 < m; j0 += tm.xcap) {
+        const uint32_t nr = min(tm.xcap, m - j0);
+        tm.sync();
+        for (uint32_t j = tm.rank; j < nr; j += tm.size) {
+          const uint32_t r = Rr[j0 + j];
+          tm.xg[j] = r < c1 ? acc[r - c0] : Yg[r];
         }
         tm.sync();
-        team_column_sum(tm, acc, width, parts, cb, s, tm.v1, tm.v0, true);
+        if (part < parts) {
+          const float* P0 = Ps + size_t(j0) * s;
+          if (cl < s)
+            for (uint32_t j = part; j < nr; j += parts) f4_fma(sum0, P0[j * s + cl], tm.xg[j]);
+          if (width + cl < s)
+            for (uint32_t j = part; j < nr; j += parts) f4_fma(sum1, P0[j * s + width + cl], tm.xg[j]);
+        }
       }
-      sn_diag_bwd_smem(tm, S, Ds, Y);
+      tm.sync();
+      team_column_sum(tm, sum0, width, parts, 0, s, acc + f, tm.v0, true);
+      if (width < s) team_column_sum(tm, sum1, width, parts, width, s, acc + f, tm.v0, true);
+      // x = inv(L_kk)^T t into acc
+      for (uint32_t c = tm.rank; c < s; c += tm.size) {
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Ds[c * s + c2], tm.v0[c2]);
+        acc[f + c] = x;
+      }
       tm.sync();
     }
   }
+  for (uint32_t c = tm.rank; c < nc; c += tm.size) Yg[c0 + c] = acc[c];
 }
 
 // Shared-memory teams of one sweep kernel block: eight warp teams and, over

@@ -425,22 +425,24 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
     S.parent = S.nrows ? f.row_sn[sns[k].below[0]] : UINT32_MAX;
     S.level = 0;
   }
-  // Bottom subtrees whose packed data fits kSubtreeFloats are swept whole by
-  // one warp; the supernodes above them are swept level by level, a top
+  // Bottom subtrees whose packed data fits kSubtreeFloats and whose columns
+  // number at most kSubtreeCols are swept whole by one warp; the supernodes
+  // above them are swept level by level, a top
   // supernode's level being one more than its highest top child (children
   // that are bottom subtrees count as below level 0).
   {
-    std::vector<uint64_t> sub(nsn, 0);
+    std::vector<uint64_t> sub(nsn, 0), cols(nsn, 0);
     std::vector<uint32_t> cnt_sub(nsn, 1);
     for (uint32_t k = 0; k < nsn; ++k) {  // children precede parents (postorder)
       sub[k] += sn_floats(f.sn[k].ncols, f.sn[k].nrows);
+      cols[k] += f.sn[k].ncols;
       uint32_t p = f.sn[k].parent;
-      if (p != UINT32_MAX) { sub[p] += sub[k]; cnt_sub[p] += cnt_sub[k]; }
+      if (p != UINT32_MAX) { sub[p] += sub[k]; cols[p] += cols[k]; cnt_sub[p] += cnt_sub[k]; }
     }
     std::vector<char> bottom(nsn, 0);
     for (int k = int(nsn) - 1; k >= 0; --k) {  // parents first
       uint32_t p = f.sn[k].parent;
-      bool fits = sub[k] <= kSubtreeFloats;
+      bool fits = sub[k] <= kSubtreeFloats && cols[k] <= kSubtreeCols;
       if (p != UINT32_MAX && bottom[p]) bottom[k] = 1;
       else if (fits) {
         bottom[k] = 1;

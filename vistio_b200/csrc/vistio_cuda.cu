@@ -23,6 +23,7 @@
 
 using namespace vistio;
 static_assert(kSubtreeFloats <= kWarpFloats, "a bottom subtree must fit one warp buffer");
+static_assert(kSubtreeCols <= kWarpVec, "a bottom subtree's vector slice must fit one warp's vector slots");
 
 struct vistio_ctx {
   int device = 0;
