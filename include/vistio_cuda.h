@@ -193,6 +193,13 @@ vistio_status vistio_solver_init_explicit(vistio_ctx* ctx, const vistio_mesh_des
                                           const uint8_t* pinned, vistio_solver** out);
 vistio_status vistio_solver_destroy(vistio_solver* s);
 const char* vistio_solver_name(const vistio_solver* s); /* "ProjectiveDynamics" */
+/* A new solver with the same set-up (mesh data, factor, configuration) and
+ * the source's current state, bound to `ctx`; it saves the set-up cost when
+ * the same garment, material and dt are simulated again. */
+vistio_status vistio_solver_clone(vistio_solver* s, vistio_ctx* ctx, vistio_solver** out);
+/* Device bytes the garment occupies inside a batch (with the self-contact
+ * buffers when self_contact != 0): the admission estimate of a server. */
+vistio_status vistio_solver_device_bytes(const vistio_solver* s, int32_t self_contact, uint64_t* bytes);
 vistio_status vistio_solver_info(const vistio_solver* s, uint32_t* nv, uint32_t* nt, uint32_t* nh,
                                  uint64_t* nnz_a, uint64_t* nnz_l, uint32_t* nsupernodes, uint32_t* nlevels);
 vistio_status vistio_solver_lumped_masses(const vistio_solver* s, float* out);
@@ -233,6 +240,86 @@ vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase);
  * vistio_batch_launch_phase), from the batch's element counts and factor sizes:
  * stored factor entries are counted at 4 bytes each. */
 vistio_status vistio_batch_phase_bytes(const vistio_batch* b, int32_t phase, uint64_t* bytes);
+
+/* ---- serving: continuous batching of drape requests ----
+ * No counterpart in the reference, whose runner simulates one scenario at a
+ * time. Requests are submitted with their own mesh, material, contact set-up,
+ * dt and step count. Host threads build each request's set-up (cached by
+ * topology, material, configuration and dt). At every vistio_server_tick the
+ * ready requests that share a step configuration are packed into a new cohort
+ * (one batch, on its own stream) when the device-memory budget allows, so
+ * requests arriving while others run are admitted at once and their work
+ * overlaps on the GPU. A finished cohort hands back its states and frees its
+ * memory without synchronising the device. One host thread calls
+ * submit / tick / query / result; the set-up threads are internal. */
+typedef struct vistio_server vistio_server;
+
+typedef struct vistio_server_config {
+  int32_t device;
+  uint64_t hbm_budget_bytes;  /* admission budget for resident cohorts */
+  uint32_t max_cohort;        /* most requests packed into one cohort */
+  uint32_t setup_threads;     /* host threads building set-ups (>= 1) */
+  uint32_t steps_per_slice;   /* steps queued per cohort ahead of the GPU (>= 1) */
+  uint64_t cache_bytes;       /* host memory for cached set-ups (0: no cache) */
+} vistio_server_config;
+
+typedef struct vistio_request {
+  vistio_mesh_desc mesh;
+  const uint8_t* pinned;          /* may be NULL */
+  vistio_solver_config config;
+  vistio_setup_desc setup;
+  int32_t has_contact;            /* 0: SolverStrategy::step, 1: step_with_ipc */
+  vistio_contact_desc contact;    /* with has_contact 0 only has_ground / ground_height are used */
+  float dt;
+  uint32_t steps;
+} vistio_request;
+
+typedef enum vistio_request_state {
+  VISTIO_REQ_QUEUED = 0,   /* waiting for a set-up thread */
+  VISTIO_REQ_SETUP = 1,    /* set-up being built */
+  VISTIO_REQ_READY = 2,    /* waiting for admission */
+  VISTIO_REQ_RUNNING = 3,  /* in a cohort on the GPU */
+  VISTIO_REQ_DONE = 4,
+  VISTIO_REQ_FAILED = 5
+} vistio_request_state;
+
+typedef struct vistio_request_info {
+  int32_t state;            /* vistio_request_state */
+  int32_t status;           /* vistio_status of a failed request */
+  uint32_t vertex_count;
+  uint32_t cohort;          /* cohort id (0 before admission) */
+  int32_t cache_hit;        /* set-up taken from the cache */
+  double submit_s, ready_s, start_s, done_s;  /* server clock, seconds */
+} vistio_request_info;
+
+typedef struct vistio_server_stats {
+  uint64_t submitted, completed, failed;
+  uint64_t cohorts_started, cohorts_active, max_cohorts_active;
+  uint64_t bytes_in_use, max_bytes_in_use;
+  uint64_t cache_hits, cache_misses;
+  uint64_t instance_steps;  /* steps of completed requests */
+  double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> done, completed requests */
+  double throughput;        /* instance_steps / (last completion - first submission) */
+} vistio_server_stats;
+
+vistio_status vistio_server_create(const vistio_server_config* cfg, vistio_server** out);
+vistio_status vistio_server_destroy(vistio_server* s);
+const char* vistio_server_last_error(const vistio_server* s);
+vistio_status vistio_server_submit(vistio_server* s, const vistio_request* r, uint64_t* id);
+/* One scheduling round: retire finished cohorts, queue the next slice of
+ * running ones, admit ready requests. *unfinished (may be NULL) = requests not
+ * yet done or failed. Does not wait for the GPU. */
+vistio_status vistio_server_tick(vistio_server* s, uint32_t* unfinished);
+/* Ticks until every submitted request is done or failed, or timeout_s passes
+ * (VISTIO_ERR_TIMEOUT). */
+vistio_status vistio_server_drain(vistio_server* s, double timeout_s);
+vistio_status vistio_server_query(vistio_server* s, uint64_t id, vistio_request_info* info);
+/* Final state of a done request (vertex_count entries each). */
+vistio_status vistio_server_result(vistio_server* s, uint64_t id, float* px, float* py, float* pz, float* vx,
+                                   float* vy, float* vz);
+/* Forgets a done or failed request (its result memory). */
+vistio_status vistio_server_release(vistio_server* s, uint64_t id);
+vistio_status vistio_server_get_stats(vistio_server* s, vistio_server_stats* st);
 
 /* ---- diagnostics (no counterpart in the reference) ---- */
 /* Runs the bounded barrier wait the sweep kernels use on a barrier nothing

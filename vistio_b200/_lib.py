@@ -65,6 +65,30 @@ class StepResultC(C.Structure):
 
 
 # Every entry point include/vistio_cuda.h declares, with its ctypes signature.
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("max_cohort", C.c_uint32),
+                ("setup_threads", C.c_uint32), ("steps_per_slice", C.c_uint32), ("cache_bytes", C.c_uint64)]
+
+
+class RequestC(C.Structure):
+    _fields_ = [("mesh", MeshDesc), ("pinned", C.POINTER(C.c_uint8)), ("config", SolverConfigC),
+                ("setup", SetupDesc), ("has_contact", C.c_int32), ("contact", ContactDesc), ("dt", C.c_float),
+                ("steps", C.c_uint32)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("vertex_count", C.c_uint32), ("cohort", C.c_uint32),
+                ("cache_hit", C.c_int32), ("submit_s", C.c_double), ("ready_s", C.c_double),
+                ("start_s", C.c_double), ("done_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "failed", "cohorts_started", "cohorts_active",
+                                          "max_cohorts_active", "bytes_in_use", "max_bytes_in_use", "cache_hits",
+                                          "cache_misses", "instance_steps")] + \
+               [(n, C.c_double) for n in ("p50_latency_s", "p99_latency_s", "mean_latency_s", "throughput")]
+
+
 _vp = C.c_void_p
 _fp = C.POINTER(C.c_float)
 _u32p = C.POINTER(C.c_uint32)
@@ -104,6 +128,18 @@ SIGNATURES = {
     "vistio_batch_launch_phase": (C.c_int, [_vp, C.c_int32]),
     "vistio_batch_phase_bytes": (C.c_int, [_vp, C.c_int32, _u64p]),
     "vistio_diag_wait_timeout": (C.c_int, [_vp, C.c_uint32]),
+    "vistio_solver_clone": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
+    "vistio_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
+    "vistio_server_destroy": (C.c_int, [_vp]),
+    "vistio_server_last_error": (C.c_char_p, [_vp]),
+    "vistio_server_submit": (C.c_int, [_vp, C.POINTER(RequestC), _u64p]),
+    "vistio_server_tick": (C.c_int, [_vp, _u32p]),
+    "vistio_server_drain": (C.c_int, [_vp, C.c_double]),
+    "vistio_server_query": (C.c_int, [_vp, C.c_uint64, C.POINTER(RequestInfo)]),
+    "vistio_server_result": (C.c_int, [_vp, C.c_uint64, _fp, _fp, _fp, _fp, _fp, _fp]),
+    "vistio_server_release": (C.c_int, [_vp, C.c_uint64]),
+    "vistio_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
+    "vistio_solver_device_bytes": (C.c_int, [_vp, C.c_int32, _u64p]),
     "vistio_sparse_factorize": (C.c_int, [_vp, C.c_uint32, _u32p, _u32p, _fp, C.POINTER(_vp)]),
     "vistio_sparse_solve": (C.c_int, [_vp, _fp, _fp]),
     "vistio_sparse_destroy": (C.c_int, [_vp]),

@@ -476,3 +476,90 @@ def ccd_hits(p0: np.ndarray, p1: np.ndarray, tris: np.ndarray, pairs: np.ndarray
                                     tris.ctypes.data_as(u32), len(pairs), pairs.ctypes.data_as(u32),
                                     hits.ctypes.data_as(u32), cap, C.byref(nh), C.byref(mt)), ctx.h)
     return hits[: nh.value], mt.value
+
+
+REQUEST_STATES = {0: "queued", 1: "setup", 2: "ready", 3: "running", 4: "done", 5: "failed"}
+
+
+class Server:
+    """Continuous batching of drape requests (vistio_server_*): each request
+    carries its own mesh, material, contact set-up, dt and step count; requests
+    that arrive while others run are admitted at the next tick as memory
+    allows and share the GPU with them. Results are read back per request."""
+
+    def __init__(self, hbm_budget_bytes: int = 8 << 30, max_cohort: int = 64, setup_threads: int = 4,
+                 steps_per_slice: int = 10, cache_bytes: int = 1 << 30, device: int = 0):
+        cfg = L.ServerConfig(device, int(hbm_budget_bytes), int(max_cohort), int(setup_threads), int(steps_per_slice),
+                             int(cache_bytes))
+        h = C.c_void_p()
+        st = L.lib().vistio_server_create(C.byref(cfg), C.byref(h))
+        if st != L.OK:
+            raise L.VistioError(st, "server creation failed")
+        self.h = h
+        self._nv = {}
+
+    def close(self):
+        if getattr(self, "h", None) and L is not None and L._lib is not None:
+            L.lib().vistio_server_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, st: int):
+        if st != L.OK:
+            raise L.VistioError(st, L.lib().vistio_server_last_error(self.h).decode())
+
+    def submit(self, mesh, config: SolverConfig, setup: SetupDesc, steps: int, dt: float,
+               contact: Optional[Contact] = None, ipc: bool = False, pinned=None) -> int:
+        """Queues a request; with ipc the steps are step_with_ipc(contact),
+        else plain steps (contact.has_ground adds the ground clamp)."""
+        px, py, pz = _f32(mesh.px), _f32(mesh.py), _f32(mesh.pz)
+        tris = np.ascontiguousarray(mesh.tris, dtype=np.uint32).reshape(-1)
+        pin = None if pinned is None else np.ascontiguousarray(pinned, dtype=np.uint8)
+        r = L.RequestC()
+        r.mesh.vertex_count = len(px)
+        r.mesh.triangle_count = len(tris) // 3
+        r.mesh.pos_x, r.mesh.pos_y, r.mesh.pos_z = _fp(px), _fp(py), _fp(pz)
+        r.mesh.indices = tris.ctypes.data_as(C.POINTER(C.c_uint32))
+        r.pinned = pin.ctypes.data_as(C.POINTER(C.c_uint8)) if pin is not None else None
+        r.config = config.to_c()
+        r.setup = setup.to_c()
+        r.has_contact = int(bool(ipc))
+        r.contact = (contact or Contact()).to_c()
+        r.dt = float(dt)
+        r.steps = int(steps)
+        rid = C.c_uint64()
+        self._check(L.lib().vistio_server_submit(self.h, C.byref(r), C.byref(rid)))
+        self._nv[rid.value] = len(px)
+        return rid.value
+
+    def tick(self) -> int:
+        n = C.c_uint32()
+        self._check(L.lib().vistio_server_tick(self.h, C.byref(n)))
+        return n.value
+
+    def drain(self, timeout_s: float = 600.0):
+        self._check(L.lib().vistio_server_drain(self.h, float(timeout_s)))
+
+    def query(self, rid: int) -> dict:
+        i = L.RequestInfo()
+        self._check(L.lib().vistio_server_query(self.h, int(rid), C.byref(i)))
+        return {"state": REQUEST_STATES[i.state], "status": i.status, "vertex_count": i.vertex_count,
+                "cohort": i.cohort, "cache_hit": bool(i.cache_hit), "submit_s": i.submit_s, "ready_s": i.ready_s,
+                "start_s": i.start_s, "done_s": i.done_s}
+
+    def result(self, rid: int):
+        nv = self._nv[rid]
+        cols = [np.zeros(nv, np.float32) for _ in range(6)]
+        self._check(L.lib().vistio_server_result(self.h, int(rid), *[_fp(c) for c in cols]))
+        return np.stack(cols[:3], 1), np.stack(cols[3:], 1)
+
+    def release(self, rid: int):
+        self._check(L.lib().vistio_server_release(self.h, int(rid)))
+        self._nv.pop(rid, None)
+
+    def stats(self) -> dict:
+        s = L.ServerStats()
+        self._check(L.lib().vistio_server_get_stats(self.h, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in L.ServerStats._fields_}

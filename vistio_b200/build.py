@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libvistio_b200.so")
-SOURCES = ["vistio_cuda.cu", "setup.cpp"]
+SOURCES = ["vistio_cuda.cu", "setup.cpp", "server.cpp"]
 HEADERS = ["pd_kernels.cuh", "contact_kernels.cuh", "self_contact.cuh", "setup.h"]
 
 NVCC_FLAGS = [

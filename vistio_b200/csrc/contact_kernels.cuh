@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) k_detect(BatchDev B, int mode) {
       const double gsq = gx * gx + gy * gy + gz * gz;
       if (gsq > double(1e-12f)) { const double gl = sqrt(gsq); nx = gx / gl; ny = gy / gl; nz = gz / gl; inc = true; }
     }
-    const double dh = P.d_hat, kap = P.kappa;
+    const double dh = P.d_hat, kap = P.kappa > 0.f ? P.kappa : I.kappa;
     if (P.has_ground) {
       const double ds = double(x.y) - double(P.ground_h);
       if (ds <= 0.0) {

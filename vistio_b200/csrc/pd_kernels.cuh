@@ -22,7 +22,7 @@ namespace vistio {
 struct InstDev {
   uint32_t vbase, nv;
   uint32_t nlvl;               // levels of the supernodal elimination tree
-  uint32_t pad0;
+  float kappa;                 // barrier stiffness estimated from this garment's own masses
   int32_t model;
   float warp, weft;
   float inv_hmat2;   // 1 / matrix_dt^2

@@ -51,16 +51,21 @@ struct SelfContactView {
   uint32_t scan_blocks;
 };
 
-// Host-side owner of those buffers (never passed to a kernel).
+// Host-side owner of those buffers (never passed to a kernel). They are
+// allocated and freed in the order of `stream`, which must outlive them.
 struct SelfContactDev : SelfContactView {
   bool ready = false;
+  cudaStream_t stream = nullptr;
   SelfContactDev() : SelfContactView{} {}
   SelfContactDev(const SelfContactDev&) = delete;
   SelfContactDev& operator=(const SelfContactDev&) = delete;
   SelfContactView view() const { return static_cast<const SelfContactView&>(*this); }
   void release() {
-    cudaFree(inst); cudaFree(tri_inst); cudaFree(box_min); cudaFree(box_max); cudaFree(cnt);
-    cudaFree(block_sums); cudaFree(pairs); cudaFree(npairs); cudaFree(adj_ptr); cudaFree(adj);
+    for (void* q : {static_cast<void*>(inst), static_cast<void*>(tri_inst), static_cast<void*>(box_min),
+                    static_cast<void*>(box_max), static_cast<void*>(cnt), static_cast<void*>(block_sums),
+                    static_cast<void*>(pairs), static_cast<void*>(npairs), static_cast<void*>(adj_ptr),
+                    static_cast<void*>(adj)})
+      if (q) cudaFreeAsync(q, stream);
     inst = nullptr; tri_inst = nullptr; box_min = box_max = nullptr; cnt = block_sums = nullptr;
     pairs = nullptr; npairs = nullptr; adj_ptr = adj = nullptr; ready = false;
   }
@@ -400,12 +405,13 @@ __global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactView S
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   double4* G = B.gacc;
   const float screen = 10.f * P.d_hat;
-  const double dh = P.d_hat, kap = P.kappa, th = P.thickness;
+  const double dh = P.d_hat, th = P.thickness;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
     uint2 pr = S.pairs[k];
     uint32_t inst = S.tri_inst[pr.x];
     InstRed& R = B.red[inst];
     if (R.al_done) continue;
+    const double kap = P.kappa > 0.f ? P.kappa : B.inst[inst].kappa;
     uint4 A = B.tri_idx[pr.x], Bt = B.tri_idx[pr.y];
     uint32_t av[3] = {A.x, A.y, A.z}, bv[3] = {Bt.x, Bt.y, Bt.z};
     uint32_t nact = 0;

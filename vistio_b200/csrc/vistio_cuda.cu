@@ -29,7 +29,41 @@ struct vistio_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   std::string last_error;
+  // Batches free their buffers in the order of this stream, so it lives until
+  // the context is destroyed and no batch uses it any more.
+  std::mutex mu;
+  int refs = 0;
+  bool closed = false;
 };
+
+namespace {
+void ctx_free(vistio_ctx* c) {
+  if (c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
+  delete c;
+}
+// A batch's hold on its context (declared first in vistio_batch, so released
+// after every buffer of the batch has been freed).
+struct CtxRef {
+  vistio_ctx* c = nullptr;
+  void bind(vistio_ctx* x) {
+    c = x;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->refs++;
+  }
+  ~CtxRef() {
+    if (!c) return;
+    bool last;
+    {
+      std::lock_guard<std::mutex> lock(c->mu);
+      last = --c->refs == 0 && c->closed;
+    }
+    if (last) ctx_free(c);
+  }
+};
+}  // namespace
 
 struct vistio_solver {
   vistio_ctx* ctx = nullptr;
@@ -63,17 +97,23 @@ vistio_status fail(vistio_ctx* ctx, vistio_status s, const std::string& msg) {
     }                                                                              \
   } while (0)
 
+// Device buffer allocated and freed in the order of one stream (the owning
+// context's), so that freeing a retired batch does not synchronise the device
+// and stall the work of other streams. The stream must outlive the buffer.
 template <class T> struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
-  ~DevBuf() { if (p) cudaFree(p); }
-  cudaError_t alloc(size_t count) {
+  cudaStream_t st = nullptr;
+  ~DevBuf() { if (p) cudaFreeAsync(p, st); }
+  cudaError_t alloc(size_t count, cudaStream_t s) {
+    if (p) { cudaFreeAsync(p, st); p = nullptr; }
+    st = s;
     n = count;
     if (count == 0) count = 1;
-    return cudaMalloc(&p, count * sizeof(T));
+    return cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), s);
   }
   cudaError_t upload(const std::vector<T>& h, cudaStream_t s) {
-    cudaError_t e = alloc(h.size());
+    cudaError_t e = alloc(h.size(), s);
     if (e != cudaSuccess || h.empty()) return e;
     return cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
   }
@@ -82,6 +122,7 @@ template <class T> struct DevBuf {
 }  // namespace
 
 struct vistio_batch {
+  CtxRef ctx_ref;  // first member: destroyed last
   vistio_ctx* ctx = nullptr;
   std::vector<vistio_solver*> solvers;
   uint32_t ninst = 0;
@@ -139,8 +180,24 @@ struct vistio_factor {
 namespace {
 
 vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch* b);
-
 inline uint64_t pad4(uint64_t n) { return (n + 3) & ~3ull; }
+float estimate_kappa(const vistio_solver_config& c, const InstanceSetup& I);
+
+// Device bytes one garment occupies in a batch (the sizes pack_batch
+// allocates), plus the self-contact buffers when those are used.
+uint64_t instance_device_bytes(const InstanceSetup& I, bool refine, bool self_contact) {
+  const Factor& F = I.factor;
+  uint64_t vals = 0;
+  for (const Supernode& X : F.sn) vals += pad4(uint64_t(X.ncols) * X.ncols) + pad4(uint64_t(X.nrows) * X.ncols);
+  const uint64_t V = I.nv, T = I.nt, H = I.nh, R = F.rows.size();
+  uint64_t b = vals * 4 + F.sn.size() * sizeof(SnDev) + R * 4 + F.fwd_sn.size() * 4 + (V + 1) * 4 +
+               F.sn.size() * 4 + R * 16;
+  b += V * (16 * 10 + 4 + 3 + 4 * 3) + T * (16 + 16 + 4 + 36 + 12) + H * (16 + 16 + 8 + 16 + 16) + (V + 1) * 8;
+  if (refine) b += (V + 1) * 4 + I.A_col.size() * 12 + V * 32;
+  if (self_contact) b += V * 32 + T * (4 + 2 * 2 * 16 + 4) + 48 * T * 8 + V * 4 + 16 * V * 4;
+  return b + 12 * V;  // whole-batch position staging
+}
+
 
 std::vector<int4> make_chunks(const std::vector<uint64_t>& base, const std::vector<uint64_t>& count) {
   std::vector<int4> ch;
@@ -153,6 +210,7 @@ std::vector<int4> make_chunks(const std::vector<uint64_t>& base, const std::vect
 vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch* b) {
   cudaStream_t st = ctx->stream;
   b->ctx = ctx;
+  b->ctx_ref.bind(ctx);
   b->solvers.assign(solvers, solvers + n);
   b->ninst = n;
   b->cfg = solvers[0]->cfg;
@@ -169,6 +227,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     d.inv_hmat2 = 1.f / (I.prm.matrix_dt * I.prm.matrix_dt);
     d.has_ground = solvers[k]->has_ground; d.ground_h = solvers[k]->ground_h;
     d.sn_base = uint32_t(NSN); d.nsn = uint32_t(I.factor.sn.size());
+    d.kappa = estimate_kappa(solvers[k]->cfg, I);
     V += I.nv; T += I.nt; H += I.nh; NSN += I.factor.sn.size(); NROWS += I.factor.rows.size();
     for (const Supernode& X : I.factor.sn) NVALS += pad4(uint64_t(X.ncols) * X.ncols) + pad4(uint64_t(X.nrows) * X.ncols);
     NLVL += I.factor.nlevels + 1; NFWD += I.factor.fwd_sn.size();
@@ -303,31 +362,31 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->prev.upload(pos, st)); CU(b->pred.upload(pos, st));
   CU(b->mass.upload(mass, st)); CU(b->pinned.upload(pin, st));
   CU(b->tri_idx.upload(tri_idx, st)); CU(b->tri_dm.upload(tri_dm, st)); CU(b->tri_w.upload(tri_w, st));
-  CU(b->tri_out.alloc(9 * T));
+  CU(b->tri_out.alloc(9 * T, st));
   CU(b->hinge_idx.upload(hinge_idx, st)); CU(b->hinge_st.upload(hinge_st, st)); CU(b->hinge_wr.upload(hinge_wr, st));
-  CU(b->hinge_out.alloc(H));
+  CU(b->hinge_out.alloc(H, st));
   CU(b->vtri_ptr.upload(vtri_ptr, st)); CU(b->vtri.upload(vtri, st));
   CU(b->vhinge_ptr.upload(vhinge_ptr, st)); CU(b->vhinge.upload(vhinge, st));
   CU(b->perm_local.upload(perm_local, st));
-  CU(b->Y.alloc(V)); CU(b->Tm.alloc(V));
+  CU(b->Y.alloc(V, st)); CU(b->Tm.alloc(V, st));
   CU(b->sn.upload(sn, st)); CU(b->rows.upload(rows, st)); CU(b->vals.upload(vals, st));
   CU(b->lvl_items.upload(items, st));
   CU(b->sub_items.upload(subs, st));
   b->n_sub = uint32_t(subs.size());
   CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
-  CU(b->U.alloc(rows.size()));
+  CU(b->U.alloc(rows.size(), st));
   if (b->refine) {
     CU(b->a_ptr.upload(a_ptr, st)); CU(b->a_col.upload(a_col, st)); CU(b->a_val.upload(a_val, st));
-    CU(b->R0.alloc(V)); CU(b->W.alloc(V));
+    CU(b->R0.alloc(V, st)); CU(b->W.alloc(V, st));
   }
-  CU(b->grad.alloc(V)); CU(b->grad_up.alloc(V)); CU(b->lam.alloc(V)); CU(b->fin_n.alloc(V));
+  CU(b->grad.alloc(V, st)); CU(b->grad_up.alloc(V, st)); CU(b->lam.alloc(V, st)); CU(b->fin_n.alloc(V, st));
   CU(cudaMemsetAsync(b->lam.p, 0, V * sizeof(float4), st));
   CU(cudaMemsetAsync(b->grad.p, 0, V * sizeof(float4), st));
   CU(cudaMemsetAsync(b->grad_up.p, 0, V * sizeof(float4), st));
-  CU(b->in_contact.alloc(V)); CU(b->in_contact_up.alloc(V)); CU(b->ever.alloc(V));
-  CU(b->red.alloc(n)); CU(cudaMemsetAsync(b->red.p, 0, n * sizeof(InstRed), st));
-  CU(b->prm.alloc(1));
-  CU(b->status.alloc(1)); CU(cudaMemsetAsync(b->status.p, 0, sizeof(uint32_t), st));
+  CU(b->in_contact.alloc(V, st)); CU(b->in_contact_up.alloc(V, st)); CU(b->ever.alloc(V, st));
+  CU(b->red.alloc(n, st)); CU(cudaMemsetAsync(b->red.p, 0, n * sizeof(InstRed), st));
+  CU(b->prm.alloc(1, st));
+  CU(b->status.alloc(1, st)); CU(cudaMemsetAsync(b->status.p, 0, sizeof(uint32_t), st));
   CU(cudaStreamSynchronize(st));
   b->factor_bytes = vals.size() * sizeof(float) + sn.size() * sizeof(SnDev) + rows.size() * 4 + fwd.size() * 4 +
                     fwd_ptr.size() * 4 + items.size() * 4 + rows.size() * 16;
@@ -352,7 +411,26 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   return VISTIO_OK;
 }
 
-StepParams make_params(const vistio_solver_config& c, float dt, const vistio_contact_desc* ct, float avg_mass) {
+// estimate_initial_kappa (barrier.rs:97-116) with the runner's inputs (no
+// configured kappa, the garment's mean free-vertex lumped mass, |g_y|, the
+// configured d_hat). Each garment gets its own, so its result does not depend
+// on the garments it is batched with.
+float estimate_kappa(const vistio_solver_config& c, const InstanceSetup& I) {
+  double sm = 0;
+  uint32_t cnt = 0;
+  for (uint32_t i = 0; i < I.nv; ++i) if (!I.pinned[i]) { sm += I.mass[i]; ++cnt; }
+  const float avg_mass = cnt ? float(sm / cnt) : 1e-3f;
+  float dhat = c.barrier_d_hat, dmid = dhat * 0.5f;
+  float dcl = std::fmin(std::fmax(dmid, dhat * 1e-3f), dhat);
+  double d64 = dcl, dd = dhat, diff = d64 - dd;
+  float gm = float(-(diff) * (2.0 * std::log(d64 / dd) + diff / d64));
+  gm = std::fabs(gm);
+  if (gm < 1e-12f) return 1e4f;
+  float kap = avg_mass * std::fabs(c.gravity[1]) / (2.f * std::sqrt(dmid) * gm);
+  return std::fmin(std::fmax(kap, 1.f), 1e6f);
+}
+
+StepParams make_params(const vistio_solver_config& c, float dt, const vistio_contact_desc* ct) {
   StepParams p{};
   p.dt = dt;
   p.inv_dt2 = 1.f / (dt * dt);
@@ -379,26 +457,8 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
     p.sphere_r = ct->sphere_radius;
     p.self_collision = ct->self_collision;
     p.thickness = ct->thickness;
-    float kap = ct->kappa;
-    if (!(kap > 0.f)) {
-      // estimate_initial_kappa (barrier.rs:97-116) with the runner's inputs:
-      // configured kappa, average vertex mass, |g_y|, configured d_hat.
-      float cfgk = c.barrier_kappa;
-      if (cfgk > 0.f) kap = cfgk;
-      else {
-        float dhat = c.barrier_d_hat, dmid = dhat * 0.5f;
-        float dcl = std::fmin(std::fmax(dmid, dhat * 1e-3f), dhat);
-        double d64 = dcl, dd = dhat, diff = d64 - dd;
-        float gm = float(-(diff) * (2.0 * std::log(d64 / dd) + diff / d64));
-        gm = std::fabs(gm);
-        if (gm < 1e-12f) kap = 1e4f;
-        else {
-          kap = avg_mass * std::fabs(c.gravity[1]) / (2.f * std::sqrt(dmid) * gm);
-          kap = std::fmin(std::fmax(kap, 1.f), 1e6f);
-        }
-      }
-    }
-    p.kappa = kap;
+    // explicit stiffness, else 0: each garment uses its own estimate (InstDev::kappa)
+    p.kappa = ct->kappa > 0.f ? ct->kappa : (c.barrier_kappa > 0.f ? c.barrier_kappa : 0.f);
   }
   return p;
 }
@@ -492,16 +552,6 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
   return VISTIO_OK;
 }
 
-float batch_avg_mass(vistio_batch* b) {
-  // The runner passes scenario.vertex_mass; the library uses the first
-  // garment's mean free-vertex lumped mass.
-  const InstanceSetup& I = b->solvers[0]->setup;
-  double s = 0;
-  uint32_t c = 0;
-  for (uint32_t i = 0; i < I.nv; ++i) if (!I.pinned[i]) { s += I.mass[i]; ++c; }
-  return c ? float(s / c) : 1e-3f;
-}
-
 vistio_status batch_run(vistio_batch* b, float dt, uint32_t nsteps, const vistio_contact_desc* ct) {
   vistio_ctx* ctx = b->ctx;
   cudaStream_t st = ctx->stream;
@@ -510,13 +560,13 @@ vistio_status batch_run(vistio_batch* b, float dt, uint32_t nsteps, const vistio
   bool self = ipc && ct->self_collision;
   if (self) {
     if (!b->gacc.p) {
-      CU(b->gacc.alloc(b->V));
+      CU(b->gacc.alloc(b->V, st));
       b->dev.gacc = b->dev_w.gacc = b->gacc.p;
     }
     vistio_status s = ensure_self_contact(b->dev, b->self, b->solvers, b->vbase, b->T, st, &ctx->last_error);
     if (s != VISTIO_OK) return s;
   }
-  StepParams p = make_params(b->cfg, dt, ct, batch_avg_mass(b));
+  StepParams p = make_params(b->cfg, dt, ct);
   CU(cudaMemcpyAsync(b->prm.p, &p, sizeof(p), cudaMemcpyHostToDevice, st));
   cudaGraphExec_t* ge = ipc ? &b->graph_ipc : &b->graph_plain;
   if (ipc && *ge && b->graph_ipc_self != int(self)) { cudaGraphExecDestroy(*ge); *ge = nullptr; }
@@ -630,6 +680,12 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   ctx = c.get();
   CU(cudaSetDevice(device));
   CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  {  // keep freed batch memory in this process's pool for reuse instead of trimming it at each synchronisation
+    cudaMemPool_t pool;
+    CU(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    CU(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   CU(cudaFuncSetAttribute(k_level<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_level<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_subtree<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
@@ -640,9 +696,13 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
 
 vistio_status vistio_ctx_destroy(vistio_ctx* ctx) {
   if (!ctx) return VISTIO_OK;
-  cudaStreamSynchronize(ctx->stream);
-  cudaStreamDestroy(ctx->stream);
-  delete ctx;
+  bool now;
+  {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->closed = true;
+    now = ctx->refs == 0;
+  }
+  if (now) ctx_free(ctx);  // else the last batch on it frees it
   return VISTIO_OK;
 }
 
@@ -705,6 +765,41 @@ vistio_status vistio_solver_destroy(vistio_solver* s) {
   if (!s) return VISTIO_OK;
   delete s->own;
   delete s;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_solver_clone(vistio_solver* s, vistio_ctx* ctx, vistio_solver** out) {
+  if (!s || !ctx || !out) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  auto c = std::make_unique<vistio_solver>();
+  c->ctx = ctx;
+  c->cfg = s->cfg;
+  c->setup = s->setup;
+  c->has_ground = s->has_ground;
+  c->ground_h = s->ground_h;
+  if (s->own) {  // the source has stepped: copy its current device state
+    const uint32_t n = s->setup.nv;
+    std::vector<float> a(6 * size_t(n));
+    vistio_status r = vistio_solver_get_state(s, a.data(), a.data() + n, a.data() + 2 * n, a.data() + 3 * n,
+                                              a.data() + 4 * n, a.data() + 5 * n);
+    if (r != VISTIO_OK) return r;
+    c->host_pos.resize(3 * size_t(n));
+    c->host_vel.resize(3 * size_t(n));
+    for (uint32_t i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) {
+        c->host_pos[3 * i + k] = a[size_t(k) * n + i];
+        c->host_vel[3 * i + k] = a[size_t(3 + k) * n + i];
+      }
+  } else {
+    c->host_pos = s->host_pos;
+    c->host_vel = s->host_vel;
+  }
+  *out = c.release();
+  return VISTIO_OK;
+}
+
+vistio_status vistio_solver_device_bytes(const vistio_solver* s, int32_t self_contact, uint64_t* bytes) {
+  if (!s || !bytes) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  *bytes = instance_device_bytes(s->setup, s->cfg.refinement_sweeps > 0, self_contact != 0);
   return VISTIO_OK;
 }
 
@@ -881,7 +976,7 @@ vistio_status vistio_batch_step(vistio_batch* b, float dt, uint32_t nsteps, cons
 vistio_status vistio_batch_upload_positions(vistio_batch* b, const float* xyz) {
   if (!b || !xyz) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
   vistio_ctx* ctx = b->ctx;
-  if (!b->xyz_stage.p) CU(b->xyz_stage.alloc(3 * b->V));
+  if (!b->xyz_stage.p) CU(b->xyz_stage.alloc(3 * b->V, ctx->stream));
   const uint32_t grid = uint32_t(std::min<uint64_t>((b->V + 255) / 256, 148 * 16));
   CU(cudaMemcpyAsync(b->xyz_stage.p, xyz, 12 * b->V, cudaMemcpyHostToDevice, ctx->stream));
   k_unpack_pos<<<grid, 256, 0, ctx->stream>>>(b->pos.p, b->xyz_stage.p, b->V);
@@ -892,7 +987,7 @@ vistio_status vistio_batch_upload_positions(vistio_batch* b, const float* xyz) {
 vistio_status vistio_batch_download_positions(vistio_batch* b, float* xyz) {
   if (!b || !xyz) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
   vistio_ctx* ctx = b->ctx;
-  if (!b->xyz_stage.p) CU(b->xyz_stage.alloc(3 * b->V));
+  if (!b->xyz_stage.p) CU(b->xyz_stage.alloc(3 * b->V, ctx->stream));
   const uint32_t grid = uint32_t(std::min<uint64_t>((b->V + 255) / 256, 148 * 16));
   k_pack_pos<<<grid, 256, 0, ctx->stream>>>(b->xyz_stage.p, b->pos.p, b->V);
   CU(cudaGetLastError());
@@ -1075,7 +1170,7 @@ vistio_status vistio_diag_wait_timeout(vistio_ctx* ctx, uint32_t polls) {
   if (polls == 0 || polls > kWaitLimit) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "polls must be in 1..2^22");
   DevBuf<uint32_t> st;
   uint32_t bits = 0;
-  CU(st.alloc(1));
+  CU(st.alloc(1, ctx->stream));
   CU(cudaMemsetAsync(st.p, 0, 4, ctx->stream));
   k_diag_wait<<<1, 32, 0, ctx->stream>>>(st.p, polls);
   CU(cudaGetLastError());
@@ -1160,13 +1255,15 @@ vistio_status self_build(SelfContactDev& S, const std::vector<std::pair<const ui
     aptr[v + 1] = uint32_t(adj.size());
   }
   S.release();
+  S.stream = st;
   S.ninst = n;
   S.T = T;
   S.pair_cap = std::max<uint64_t>(1024, 48 * T);
   S.scan_blocks = uint32_t((T + kScanBlock - 1) / kScanBlock);
   if (S.scan_blocks == 0) S.scan_blocks = 1;
   cudaError_t e;
-#define SA(ptr, bytes) if ((e = cudaMalloc(&ptr, bytes)) != cudaSuccess) return bad(e, "cudaMalloc")
+#define SA(ptr, bytes) \
+  if ((e = cudaMallocAsync(reinterpret_cast<void**>(&ptr), bytes, st)) != cudaSuccess) return bad(e, "cudaMallocAsync")
   SA(S.inst, n * sizeof(SelfInst));
   SA(S.tri_inst, std::max<uint64_t>(T, 1) * 4);
   SA(S.box_min, std::max<uint64_t>(boxes, 1) * sizeof(float4));
@@ -1220,11 +1317,11 @@ vistio_status broadphase_pairs_impl(vistio_ctx* ctx, uint32_t nv, const float* p
   DevBuf<float4> dpos; DevBuf<uint4> dti; DevBuf<int4> dch; DevBuf<InstRed> dred; DevBuf<StepParams> dprm;
   DevBuf<uint32_t> dstatus;
   CU(dpos.upload(pos, st)); CU(dti.upload(ti, st)); CU(dch.upload(ch, st));
-  CU(dred.alloc(1)); CU(cudaMemsetAsync(dred.p, 0, sizeof(InstRed), st));
+  CU(dred.alloc(1, st)); CU(cudaMemsetAsync(dred.p, 0, sizeof(InstRed), st));
   StepParams p{};
   std::vector<StepParams> pv{p};
   CU(dprm.upload(pv, st));
-  CU(dstatus.alloc(1)); CU(cudaMemsetAsync(dstatus.p, 0, 4, st));
+  CU(dstatus.alloc(1, st)); CU(cudaMemsetAsync(dstatus.p, 0, 4, st));
   BatchDev d{};
   d.pos = dpos.p; d.tri_idx = dti.p; d.tri_chunks = dch.p; d.red = dred.p; d.prm = dprm.p; d.status = dstatus.p;
   SelfContactDev S;
@@ -1241,9 +1338,10 @@ vistio_status broadphase_pairs_impl(vistio_ctx* ctx, uint32_t nv, const float* p
   CU(cudaMemcpyAsync(&total, S.npairs, 4, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   if (total > S.pair_cap) {  // grow and recount
-    cudaFree(S.pairs);
+    cudaFreeAsync(S.pairs, st);
+    S.pairs = nullptr;
     S.pair_cap = total;
-    CU(cudaMalloc(&S.pairs, uint64_t(total) * sizeof(uint2)));
+    CU(cudaMallocAsync(reinterpret_cast<void**>(&S.pairs), uint64_t(total) * sizeof(uint2), st));
   }
   k_self_write<<<uint32_t(ch.size()), 256, 0, st>>>(d, S.view());
   CU(cudaGetLastError());
@@ -1298,7 +1396,7 @@ vistio_status ccd_hits_impl(vistio_ctx* ctx, uint32_t nv, const float* p0, const
   std::vector<uint32_t> tv(tris, tris + 3ull * nt), pv(pairs, pairs + 2 * npairs);
   DevBuf<float> d0, d1; DevBuf<uint32_t> dt, dp; DevBuf<uint2> dh; DevBuf<double> dtoi;
   CU(d0.upload(a, st)); CU(d1.upload(b, st)); CU(dt.upload(tv, st)); CU(dp.upload(pv, st));
-  CU(dh.alloc(6 * std::max<uint64_t>(npairs, 1))); CU(dtoi.alloc(6 * std::max<uint64_t>(npairs, 1)));
+  CU(dh.alloc(6 * std::max<uint64_t>(npairs, 1), st)); CU(dtoi.alloc(6 * std::max<uint64_t>(npairs, 1), st));
   if (npairs) k_ccd_hits<<<uint32_t((npairs + 127) / 128), 128, 0, st>>>(d0.p, d1.p, dt.p, dp.p, npairs, dh.p, dtoi.p);
   CU(cudaGetLastError());
   std::vector<uint2> hh(6 * npairs);
