@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--no-baselines", action="store_true", help="skip the CPU and plain-GPU side measurements")
+    ap.add_argument("--serve-seconds", type=float, default=1.0,
+                    help="arrival window of the served-stream measurement (0 skips it)")
     ap.add_argument("--refine", type=int, default=None,
                     help="FP64 refinement sweeps of the global solve (default: the solver's default)")
     return ap.parse_args()
@@ -174,6 +176,61 @@ def reference_arm(args):
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference is Rust (no toolchain here): its CPU path is timed through the oracle restatement"}
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------- served stream
+def served_stream(window_s, rate=200.0, seed=20261203, threads=None):
+    """The served drape stream: Poisson arrivals at `rate` req/s during
+    `window_s` seconds, half sphere drapes (the sphere-drape geometry at the
+    drawn side, IPC d_hat 1e-3, kappa 1e4, AL <= 5, 15 iterations) and half
+    hanging sheets (10 iterations); grid side log-uniform in [20, 192],
+    materials as in the batched workload, 300 steps each, 120 GB admission
+    budget. Latency runs from a request's arrival to its completion."""
+    from vistio_b200 import api, scenarios
+    rng = np.random.default_rng(seed)
+    t, arrivals = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= window_s:
+            break
+        side = int(round(math.exp(rng.uniform(math.log(20), math.log(192)))))
+        arrivals.append(dict(t=t, sphere=bool(rng.random() < 0.5), side=side,
+                             stretch=float(math.exp(rng.uniform(math.log(2e2), math.log(5e3)))),
+                             bending=float(math.exp(rng.uniform(math.log(1e-5), math.log(1e-3)))),
+                             density=float(rng.uniform(0.08, 0.30) * 1000.0)))
+    sphere = api.Contact(has_ground=True, ground_height=-0.3, has_sphere=True, sphere_center=(0.0, 0.0, 0.0),
+                         sphere_radius=0.3, kappa=1e4)
+    cfg_s = api.drape_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=1e-3, barrier_kappa=1e4)
+    cfg_p = api.drape_config(max_iterations=ITERS)
+    srv = api.Server(hbm_budget_bytes=120 << 30, max_cohort=64, setup_threads=threads or (os.cpu_count() or 4),
+                     steps_per_slice=10, cache_bytes=2 << 30)
+    t0 = time.perf_counter()
+    k = 0
+    while k < len(arrivals):
+        now = time.perf_counter() - t0
+        while k < len(arrivals) and arrivals[k]["t"] <= now:
+            a = arrivals[k]
+            setup = api.SetupDesc(stiffness=a["stretch"], bend_stiffness=a["bending"], density_gsm=a["density"])
+            if a["sphere"]:
+                m = scenarios.sphere_drape(side=a["side"], length=1.5, height=0.5)
+                srv.submit(m, cfg_s, setup, 300, DT, contact=sphere, ipc=True)
+            else:
+                m = scenarios.hanging_sheet(a["side"], 1.0)
+                srv.submit(m, cfg_p, setup, 300, DT, pinned=m.pinned)
+            k += 1
+        srv.tick()
+        time.sleep(0.0005)
+    srv.drain(3600)
+    st = srv.stats()
+    srv.close()
+    return {"window_s": window_s, "rate_per_s": rate, "requests": len(arrivals),
+            "sphere_requests": sum(a["sphere"] for a in arrivals),
+            "completed": st["completed"], "failed": st["failed"],
+            "throughput_instance_steps_per_s": st["throughput"],
+            "latency_s": {"p50": st["p50_latency_s"], "p99": st["p99_latency_s"], "mean": st["mean_latency_s"]},
+            "max_cohorts_active": st["max_cohorts_active"], "peak_device_bytes": st["max_bytes_in_use"],
+            "setup_cache": {"hits": st["cache_hits"], "misses": st["cache_misses"]},
+            "how": "Poisson arrivals at the stated rate during the window, then drained; each request 300 steps"}
 
 
 # ------------------------------------------------------------------- our arm
@@ -405,6 +462,8 @@ def main():
         out["cpu_baseline"] = {"value": units / secs, "unit": UNIT, "cores": 1, "kind": "port",
                                "sample": f"one instance of each of the {len(sample)} topologies x {cpu_steps} steps "
                                          f"({secs:.1f} s); each topology is 1/8 of the workload"}
+        if args.serve_seconds > 0:
+            out["serving"] = served_stream(args.serve_seconds)
         # accuracy of the measured run: the metric is quoted at <= 1e-4 m against FP64
         out["error_vs_fp64"] = fp64_error(specs, order, batch, args.warmup + args.steps + e2e_steps,
                                           os.cpu_count() or 1)
