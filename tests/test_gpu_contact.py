@@ -63,6 +63,22 @@ def test_broadphase_pairs_bit_exact(gap, margin):
     assert fset <= set(map(tuple, ref))
 
 
+def test_broadphase_pairs_independent_of_triangle_order():
+    """The LBVH sorts triangles by the Morton code of their centroids, so a
+    mesh stored in a random triangle order gives the same complete pair set
+    (bit-exact against the oracle on the permuted mesh)."""
+    pos, tris = folded_ribbon(gap=0.004)
+    perm = np.random.default_rng(7).permutation(len(tris))
+    shuffled = np.ascontiguousarray(tris[perm])
+    ref = O.tri_pairs(pos, shuffled, 7.5e-4, mode=0)
+    got = api.broadphase_pairs(pos, shuffled, 7.5e-4)
+    assert np.array_equal(got, ref)
+    # and, mapped back to the original triangle ids, the unshuffled set
+    back = np.sort(perm[got], axis=1)
+    back = back[np.lexsort((back[:, 1], back[:, 0]))]
+    assert np.array_equal(back, O.tri_pairs(pos, tris, 7.5e-4, mode=0))
+
+
 def test_broadphase_empty_and_degenerate():
     pos = np.zeros((3, 3), np.float32)
     tris = np.array([[0, 1, 2]], np.uint32)

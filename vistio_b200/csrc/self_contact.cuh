@@ -49,6 +49,17 @@ struct SelfContactView {
   uint32_t* adj_ptr;   // 1-ring exclusion lists (sorted, include the vertex itself)
   uint32_t* adj;
   uint32_t scan_blocks;
+  // LBVH leaf order: triangles sorted by (garment, Morton code of the
+  // centroid). leaf_tri[tbase + i] is the global triangle of leaf i (the last
+  // sort buffer); null keeps mesh order.
+  uint32_t* leaf_tri;
+  uint64_t* keys;        // sort keys, ping-pong pair with keys_alt
+  uint64_t* keys_alt;
+  uint32_t* order;       // sorted triangle ids, ping-pong pair with order_alt
+  uint32_t* order_alt;
+  uint32_t* sort_hist;   // 256 digit counts per sort block, then their offsets
+  uint32_t* sort_sums;   // scan block sums of sort_hist (+1: the total)
+  uint32_t sort_blocks, sort_scan_blocks, sort_passes;
 };
 
 // Host-side owner of those buffers (never passed to a kernel). They are
@@ -64,15 +75,129 @@ struct SelfContactDev : SelfContactView {
     for (void* q : {static_cast<void*>(inst), static_cast<void*>(tri_inst), static_cast<void*>(box_min),
                     static_cast<void*>(box_max), static_cast<void*>(cnt), static_cast<void*>(block_sums),
                     static_cast<void*>(pairs), static_cast<void*>(npairs), static_cast<void*>(adj_ptr),
-                    static_cast<void*>(adj)})
+                    static_cast<void*>(adj), static_cast<void*>(keys), static_cast<void*>(keys_alt),
+                    static_cast<void*>(order), static_cast<void*>(order_alt), static_cast<void*>(sort_hist),
+                    static_cast<void*>(sort_sums)})
       if (q) cudaFreeAsync(q, stream);
     inst = nullptr; tri_inst = nullptr; box_min = box_max = nullptr; cnt = block_sums = nullptr;
     pairs = nullptr; npairs = nullptr; adj_ptr = adj = nullptr; ready = false;
+    keys = keys_alt = nullptr; order = order_alt = leaf_tri = sort_hist = sort_sums = nullptr;
   }
   ~SelfContactDev() { release(); }
 };
 
 constexpr int kScanBlock = 1024;
+constexpr uint32_t kSortTile = 2048;  // keys per radix-sort block (256 threads x 8)
+
+// ------------------------------------------------------------------ LBVH
+// 30-bit Morton code: 10 bits per axis interleaved (x in the lowest bit).
+__device__ __forceinline__ uint32_t morton_spread10(uint32_t v) {
+  v &= 1023u;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+// Sort keys of one garment per block: its triangles' centroids, quantized to
+// 10 bits per axis within the garment's centroid bounds, as a Morton code
+// below the garment index (so each garment stays in its own range).
+__global__ void __launch_bounds__(1024) k_self_keys(BatchDev B, SelfContactView S) {
+  const SelfInst I = S.inst[blockIdx.x];
+  __shared__ float red[6][32];
+  float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+  auto centroid = [&](uint32_t i) {
+    const uint4 id = B.tri_idx[I.tbase + i];
+    const float4 a = B.pos[id.x], b = B.pos[id.y], c = B.pos[id.z];
+    return make_float3((a.x + b.x + c.x) * (1.f / 3.f), (a.y + b.y + c.y) * (1.f / 3.f), (a.z + b.z + c.z) * (1.f / 3.f));
+  };
+  for (uint32_t i = threadIdx.x; i < I.nt; i += blockDim.x) {
+    const float3 c = centroid(i);
+    lo[0] = fminf(lo[0], c.x); lo[1] = fminf(lo[1], c.y); lo[2] = fminf(lo[2], c.z);
+    hi[0] = fmaxf(hi[0], c.x); hi[1] = fmaxf(hi[1], c.y); hi[2] = fmaxf(hi[2], c.z);
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int k = 0; k < 3; ++k) { red[k][w] = lo[k]; red[3 + k][w] = hi[k]; }
+  __syncthreads();
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = red[k][0];
+    hi[k] = red[3 + k][0];
+    for (uint32_t q = 1; q < (blockDim.x >> 5); ++q) { lo[k] = fminf(lo[k], red[k][q]); hi[k] = fmaxf(hi[k], red[3 + k][q]); }
+  }
+  float sc[3];
+  for (int k = 0; k < 3; ++k) sc[k] = hi[k] > lo[k] ? 1023.f / (hi[k] - lo[k]) : 0.f;
+  for (uint32_t i = threadIdx.x; i < I.nt; i += blockDim.x) {
+    const float3 c = centroid(i);
+    const uint32_t qx = uint32_t(fminf(fmaxf((c.x - lo[0]) * sc[0], 0.f), 1023.f));
+    const uint32_t qy = uint32_t(fminf(fmaxf((c.y - lo[1]) * sc[1], 0.f), 1023.f));
+    const uint32_t qz = uint32_t(fminf(fmaxf((c.z - lo[2]) * sc[2], 0.f), 1023.f));
+    const uint32_t code = morton_spread10(qx) | (morton_spread10(qy) << 1) | (morton_spread10(qz) << 2);
+    S.keys[I.tbase + i] = (uint64_t(blockIdx.x) << 30) | code;
+    S.order[I.tbase + i] = I.tbase + i;
+  }
+}
+
+// Stable LSD radix sort of (key, value) pairs, 8-bit digits, over all
+// triangles of the batch: per pass a digit histogram per block of kSortTile
+// keys (digit-major), an exclusive scan of those counts, and a stable scatter
+// (ranks within a block from warp match masks and per-warp digit counts).
+__global__ void __launch_bounds__(256) k_rs_hist(const uint64_t* __restrict__ keys, uint32_t n, uint32_t shift,
+                                                 uint32_t* __restrict__ hist, uint32_t nblocks) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t b0 = blockIdx.x * kSortTile, b1 = min(n, b0 + kSortTile);
+  for (uint32_t i = b0 + threadIdx.x; i < b1; i += 256) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+  __syncthreads();
+  hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                    uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                    uint32_t n, uint32_t shift, const uint32_t* __restrict__ offs,
+                                                    uint32_t nblocks) {
+  __shared__ uint32_t wcnt[8][256];
+  __shared__ uint32_t woff[8][256];
+  __shared__ uint32_t run[256];
+  const uint32_t t = threadIdx.x, w = t >> 5, lane = t & 31;
+  for (uint32_t q = 0; q < 8; ++q) wcnt[q][t] = 0;
+  run[t] = offs[t * nblocks + blockIdx.x];
+  __syncthreads();
+  const uint32_t b0 = blockIdx.x * kSortTile;
+  for (uint32_t c0 = b0; c0 < min(n, b0 + kSortTile); c0 += 256) {
+    const uint32_t i = c0 + t;
+    const bool valid = i < n;
+    const uint64_t key = valid ? kin[i] : 0ull;
+    const uint32_t d = valid ? uint32_t((key >> shift) & 255u) : 256u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    if (valid && rank == 0) wcnt[w][d] = __popc(peers);
+    __syncthreads();
+    {  // thread t: digit t's offsets for each warp of this chunk
+      uint32_t r = run[t];
+      for (uint32_t q = 0; q < 8; ++q) {
+        woff[q][t] = r;
+        r += wcnt[q][t];
+        wcnt[q][t] = 0;
+      }
+      run[t] = r;
+    }
+    __syncthreads();
+    if (valid) {
+      const uint32_t dst = woff[w][d] + rank;
+      kout[dst] = key;
+      vout[dst] = vin[i];
+    }
+    __syncthreads();
+  }
+}
 
 // ---------------------------------------------------------------- trees
 // Leaf boxes (bvh.rs:29-43, inflated by the margin) and the level-by-level
@@ -84,7 +209,8 @@ __global__ void __launch_bounds__(1024) k_self_boxes(BatchDev B, SelfContactView
   float4* mn = S.box_min + I.box_base;
   float4* mx = S.box_max + I.box_base;
   for (uint32_t i = threadIdx.x; i < I.nt; i += blockDim.x) {
-    uint4 id = B.tri_idx[I.tbase + i];
+    const uint32_t tri = S.leaf_tri ? S.leaf_tri[I.tbase + i] : I.tbase + i;
+    uint4 id = B.tri_idx[tri];
     float4 a = B.pos[id.x], b = B.pos[id.y], c = B.pos[id.z];
     mn[i] = make_float4(fminf(fminf(a.x, b.x), c.x) - margin, fminf(fminf(a.y, b.y), c.y) - margin,
                         fminf(fminf(a.z, b.z), c.z) - margin, 0.f);
@@ -139,7 +265,14 @@ __device__ void self_traverse(const SelfContactView& S, const SelfInst& I, uint3
     if (l == 0) {
       if (MODE == 1) {
         uint32_t slot = base + found;
-        if (slot < cap) out[slot] = make_uint2(I.tbase + i, I.tbase + k);
+        if (slot < cap) {
+          uint32_t a = I.tbase + i, b = I.tbase + k;
+          if (S.leaf_tri) {
+            a = S.leaf_tri[a];
+            b = S.leaf_tri[b];
+          }
+          out[slot] = make_uint2(min(a, b), max(a, b));
+        }
       }
       ++found;
       continue;
@@ -580,12 +713,35 @@ __global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactView S)
 }
 
 // ---------------------------------------------------------------- host side
-inline uint32_t self_detect_launches() { return 7; }
 inline uint32_t self_ccd_launches() { return 1; }
 
-inline void launch_self_detect(const BatchDev& d, const SelfContactView& S, uint32_t n_vtx_chunks,
-                               uint32_t n_tri_chunks, int mode, cudaStream_t st) {
+// The LBVH leaf order: Morton keys, then sort_passes radix passes (5 launches each).
+inline uint32_t launch_self_sort(const BatchDev& d, const SelfContactView& S, cudaStream_t st) {
+  if (!S.leaf_tri) return 0;
+  const uint32_t n = uint32_t(S.T);
+  k_self_keys<<<S.ninst, 1024, 0, st>>>(d, S);
+  uint64_t* k0 = S.keys;
+  uint64_t* k1 = S.keys_alt;
+  uint32_t* v0 = S.order;
+  uint32_t* v1 = S.order_alt;
+  const uint32_t L = 256u * S.sort_blocks;
+  for (uint32_t p = 0; p < S.sort_passes; ++p) {
+    k_rs_hist<<<S.sort_blocks, 256, 0, st>>>(k0, n, 8 * p, S.sort_hist, S.sort_blocks);
+    k_scan_local<<<S.sort_scan_blocks, kScanBlock, 0, st>>>(S.sort_hist, L, S.sort_sums);
+    k_scan_sums<<<1, kScanBlock, 0, st>>>(S.sort_sums, S.sort_scan_blocks, S.sort_sums + S.sort_scan_blocks);
+    k_scan_add<<<S.sort_scan_blocks, kScanBlock, 0, st>>>(S.sort_hist, L, S.sort_sums);
+    k_rs_scatter<<<S.sort_blocks, 256, 0, st>>>(k0, v0, k1, v1, n, 8 * p, S.sort_hist, S.sort_blocks);
+    std::swap(k0, k1);
+    std::swap(v0, v1);
+  }
+  return 1 + 5 * S.sort_passes;
+}
+
+// Returns the kernels launched.
+inline uint32_t launch_self_detect(const BatchDev& d, const SelfContactView& S, uint32_t n_vtx_chunks,
+                                   uint32_t n_tri_chunks, int mode, cudaStream_t st) {
   k_clear_grad<<<n_vtx_chunks, 256, 0, st>>>(d);
+  const uint32_t ns = launch_self_sort(d, S, st);
   k_self_boxes<<<S.ninst, 1024, 0, st>>>(d, S, -1.f);  // margin: StepParams::thickness
   k_self_count<<<n_tri_chunks, 256, 0, st>>>(d, S);
   k_scan_local<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);
@@ -593,6 +749,7 @@ inline void launch_self_detect(const BatchDev& d, const SelfContactView& S, uint
   k_scan_add<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);
   k_self_write<<<n_tri_chunks, 256, 0, st>>>(d, S);
   k_self_grad<<<4 * 148, 256, 0, st>>>(d, S, mode);
+  return 8 + ns;
 }
 
 inline void launch_self_ccd(const BatchDev& d, const SelfContactView& S, cudaStream_t st) {

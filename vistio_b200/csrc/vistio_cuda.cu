@@ -525,7 +525,7 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
   } else {
     for (uint32_t al = 0; al < b->cfg.al_max_iterations; ++al) {
       k_al_begin<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
-      if (self) { launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 0, st); L += self_detect_launches(); }
+      if (self) L += launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 0, st);
       k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 0);
       for (uint32_t it = 0; it < iters; ++it) {
         // With backtracking (alpha < 1) part of each sweep's error stays in x:
@@ -535,7 +535,7 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
         k_ccd<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
         k_ipc_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
       }
-      if (self) { launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 1, st); L += self_detect_launches(); }
+      if (self) L += launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 1, st);
       k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 1);
       k_al_end<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
       k_al_finish<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
@@ -1274,6 +1274,22 @@ vistio_status self_build(SelfContactDev& S, const std::vector<std::pair<const ui
   SA(S.npairs, 8);
   SA(S.adj_ptr, (V + 1) * 4);
   SA(S.adj, std::max<size_t>(adj.size(), 1) * 4);
+  // LBVH sort buffers: keys carry the garment index above a 30-bit Morton code
+  {
+    const uint64_t Tn = std::max<uint64_t>(T, 1);
+    uint32_t gbits = 0;
+    while ((1ull << gbits) < n) ++gbits;
+    S.sort_passes = (30 + gbits + 7) / 8;
+    S.sort_blocks = uint32_t((Tn + kSortTile - 1) / kSortTile);
+    S.sort_scan_blocks = uint32_t((256ull * S.sort_blocks + kScanBlock - 1) / kScanBlock);
+    SA(S.keys, Tn * 8);
+    SA(S.keys_alt, Tn * 8);
+    SA(S.order, Tn * 4);
+    SA(S.order_alt, Tn * 4);
+    SA(S.sort_hist, 256ull * S.sort_blocks * 4);
+    SA(S.sort_sums, (S.sort_scan_blocks + 1ull) * 4);
+    S.leaf_tri = S.sort_passes % 2 == 0 ? S.order : S.order_alt;  // where the last pass leaves the order
+  }
 #undef SA
   if ((e = cudaMemcpyAsync(S.inst, si.data(), n * sizeof(SelfInst), cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
   if (T && (e = cudaMemcpyAsync(S.tri_inst, tri_inst.data(), T * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
@@ -1329,6 +1345,7 @@ vistio_status broadphase_pairs_impl(vistio_ctx* ctx, uint32_t nv, const float* p
   std::vector<uint32_t> nvs{nv}, vb{0};
   vistio_status r = self_build(S, tl, nvs, vb, nt, st, err);
   if (r != VISTIO_OK) return r;
+  launch_self_sort(d, S.view(), st);
   k_self_boxes<<<1, 1024, 0, st>>>(d, S.view(), margin);
   k_self_count<<<uint32_t(ch.size()), 256, 0, st>>>(d, S.view());
   k_scan_local<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, nt, S.block_sums);
