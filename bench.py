@@ -56,6 +56,23 @@ def workload(n_instances, rank=0):
     return scenarios.batched_specs(n_instances=n_instances, seed=scenarios.SEED + rank)
 
 
+def max_over_ranks(x, world, device):
+    """The largest of every rank's x (a device-timed duration): the job's time."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(instances_per_rank, world, steps, total_ms):
+    """Whole-job instance-steps per second: every rank advances its own
+    instances (weak scaling), timed by the slowest rank."""
+    return instances_per_rank * world * steps / (total_ms / 1e3)
+
+
 def config_block(n, gpus, refine=None):
     return {"workload": f"batched hanging sheets: {n} instances/GPU, grid side 16-128 (8 topologies), "
                         f"{ITERS} PD iterations, dt=1/60 s",
@@ -323,12 +340,7 @@ def main():
         if world > 1:
             dist.barrier(device_ids=[local])
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    device = f"cuda:{local}"
 
     for _ in range(args.warmup):
         batch.step(DT, 1)
@@ -348,8 +360,8 @@ def main():
         torch.cuda.synchronize()
     barrier()
     step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
-    total_ms = max_over_ranks(evs[0].elapsed_time(evs[-1]))
-    value = len(specs) * world * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(evs[0].elapsed_time(evs[-1]), world, device)
+    value = job_value(len(specs), world, args.steps, total_ms)
     clocks = clk.summary()
 
     # ---- end to end: positions from pinned host memory in, positions back out, each step
@@ -369,8 +381,8 @@ def main():
         e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = len(specs) * world * e2e_steps / (e2e_ms / 1e3)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, device)
+    e2e_value = job_value(len(specs), world, e2e_steps, e2e_ms)
 
     # ---- per-kernel timing of one plain iteration's phases (live, CUDA events)
     phases = ["membrane", "bending", "gather", "solve"]
