@@ -488,6 +488,26 @@ __device__ __forceinline__ const float* stage(Team& tm, const float* __restrict_
   return tm.buf + (a - lo) / 4;
 }
 
+// The same copy in two halves, so that other work overlaps it: stage_issue
+// starts the copy (after the team's previous readers of the buffer are done),
+// stage_wait waits for it (bounded) and returns where src[0] landed.
+__device__ __forceinline__ void stage_issue(Team& tm, const float* __restrict__ src, uint32_t n) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uintptr_t lo = a & ~uintptr_t(15);
+  const uintptr_t hi = (a + uintptr_t(n) * 4 + 15) & ~uintptr_t(15);
+  tm.sync();
+  if (tm.rank == 0) bulk_g2s(tm.buf, reinterpret_cast<const void*>(lo), uint32_t(hi - lo), tm.bar);
+}
+__device__ __forceinline__ const float* stage_wait(Team& tm, const float* __restrict__ src, uint32_t* status) {
+  const bool ok = mbar_wait(tm.bar, tm.parity);
+  tm.parity ^= 1u;
+  if (!ok) {
+    atomicOr(status, 4u);
+    *tm.abort = 1u;
+  }
+  return tm.buf + (reinterpret_cast<uintptr_t>(src) & 15) / 4;
+}
+
 // Pull for the rows of supernode S: t = r - sum of the updates U that its
 // descendants pushed (lanes / threads over columns).
 __device__ __forceinline__ void sn_pull(const BatchDev& B, const Team& tm, const SnDev& S, const float4* Y) {
@@ -532,6 +552,19 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const Sn
   float4* Y = B.Y + S.vbase;
   const float* D = B.vals + S.d_off;
   const float* Pp = B.vals + S.p_off;
+  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * s;  // [D | P] is one contiguous region
+  if (whole + 8 <= tm.cap) {
+    // the whole supernode in one copy, in flight while the pull gathers
+    stage_issue(tm, D, whole);
+    sn_pull(B, tm, S, Y);
+    const float* Ds = stage_wait(tm, D, B.status);
+    tm.sync();
+    sn_diag_fwd_smem(tm, S, Ds, Y);
+    tm.sync();
+    if (m) sn_push_rows(B, tm, S, Ds + (S.p_off - S.d_off), 0, m);
+    tm.sync();
+    return;
+  }
   sn_pull(B, tm, S, Y);
   if (s * s + 8 <= tm.cap) {
     const float* Ds = stage(tm, D, s * s, B.status);
@@ -615,6 +648,39 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
   const float* D = B.vals + S.d_off;
   const float* Pp = B.vals + S.p_off;
   const uint32_t* Rr = B.rows + S.rows_off;
+  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * s;
+  if (whole + 8 <= tm.cap) {
+    // the whole supernode in one copy, in flight while y and the first
+    // chunk of x[R] are gathered; columns in at most two rounds of the team
+    // width (warp items have s <= 42, block items s <= 256 <= the block width)
+    stage_issue(tm, D, whole);
+    for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
+    const uint32_t width = team_width(tm, s), parts = tm.size / width;
+    const uint32_t cl = tm.rank % width, part = tm.rank / width;
+    float4 sum0 = make_float4(0.f, 0.f, 0.f, 0.f), sum1 = sum0;
+    const float* Ds = nullptr;
+    for (uint32_t j0 = 0; j0 < m; j0 += tm.xcap) {
+      const uint32_t nr = min(tm.xcap, m - j0);
+      tm.sync();
+      for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = Y[Rr[j0 + j]];
+      if (!Ds) Ds = stage_wait(tm, D, B.status);
+      tm.sync();
+      if (part < parts) {
+        const float* P0 = Ds + (S.p_off - S.d_off) + size_t(j0) * s;
+        if (cl < s)
+          for (uint32_t j = part; j < nr; j += parts) f4_fma(sum0, P0[j * s + cl], tm.xg[j]);
+        if (width + cl < s)
+          for (uint32_t j = part; j < nr; j += parts) f4_fma(sum1, P0[j * s + width + cl], tm.xg[j]);
+      }
+    }
+    if (!Ds) Ds = stage_wait(tm, D, B.status);
+    tm.sync();
+    team_column_sum(tm, sum0, width, parts, 0, s, tm.v1, tm.v0, true);
+    if (width < s) team_column_sum(tm, sum1, width, parts, width, s, tm.v1, tm.v0, true);
+    sn_diag_bwd_smem(tm, S, Ds, Y);
+    tm.sync();
+    return;
+  }
   for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
   const uint32_t width = team_width(tm, s);
   const uint32_t parts = tm.size / width;
