@@ -387,14 +387,17 @@ __device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
 // kWarpFloats floats and kWarpVec float4 vector slots; a narrow level uses
 // all of them as one block-wide buffer.
 constexpr uint32_t kSolveWarps = 8;
-constexpr uint32_t kWarpFloats = 1792;
-constexpr uint32_t kWarpVec = 48;
+// Sized so that four 256-thread blocks fit an SM (56 KB each): the sweeps
+// are bound by the latency of global loads, so warps in flight matter more
+// than larger staging buffers.
+constexpr uint32_t kWarpFloats = 1280;
+constexpr uint32_t kWarpVec = 40;
 constexpr uint32_t kSolveSmem = kSolveWarps * (kWarpFloats * 4 + 3 * kWarpVec * 16);
 constexpr uint32_t kMaxSupernode = 256;  // enforced by the host set-up
 // A supernode is a warp item when its vectors and diagonal block fit a warp's
 // slots and its block is small; larger ones get a whole block.
 __host__ __device__ constexpr bool warp_item(uint32_t s, uint32_t m) {
-  return s <= 42 && uint64_t(s) * (s + m) <= 6144;
+  return s <= kWarpVec && uint64_t(s) * (s + m) <= 6144;
 }
 
 // ------------------------------------------------ TMA bulk staging
@@ -652,7 +655,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
   if (whole + 8 <= tm.cap) {
     // the whole supernode in one copy, in flight while y and the first
     // chunk of x[R] are gathered; columns in at most two rounds of the team
-    // width (warp items have s <= 42, block items s <= 256 <= the block width)
+    // width (warp items have s <= kWarpVec, block items s <= 256 <= the block width)
     stage_issue(tm, D, whole);
     for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
     const uint32_t width = team_width(tm, s), parts = tm.size / width;
@@ -711,12 +714,16 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
     for (uint32_t c0 = 0; c0 < s; c0 += cw) {
       uint32_t c1 = min(s, c0 + cw);
       const float* Dc = stage(tm, D + uint64_t(c0) * s, (c1 - c0) * s, B.status);
+      // a chunk can be wider than the team: columns in rounds of the team width
       const uint32_t w = team_width(tm, c1 - c0), np = tm.size / w;
-      const uint32_t ccl = tm.rank % w, pp = tm.rank / w, cc = c0 + ccl;
-      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (cc < c1 && pp < np)
-        for (uint32_t r = cc + pp; r < s; r += np) f4_fma(acc, Dc[(cc - c0) * s + r], tm.v0[r]);
-      team_column_sum(tm, acc, w, np, c0, c1, nullptr, Y + f, false);
+      const uint32_t ccl = tm.rank % w, pp = tm.rank / w;
+      for (uint32_t cb = c0; cb < c1; cb += w) {
+        const uint32_t cc = cb + ccl;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (cc < c1 && pp < np)
+          for (uint32_t r = cc + pp; r < s; r += np) f4_fma(acc, Dc[(cc - c0) * s + r], tm.v0[r]);
+        team_column_sum(tm, acc, w, np, cb, c1, nullptr, Y + f, false);
+      }
     }
   }
   tm.sync();
@@ -835,11 +842,11 @@ __device__ __forceinline__ SweepTeams make_teams(float4* smem4, uint64_t* s_bar,
   t.wt = Team{lane, 32, fbuf + warp * kWarpFloats, kWarpFloats, vbuf + warp * 3 * kWarpVec,
               vbuf + warp * 3 * kWarpVec + kWarpVec, vbuf + warp * 3 * kWarpVec + 2 * kWarpVec, kWarpVec, kWarpVec,
               false, &s_bar[warp], 0u, s_abort};
-  // block team: all warps' buffers; the 1152 vector slots split 448 / 448 / 256
-  // (supernodes have at most kMaxSupernode <= 448 columns; xg doubles as the
-  // NT-entry reduction buffer).
-  static_assert(3 * kWarpVec * kSolveWarps >= 448 + 448 + NT, "block-team vector slots");
-  t.bt = Team{tid, NT, fbuf, NW * kWarpFloats, vbuf, vbuf + 448, vbuf + 896, 448, NT, true, &s_bar[NW], 0u, s_abort};
+  // block team: all warps' buffers; the vector slots split kMaxSupernode /
+  // kMaxSupernode / NT (xg doubles as the NT-entry reduction buffer).
+  static_assert(3 * kWarpVec * kSolveWarps >= 2 * kMaxSupernode + NT, "block-team vector slots");
+  t.bt = Team{tid, NT, fbuf, NW * kWarpFloats, vbuf, vbuf + kMaxSupernode, vbuf + 2 * kMaxSupernode, kMaxSupernode, NT,
+              true, &s_bar[NW], 0u, s_abort};
   return t;
 }
 
