@@ -387,12 +387,15 @@ __device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
 // kWarpFloats floats and kWarpVec float4 vector slots; a narrow level uses
 // all of them as one block-wide buffer.
 constexpr uint32_t kSolveWarps = 8;
-// Sized so that four 256-thread blocks fit an SM (56 KB each): the sweeps
+// Sized so that five 256-thread blocks fit an SM (45 KB each): the sweeps
 // are bound by the latency of global loads, so warps in flight matter more
 // than larger staging buffers.
-constexpr uint32_t kWarpFloats = 1280;
-constexpr uint32_t kWarpVec = 40;
+constexpr uint32_t kWarpFloats = 1024;
+constexpr uint32_t kWarpVec = 32;
 constexpr uint32_t kSolveSmem = kSolveWarps * (kWarpFloats * 4 + 3 * kWarpVec * 16);
+// Blocks per SM the sweep kernels are compiled for (registers of a 256-thread
+// block at most 65536 / 5): shared memory admits five.
+constexpr int kSolveMinBlocks = 5;
 constexpr uint32_t kMaxSupernode = 256;  // enforced by the host set-up
 // A supernode is a warp item when its vectors and diagonal block fit a warp's
 // slots and its block is small; larger ones get a whole block.
@@ -857,7 +860,7 @@ __device__ __forceinline__ SweepTeams make_teams(float4* smem4, uint64_t* s_bar,
 // per warp. Supernodes of a level are independent; levels are ordered by
 // kernel boundaries.
 template <int DIR>
-__global__ void __launch_bounds__(32 * kSolveWarps) k_level(BatchDev B, uint32_t off, uint32_t nblock, uint32_t nwarp) {
+__global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_level(BatchDev B, uint32_t off, uint32_t nblock, uint32_t nwarp) {
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
   __shared__ uint32_t s_abort;
@@ -880,7 +883,7 @@ __global__ void __launch_bounds__(32 * kSolveWarps) k_level(BatchDev B, uint32_t
 
 // Bottom subtrees of every instance, one per warp.
 template <int DIR>
-__global__ void __launch_bounds__(32 * kSolveWarps) k_subtree(BatchDev B, uint32_t nitems) {
+__global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_subtree(BatchDev B, uint32_t nitems) {
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
   __shared__ uint32_t s_abort;
