@@ -33,7 +33,8 @@ struct InstDev {
 
 // One supernode in HBM: one contiguous, 16-byte aligned region holding
 //   D  inv(L_kk), s x s column-major (Linv[c][c2] at c2*s + c), then
-//   P  the m x s panel below the diagonal block, row-major (P[j][c] at j*s + c).
+//   P  the m x s panel below the diagonal block, row-major (P[j][c] at j*s + c),
+//      followed by its m row indices (u32 bits; the same as rows[rows_off..]).
 // Both sweeps stage it through shared memory in row chunks.
 struct SnDev {
   uint32_t first;    // first column (instance-local permuted row)
@@ -558,7 +559,7 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const Sn
   float4* Y = B.Y + S.vbase;
   const float* D = B.vals + S.d_off;
   const float* Pp = B.vals + S.p_off;
-  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * s;  // [D | P] is one contiguous region
+  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * s + m;  // [D | P | rows] is one contiguous region
   if (whole + 8 <= tm.cap) {
     // the whole supernode in one copy, in flight while the pull gathers
     stage_issue(tm, D, whole);
@@ -654,7 +655,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
   const float* D = B.vals + S.d_off;
   const float* Pp = B.vals + S.p_off;
   const uint32_t* Rr = B.rows + S.rows_off;
-  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * s;
+  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * s + m;
   if (whole + 8 <= tm.cap) {
     // the whole supernode in one copy, in flight while y and the first
     // chunk of x[R] are gathered; columns in at most two rounds of the team
@@ -744,7 +745,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
 template <int DIR>
 __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint32_t first, uint32_t last) {
   const SnDev F = B.sn[first], Lz = B.sn[last];
-  const uint64_t end = Lz.p_off + ((uint64_t(Lz.nrows) * Lz.ncols + 3) & ~3ull);
+  const uint64_t end = Lz.p_off + ((uint64_t(Lz.nrows) * Lz.ncols + Lz.nrows + 3) & ~3ull);
   const float* src = B.vals + F.d_off;  // 16-byte aligned: d_off is a multiple of 4
   const uint32_t bytes = uint32_t(end - F.d_off) * 4u;
   tm.sync();  // previous readers of the buffer are done
@@ -766,8 +767,8 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
     const SnDev S = B.sn[k];
     const float* Ds = base + (S.d_off - F.d_off);
     const float* Ps = base + (S.p_off - F.d_off);
-    const uint32_t* Rr = B.rows + S.rows_off;
     const uint32_t s = S.ncols, m = S.nrows, f = S.first - c0;
+    const uint32_t* Rr = reinterpret_cast<const uint32_t*>(Ps + m * s);  // staged with the panel
     if (DIR == 0) {
       // t = acc (all descendant updates are in); y = inv(L_kk) t into acc
       for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v0[c] = acc[f + c];

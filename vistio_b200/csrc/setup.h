@@ -30,15 +30,17 @@ struct SetupParams {
 // Largest supernode (columns); the GPU sweeps size their shared-memory vectors for it.
 constexpr uint32_t kMaxSupernodeCols = 256;
 // Bottom subtrees of the supernodal elimination tree whose factor data (in
-// floats, as packed for the GPU: pad4(s*s) + pad4(m*s) per supernode) fits
-// this budget are swept as one unit by one warp.
+// floats, as packed for the GPU: sn_floats per supernode) fits this budget
+// are swept as one unit by one warp.
 constexpr uint32_t kSubtreeFloats = 1024;
 // ... and whose columns (contiguous in postorder) number at most this: the
 // warp keeps the subtree's slice of the vector in shared memory.
 constexpr uint32_t kSubtreeCols = 32;
 constexpr uint32_t kBottomLevel = 0xffffffffu;
+// Floats of one supernode's packed region: inv(L_kk) (s x s), then the panel
+// (m x s) followed by its m row indices, each part padded to 4 floats.
 inline uint64_t sn_floats(uint32_t s, uint32_t m) {
-  return ((uint64_t(s) * s + 3) & ~3ull) + ((uint64_t(m) * s + 3) & ~3ull);
+  return ((uint64_t(s) * s + 3) & ~3ull) + ((uint64_t(m) * s + m + 3) & ~3ull);
 }
 
 // Supernodal factor of P A P^T = L L^T in the layout the GPU sweeps read.

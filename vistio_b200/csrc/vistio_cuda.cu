@@ -188,7 +188,7 @@ float estimate_kappa(const vistio_solver_config& c, const InstanceSetup& I);
 uint64_t instance_device_bytes(const InstanceSetup& I, bool refine, bool self_contact) {
   const Factor& F = I.factor;
   uint64_t vals = 0;
-  for (const Supernode& X : F.sn) vals += pad4(uint64_t(X.ncols) * X.ncols) + pad4(uint64_t(X.nrows) * X.ncols);
+  for (const Supernode& X : F.sn) vals += sn_floats(X.ncols, X.nrows);
   const uint64_t V = I.nv, T = I.nt, H = I.nh, R = F.rows.size();
   uint64_t b = vals * 4 + F.sn.size() * sizeof(SnDev) + R * 4 + F.fwd_sn.size() * 4 + (V + 1) * 4 +
                F.sn.size() * 4 + R * 16;
@@ -229,7 +229,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     d.sn_base = uint32_t(NSN); d.nsn = uint32_t(I.factor.sn.size());
     d.kappa = estimate_kappa(solvers[k]->cfg, I);
     V += I.nv; T += I.nt; H += I.nh; NSN += I.factor.sn.size(); NROWS += I.factor.rows.size();
-    for (const Supernode& X : I.factor.sn) NVALS += pad4(uint64_t(X.ncols) * X.ncols) + pad4(uint64_t(X.nrows) * X.ncols);
+    for (const Supernode& X : I.factor.sn) NVALS += sn_floats(X.ncols, X.nrows);
     NLVL += I.factor.nlevels + 1; NFWD += I.factor.fwd_sn.size();
   }
   if (V >= (1ull << 31) || 3 * T >= (1ull << 30) || 4 * H >= (1ull << 30))
@@ -289,7 +289,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       d.first = X.first; d.ncols = sc; d.nrows = m;
       d.rows_off = uint32_t(rowsb + X.rows_off);
       d.d_off = valsb; valsb += pad4(uint64_t(sc) * sc);
-      d.p_off = valsb; valsb += pad4(uint64_t(m) * sc);
+      d.p_off = valsb; valsb += pad4(uint64_t(m) * sc + m);  // panel, then its row indices
       d.vbase = uint32_t(v0);
       d.inst = k;
       if (X.level != kBottomLevel) (warp_item(sc, m) ? lvl_warp : lvl_block)[X.level].push_back(uint32_t(snb + q));
@@ -297,6 +297,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
       for (uint64_t e = 0; e < uint64_t(m) * sc; ++e) vals[d.p_off + e] = float(Pn[e]);
       for (uint64_t e = 0; e < uint64_t(sc) * sc; ++e) vals[d.d_off + e] = float(Dn[e]);
+      // the panel's row indices (u32 bits), staged with the panel by the sweeps
+      std::memcpy(vals.data() + d.p_off + uint64_t(m) * sc, F.rows.data() + X.rows_off, size_t(m) * 4);
     }
     rows.insert(rows.end(), F.rows.begin(), F.rows.end());
     for (size_t q = 0; q < F.sub_first.size(); ++q)
