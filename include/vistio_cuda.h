@@ -227,6 +227,16 @@ vistio_status vistio_batch_download_positions(vistio_batch* b, float* xyz);
 vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, uint64_t* total_vertices,
                                 uint64_t* total_triangles, uint64_t* total_hinges, uint64_t* factor_bytes,
                                 uint64_t* device_bytes);
+/* Autotuner of the sweeps' level schedule (no counterpart in the reference).
+ * Which top-level supernodes a single warp takes and which a whole block is
+ * decided by a limit on s (s + m); this times the forward and backward sweeps
+ * of this batch's factor for the limits 0, 1024, 2048, 4096, 6144, 12288 and
+ * 2^30 (candidate_ms, 7 entries, may be NULL) and keeps the fastest
+ * (*chosen_limit). The default without tuning is 6144. Captured step graphs
+ * are rebuilt on the next step. Synchronises the batch's stream. */
+vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms);
+/* Sets that limit directly (any value; see vistio_batch_tune). */
+vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit);
 /* Kernel launches in one batch step (graph nodes), for launch accounting. */
 vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* launches);
 /* The stream the batch runs on (cudaStream_t as void*), for event timing. */

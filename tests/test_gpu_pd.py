@@ -226,3 +226,35 @@ def test_long_ribbon_steps_match_fp64(cols):
     e = rel(gpu.state()[0], ref.state()[0])
     print(f"ribbon {cols}x400: 3 steps, rel error {e:.2e}")
     assert e <= 1e-5, e
+
+
+def test_level_schedules_and_autotuner():
+    """Every candidate level schedule of the autotuner (from all top-level
+    supernodes on whole blocks to every narrow one on a single warp) steps a
+    batch of uneven sheets and a long ribbon to within 1e-5 of FP64; the tuner
+    picks one of the candidates and times them all."""
+    dt = 1.0 / 120.0
+    meshes = [(scenarios.hanging_sheet(40, 1.0), 1.0 / 60.0), (scenarios.hanging_sheet(23, 0.6), 1.0 / 60.0),
+              (scenarios.self_fold(30, 400, 0.2, 2.0, lowest=0.5), dt)]
+    cfg = api.drape_config(max_iterations=10)
+    for lim in api.Batch.TUNE_LIMITS:
+        for mesh, h in meshes:
+            setup = api.SetupDesc(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0, matrix_dt=h)
+            s = api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
+            batch = api.Batch([s])
+            batch.set_warp_limit(lim)
+            ref = O.OracleSim(mesh, O.init_params(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0, matrix_dt=h),
+                              O.default_config(max_iterations=10), precision=1)
+            batch.step(h, 2)
+            ref.step(h)
+            ref.step(h)
+            e = rel(batch.state(0)[0], ref.state()[0])
+            assert e <= 1e-5, (lim, mesh.nv, e)
+    solvers = [api.ProjectiveDynamicsSolver().init(scenarios.hanging_sheet(sd, 1.0), cfg,
+                                                   pinned=scenarios.hanging_sheet(sd, 1.0).pinned) for sd in (31, 47, 64)]
+    batch = api.Batch(solvers)
+    t = batch.tune()
+    print(t)
+    assert t["warp_item_limit"] in api.Batch.TUNE_LIMITS
+    assert all(v > 0 for v in t["sweep_ms"].values())
+    batch.step(1.0 / 60.0, 1)

@@ -128,6 +128,8 @@ SIGNATURES = {
     "vistio_batch_launch_phase": (C.c_int, [_vp, C.c_int32]),
     "vistio_batch_phase_bytes": (C.c_int, [_vp, C.c_int32, _u64p]),
     "vistio_diag_wait_timeout": (C.c_int, [_vp, C.c_uint32]),
+    "vistio_batch_tune": (C.c_int, [_vp, _u32p, _fp]),
+    "vistio_batch_set_warp_limit": (C.c_int, [_vp, C.c_uint32]),
     "vistio_solver_clone": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
     "vistio_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
     "vistio_server_destroy": (C.c_int, [_vp]),

@@ -375,6 +375,20 @@ class Batch:
 
     PHASES = {"predict": 0, "membrane": 1, "bending": 2, "gather": 3, "solve": 4, "finalize": 5, "refine": 6}
 
+    TUNE_LIMITS = (0, 1024, 2048, 4096, 6144, 12288, 1 << 30)
+
+    def tune(self) -> dict:
+        """Autotunes the sweeps' level schedule on this batch (vistio_batch_tune):
+        returns the chosen warp-item limit and the sweep time of each candidate."""
+        chosen = C.c_uint32()
+        ms = (C.c_float * 7)()
+        L.check(L.lib().vistio_batch_tune(self.h, C.byref(chosen), ms), self.ctx.h)
+        return {"warp_item_limit": chosen.value,
+                "sweep_ms": {str(lim): float(ms[i]) for i, lim in enumerate(self.TUNE_LIMITS)}}
+
+    def set_warp_limit(self, limit: int):
+        L.check(L.lib().vistio_batch_set_warp_limit(self.h, int(limit)), self.ctx.h)
+
     def launch_phase(self, phase: str):
         L.check(L.lib().vistio_batch_launch_phase(self.h, self.PHASES[phase]), self.ctx.h)
 

@@ -400,8 +400,10 @@ constexpr int kSolveMinBlocks = 5;
 constexpr uint32_t kMaxSupernode = 256;  // enforced by the host set-up
 // A supernode is a warp item when its vectors and diagonal block fit a warp's
 // slots and its block is small; larger ones get a whole block.
-__host__ __device__ constexpr bool warp_item(uint32_t s, uint32_t m) {
-  return s <= kWarpVec && uint64_t(s) * (s + m) <= 6144;
+// Default limit of s (s + m) for a warp item; vistio_batch_tune picks one per batch.
+constexpr uint32_t kWarpItemLimit = 6144;
+__host__ __device__ constexpr bool warp_item(uint32_t s, uint32_t m, uint32_t limit = kWarpItemLimit) {
+  return s <= kWarpVec && uint64_t(s) * (s + m) <= limit;
 }
 
 // ------------------------------------------------ TMA bulk staging

@@ -149,6 +149,10 @@ struct vistio_batch {
   BatchDev dev_w{};          // dev with Y = W: the sweeps of a refinement
   // batch levels of the sweeps: offset into lvl_items, block items, warp items
   std::vector<uint32_t> lvl_off, lvl_nb, lvl_nw;
+  std::vector<std::pair<uint32_t, uint32_t>> top;  // (level, supernode) of every top-level supernode
+  std::vector<SnDev> sn_host;                       // supernode table, for re-scheduling
+  uint32_t warp_limit = kWarpItemLimit;             // s (s + m) limit of a warp item
+  float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
   DevBuf<SnDev> sn;
   DevBuf<float4> U;
   DevBuf<InstRed> red;
@@ -180,6 +184,33 @@ struct vistio_factor {
 namespace {
 
 vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch* b);
+
+// The level schedule of a batch for a warp-item limit: per level, the
+// supernodes for a whole block (heaviest first), then those for one warp
+// (heaviest first). Fills lvl_off / lvl_nb / lvl_nw and returns the items.
+std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
+  uint32_t L = 0;
+  for (auto& t : b->top) L = std::max(L, t.first + 1);
+  std::vector<std::vector<uint32_t>> blk(L), wrp(L);
+  for (auto& t : b->top) {
+    const SnDev& S = b->sn_host[t.second];
+    (warp_item(S.ncols, S.nrows, limit) ? wrp : blk)[t.first].push_back(t.second);
+  }
+  auto weight = [&](uint32_t q) { return uint64_t(b->sn_host[q].ncols) * (b->sn_host[q].ncols + b->sn_host[q].nrows); };
+  std::vector<uint32_t> items;
+  b->lvl_off.clear(); b->lvl_nb.clear(); b->lvl_nw.clear();
+  for (uint32_t l = 0; l < L; ++l) {
+    std::stable_sort(blk[l].begin(), blk[l].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
+    std::stable_sort(wrp[l].begin(), wrp[l].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
+    b->lvl_off.push_back(uint32_t(items.size()));
+    b->lvl_nb.push_back(uint32_t(blk[l].size()));
+    b->lvl_nw.push_back(uint32_t(wrp[l].size()));
+    items.insert(items.end(), blk[l].begin(), blk[l].end());
+    items.insert(items.end(), wrp[l].begin(), wrp[l].end());
+  }
+  b->warp_limit = limit;
+  return items;
+}
 inline uint64_t pad4(uint64_t n) { return (n + 3) & ~3ull; }
 float estimate_kappa(const vistio_solver_config& c, const InstanceSetup& I);
 
@@ -254,7 +285,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   rows.reserve(NROWS);
   uint32_t LMAX = 0;
   for (uint32_t k = 0; k < n; ++k) LMAX = std::max(LMAX, solvers[k]->setup.factor.nlevels);
-  std::vector<std::vector<uint32_t>> lvl_block(LMAX), lvl_warp(LMAX);
+  (void)LMAX;
   std::vector<uint2> subs;
   uint64_t snb = 0, rowsb = 0, valsb = 0, fwdb = 0;
   for (uint32_t k = 0; k < n; ++k) {
@@ -292,7 +323,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       d.p_off = valsb; valsb += pad4(uint64_t(m) * sc + m);  // panel, then its row indices
       d.vbase = uint32_t(v0);
       d.inst = k;
-      if (X.level != kBottomLevel) (warp_item(sc, m) ? lvl_warp : lvl_block)[X.level].push_back(uint32_t(snb + q));
+      if (X.level != kBottomLevel) b->top.push_back({X.level, uint32_t(snb + q)});
       const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
       const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
       for (uint64_t e = 0; e < uint64_t(m) * sc; ++e) vals[d.p_off + e] = float(Pn[e]);
@@ -325,18 +356,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     for (uint32_t k = 0; k < n; ++k) append_permuted_matrix(solvers[k]->setup, uint32_t(vb[k]), a_ptr, a_col, a_val);
     b->refine = b->cfg.refinement_sweeps;
   }
-  // batch levels: block items (heaviest first), then warp items
-  std::vector<uint32_t> items;
-  for (uint32_t l = 0; l < LMAX; ++l) {
-    auto weight = [&](uint32_t q) { return uint64_t(sn[q].ncols) * (sn[q].ncols + sn[q].nrows); };
-    std::stable_sort(lvl_block[l].begin(), lvl_block[l].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
-    std::stable_sort(lvl_warp[l].begin(), lvl_warp[l].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
-    b->lvl_off.push_back(uint32_t(items.size()));
-    b->lvl_nb.push_back(uint32_t(lvl_block[l].size()));
-    b->lvl_nw.push_back(uint32_t(lvl_warp[l].size()));
-    items.insert(items.end(), lvl_block[l].begin(), lvl_block[l].end());
-    items.insert(items.end(), lvl_warp[l].begin(), lvl_warp[l].end());
-  }
+  b->sn_host = sn;
+  std::vector<uint32_t> items = schedule_levels(b, b->warp_limit);
   // vertex incidence
   for (uint64_t t = 0; t < T; ++t) { vtri_ptr[tri_idx[t].x + 1]++; vtri_ptr[tri_idx[t].y + 1]++; vtri_ptr[tri_idx[t].z + 1]++; }
   for (uint64_t h = 0; h < H; ++h) {
@@ -1017,6 +1038,64 @@ vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* la
 }
 
 void* vistio_batch_stream(vistio_batch* b) { return b ? (void*)b->ctx->stream : nullptr; }
+
+// Level-schedule autotuner. The candidate warp-item limits of s (s + m):
+// 0 (every top supernode for a block) ... 2^30 (every one of at most
+// kWarpVec columns for a warp).
+static const uint32_t kTuneLimits[7] = {0u, 1024u, 2048u, 4096u, 6144u, 12288u, 1u << 30};
+
+vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  vistio_ctx* ctx = b->ctx;
+  cudaStream_t st = ctx->stream;
+  StepParams p{};
+  p.dt = 1.f / 60.f;
+  CU(cudaMemcpyAsync(b->prm.p, &p, sizeof(p), cudaMemcpyHostToDevice, st));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  float best = 0.f;
+  uint32_t best_limit = b->warp_limit;
+  for (int c = 0; c < 7; ++c) {
+    std::vector<uint32_t> items = schedule_levels(b, kTuneLimits[c]);
+    if (!items.empty())
+      CU(cudaMemcpyAsync(b->lvl_items.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(b->Y.p, 0, b->V * sizeof(float4), st));
+    launch_sweeps(b, b->dev, st);  // warm-up
+    CU(cudaEventRecord(e0, st));
+    for (int r = 0; r < 3; ++r) launch_sweeps(b, b->dev, st);
+    CU(cudaEventRecord(e1, st));
+    CU(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, e0, e1));
+    ms /= 3.f;
+    if (candidate_ms) candidate_ms[c] = ms;
+    if (c == 0 || ms < best) { best = ms; best_limit = kTuneLimits[c]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::vector<uint32_t> items = schedule_levels(b, best_limit);
+  if (!items.empty()) CU(cudaMemcpyAsync(b->lvl_items.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaStreamSynchronize(st));
+  b->tuned_ms = best;
+  // captured steps bake the old schedule into their launches
+  if (b->graph_plain) { cudaGraphExecDestroy(b->graph_plain); b->graph_plain = nullptr; }
+  if (b->graph_ipc) { cudaGraphExecDestroy(b->graph_ipc); b->graph_ipc = nullptr; }
+  if (chosen_limit) *chosen_limit = best_limit;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  vistio_ctx* ctx = b->ctx;
+  std::vector<uint32_t> items = schedule_levels(b, limit);
+  if (!items.empty())
+    CU(cudaMemcpyAsync(b->lvl_items.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  if (b->graph_plain) { cudaGraphExecDestroy(b->graph_plain); b->graph_plain = nullptr; }
+  if (b->graph_ipc) { cudaGraphExecDestroy(b->graph_ipc); b->graph_ipc = nullptr; }
+  return VISTIO_OK;
+}
 
 vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase) {
   if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
