@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import argparse
 import concurrent.futures as cf
+import dataclasses
 import json
 import math
 import os
@@ -443,7 +444,8 @@ def main():
            "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
            "clocks": clocks, "roofline": roofline,
            "batch": {"vertices": V, "triangles": T, "hinges": H, "factor_bytes": info["factor_bytes"],
-                     "setup_s": setup_s}}
+                     "setup_s": setup_s,
+                     "factorization": dict(batch.factor_stats(), where="GPU, multifrontal FP64, every garment")}}
 
     if rank == 0 and not args.no_baselines:
         # plain one-instance-per-launch GPU PD on one instance of each topology
@@ -465,6 +467,20 @@ def main():
                 p.step(DT)
         torch.cuda.synchronize()
         plain_v = len(plain) * psteps / (time.perf_counter() - t0)
+        # the host's numeric FP64 factorization of the same garments, one thread,
+        # for comparison with the batch's device factorization above
+        host_ms = 0.0
+        for s in sample:
+            m = scenarios.hanging_sheet(s.side, s.length)
+            setup = api.SetupDesc(stiffness=s.stretch, bend_stiffness=s.bending, density_gsm=s.density_gsm)
+            t = []
+            for host in (True, False):
+                c = dataclasses.replace(cfg, host_factorization=host)
+                t1 = time.perf_counter()
+                api.ProjectiveDynamicsSolver().init_explicit(m, c, setup, pinned=m.pinned)
+                t.append(time.perf_counter() - t1)
+            host_ms += 1e3 * max(0.0, t[0] - t[1]) * len(specs) / len(sample)
+        out["batch"]["factorization"]["host_1thread_ms_est"] = host_ms
         out["plain_gpu"] = {"value": plain_v, "unit": UNIT,
                             "how": "each instance stepped alone (one graph launch per instance-step, result read "
                                    "back each step), one instance of each topology",

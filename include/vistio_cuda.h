@@ -100,6 +100,12 @@ typedef struct vistio_solver_config {
    * solve; the plain step refines its last iteration's solve (each earlier
    * iteration's error is corrected by the next iteration's residual). */
   uint32_t refinement_sweeps;
+  /* Where the numeric FP64 Cholesky factorization of the system matrix runs
+   * (faer's LL^T in the reference, faer_solver.rs:67-93). 0: on the GPU,
+   * multifrontal, when the garment is first packed into a batch; the host
+   * computes the ordering and the symbolic structure. 1: on the host. */
+  uint32_t host_factorization;
+  uint32_t reserved0; /* must be 0 */
 } vistio_solver_config;
 
 /* FabricProperties (crates/vistio-material/src/properties.rs:23-58). */
@@ -237,6 +243,11 @@ vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, ui
 vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms);
 /* Sets that limit directly (any value; see vistio_batch_tune). */
 vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit);
+/* The device factorization done when the batch was created (the garments
+ * whose solver config has host_factorization = 0): its kernel launches (one
+ * per height of the supernodal trees per group of garments) and their device
+ * time in milliseconds; 0 and 0 when every garment was factorized on the host. */
+vistio_status vistio_batch_factor_stats(const vistio_batch* b, uint32_t* launches, float* device_ms);
 /* Kernel launches in one batch step (graph nodes), for launch accounting. */
 vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* launches);
 /* The stream the batch runs on (cudaStream_t as void*), for event timing. */

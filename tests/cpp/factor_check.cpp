@@ -5,6 +5,7 @@
 // residual of A x = b. Prints one JSON object.
 //
 // usage: factor_check cols rows width [bending] [pinned_row]
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -75,6 +76,101 @@ static void sweep(const Factor& F, const std::vector<T>& vals, std::vector<T>& Y
     for (int k = int(F.sub_last[q]); k >= int(F.sub_first[q]); --k) bwd_sn(F, vals, Y, Tm, uint32_t(k));
 }
 
+// Replays the device factorization (k_front in factor_kernels.cuh) on the
+// CPU: one dense front per supernode (columns, then rows), assembled from the
+// permuted A and the children's update matrices through the map of each
+// child row into its parent's front, partial Cholesky of the supernode's
+// columns, inv(L_kk) by forward substitution. Returns the largest difference
+// to the host factor's values, relative to the largest value.
+static double multifrontal_replay(const InstanceSetup& I) {
+  const Factor& F = I.factor;
+  const uint32_t nsn = uint32_t(F.sn.size());
+  std::vector<uint32_t> ap{0}, ac;
+  std::vector<double> av;
+  append_permuted_matrix(I, 0, ap, ac, av);
+  std::vector<std::vector<double>> fronts(nsn);
+  std::vector<double> out(F.vals.size(), 0.0);
+  auto pos_in = [&](uint32_t k, uint32_t r) -> int64_t {  // position of row r in supernode k's front
+    const Supernode& S = F.sn[k];
+    if (r >= S.first && r < S.first + S.ncols) return r - S.first;
+    const uint32_t* R = F.rows.data() + S.rows_off;
+    const uint32_t* it = std::lower_bound(R, R + S.nrows, r);
+    if (it == R + S.nrows || *it != r) return -1;
+    return S.ncols + (it - R);
+  };
+  for (uint32_t k = 0; k < nsn; ++k) {  // children precede parents
+    const Supernode& S = F.sn[k];
+    const uint32_t s = S.ncols, m = S.nrows, nf = s + m, f = S.first;
+    std::vector<double>& Fk = fronts[k];
+    Fk.assign(size_t(nf) * nf, 0.0);
+    for (uint32_t c = 0; c < s; ++c)
+      for (uint32_t q = ap[f + c]; q < ap[f + c + 1]; ++q) {
+        if (ac[q] < f + c) continue;
+        int64_t at = pos_in(k, ac[q]);
+        if (at < 0) return 1e30;
+        Fk[size_t(c) * nf + at] += av[q];
+      }
+    for (uint32_t ch = 0; ch < k; ++ch) {
+      if (F.sn[ch].parent != k) continue;
+      const Supernode& C = F.sn[ch];
+      const uint32_t sc = C.ncols, mc = C.nrows, nfc = sc + mc;
+      std::vector<int64_t> map(mc);
+      for (uint32_t j = 0; j < mc; ++j) {
+        map[j] = pos_in(k, F.rows[C.rows_off + j]);
+        if (map[j] < 0) return 1e30;
+      }
+      for (uint32_t j = 0; j < mc; ++j)
+        for (uint32_t i = j; i < mc; ++i)
+          Fk[size_t(map[j]) * nf + map[i]] += fronts[ch][size_t(sc + j) * nfc + sc + i];
+      fronts[ch].clear();
+    }
+    for (uint32_t j = 0; j < s; ++j) {
+      double d = Fk[size_t(j) * nf + j];
+      if (!(d > 0.0)) return 1e30;
+      d = std::sqrt(d);
+      Fk[size_t(j) * nf + j] = d;
+      for (uint32_t i = j + 1; i < nf; ++i) Fk[size_t(j) * nf + i] /= d;
+      for (uint32_t l = j + 1; l < nf; ++l)
+        for (uint32_t i = l; i < nf; ++i) Fk[size_t(l) * nf + i] -= Fk[size_t(j) * nf + i] * Fk[size_t(j) * nf + l];
+    }
+    double* Dv = out.data() + S.diag_off;
+    for (uint32_t c = 0; c < s; ++c) {
+      Dv[size_t(c) * s + c] = 1.0 / Fk[size_t(c) * nf + c];
+      for (uint32_t i = c + 1; i < s; ++i) {
+        double acc = 0.0;
+        for (uint32_t q = c; q < i; ++q) acc += Fk[size_t(q) * nf + i] * Dv[size_t(c) * s + q];
+        Dv[size_t(c) * s + i] = -acc / Fk[size_t(i) * nf + i];
+      }
+    }
+    double* Pv = out.data() + S.panel_off;
+    for (uint32_t r = 0; r < m; ++r)
+      for (uint32_t c = 0; c < s; ++c) Pv[size_t(r) * s + c] = Fk[size_t(c) * nf + s + r];
+  }
+  double big = 0, diff = 0;
+  for (size_t e = 0; e < out.size(); ++e) {
+    big = std::max(big, std::fabs(F.vals[e]));
+    diff = std::max(diff, std::fabs(out[e] - F.vals[e]));
+  }
+  return diff / big;
+}
+
+// The symbolic-only set-up (numeric factorization left to the device) has
+// the same ordering, supernodes, rows, schedule and pull lists.
+static bool same_structure(const Factor& a, const Factor& b) {
+  if (a.perm != b.perm || a.rows != b.rows || a.nlevels != b.nlevels || a.level_sn != b.level_sn ||
+      a.level_sn_ptr != b.level_sn_ptr || a.sub_first != b.sub_first || a.sub_last != b.sub_last ||
+      a.fwd_ptr != b.fwd_ptr || a.fwd_sn != b.fwd_sn || a.fwd_pos != b.fwd_pos || a.sn.size() != b.sn.size() ||
+      a.nnz_stored != b.nnz_stored || b.numeric || !b.vals.empty())
+    return false;
+  for (size_t k = 0; k < a.sn.size(); ++k) {
+    const Supernode &x = a.sn[k], &y = b.sn[k];
+    if (x.first != y.first || x.ncols != y.ncols || x.nrows != y.nrows || x.rows_off != y.rows_off ||
+        x.panel_off != y.panel_off || x.diag_off != y.diag_off || x.parent != y.parent || x.level != y.level)
+      return false;
+  }
+  return true;
+}
+
 int main(int argc, char** argv) {
   uint32_t cols = argc > 1 ? atoi(argv[1]) : 20, rows = argc > 2 ? atoi(argv[2]) : 20;
   float width = argc > 3 ? float(atof(argv[3])) : 1.f;
@@ -114,6 +210,13 @@ int main(int argc, char** argv) {
     return 1;
   }
   const Factor& F = I.factor;
+  InstanceSetup Isym;
+  SetupParams psym = p;
+  psym.numeric = false;
+  err = build_instance(nv, px.data(), py.data(), pz.data(), uint32_t(tris.size() / 3), tris.data(), pinned.data(),
+                       psym, Isym, &st);
+  const int symbolic_same = err.empty() && same_structure(F, Isym.factor);
+  const double mf_diff = multifrontal_replay(I);
   std::mt19937_64 rng(20261203);
   std::normal_distribution<double> nd;
   std::vector<double> b(nv), yd(nv);
@@ -155,8 +258,10 @@ int main(int argc, char** argv) {
   for (auto& S : F.sn) maxs = std::max(maxs, S.ncols);
   printf("{\"nv\": %u, \"nh\": %u, \"nnz_a\": %zu, \"nnz_l\": %llu, \"stored\": %llu, \"supernodes\": %zu, "
          "\"levels\": %u, \"subtrees\": %zu, \"max_snode\": %u, \"fwd_entries\": %zu, \"resid64\": %.3e, \"resid32\": %.3e, "
-         "\"resid32_refined\": %.3e, \"err32\": %.3e, \"err32_refined\": %.3e}\n",
+         "\"resid32_refined\": %.3e, \"err32\": %.3e, \"err32_refined\": %.3e, \"symbolic_same\": %d, "
+         "\"multifrontal_diff\": %.3e}\n",
          nv, I.nh, I.A_col.size(), (unsigned long long)F.nnz_L, (unsigned long long)F.nnz_stored, F.sn.size(),
-         F.nlevels, F.sub_first.size(), maxs, F.fwd_sn.size(), resid(yd), resid(yf), resid(yr), dist64(yf), dist64(yr));
+         F.nlevels, F.sub_first.size(), maxs, F.fwd_sn.size(), resid(yd), resid(yf), resid(yr), dist64(yf), dist64(yr),
+         symbolic_same, mf_diff);
   return 0;
 }

@@ -63,7 +63,11 @@ def test_supernodal_layout_replays_exactly(factor_check_bin, grid):
     """The level-scheduled supernodal sweeps over the packed factor solve A x = b
     (FP64 replay ~1e-14, FP32 replay ~1e-5 relative residual). One FP64
     refinement with the permuted f64 matrix, formed as the GPU forms it, brings
-    the FP32 solution to within FP32 rounding (~3e-8) of the FP64 solution."""
+    the FP32 solution to within FP32 rounding (~3e-8) of the FP64 solution.
+    The symbolic-only set-up (numeric factorization on the device) has the same
+    structure, and a CPU replay of the device's multifrontal factorization
+    (fronts, extend-add through the child-row maps, partial Cholesky, inverted
+    diagonal blocks) reproduces the host factor to FP64 rounding."""
     out = subprocess.check_output([factor_check_bin] + [str(g) for g in grid])
     r = json.loads(out)
     assert r["resid64"] < 1e-11, r
@@ -71,6 +75,8 @@ def test_supernodal_layout_replays_exactly(factor_check_bin, grid):
     assert r["resid32_refined"] < r["resid32"], r
     assert r["err32_refined"] < min(6e-8, r["err32"] / 3), r
     assert r["levels"] <= 32
+    assert r["symbolic_same"] == 1, r
+    assert r["multifrontal_diff"] < 1e-12, r
 
 
 def test_hanging_sheet_sizes_and_hinges():

@@ -258,3 +258,30 @@ def test_level_schedules_and_autotuner():
     assert t["warp_item_limit"] in api.Batch.TUNE_LIMITS
     assert all(v > 0 for v in t["sweep_ms"].values())
     batch.step(1.0 / 60.0, 1)
+
+
+@pytest.mark.parametrize("side,length", [(20, 1.0), (48, 1.5)])
+def test_device_factorization_matches_host_factorization(side, length):
+    """The FP64 Cholesky factor computed on the GPU (multifrontal, the default)
+    and the one computed on the host give the same trajectories: both are
+    FP64 factors of the same matrix rounded to FP32 for the sweeps, so they
+    differ by FP64 rounding only (<= 1e-6 m after 10 steps). A batch holding
+    one garment of each kind gives each the result it gives alone."""
+    mesh = scenarios.hanging_sheet(side, length)
+    setup = api.SetupDesc(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0)
+    runs = {}
+    for host in (False, True):
+        cfg = api.drape_config(max_iterations=10, host_factorization=host)
+        s = api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
+        for _ in range(10):
+            s.step(DT)
+        runs[host] = s.state()[0]
+    diff = float(np.abs(runs[False] - runs[True]).max())
+    print(f"max |device factor - host factor| after 10 steps = {diff:.3e} m")
+    assert diff <= 1e-6, diff
+    pair = [api.ProjectiveDynamicsSolver().init_explicit(mesh, api.drape_config(max_iterations=10, host_factorization=h),
+                                                         setup, pinned=mesh.pinned) for h in (False, True)]
+    batch = api.Batch(pair)
+    batch.step(DT, 10)
+    assert np.array_equal(batch.state(0)[0], runs[False])
+    assert np.array_equal(batch.state(1)[0], runs[True])

@@ -91,16 +91,20 @@ def test_requests_in_the_mix_equal_requests_alone():
 
 
 def test_memory_budget_admission_and_oversize_request():
-    reqs = [plain_request(10, 0.6, 600.0, 1e-4, 150.0, 20), plain_request(14, 0.9, 900.0, 1e-4, 150.0, 20),
-            plain_request(11, 0.7, 700.0, 1e-4, 150.0, 20)]
-    probe = api.ProjectiveDynamicsSolver().init_explicit(reqs[1]["mesh"], reqs[1]["config"], reqs[1]["setup"],
-                                                         pinned=reqs[1]["pinned"])
+    reqs = [plain_request(12, 0.6, 600.0, 1e-4, 150.0, 20), plain_request(14, 0.9, 900.0, 1e-4, 150.0, 20),
+            plain_request(13, 0.7, 700.0, 1e-4, 150.0, 20)]
     from vistio_b200 import _lib
     import ctypes as C
-    need = C.c_uint64()
-    _lib.check(_lib.lib().vistio_solver_device_bytes(probe.h, 0, C.byref(need)))
+    needs = []
+    for r in reqs:
+        probe = api.ProjectiveDynamicsSolver().init_explicit(r["mesh"], r["config"], r["setup"], pinned=r["pinned"])
+        need = C.c_uint64()
+        _lib.check(_lib.lib().vistio_solver_device_bytes(probe.h, 0, C.byref(need)))
+        needs.append(need.value)
     # room for the largest request alone, and for no two of the three together
-    srv = api.Server(hbm_budget_bytes=int(need.value * 1.05), max_cohort=8, setup_threads=2, steps_per_slice=5)
+    budget = max(needs) + min(needs) // 2
+    assert budget < sorted(needs)[0] + sorted(needs)[1]
+    srv = api.Server(hbm_budget_bytes=budget, max_cohort=8, setup_threads=2, steps_per_slice=5)
     ids = [submit(srv, r) for r in reqs]
     big = plain_request(40, 1.0, 1e3, 1e-4, 150.0, 5)  # never fits this budget
     big_id = submit(srv, big)

@@ -31,7 +31,8 @@ class SolverConfigC(C.Structure):
                 ("al_tolerance", C.c_float), ("friction_coefficient", C.c_float), ("contact_damping", C.c_float),
                 ("compliant_d_hat_scale", C.c_float), ("contact_damping_max", C.c_float),
                 ("contact_velocity_threshold", C.c_float), ("compliant_contact", C.c_int32),
-                ("adaptive_contact_damping", C.c_int32), ("refinement_sweeps", C.c_uint32)]
+                ("adaptive_contact_damping", C.c_int32), ("refinement_sweeps", C.c_uint32),
+                ("host_factorization", C.c_uint32), ("reserved0", C.c_uint32)]
 
 
 class MaterialDesc(C.Structure):
@@ -124,6 +125,7 @@ SIGNATURES = {
     "vistio_batch_download_positions": (C.c_int, [_vp, _fp]),
     "vistio_batch_info": (C.c_int, [_vp, _u32p, _u64p, _u64p, _u64p, _u64p, _u64p]),
     "vistio_batch_launches_per_step": (C.c_int, [_vp, _u32p]),
+    "vistio_batch_factor_stats": (C.c_int, [_vp, _u32p, _fp]),
     "vistio_batch_stream": (_vp, [_vp]),
     "vistio_batch_launch_phase": (C.c_int, [_vp, C.c_int32]),
     "vistio_batch_phase_bytes": (C.c_int, [_vp, C.c_int32, _u64p]),

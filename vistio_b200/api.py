@@ -48,6 +48,10 @@ class SolverConfig:
     # projections and barriers in FP64 the FP32 sweeps already keep a step
     # within 1e-5 of FP64 on the drape workloads, and a sweep costs ~7% there.
     refinement_sweeps: int = 0
+    # False (default): the numeric FP64 Cholesky factorization runs on the GPU
+    # when the garment is first packed; True: on the host (both produce the
+    # same factor up to FP64 rounding).
+    host_factorization: bool = False
 
     def to_c(self) -> L.SolverConfigC:
         c = L.SolverConfigC()
@@ -62,6 +66,7 @@ class SolverConfig:
         c.compliant_contact = int(bool(self.compliant_contact))
         c.adaptive_contact_damping = int(bool(self.adaptive_contact_damping))
         c.refinement_sweeps = int(self.refinement_sweeps)
+        c.host_factorization = int(bool(self.host_factorization))
         return c
 
 
@@ -364,6 +369,14 @@ class Batch:
         L.check(L.lib().vistio_batch_info(self.h, *[C.byref(v) for v in vals]), self.ctx.h)
         keys = ("instances", "vertices", "triangles", "hinges", "factor_bytes", "device_bytes")
         return {k: v.value for k, v in zip(keys, vals)}
+
+    def factor_stats(self) -> dict:
+        """The device factorization done when the batch was created: kernel
+        launches and device milliseconds (0, 0 if every garment was factorized
+        on the host)."""
+        n, ms = C.c_uint32(), C.c_float()
+        L.check(L.lib().vistio_batch_factor_stats(self.h, C.byref(n), C.byref(ms)), self.ctx.h)
+        return {"launches": n.value, "device_ms": ms.value}
 
     def launches_per_step(self) -> int:
         v = C.c_uint32()

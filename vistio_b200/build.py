@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libvistio_b200.so")
 SOURCES = ["vistio_cuda.cu", "setup.cpp", "server.cpp"]
-HEADERS = ["pd_kernels.cuh", "contact_kernels.cuh", "self_contact.cuh", "setup.h"]
+HEADERS = ["pd_kernels.cuh", "contact_kernels.cuh", "factor_kernels.cuh", "self_contact.cuh", "setup.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -191,10 +191,11 @@ class Dissector {
 
 // ------------------------------------------------------------- factorize
 std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,
-                          const float* coords, Factor& f, int* status) {
+                          const float* coords, Factor& f, int* status, bool numeric) {
   *status = 0;
   f = Factor();
   f.n = n;
+  f.numeric = numeric;
   if (n == 0) { *status = 3; return "cannot factorize an empty matrix"; }
   // Symmetric adjacency (pattern of A + A^T without the diagonal).
   Graph g;
@@ -315,11 +316,18 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
   std::vector<uint64_t> Lp(n + 1, 0);
   for (uint32_t k = 0; k < n; ++k) Lp[k + 1] = Lp[k] + cnt[k];
   std::vector<uint32_t> Li(Lp[n]);
-  std::vector<double> Lx(Lp[n]);
+  std::vector<double> Lx(numeric ? Lp[n] : 0);
   std::vector<uint64_t> cur(Lp.begin(), Lp.end() - 1);
   std::vector<double> x(n, 0.0);
   std::fill(mark.begin(), mark.end(), -1);
-  for (uint32_t k = 0; k < n; ++k) {
+  if (!numeric) {  // the pattern of L only (row k from the etree reach)
+    for (uint32_t k = 0; k < n; ++k) {
+      int top = ereach(k);
+      for (int p = top; p < int(n); ++p) Li[cur[uint32_t(pat[p])]++] = k;
+      Li[cur[k]++] = k;
+    }
+  }
+  for (uint32_t k = 0; k < n && numeric; ++k) {
     int top = ereach(k);
     for (uint32_t p = bp[k]; p < bp[k + 1]; ++p) x[bent[p].first] += bent[p].second;
     double d = x[k];
@@ -461,12 +469,12 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
       if (p != UINT32_MAX) top_lvl[p] = std::max(top_lvl[p], top_lvl[k] + 1);
     }
   }
-  f.vals.assign(off, 0.0);
   f.nnz_stored = off;
+  if (numeric) f.vals.assign(off, 0.0);
   // Scatter the simplicial columns into panels and diagonal blocks.
   std::vector<int> pos(n, -1);
   std::vector<double> Lkk;
-  for (uint32_t k = 0; k < nsn; ++k) {
+  for (uint32_t k = 0; k < nsn && numeric; ++k) {
     Supernode& S = f.sn[k];
     const uint32_t* R = f.rows.data() + S.rows_off;
     for (uint32_t r = 0; r < S.nrows; ++r) pos[R[r]] = int(r);
@@ -695,7 +703,8 @@ std::string build_instance(uint32_t nv, const float* px, const float* py, const 
     k = j;
   }
   for (uint32_t i = 0; i < nv; ++i) I.A_ptr[i + 1] += I.A_ptr[i];
-  std::string err = factorize_csr(nv, I.A_ptr.data(), I.A_col.data(), I.A_val.data(), I.rest.data(), I.factor, status);
+  std::string err = factorize_csr(nv, I.A_ptr.data(), I.A_col.data(), I.A_val.data(), I.rest.data(), I.factor, status,
+                                  prm.numeric);
   if (!err.empty()) return "Cholesky factorization failed: " + err;
   return "";
 }

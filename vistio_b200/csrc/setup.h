@@ -25,6 +25,7 @@ struct SetupParams {
   float warp = 0.f, weft = 0.f;   // membrane model warp/weft
   float bend_warp = 0.f, bend_weft = 0.f;
   float matrix_dt = 1.0f / 60.0f; // dt used in A (the reference always assembles with 1/60)
+  bool numeric = true;            // false: symbolic factorization only (the numbers on the GPU)
 };
 
 // Largest supernode (columns); the GPU sweeps size their shared-memory vectors for it.
@@ -78,6 +79,7 @@ struct Factor {
   std::vector<uint32_t> fwd_sn;     // supernode id
   std::vector<uint32_t> fwd_pos;    // row position inside that supernode's panel
   uint64_t nnz_L = 0;               // nonzeros of the simplicial factor (incl. diagonal)
+  bool numeric = true;              // vals holds the factor (else symbolic only)
   uint64_t nnz_stored = 0;          // entries stored in panels + diagonal blocks
 };
 
@@ -116,7 +118,10 @@ void append_permuted_matrix(const InstanceSetup& I, uint32_t base, std::vector<u
 
 // Factorizes a general SPD matrix (CSR, either triangle or both) into the GPU layout.
 // coords (3*n) steer the nested dissection; may be null (a BFS-based split is used).
+// With numeric == false only the symbolic analysis is done (ordering,
+// supernodes, row structures, schedules; vals stays empty): the GPU computes
+// the numbers (multifrontal, FP64) when the garment is packed into a batch.
 std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
-                          const double* vals, const float* coords, Factor& f, int* status);
+                          const double* vals, const float* coords, Factor& f, int* status, bool numeric = true);
 
 }  // namespace vistio

@@ -18,6 +18,7 @@
 
 #include "../../include/vistio_cuda.h"
 #include "contact_kernels.cuh"
+#include "factor_kernels.cuh"
 #include "self_contact.cuh"
 #include "setup.h"
 
@@ -117,6 +118,11 @@ template <class T> struct DevBuf {
     if (e != cudaSuccess || h.empty()) return e;
     return cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
   }
+  void reset() {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    n = 0;
+  }
 };
 
 }  // namespace
@@ -141,6 +147,8 @@ struct vistio_batch {
   DevBuf<uint32_t> vtri_ptr, vtri, vhinge_ptr, vhinge, perm_local, rows, lvl_items, fwd_ptr, fwd, status;
   DevBuf<uint2> sub_items;
   uint32_t n_sub = 0;
+  uint32_t factor_launches = 0;  // k_front launches of the device factorization
+  float factor_ms = 0.f;         // their device time
   // FP64 refinement: permuted f64 CSR of A, kept right-hand side, correction
   DevBuf<uint32_t> a_ptr, a_col;
   DevBuf<double> a_val;
@@ -214,6 +222,11 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
 inline uint64_t pad4(uint64_t n) { return (n + 3) & ~3ull; }
 float estimate_kappa(const vistio_solver_config& c, const InstanceSetup& I);
 
+// Fronts of the device factorization are allocated for groups of garments
+// of at most this many bytes (at least one garment per group); one buffer
+// serves the groups one after another.
+constexpr uint64_t kFrontBudget = 1ull << 30;
+
 // Device bytes one garment occupies in a batch (the sizes pack_batch
 // allocates), plus the self-contact buffers when those are used.
 uint64_t instance_device_bytes(const InstanceSetup& I, bool refine, bool self_contact) {
@@ -224,7 +237,14 @@ uint64_t instance_device_bytes(const InstanceSetup& I, bool refine, bool self_co
   uint64_t b = vals * 4 + F.sn.size() * sizeof(SnDev) + R * 4 + F.fwd_sn.size() * 4 + (V + 1) * 4 +
                F.sn.size() * 4 + R * 16;
   b += V * (16 * 10 + 4 + 3 + 4 * 3) + T * (16 + 16 + 4 + 36 + 12) + H * (16 + 16 + 8 + 16 + 16) + (V + 1) * 8;
-  if (refine) b += (V + 1) * 4 + I.A_col.size() * 12 + V * 32;
+  if (refine || !F.numeric) b += (V + 1) * 4 + I.A_col.size() * 12;
+  if (refine) b += V * 32;
+  if (!F.numeric) {  // the fronts of the device factorization, freed once it is done (at most kFrontBudget
+                     // bytes for a batch of garments that each need less)
+    uint64_t fronts = 0;
+    for (const Supernode& X : F.sn) fronts += 8 * uint64_t(X.ncols + X.nrows) * (X.ncols + X.nrows);
+    b += std::min(fronts, kFrontBudget) + R * 4 + F.sn.size() * 24;
+  }
   if (self_contact) b += V * 32 + T * (4 + 2 * 2 * 16 + 4) + 48 * T * 8 + V * 4 + 16 * V * 4;
   return b + 12 * V;  // whole-batch position staging
 }
@@ -236,6 +256,127 @@ std::vector<int4> make_chunks(const std::vector<uint64_t>& base, const std::vect
     for (uint64_t s = 0; s < count[k]; s += kElemThreads)
       ch.push_back(make_int4(int(k), int(base[k] + s), int(std::min<uint64_t>(kElemThreads, count[k] - s)), 0));
   return ch;
+}
+
+// Numeric FP64 factorization, on the device, of the garments whose host
+// set-up is symbolic only (k_front, one block per supernode, one launch per
+// height of the supernodal trees). The batch's supernodes, rows, permuted A
+// and (zeroed) factor values are on the device already.
+vistio_status factor_on_device(vistio_ctx* ctx, vistio_batch* b, vistio_solver* const* solvers, uint32_t n,
+                               const std::vector<InstDev>& hi, const std::vector<SnDev>& sn,
+                               const std::vector<uint32_t>& rows) {
+  cudaStream_t st = ctx->stream;
+  const uint64_t NSN = sn.size();
+  std::vector<uint32_t> parent(NSN, UINT32_MAX), height(NSN, 0), kid_ptr(NSN + 1, 0), kids, relmap(rows.size(), 0);
+  std::vector<uint64_t> front_off(NSN, 0);
+  for (uint32_t k = 0; k < n; ++k) {
+    const Factor& F = solvers[k]->setup.factor;
+    if (F.numeric) continue;
+    const uint32_t base = hi[k].sn_base;
+    for (uint32_t q = 0; q < F.sn.size(); ++q) {
+      if (F.sn[q].parent == UINT32_MAX) continue;
+      const uint32_t g = base + q, p = base + F.sn[q].parent;
+      parent[g] = p;
+      kid_ptr[p + 1]++;
+      height[p] = std::max(height[p], height[g] + 1);  // children precede parents
+    }
+  }
+  for (uint64_t g = 0; g < NSN; ++g) kid_ptr[g + 1] += kid_ptr[g];
+  kids.resize(kid_ptr[NSN]);
+  {
+    std::vector<uint32_t> cur(kid_ptr.begin(), kid_ptr.end() - 1);
+    for (uint64_t g = 0; g < NSN; ++g)
+      if (parent[g] != UINT32_MAX) kids[cur[parent[g]]++] = uint32_t(g);
+  }
+  // each child row's position in its parent's front: a column of the parent
+  // or one of the parent's rows (the child's rows are a subset of those)
+  for (uint64_t g = 0; g < NSN; ++g) {
+    if (parent[g] == UINT32_MAX) continue;
+    const SnDev &C = sn[g], &P = sn[parent[g]];
+    const uint32_t* Rp = rows.data() + P.rows_off;
+    for (uint32_t j = 0; j < C.nrows; ++j) {
+      const uint32_t r = rows[C.rows_off + j];
+      uint32_t at;
+      if (r >= P.first && r < P.first + P.ncols) {
+        at = r - P.first;
+      } else {
+        const uint32_t* it = std::lower_bound(Rp, Rp + P.nrows, r);
+        if (it == Rp + P.nrows || *it != r)
+          return fail(ctx, VISTIO_ERR_INVARIANT, "supernode rows are not contained in the parent's front");
+        at = P.ncols + uint32_t(it - Rp);
+      }
+      relmap[C.rows_off + j] = at;
+    }
+  }
+  // groups of garments, and per group the supernodes by height
+  std::vector<uint32_t> items;
+  std::vector<uint2> launches;  // (first item, count)
+  uint64_t gsize = 0, max_gsize = 0;
+  std::vector<uint32_t> group;
+  auto flush = [&]() {
+    if (group.empty()) return;
+    uint32_t hmax = 0;
+    for (uint32_t k : group)
+      for (uint32_t g = hi[k].sn_base; g < hi[k].sn_base + hi[k].nsn; ++g) hmax = std::max(hmax, height[g]);
+    for (uint32_t h = 0; h <= hmax; ++h) {
+      const uint32_t first = uint32_t(items.size());
+      for (uint32_t k : group)
+        for (uint32_t g = hi[k].sn_base; g < hi[k].sn_base + hi[k].nsn; ++g)
+          if (height[g] == h) items.push_back(g);
+      if (items.size() > first) launches.push_back(make_uint2(first, uint32_t(items.size()) - first));
+    }
+    max_gsize = std::max(max_gsize, gsize);
+    group.clear();
+    gsize = 0;
+  };
+  for (uint32_t k = 0; k < n; ++k) {
+    if (solvers[k]->setup.factor.numeric) continue;
+    uint64_t fb = 0;
+    for (uint32_t g = hi[k].sn_base; g < hi[k].sn_base + hi[k].nsn; ++g) {
+      const uint64_t nf = uint64_t(sn[g].ncols) + sn[g].nrows;
+      if (nf >= 65536) return fail(ctx, VISTIO_ERR_CAPACITY, "supernode front too large for the device factorization");
+      fb += nf * nf;
+    }
+    if (!group.empty() && (gsize + fb) * 8 > kFrontBudget) flush();
+    for (uint32_t g = hi[k].sn_base; g < hi[k].sn_base + hi[k].nsn; ++g) {
+      const uint64_t nf = uint64_t(sn[g].ncols) + sn[g].nrows;
+      front_off[g] = gsize;
+      gsize += nf * nf;
+    }
+    group.push_back(k);
+  }
+  flush();
+  DevBuf<uint32_t> d_kid_ptr, d_kids, d_relmap, d_items, d_status;
+  DevBuf<uint64_t> d_front_off;
+  DevBuf<double> d_fronts;
+  CU(d_kid_ptr.upload(kid_ptr, st)); CU(d_kids.upload(kids, st)); CU(d_relmap.upload(relmap, st));
+  CU(d_items.upload(items, st)); CU(d_front_off.upload(front_off, st));
+  CU(d_fronts.alloc(max_gsize, st));
+  CU(d_status.alloc(1, st)); CU(cudaMemsetAsync(d_status.p, 0, sizeof(uint32_t), st));
+  FrontDev D;
+  D.sn = b->sn.p; D.rows = b->rows.p;
+  D.a_ptr = b->a_ptr.p; D.a_col = b->a_col.p; D.a_val = b->a_val.p;
+  D.front_off = d_front_off.p; D.kid_ptr = d_kid_ptr.p; D.kids = d_kids.p; D.relmap = d_relmap.p;
+  D.fronts = d_fronts.p; D.vals = b->vals.p; D.status = d_status.p;
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  CU(cudaEventRecord(e0, st));
+  for (const uint2& L : launches) k_front<<<L.y, kFrontThreads, 0, st>>>(D, d_items.p + L.x);
+  CU(cudaGetLastError());
+  CU(cudaEventRecord(e1, st));
+  uint32_t status = 0;
+  CU(cudaMemcpyAsync(&status, d_status.p, sizeof(status), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  CU(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->factor_ms = ms;
+  if (status & 32u) return fail(ctx, VISTIO_ERR_NOT_SPD, "matrix is not symmetric positive definite (device Cholesky pivot)");
+  if (status & 64u) return fail(ctx, VISTIO_ERR_INVARIANT, "matrix entry outside the symbolic factor structure");
+  b->factor_launches = uint32_t(launches.size());
+  return VISTIO_OK;
 }
 
 vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch* b) {
@@ -324,10 +465,12 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       d.vbase = uint32_t(v0);
       d.inst = k;
       if (X.level != kBottomLevel) b->top.push_back({X.level, uint32_t(snb + q)});
-      const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
-      const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
-      for (uint64_t e = 0; e < uint64_t(m) * sc; ++e) vals[d.p_off + e] = float(Pn[e]);
-      for (uint64_t e = 0; e < uint64_t(sc) * sc; ++e) vals[d.d_off + e] = float(Dn[e]);
+      if (F.numeric) {  // else the device factorization writes D and P
+        const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
+        const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
+        for (uint64_t e = 0; e < uint64_t(m) * sc; ++e) vals[d.p_off + e] = float(Pn[e]);
+        for (uint64_t e = 0; e < uint64_t(sc) * sc; ++e) vals[d.d_off + e] = float(Dn[e]);
+      }
       // the panel's row indices (u32 bits), staged with the panel by the sweeps
       std::memcpy(vals.data() + d.p_off + uint64_t(m) * sc, F.rows.data() + X.rows_off, size_t(m) * 4);
     }
@@ -343,8 +486,11 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   // f64 CSR of each instance's A with rows and columns in solve order (global ids)
   std::vector<uint32_t> a_ptr, a_col;
   std::vector<double> a_val;
-  bool have_a = b->cfg.refinement_sweeps > 0;
+  bool on_device = false;
+  for (uint32_t k = 0; k < n; ++k) on_device = on_device || !solvers[k]->setup.factor.numeric;
+  bool have_a = b->cfg.refinement_sweeps > 0 || on_device;
   for (uint32_t k = 0; k < n && have_a; ++k) have_a = !solvers[k]->setup.A_ptr.empty();
+  if (on_device && !have_a) return fail(ctx, VISTIO_ERR_INVARIANT, "device factorization without the system matrix");
   if (have_a) {
     uint64_t nnz = 0;
     for (uint32_t k = 0; k < n; ++k) nnz += solvers[k]->setup.A_col.size();
@@ -398,9 +544,12 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   b->n_sub = uint32_t(subs.size());
   CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
   CU(b->U.alloc(rows.size(), st));
-  if (b->refine) {
-    CU(b->a_ptr.upload(a_ptr, st)); CU(b->a_col.upload(a_col, st)); CU(b->a_val.upload(a_val, st));
-    CU(b->R0.alloc(V, st)); CU(b->W.alloc(V, st));
+  if (have_a) { CU(b->a_ptr.upload(a_ptr, st)); CU(b->a_col.upload(a_col, st)); CU(b->a_val.upload(a_val, st)); }
+  if (b->refine) { CU(b->R0.alloc(V, st)); CU(b->W.alloc(V, st)); }
+  if (on_device) {
+    vistio_status r = factor_on_device(ctx, b, solvers, n, hi, sn, rows);
+    if (r != VISTIO_OK) return r;
+    if (!b->refine) { b->a_ptr.reset(); b->a_col.reset(); b->a_val.reset(); }
   }
   CU(b->grad.alloc(V, st)); CU(b->grad_up.alloc(V, st)); CU(b->lam.alloc(V, st)); CU(b->fin_n.alloc(V, st));
   CU(cudaMemsetAsync(b->lam.p, 0, V * sizeof(float4), st));
@@ -651,8 +800,10 @@ vistio_status init_common(vistio_ctx* ctx, const vistio_mesh_desc* mesh, const v
   s->ctx = ctx;
   s->cfg = *cfg;
   int st = 0;
+  SetupParams sp = prm;
+  sp.numeric = cfg->host_factorization != 0;
   std::string err = build_instance(mesh->vertex_count, mesh->pos_x, mesh->pos_y, mesh->pos_z, mesh->triangle_count,
-                                   mesh->indices, pin.data(), prm, s->setup, &st);
+                                   mesh->indices, pin.data(), sp, s->setup, &st);
   if (!err.empty()) {
     vistio_status code = st == 1 ? VISTIO_ERR_INVALID_MESH : st == 11 ? VISTIO_ERR_NOT_SPD : VISTIO_ERR_INVALID_CONFIG;
     return fail(ctx, code, err);
@@ -1031,6 +1182,13 @@ vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* ni, uint64_t* t
   return VISTIO_OK;
 }
 
+vistio_status vistio_batch_factor_stats(const vistio_batch* b, uint32_t* launches, float* device_ms) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  if (launches) *launches = b->factor_launches;
+  if (device_ms) *device_ms = b->factor_ms;
+  return VISTIO_OK;
+}
+
 vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* launches) {
   if (!b || !launches) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
   *launches = b->graph_ipc ? b->launches_ipc : b->launches_plain;
@@ -1181,8 +1339,10 @@ vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_
       if (f->A_col[p] >= i) { up_col.push_back(f->A_col[p]); up_val.push_back(f->A_val[p]); }
     up_ptr[i + 1] = uint32_t(up_col.size());
   }
+  // the host finds the ordering and the symbolic structure; the numeric
+  // factorization runs on the device (k_front) when the batch is packed
   int st = 0;
-  std::string err = factorize_csr(n, up_ptr.data(), up_col.data(), up_val.data(), nullptr, f->f, &st);
+  std::string err = factorize_csr(n, up_ptr.data(), up_col.data(), up_val.data(), nullptr, f->f, &st, false);
   if (!err.empty()) return fail(ctx, st == 11 ? VISTIO_ERR_NOT_SPD : VISTIO_ERR_INVALID_CONFIG, err);
   // Device layout: a one-instance batch with no elements.
   auto* s = new vistio_solver();
@@ -1190,6 +1350,25 @@ vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_
   s->cfg.max_iterations = 1;
   s->setup.nv = n;
   s->setup.factor = f->f;
+  {  // the symmetric matrix the upper triangle defines, rows in original order
+    std::vector<uint32_t>& P = s->setup.A_ptr;
+    P.assign(n + 1, 0);
+    for (uint32_t i = 0; i < n; ++i)
+      for (uint32_t q = up_ptr[i]; q < up_ptr[i + 1]; ++q) {
+        P[i + 1]++;
+        if (up_col[q] != i) P[up_col[q] + 1]++;
+      }
+    for (uint32_t i = 0; i < n; ++i) P[i + 1] += P[i];
+    s->setup.A_col.resize(P[n]);
+    s->setup.A_val.resize(P[n]);
+    std::vector<uint32_t> cur(P.begin(), P.end() - 1);
+    for (uint32_t i = 0; i < n; ++i)
+      for (uint32_t q = up_ptr[i]; q < up_ptr[i + 1]; ++q) {
+        const uint32_t j = up_col[q];
+        s->setup.A_col[cur[i]] = j; s->setup.A_val[cur[i]++] = up_val[q];
+        if (j != i) { s->setup.A_col[cur[j]] = i; s->setup.A_val[cur[j]++] = up_val[q]; }
+      }
+  }
   s->setup.mass.assign(n, 0.f);
   s->setup.pinned.assign(n, 0);
   s->setup.prm.matrix_dt = 1.f;
