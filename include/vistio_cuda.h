@@ -233,16 +233,25 @@ vistio_status vistio_batch_download_positions(vistio_batch* b, float* xyz);
 vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, uint64_t* total_vertices,
                                 uint64_t* total_triangles, uint64_t* total_hinges, uint64_t* factor_bytes,
                                 uint64_t* device_bytes);
-/* Autotuner of the sweeps' level schedule (no counterpart in the reference).
- * Which top-level supernodes a single warp takes and which a whole block is
- * decided by a limit on s (s + m); this times the forward and backward sweeps
- * of this batch's factor for the limits 0, 1024, 2048, 4096, 6144, 12288 and
- * 2^30 (candidate_ms, 7 entries, may be NULL) and keeps the fastest
- * (*chosen_limit). The default without tuning is 6144. Captured step graphs
- * are rebuilt on the next step. Synchronises the batch's stream. */
+/* Autotuner of the sweeps (no counterpart in the reference). Two things are
+ * chosen by timing this batch's forward and backward sweeps:
+ * - the sweep kind: 0 = one kernel launch per level of the supernodal trees;
+ *   1 = one dependency-driven launch per direction, in which each supernode
+ *   waits only for its own children (forward) or parent (backward);
+ * - which top-level supernodes a single warp takes and which a whole block,
+ *   by a limit on s (s + m): 0, 1024, 2048, 4096, 6144, 12288 and 2^30.
+ * candidate_ms (14 entries, may be NULL) receives the time of each limit for
+ * kind 0 (entries 0-6), then for kind 1 (entries 7-13); the fastest pair is
+ * kept (*chosen_limit; the kind from vistio_batch_get_sweep_mode). Without
+ * tuning: kind 1 with the limit 6144. Captured step graphs are rebuilt on the
+ * next step. Synchronises the batch's stream. */
 vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms);
-/* Sets that limit directly (any value; see vistio_batch_tune). */
+/* Sets the warp-item limit directly (any value; see vistio_batch_tune). */
 vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit);
+/* Sets the sweep kind (0 or 1; see vistio_batch_tune). */
+vistio_status vistio_batch_set_sweep_mode(vistio_batch* b, uint32_t mode);
+/* The sweep kind and warp-item limit in use. */
+vistio_status vistio_batch_get_sweep_mode(const vistio_batch* b, uint32_t* mode, uint32_t* warp_limit);
 /* The device factorization done when the batch was created (the garments
  * whose solver config has host_factorization = 0): its kernel launches (one
  * per height of the supernodal trees per group of garments) and their device

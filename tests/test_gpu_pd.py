@@ -229,10 +229,12 @@ def test_long_ribbon_steps_match_fp64(cols):
 
 
 def test_level_schedules_and_autotuner():
-    """Every candidate level schedule of the autotuner (from all top-level
+    """Every candidate schedule of the autotuner (from all top-level
     supernodes on whole blocks to every narrow one on a single warp) steps a
-    batch of uneven sheets and a long ribbon to within 1e-5 of FP64; the tuner
-    picks one of the candidates and times them all."""
+    batch of uneven sheets and a long ribbon to within 1e-5 of FP64, with
+    one launch per level and with the dependency-driven sweeps; the two sweep
+    kinds give bit-identical results (the same arithmetic per supernode). The
+    tuner picks one of the candidates and times them all."""
     dt = 1.0 / 120.0
     meshes = [(scenarios.hanging_sheet(40, 1.0), 1.0 / 60.0), (scenarios.hanging_sheet(23, 0.6), 1.0 / 60.0),
               (scenarios.self_fold(30, 400, 0.2, 2.0, lowest=0.5), dt)]
@@ -240,24 +242,55 @@ def test_level_schedules_and_autotuner():
     for lim in api.Batch.TUNE_LIMITS:
         for mesh, h in meshes:
             setup = api.SetupDesc(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0, matrix_dt=h)
-            s = api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
-            batch = api.Batch([s])
-            batch.set_warp_limit(lim)
+            out = {}
+            for mode in api.Batch.SWEEP_MODES:
+                s = api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
+                batch = api.Batch([s])
+                batch.set_warp_limit(lim)
+                batch.set_sweep_mode(mode)
+                assert batch.sweep_mode() == (mode, lim)
+                batch.step(h, 2)
+                out[mode] = batch.state(0)[0]
             ref = O.OracleSim(mesh, O.init_params(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0, matrix_dt=h),
                               O.default_config(max_iterations=10), precision=1)
-            batch.step(h, 2)
             ref.step(h)
             ref.step(h)
-            e = rel(batch.state(0)[0], ref.state()[0])
+            e = rel(out["levels"], ref.state()[0])
             assert e <= 1e-5, (lim, mesh.nv, e)
+            assert np.array_equal(out["levels"], out["dataflow"]), (lim, mesh.nv)
     solvers = [api.ProjectiveDynamicsSolver().init(scenarios.hanging_sheet(sd, 1.0), cfg,
                                                    pinned=scenarios.hanging_sheet(sd, 1.0).pinned) for sd in (31, 47, 64)]
     batch = api.Batch(solvers)
     t = batch.tune()
     print(t)
     assert t["warp_item_limit"] in api.Batch.TUNE_LIMITS
-    assert all(v > 0 for v in t["sweep_ms"].values())
+    assert t["sweep_mode"] in api.Batch.SWEEP_MODES
+    assert batch.sweep_mode() == (t["sweep_mode"], t["warp_item_limit"])
+    assert all(v > 0 for m in t["sweep_ms"].values() for v in m.values())
     batch.step(1.0 / 60.0, 1)
+
+
+def test_dataflow_sweeps_match_levels_on_a_mixed_batch():
+    """A batch of many garments of different sizes (so that the dependency-
+    driven sweeps interleave supernodes of different levels and garments)
+    steps bit-identically with both sweep kinds, plain and with IPC."""
+    sides = [12, 37, 20, 64, 9, 48, 31, 25] * 3
+    cfg = api.drape_config(max_iterations=10, al_max_iterations=3, barrier_d_hat=1e-3, barrier_kappa=1e4)
+    contact = api.Contact(has_ground=True, ground_height=0.6, kappa=1e4)
+    res = {}
+    for mode in api.Batch.SWEEP_MODES:
+        solvers = []
+        for k, sd in enumerate(sides):
+            m = scenarios.hanging_sheet(sd, 0.5 + 0.03 * k)
+            setup = api.SetupDesc(stiffness=800.0 + 50 * k, bend_stiffness=1e-4, density_gsm=150.0)
+            solvers.append(api.ProjectiveDynamicsSolver().init_explicit(m, cfg, setup, pinned=m.pinned))
+        batch = api.Batch(solvers)
+        batch.set_sweep_mode(mode)
+        batch.step(DT, 3)
+        batch.step(DT, 3, contact=contact)
+        res[mode] = [batch.state(k)[0] for k in range(len(sides))]
+    for a, b in zip(res["levels"], res["dataflow"]):
+        assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("side,length", [(20, 1.0), (48, 1.5)])

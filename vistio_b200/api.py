@@ -390,17 +390,32 @@ class Batch:
 
     TUNE_LIMITS = (0, 1024, 2048, 4096, 6144, 12288, 1 << 30)
 
+    SWEEP_MODES = ("levels", "dataflow")
+
     def tune(self) -> dict:
-        """Autotunes the sweeps' level schedule on this batch (vistio_batch_tune):
-        returns the chosen warp-item limit and the sweep time of each candidate."""
+        """Autotunes the sweeps on this batch (vistio_batch_tune): returns the
+        chosen sweep kind and warp-item limit, and the sweep time of every
+        candidate (per kind, per limit)."""
         chosen = C.c_uint32()
-        ms = (C.c_float * 7)()
+        ms = (C.c_float * 14)()
         L.check(L.lib().vistio_batch_tune(self.h, C.byref(chosen), ms), self.ctx.h)
-        return {"warp_item_limit": chosen.value,
-                "sweep_ms": {str(lim): float(ms[i]) for i, lim in enumerate(self.TUNE_LIMITS)}}
+        return {"sweep_mode": self.sweep_mode()[0], "warp_item_limit": chosen.value,
+                "sweep_ms": {mode: {str(lim): float(ms[7 * m + i]) for i, lim in enumerate(self.TUNE_LIMITS)}
+                             for m, mode in enumerate(self.SWEEP_MODES)}}
 
     def set_warp_limit(self, limit: int):
         L.check(L.lib().vistio_batch_set_warp_limit(self.h, int(limit)), self.ctx.h)
+
+    def set_sweep_mode(self, mode: str):
+        """"levels": one launch per level; "dataflow": one dependency-driven
+        launch per direction."""
+        L.check(L.lib().vistio_batch_set_sweep_mode(self.h, self.SWEEP_MODES.index(mode)), self.ctx.h)
+
+    def sweep_mode(self) -> tuple:
+        """(sweep kind, warp-item limit) in use."""
+        m, lim = C.c_uint32(), C.c_uint32()
+        L.check(L.lib().vistio_batch_get_sweep_mode(self.h, C.byref(m), C.byref(lim)), self.ctx.h)
+        return self.SWEEP_MODES[m.value], lim.value
 
     def launch_phase(self, phase: str):
         L.check(L.lib().vistio_batch_launch_phase(self.h, self.PHASES[phase]), self.ctx.h)

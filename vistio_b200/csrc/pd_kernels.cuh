@@ -126,6 +126,17 @@ struct BatchDev {
   float4* U;                   // forward updates, one per (supernode, panel row)
   const uint32_t* lvl_items;   // supernodes of each batch level (block items first)
   const uint2* sub_items;      // bottom subtrees: (first, last) supernode of each
+  // dependency-driven sweeps (k_sweep): work units in forward order (see
+  // SweepUnit), the supernodal tree, per-supernode counters (zero between
+  // sweeps) and the two work queues
+  const uint2* df_units;
+  const uint32_t* df_parent;   // parent supernode (global id) or kNoParent
+  const uint32_t* df_nkids;
+  const uint32_t* df_kid_ptr;
+  const uint32_t* df_kids;
+  uint32_t* df_cnt;            // forward: children finished
+  uint32_t* df_flag;           // backward: parent finished
+  uint32_t* df_queue;          // next unit: [0] forward, [1] backward
   // FP64 refinement: the factored matrix A (f64, rows and columns in each
   // instance's solve order, global row ids), the right-hand side the first
   // sweep solved (R0) and the correction vector the refinement sweeps solve in
@@ -422,7 +433,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
 __device__ __forceinline__ void mbar_fence_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// One thread: expect `bytes` on the barrier and start the bulk copy.
+// One thread: expect `bytes` on the barrier and start the bulk copy. Callers
+// reconverge the issuing warp (__syncwarp) before any lane polls the barrier:
+// a warp whose other lanes spin in mbar_wait while the issuing lane sits on
+// the other side of a branch was seen to run the spinning side until its poll
+// budget ran out, the copy never issued.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
@@ -488,6 +503,7 @@ __device__ __forceinline__ const float* stage(Team& tm, const float* __restrict_
   const uintptr_t hi = (a + uintptr_t(n) * 4 + 15) & ~uintptr_t(15);
   tm.sync();  // previous readers of the buffer are done
   if (tm.rank == 0) bulk_g2s(tm.buf, reinterpret_cast<const void*>(lo), uint32_t(hi - lo), tm.bar);
+  __syncwarp();  // the issuing lane first: polling lanes must not starve it
   bool ok = mbar_wait(tm.bar, tm.parity);
   tm.parity ^= 1u;
   if (!ok) {
@@ -506,6 +522,7 @@ __device__ __forceinline__ void stage_issue(Team& tm, const float* __restrict__ 
   const uintptr_t hi = (a + uintptr_t(n) * 4 + 15) & ~uintptr_t(15);
   tm.sync();
   if (tm.rank == 0) bulk_g2s(tm.buf, reinterpret_cast<const void*>(lo), uint32_t(hi - lo), tm.bar);
+  __syncwarp();
 }
 __device__ __forceinline__ const float* stage_wait(Team& tm, const float* __restrict__ src, uint32_t* status) {
   const bool ok = mbar_wait(tm.bar, tm.parity);
@@ -525,7 +542,7 @@ __device__ __forceinline__ void sn_pull(const BatchDev& B, const Team& tm, const
     float4 t = Y[f + c];
     uint32_t q = B.fwd_ptr[vb + f + c], qe = B.fwd_ptr[vb + f + c + 1];
 #pragma unroll 4
-    for (; q < qe; ++q) t = f4_sub(t, B.U[B.fwd[q]]);
+    for (; q < qe; ++q) t = f4_sub(t, __ldcg(B.U + B.fwd[q]));
     tm.v0[c] = t;
   }
 }
@@ -671,7 +688,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
     for (uint32_t j0 = 0; j0 < m; j0 += tm.xcap) {
       const uint32_t nr = min(tm.xcap, m - j0);
       tm.sync();
-      for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = Y[Rr[j0 + j]];
+      for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = __ldcg(Y + Rr[j0 + j]);
       if (!Ds) Ds = stage_wait(tm, D, B.status);
       tm.sync();
       if (part < parts) {
@@ -701,7 +718,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
     for (uint32_t j0 = 0; j0 < m; j0 += rc) {
       uint32_t nr = min(rc, m - j0);
       tm.sync();  // previous readers of xg are done
-      for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = Y[Rr[j0 + j]];
+      for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = __ldcg(Y + Rr[j0 + j]);
       const float* Ps = stage(tm, Pp + uint64_t(j0) * s, nr * s, B.status);
       tm.sync();
       if (c < s && part < parts)
@@ -752,6 +769,7 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
   const uint32_t bytes = uint32_t(end - F.d_off) * 4u;
   tm.sync();  // previous readers of the buffer are done
   if (tm.rank == 0) bulk_g2s(tm.buf, src, bytes, tm.bar);
+  __syncwarp();
   const uint32_t c0 = F.first, c1 = Lz.first + Lz.ncols, nc = c1 - c0;
   float4* Yg = B.Y + F.vbase;
   float4* acc = tm.v1;  // rows c0 .. c1 of this instance (nc <= vcap, enforced by the set-up)
@@ -804,7 +822,7 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
         tm.sync();
         for (uint32_t j = tm.rank; j < nr; j += tm.size) {
           const uint32_t r = Rr[j0 + j];
-          tm.xg[j] = r < c1 ? acc[r - c0] : Yg[r];
+          tm.xg[j] = r < c1 ? acc[r - c0] : __ldcg(Yg + r);
         }
         tm.sync();
         if (part < parts) {
@@ -899,6 +917,128 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_subtree(B
 }
 
 // Clears the per-instance residual sums before a sweep.
+// ---------------------------------------------- dependency-driven sweeps
+// One launch per direction instead of one per level. Blocks stay resident and
+// take work units from a global queue in a topological order of the
+// supernodal tree (forward: bottom subtrees, then the top levels upwards;
+// backward: the reverse), so a unit only waits for units handed out before
+// it, whose blocks are running: no deadlock whatever the number of resident
+// blocks. A unit waits for its own inputs only, not for the whole level
+// below it:
+//   forward   a top supernode waits until all its children have pushed their
+//             updates (df_cnt counts them), then counts itself in at its parent;
+//   backward  a supernode or bottom subtree waits until its parent has its
+//             final values (df_flag), then flags its own children.
+// A waiting supernode resets its counter once the wait is over (no one
+// writes it again in this sweep), so the counters are zero between sweeps.
+// Writers fence before they signal; readers of data produced in the same
+// launch (U, ancestors' Y) load it through L2 (__ldcg). Every wait is
+// bounded; a wait that gives up sets status bit 4, and every later wait
+// returns at once, so a failing sweep ends quickly with the error recorded.
+//
+// SweepUnit (uint2): x = kind | count << 2; kind 0: `count` bottom subtrees
+// from sub_items[y]; kind 1: the top supernode y with the whole block; kind
+// 2: `count` top supernodes, one per warp, from lvl_items[y].
+constexpr uint32_t kNoParent = 0xffffffffu;
+constexpr uint32_t kDepPolls = 1u << 21;
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits (bounded) until *word >= target; false if it gave up or an earlier
+// wait of the batch did.
+__device__ __forceinline__ bool dep_wait(const BatchDev& B, const uint32_t* word, uint32_t target) {
+  for (uint32_t it = 0; it < kDepPolls; ++it) {
+    if (ld_acquire_u32(word) >= target) return true;
+    if ((it & 31u) == 31u && (*reinterpret_cast<volatile uint32_t*>(B.status) & 4u)) return false;
+    __nanosleep(64);
+  }
+  atomicOr(B.status, 4u);
+  return false;
+}
+
+// Forward: wait for the children of supernode k; backward: for its parent.
+template <int DIR>
+__device__ __forceinline__ void dep_enter(const BatchDev& B, uint32_t k) {
+  if (DIR == 0) {
+    const uint32_t need = B.df_nkids[k];
+    if (need && dep_wait(B, B.df_cnt + k, need)) B.df_cnt[k] = 0u;
+  } else if (B.df_parent[k] != kNoParent) {
+    if (dep_wait(B, B.df_flag + k, 1u)) B.df_flag[k] = 0u;
+  }
+}
+
+// Forward: count k in at its parent; backward: release k's children (lanes
+// `rank` of `size` share the children).
+template <int DIR>
+__device__ __forceinline__ void dep_leave(const BatchDev& B, uint32_t k, uint32_t rank, uint32_t size) {
+  if (DIR == 0) {
+    const uint32_t p = B.df_parent[k];
+    if (rank == 0 && p != kNoParent) atomicAdd(B.df_cnt + p, 1u);
+  } else {
+    for (uint32_t q = B.df_kid_ptr[k] + rank, qe = B.df_kid_ptr[k + 1]; q < qe; q += size)
+      atomicExch(B.df_flag + B.df_kids[q], 1u);
+  }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_sweep(BatchDev B, uint32_t nunits) {
+  extern __shared__ float4 smem4[];
+  __shared__ uint64_t s_bar[kSolveWarps + 1];
+  __shared__ uint32_t s_abort, s_unit;
+  SweepTeams t = make_teams(smem4, s_bar, &s_abort);
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // the other direction's queue restarts for its next launch (it is not running)
+  if (blockIdx.x == 0 && tid == 0) B.df_queue[DIR ^ 1] = 0u;
+  const bool ipc = B.prm->ipc != 0;
+  for (;;) {
+    __syncthreads();  // every warp is done with the previous unit
+    if (tid == 0) s_unit = atomicAdd(B.df_queue + DIR, 1u);
+    __syncthreads();
+    const uint32_t q = s_unit;
+    if (q >= nunits) break;
+    const uint2 u = B.df_units[DIR == 0 ? q : nunits - 1 - q];
+    const uint32_t kind = u.x & 3u, count = u.x >> 2;
+    if (kind == 1) {
+      const uint32_t k = u.y;
+      const SnDev S = B.sn[k];
+      if (ipc && B.red[S.inst].al_done) continue;
+      if (tid == 0) dep_enter<DIR>(B, k);
+      __syncthreads();
+      if (DIR == 0) sn_forward(B, t.bt, S);
+      else sn_backward(B, t.bt, S);
+      __threadfence();
+      __syncthreads();
+      dep_leave<DIR>(B, k, tid, 32 * kSolveWarps);
+    } else if (warp < count) {
+      if (kind == 0) {
+        const uint2 it = B.sub_items[u.y + warp];
+        if (ipc && B.red[B.sn[it.x].inst].al_done) continue;
+        if (DIR == 1 && lane == 0) dep_enter<1>(B, it.y);
+        __syncwarp();
+        subtree_sweep<DIR>(B, t.wt, it.x, it.y);
+        __threadfence();
+        __syncwarp();
+        if (DIR == 0) dep_leave<0>(B, it.y, lane, 32);
+      } else {
+        const uint32_t k = B.lvl_items[u.y + warp];
+        const SnDev S = B.sn[k];
+        if (ipc && B.red[S.inst].al_done) continue;
+        if (lane == 0) dep_enter<DIR>(B, k);
+        __syncwarp();
+        if (DIR == 0) sn_forward(B, t.wt, S);
+        else sn_backward(B, t.wt, S);
+        __threadfence();
+        __syncwarp();
+        dep_leave<DIR>(B, k, lane, 32);
+      }
+    }
+  }
+}
+
 __global__ void k_red_reset(BatchDev B, uint32_t ninst) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ninst) return;

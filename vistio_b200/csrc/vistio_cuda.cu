@@ -35,6 +35,7 @@ struct vistio_ctx {
   std::mutex mu;
   int refs = 0;
   bool closed = false;
+  uint32_t sweep_blocks = 0;  // resident k_sweep blocks on this device (SMs x blocks per SM)
 };
 
 namespace {
@@ -161,6 +162,12 @@ struct vistio_batch {
   std::vector<SnDev> sn_host;                       // supernode table, for re-scheduling
   uint32_t warp_limit = kWarpItemLimit;             // s (s + m) limit of a warp item
   float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
+  // sweeps: 0 = one launch per level (k_level), 1 = dependency-driven (k_sweep)
+  uint32_t sweep_mode = 1;
+  std::vector<uint2> units_host;                    // k_sweep work units in forward order
+  uint32_t n_units = 0;
+  DevBuf<uint2> df_units;
+  DevBuf<uint32_t> df_parent, df_nkids, df_kid_ptr, df_kids, df_cnt, df_flag, df_queue;
   DevBuf<SnDev> sn;
   DevBuf<float4> U;
   DevBuf<InstRed> red;
@@ -217,7 +224,30 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
     items.insert(items.end(), wrp[l].begin(), wrp[l].end());
   }
   b->warp_limit = limit;
+  // k_sweep units in forward order: bottom subtrees by eight, then each level's
+  // block supernodes one by one and its warp supernodes by eight
+  b->units_host.clear();
+  for (uint32_t q = 0; q < b->n_sub; q += kSolveWarps)
+    b->units_host.push_back(make_uint2(0u | (std::min(kSolveWarps, b->n_sub - q) << 2), q));
+  for (uint32_t l = 0; l < L; ++l) {
+    const uint32_t off = b->lvl_off[l], nb = b->lvl_nb[l], nw = b->lvl_nw[l];
+    for (uint32_t i = 0; i < nb; ++i) b->units_host.push_back(make_uint2(1u | (1u << 2), items[off + i]));
+    for (uint32_t i = 0; i < nw; i += kSolveWarps)
+      b->units_host.push_back(make_uint2(2u | (std::min(kSolveWarps, nw - i) << 2), off + nb + i));
+  }
+  b->n_units = uint32_t(b->units_host.size());
   return items;
+}
+
+// Uploads a schedule from schedule_levels (the unit buffer holds the largest
+// possible count, every top supernode its own unit).
+cudaError_t upload_schedule(vistio_batch* b, const std::vector<uint32_t>& items, cudaStream_t st) {
+  cudaError_t e = cudaSuccess;
+  if (!items.empty()) e = cudaMemcpyAsync(b->lvl_items.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !b->units_host.empty())
+    e = cudaMemcpyAsync(b->df_units.p, b->units_host.data(), b->units_host.size() * sizeof(uint2),
+                        cudaMemcpyHostToDevice, st);
+  return e;
 }
 inline uint64_t pad4(uint64_t n) { return (n + 3) & ~3ull; }
 float estimate_kappa(const vistio_solver_config& c, const InstanceSetup& I);
@@ -503,7 +533,26 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     b->refine = b->cfg.refinement_sweeps;
   }
   b->sn_host = sn;
+  b->n_sub = uint32_t(subs.size());
   std::vector<uint32_t> items = schedule_levels(b, b->warp_limit);
+  // the supernodal tree for the dependency-driven sweeps (global ids)
+  std::vector<uint32_t> df_parent(NSN, kNoParent), df_nkids(NSN, 0), df_kid_ptr(NSN + 1, 0), df_kids;
+  for (uint32_t k = 0; k < n; ++k) {
+    const Factor& F = solvers[k]->setup.factor;
+    const uint32_t base = hi[k].sn_base;
+    for (uint32_t q = 0; q < F.sn.size(); ++q)
+      if (F.sn[q].parent != UINT32_MAX) {
+        df_parent[base + q] = base + F.sn[q].parent;
+        df_nkids[base + F.sn[q].parent]++;
+      }
+  }
+  for (uint64_t g = 0; g < NSN; ++g) df_kid_ptr[g + 1] = df_kid_ptr[g] + df_nkids[g];
+  df_kids.resize(df_kid_ptr[NSN]);
+  {
+    std::vector<uint32_t> cur(df_kid_ptr.begin(), df_kid_ptr.end() - 1);
+    for (uint64_t g = 0; g < NSN; ++g)
+      if (df_parent[g] != kNoParent) df_kids[cur[df_parent[g]]++] = uint32_t(g);
+  }
   // vertex incidence
   for (uint64_t t = 0; t < T; ++t) { vtri_ptr[tri_idx[t].x + 1]++; vtri_ptr[tri_idx[t].y + 1]++; vtri_ptr[tri_idx[t].z + 1]++; }
   for (uint64_t h = 0; h < H; ++h) {
@@ -541,7 +590,13 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->sn.upload(sn, st)); CU(b->rows.upload(rows, st)); CU(b->vals.upload(vals, st));
   CU(b->lvl_items.upload(items, st));
   CU(b->sub_items.upload(subs, st));
-  b->n_sub = uint32_t(subs.size());
+  CU(b->df_units.alloc((b->n_sub + kSolveWarps - 1) / kSolveWarps + b->top.size() + 1, st));
+  CU(upload_schedule(b, items, st));
+  CU(b->df_parent.upload(df_parent, st)); CU(b->df_nkids.upload(df_nkids, st));
+  CU(b->df_kid_ptr.upload(df_kid_ptr, st)); CU(b->df_kids.upload(df_kids, st));
+  CU(b->df_cnt.alloc(NSN, st)); CU(cudaMemsetAsync(b->df_cnt.p, 0, NSN * 4, st));
+  CU(b->df_flag.alloc(NSN, st)); CU(cudaMemsetAsync(b->df_flag.p, 0, NSN * 4, st));
+  CU(b->df_queue.alloc(2, st)); CU(cudaMemsetAsync(b->df_queue.p, 0, 8, st));
   CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
   CU(b->U.alloc(rows.size(), st));
   if (have_a) { CU(b->a_ptr.upload(a_ptr, st)); CU(b->a_col.upload(a_col, st)); CU(b->a_val.upload(a_val, st)); }
@@ -563,7 +618,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   b->factor_bytes = vals.size() * sizeof(float) + sn.size() * sizeof(SnDev) + rows.size() * 4 + fwd.size() * 4 +
                     fwd_ptr.size() * 4 + items.size() * 4 + rows.size() * 16;
   b->device_bytes = b->factor_bytes + V * (16 * 10 + 4 + 3 + 4 * 3) + T * (16 + 16 + 4 + 36 + 12) +
-                    H * (16 + 16 + 8 + 16 + 16) + (V + 1) * 8;
+                    H * (16 + 16 + 8 + 16 + 16) + (V + 1) * 8 + NSN * 28 + b->df_units.n * 8;
   if (b->refine) b->device_bytes += (V + 1) * 4 + a_col.size() * 12 + V * 32;
   BatchDev& d = b->dev;
   d.inst = b->inst.p; d.tri_chunks = b->tri_chunks.p; d.hinge_chunks = b->hinge_chunks.p; d.vtx_chunks = b->vtx_chunks.p;
@@ -574,6 +629,9 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   d.perm_local = b->perm_local.p; d.row_vertex = nullptr; d.Y = b->Y.p; d.T = b->Tm.p;
   d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.lvl_items = b->lvl_items.p; d.sub_items = b->sub_items.p;
   d.fwd_ptr = b->fwd_ptr.p; d.fwd = b->fwd.p; d.U = b->U.p;
+  d.df_units = b->df_units.p; d.df_parent = b->df_parent.p; d.df_nkids = b->df_nkids.p;
+  d.df_kid_ptr = b->df_kid_ptr.p; d.df_kids = b->df_kids.p; d.df_cnt = b->df_cnt.p; d.df_flag = b->df_flag.p;
+  d.df_queue = b->df_queue.p;
   d.a_ptr = b->a_ptr.p; d.a_col = b->a_col.p; d.a_val = b->a_val.p; d.R0 = b->R0.p; d.W = b->W.p;
   d.grad = b->grad.p; d.grad_up = b->grad_up.p; d.lam = b->lam.p; d.fin_n = b->fin_n.p;
   d.in_contact = b->in_contact.p; d.in_contact_up = b->in_contact_up.p; d.ever = b->ever.p;
@@ -638,6 +696,12 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
 // Forward then backward sweep, level by level over the whole batch, in place
 // on dv.Y (right-hand side in, solution out). Returns the launches.
 uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
+  if (b->sweep_mode == 1 && b->n_units) {
+    const uint32_t grid = std::min(b->n_units, b->ctx->sweep_blocks);
+    k_sweep<0><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units);
+    k_sweep<1><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units);
+    return 2;
+  }
   uint32_t L = uint32_t(b->lvl_off.size()), n = 0;
   const uint32_t sub_grid = (b->n_sub + kSolveWarps - 1) / kSolveWarps;
   if (sub_grid) { k_subtree<0><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_sub); ++n; }
@@ -864,6 +928,14 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   CU(cudaFuncSetAttribute(k_level<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_subtree<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_subtree<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_sweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  {
+    int per_sm = 0, sms = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<0>, kSolveThreads, kSolveSmem));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    c->sweep_blocks = uint32_t(std::max(1, per_sm) * std::max(1, sms));
+  }
   *out = c.release();
   return VISTIO_OK;
 }
@@ -1197,10 +1269,19 @@ vistio_status vistio_batch_launches_per_step(const vistio_batch* b, uint32_t* la
 
 void* vistio_batch_stream(vistio_batch* b) { return b ? (void*)b->ctx->stream : nullptr; }
 
-// Level-schedule autotuner. The candidate warp-item limits of s (s + m):
-// 0 (every top supernode for a block) ... 2^30 (every one of at most
-// kWarpVec columns for a warp).
+// Sweep autotuner. The candidates are the two sweep kinds (one launch per
+// level; dependency-driven) times the warp-item limits of s (s + m): 0 (every
+// top supernode for a block) ... 2^30 (every one of at most kWarpVec columns
+// for a warp).
 static const uint32_t kTuneLimits[7] = {0u, 1024u, 2048u, 4096u, 6144u, 12288u, 1u << 30};
+
+namespace {
+vistio_status drop_graphs(vistio_batch* b) {  // captured steps bake the schedule into their launches
+  if (b->graph_plain) { cudaGraphExecDestroy(b->graph_plain); b->graph_plain = nullptr; }
+  if (b->graph_ipc) { cudaGraphExecDestroy(b->graph_ipc); b->graph_ipc = nullptr; }
+  return VISTIO_OK;
+}
+}  // namespace
 
 vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms) {
   if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
@@ -1213,11 +1294,11 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
   float best = 0.f;
-  uint32_t best_limit = b->warp_limit;
-  for (int c = 0; c < 7; ++c) {
-    std::vector<uint32_t> items = schedule_levels(b, kTuneLimits[c]);
-    if (!items.empty())
-      CU(cudaMemcpyAsync(b->lvl_items.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st));
+  uint32_t best_limit = b->warp_limit, best_mode = b->sweep_mode;
+  for (int c = 0; c < 14; ++c) {
+    b->sweep_mode = uint32_t(c / 7);
+    std::vector<uint32_t> items = schedule_levels(b, kTuneLimits[c % 7]);
+    CU(upload_schedule(b, items, st));
     CU(cudaMemsetAsync(b->Y.p, 0, b->V * sizeof(float4), st));
     launch_sweeps(b, b->dev, st);  // warm-up
     CU(cudaEventRecord(e0, st));
@@ -1228,17 +1309,19 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
     CU(cudaEventElapsedTime(&ms, e0, e1));
     ms /= 3.f;
     if (candidate_ms) candidate_ms[c] = ms;
-    if (c == 0 || ms < best) { best = ms; best_limit = kTuneLimits[c]; }
+    if (c == 0 || ms < best) { best = ms; best_limit = kTuneLimits[c % 7]; best_mode = b->sweep_mode; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  uint32_t status = 0;
+  CU(cudaMemcpyAsync(&status, b->status.p, sizeof(status), cudaMemcpyDeviceToHost, st));
+  b->sweep_mode = best_mode;
   std::vector<uint32_t> items = schedule_levels(b, best_limit);
-  if (!items.empty()) CU(cudaMemcpyAsync(b->lvl_items.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st));
+  CU(upload_schedule(b, items, st));
   CU(cudaStreamSynchronize(st));
+  if (status & 4u) return fail(ctx, VISTIO_ERR_TIMEOUT, "a bounded wait of the sweeps gave up while tuning");
   b->tuned_ms = best;
-  // captured steps bake the old schedule into their launches
-  if (b->graph_plain) { cudaGraphExecDestroy(b->graph_plain); b->graph_plain = nullptr; }
-  if (b->graph_ipc) { cudaGraphExecDestroy(b->graph_ipc); b->graph_ipc = nullptr; }
+  drop_graphs(b);
   if (chosen_limit) *chosen_limit = best_limit;
   return VISTIO_OK;
 }
@@ -1247,11 +1330,22 @@ vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit) {
   if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
   vistio_ctx* ctx = b->ctx;
   std::vector<uint32_t> items = schedule_levels(b, limit);
-  if (!items.empty())
-    CU(cudaMemcpyAsync(b->lvl_items.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CU(upload_schedule(b, items, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
-  if (b->graph_plain) { cudaGraphExecDestroy(b->graph_plain); b->graph_plain = nullptr; }
-  if (b->graph_ipc) { cudaGraphExecDestroy(b->graph_ipc); b->graph_ipc = nullptr; }
+  return drop_graphs(b);
+}
+
+vistio_status vistio_batch_set_sweep_mode(vistio_batch* b, uint32_t mode) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  if (mode > 1) return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "sweep mode must be 0 or 1");
+  b->sweep_mode = mode;
+  return drop_graphs(b);
+}
+
+vistio_status vistio_batch_get_sweep_mode(const vistio_batch* b, uint32_t* mode, uint32_t* warp_limit) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  if (mode) *mode = b->sweep_mode;
+  if (warp_limit) *warp_limit = b->warp_limit;
   return VISTIO_OK;
 }
 
