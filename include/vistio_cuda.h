@@ -291,6 +291,16 @@ typedef struct vistio_server_config {
   uint32_t setup_threads;     /* host threads building set-ups (>= 1) */
   uint32_t steps_per_slice;   /* steps queued per cohort ahead of the GPU (>= 1) */
   uint64_t cache_bytes;       /* host memory for cached set-ups (0: no cache) */
+  /* 0: the set-up threads compute each request's numeric factorization on the
+   * host, in parallel with the GPU's work (each request's host_factorization
+   * is overridden); 1: each request's own setting (0 = its cohort factorizes
+   * on the GPU when it starts, on the thread that calls vistio_server_tick). */
+  uint32_t gpu_factorization;
+  /* Sweep kind of every cohort (vistio_batch_set_sweep_mode): 0 = one launch
+   * per level, 1 = dependency-driven. Cohorts run side by side on their own
+   * streams, and the dependency-driven sweeps keep blocks resident that wait
+   * for one another, so 0 suits a busy server. */
+  uint32_t sweep_mode;
 } vistio_server_config;
 
 typedef struct vistio_request {

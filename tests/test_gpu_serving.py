@@ -11,6 +11,7 @@ drape requests of different sizes, materials and kinds.
   wait for memory and still complete; one that can never fit fails with
   VISTIO_ERR_OOM.
 """
+import dataclasses
 import time
 
 import numpy as np
@@ -97,7 +98,9 @@ def test_memory_budget_admission_and_oversize_request():
     import ctypes as C
     needs = []
     for r in reqs:
-        probe = api.ProjectiveDynamicsSolver().init_explicit(r["mesh"], r["config"], r["setup"], pinned=r["pinned"])
+        # as the server's set-up threads build it: factorized on the host
+        cfg = dataclasses.replace(r["config"], host_factorization=True)
+        probe = api.ProjectiveDynamicsSolver().init_explicit(r["mesh"], cfg, r["setup"], pinned=r["pinned"])
         need = C.c_uint64()
         _lib.check(_lib.lib().vistio_solver_device_bytes(probe.h, 0, C.byref(need)))
         needs.append(need.value)

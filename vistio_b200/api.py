@@ -530,9 +530,13 @@ class Server:
     allows and share the GPU with them. Results are read back per request."""
 
     def __init__(self, hbm_budget_bytes: int = 8 << 30, max_cohort: int = 64, setup_threads: int = 4,
-                 steps_per_slice: int = 10, cache_bytes: int = 1 << 30, device: int = 0):
+                 steps_per_slice: int = 10, cache_bytes: int = 1 << 30, device: int = 0,
+                 gpu_factorization: bool = False, sweep_mode: str = "levels"):
+        """gpu_factorization False: the set-up threads factorize on the host,
+        beside the GPU's work; True: each request's own host_factorization.
+        sweep_mode: the sweep kind of every cohort (Batch.SWEEP_MODES)."""
         cfg = L.ServerConfig(device, int(hbm_budget_bytes), int(max_cohort), int(setup_threads), int(steps_per_slice),
-                             int(cache_bytes))
+                             int(cache_bytes), int(bool(gpu_factorization)), Batch.SWEEP_MODES.index(sweep_mode))
         h = C.c_void_p()
         st = L.lib().vistio_server_create(C.byref(cfg), C.byref(h))
         if st != L.OK:

@@ -199,7 +199,9 @@ void setup_worker(vistio_server* S, vistio_ctx* ctx) {
     } else {
       vistio_mesh_desc m{uint32_t(r->px.size()), uint32_t(r->tris.size() / 3), r->px.data(), r->py.data(),
                          r->pz.data(), r->tris.data()};
-      st = vistio_solver_init_explicit(ctx, &m, &r->cfg, &r->setup, r->pinned.empty() ? nullptr : r->pinned.data(),
+      vistio_solver_config cfg = r->cfg;
+      if (!S->cfg.gpu_factorization) cfg.host_factorization = 1;  // in this thread, beside the GPU's work
+      st = vistio_solver_init_explicit(ctx, &m, &cfg, &r->setup, r->pinned.empty() ? nullptr : r->pinned.data(),
                                        &sol);
       if (st == VISTIO_OK && r->ipc == 0 && r->contact.has_ground)
         st = vistio_solver_set_ground(sol, 1, r->contact.ground_height);
@@ -320,6 +322,7 @@ vistio_status start_cohort(vistio_server* S, const std::vector<Request*>& take, 
   std::vector<vistio_solver*> sv;
   for (Request* r : take) sv.push_back(r->solver);
   st = vistio_batch_create(c.ctx, sv.data(), uint32_t(sv.size()), &c.batch);
+  if (st == VISTIO_OK) st = vistio_batch_set_sweep_mode(c.batch, S->cfg.sweep_mode);
   if (st != VISTIO_OK) {
     std::string err = vistio_last_error(c.ctx);
     vistio_ctx_destroy(c.ctx);
@@ -402,7 +405,8 @@ extern "C" {
 
 vistio_status vistio_server_create(const vistio_server_config* cfg, vistio_server** out) {
   if (!cfg || !out) return VISTIO_ERR_INVALID_CONFIG;
-  if (cfg->max_cohort == 0 || cfg->setup_threads == 0 || cfg->steps_per_slice == 0 || cfg->hbm_budget_bytes == 0)
+  if (cfg->max_cohort == 0 || cfg->setup_threads == 0 || cfg->steps_per_slice == 0 || cfg->hbm_budget_bytes == 0 ||
+      cfg->sweep_mode > 1)
     return VISTIO_ERR_INVALID_CONFIG;
   auto S = std::make_unique<vistio_server>();
   S->cfg = *cfg;
