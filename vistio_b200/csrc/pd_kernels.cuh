@@ -362,17 +362,20 @@ __global__ void __launch_bounds__(256) k_gather(BatchDev B, int keep_rhs) {
   float3 x = f3(B.pos[g]), q = f3(B.pred[g]);
   float cm = m * I.inv_hmat2, cr = m * P.inv_dt2;
   float3 r = (q - x) * cm + q * (cr - cm);
+  // element outputs are read-only here: non-coherent loads, and of a hinge's
+  // stencil only this vertex's weight (gather 0.313 -> 0.278 ms per iteration)
+#pragma unroll 4
   for (uint32_t e = B.vtri_ptr[g], ee = B.vtri_ptr[g + 1]; e < ee; ++e) {
-    uint32_t code = B.vtri[e];
+    uint32_t code = __ldg(B.vtri + e);
     const float* o = B.tri_out + 9ull * (code >> 2) + 3 * (code & 3u);
-    r.x += o[0]; r.y += o[1]; r.z += o[2];
+    r.x += __ldg(o); r.y += __ldg(o + 1); r.z += __ldg(o + 2);
   }
+#pragma unroll 4
   for (uint32_t e = B.vhinge_ptr[g], ee = B.vhinge_ptr[g + 1]; e < ee; ++e) {
-    uint32_t code = B.vhinge[e];
+    uint32_t code = __ldg(B.vhinge + e);
     uint32_t h = code >> 2, k = code & 3u;
-    float4 st = B.hinge_st[h];
-    float s = k == 0 ? st.x : k == 1 ? st.y : k == 2 ? st.z : st.w;
-    float4 o = B.hinge_out[h];
+    float s = __ldg(reinterpret_cast<const float*>(B.hinge_st + h) + k);
+    float4 o = __ldg(B.hinge_out + h);
     r.x += s * o.x; r.y += s * o.y; r.z += s * o.z;
   }
   if (P.ipc) {  // assemble_barrier_rhs (assembly.rs:272-282)
