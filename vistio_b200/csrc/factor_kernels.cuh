@@ -18,7 +18,8 @@
 //   invert    inv(L_kk) by forward substitution, one column per thread, kept
 //             in the (unused) strict upper triangle;
 //   write     D = inv(L_kk) and P = L_Rk in FP32 into the supernode's packed
-//             region (the row indices after P are written by the host).
+//             region, leading dimension sn_ld(s) (the row indices after P
+//             are written by the host).
 #pragma once
 #include "pd_kernels.cuh"
 
@@ -126,18 +127,19 @@ __global__ void __launch_bounds__(kFrontThreads) k_front(FrontDev D, const uint3
     }
   }
   __syncthreads();
-  float* Dv = D.vals + S.d_off;  // Linv[i][c] at c * s + i
+  const uint32_t ld = sn_ld(s);
+  float* Dv = D.vals + S.d_off;  // Linv[i][c] at c * ld + i
   for (uint32_t t = tid; t < s * s; t += kFrontThreads) {
     const uint32_t c = t / s, i = t % s;
     double v = 0.0;
     if (i == c) v = 1.0 / Fk[uint64_t(c) * nf + c];
     else if (i > c) v = Fk[uint64_t(i) * nf + c];
-    Dv[t] = float(v);
+    Dv[c * ld + i] = float(v);
   }
-  float* Pv = D.vals + S.p_off;  // P[r][c] at r * s + c
+  float* Pv = D.vals + S.p_off;  // P[r][c] at r * ld + c
   for (uint32_t t = tid; t < m * s; t += kFrontThreads) {
     const uint32_t r = t / s, c = t % s;
-    Pv[t] = float(Fk[uint64_t(c) * nf + s + r]);
+    Pv[r * ld + c] = float(Fk[uint64_t(c) * nf + s + r]);
   }
   if (tid == 0 && s_bad) atomicOr(D.status, 32u);
 }

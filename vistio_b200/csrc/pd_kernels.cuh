@@ -17,6 +17,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "setup.h"
+
 namespace vistio {
 
 struct InstDev {
@@ -32,8 +34,9 @@ struct InstDev {
 };
 
 // One supernode in HBM: one contiguous, 16-byte aligned region holding
-//   D  inv(L_kk), s x s column-major (Linv[c][c2] at c2*s + c), then
-//   P  the m x s panel below the diagonal block, row-major (P[j][c] at j*s + c),
+//   D  inv(L_kk), s x s column-major with leading dimension ld = sn_ld(s)
+//      (odd; Linv[c][c2] at c2*ld + c), then
+//   P  the m x s panel below the diagonal block, row-major (P[j][c] at j*ld + c),
 //      followed by its m row indices (u32 bits; the same as rows[rows_off..]).
 // Both sweeps stage it through shared memory in row chunks.
 struct SnDev {
@@ -556,10 +559,10 @@ __device__ __forceinline__ void sn_pull(const BatchDev& B, const Team& tm, const
 
 // y = inv(L_kk) t with the whole diagonal block in shared memory (Ds, column-major).
 __device__ __forceinline__ void sn_diag_fwd_smem(const Team& tm, const SnDev& S, const float* Ds, float4* Y) {
-  const uint32_t s = S.ncols, f = S.first;
+  const uint32_t s = S.ncols, f = S.first, ld = sn_ld(s);
   for (uint32_t c = tm.rank; c < s; c += tm.size) {
     float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, Ds[c2 * s + c], tm.v0[c2]);
+    for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, Ds[c2 * ld + c], tm.v0[c2]);
     tm.v1[c] = y;
     Y[f + c] = y;
   }
@@ -568,10 +571,10 @@ __device__ __forceinline__ void sn_diag_fwd_smem(const Team& tm, const SnDev& S,
 // U[j] = P[j,:] . y for nr rows staged at Ps (row-major, s columns).
 __device__ __forceinline__ void sn_push_rows(const BatchDev& B, const Team& tm, const SnDev& S, const float* Ps,
                                              uint32_t j0, uint32_t nr) {
-  const uint32_t s = S.ncols;
+  const uint32_t s = S.ncols, ld = sn_ld(s);
   for (uint32_t j = tm.rank; j < nr; j += tm.size) {
     float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float* row = Ps + j * s;
+    const float* row = Ps + j * ld;
     for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], tm.v1[c]);
     B.U[S.rows_off + j0 + j] = u;
   }
@@ -581,11 +584,11 @@ __device__ __forceinline__ void sn_push_rows(const BatchDev& B, const Team& tm, 
 // diagonal block and the panel are staged through the team buffer (the
 // block in column chunks when it does not fit, the panel in row chunks).
 __device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const SnDev& S) {
-  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first, ld = sn_ld(s);
   float4* Y = B.Y + S.vbase;
   const float* D = B.vals + S.d_off;
   const float* Pp = B.vals + S.p_off;
-  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * s + m;  // [D | P | rows] is one contiguous region
+  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * ld + m;  // [D | P | rows] is one contiguous region
   if (whole + 8 <= tm.cap) {
     // the whole supernode in one copy, in flight while the pull gathers
     stage_issue(tm, D, whole);
@@ -599,21 +602,21 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const Sn
     return;
   }
   sn_pull(B, tm, S, Y);
-  if (s * s + 8 <= tm.cap) {
-    const float* Ds = stage(tm, D, s * s, B.status);
+  if (s * ld + 8 <= tm.cap) {
+    const float* Ds = stage(tm, D, s * ld, B.status);
     tm.sync();
     sn_diag_fwd_smem(tm, S, Ds, Y);
   } else {
     // column chunks [c0, c1) of D; y accumulates in v1
     for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-    const uint32_t cw = max(1u, (tm.cap - 8) / s);
+    const uint32_t cw = max(1u, (tm.cap - 8) / ld);
     for (uint32_t c0 = 0; c0 < s; c0 += cw) {
       uint32_t c1 = min(s, c0 + cw);
-      const float* Dc = stage(tm, D + uint64_t(c0) * s, (c1 - c0) * s, B.status);
+      const float* Dc = stage(tm, D + uint64_t(c0) * ld, (c1 - c0) * ld, B.status);
       for (uint32_t c = c0 + tm.rank; c < s; c += tm.size) {
         float4 y = tm.v1[c];
         uint32_t ce = min(c1, c + 1);
-        for (uint32_t c2 = c0; c2 < ce; ++c2) f4_fma(y, Dc[(c2 - c0) * s + c], tm.v0[c2]);
+        for (uint32_t c2 = c0; c2 < ce; ++c2) f4_fma(y, Dc[(c2 - c0) * ld + c], tm.v0[c2]);
         tm.v1[c] = y;
       }
     }
@@ -622,10 +625,10 @@ __device__ __forceinline__ void sn_forward(const BatchDev& B, Team& tm, const Sn
   }
   tm.sync();
   if (m == 0) return;
-  const uint32_t rc = max(1u, (tm.cap - 8) / s);
+  const uint32_t rc = max(1u, (tm.cap - 8) / ld);
   for (uint32_t j0 = 0; j0 < m; j0 += rc) {
     uint32_t nr = min(rc, m - j0);
-    const float* Ps = stage(tm, Pp + uint64_t(j0) * s, nr * s, B.status);
+    const float* Ps = stage(tm, Pp + uint64_t(j0) * ld, nr * ld, B.status);
     sn_push_rows(B, tm, S, Ps, j0, nr);
   }
   tm.sync();
@@ -666,22 +669,22 @@ __device__ __forceinline__ uint32_t team_width(const Team& tm, uint32_t s) {
 
 // x = inv(L_kk)^T t with the whole diagonal block in shared memory (Ds).
 __device__ __forceinline__ void sn_diag_bwd_smem(const Team& tm, const SnDev& S, const float* Ds, float4* Y) {
-  const uint32_t s = S.ncols, f = S.first;
+  const uint32_t s = S.ncols, f = S.first, ld = sn_ld(s);
   for (uint32_t c = tm.rank; c < s; c += tm.size) {
     float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Ds[c * s + c2], tm.v0[c2]);
+    for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Ds[c * ld + c2], tm.v0[c2]);
     Y[f + c] = x;
   }
 }
 
 // Backward step of one supernode: t = y - P^T x[R]; x = inv(L_kk)^T t.
 __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const SnDev& S) {
-  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first, ld = sn_ld(s);
   float4* Y = B.Y + S.vbase;
   const float* D = B.vals + S.d_off;
   const float* Pp = B.vals + S.p_off;
   const uint32_t* Rr = B.rows + S.rows_off;
-  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * s + m;
+  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * ld + m;
   if (whole + 8 <= tm.cap) {
     // the whole supernode in one copy, in flight while y and the first
     // chunk of x[R] are gathered; columns in at most two rounds of the team
@@ -699,11 +702,11 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
       if (!Ds) Ds = stage_wait(tm, D, B.status);
       tm.sync();
       if (part < parts) {
-        const float* P0 = Ds + (S.p_off - S.d_off) + size_t(j0) * s;
+        const float* P0 = Ds + (S.p_off - S.d_off) + size_t(j0) * ld;
         if (cl < s)
-          for (uint32_t j = part; j < nr; j += parts) f4_fma(sum0, P0[j * s + cl], tm.xg[j]);
+          for (uint32_t j = part; j < nr; j += parts) f4_fma(sum0, P0[j * ld + cl], tm.xg[j]);
         if (width + cl < s)
-          for (uint32_t j = part; j < nr; j += parts) f4_fma(sum1, P0[j * s + width + cl], tm.xg[j]);
+          for (uint32_t j = part; j < nr; j += parts) f4_fma(sum1, P0[j * ld + width + cl], tm.xg[j]);
       }
     }
     if (!Ds) Ds = stage_wait(tm, D, B.status);
@@ -718,7 +721,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
   const uint32_t width = team_width(tm, s);
   const uint32_t parts = tm.size / width;
   const uint32_t cl = tm.rank % width, part = tm.rank / width;
-  const uint32_t rc = max(1u, min((tm.cap - 8) / s, tm.xcap));
+  const uint32_t rc = max(1u, min((tm.cap - 8) / ld, tm.xcap));
   for (uint32_t cb = 0; cb < s; cb += width) {
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t c = cb + cl;
@@ -726,24 +729,24 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
       uint32_t nr = min(rc, m - j0);
       tm.sync();  // previous readers of xg are done
       for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = __ldcg(Y + Rr[j0 + j]);
-      const float* Ps = stage(tm, Pp + uint64_t(j0) * s, nr * s, B.status);
+      const float* Ps = stage(tm, Pp + uint64_t(j0) * ld, nr * ld, B.status);
       tm.sync();
       if (c < s && part < parts)
-        for (uint32_t j = part; j < nr; j += parts) f4_fma(acc, Ps[j * s + c], tm.xg[j]);
+        for (uint32_t j = part; j < nr; j += parts) f4_fma(acc, Ps[j * ld + c], tm.xg[j]);
     }
     tm.sync();
     team_column_sum(tm, acc, width, parts, cb, s, tm.v1, tm.v0, true);
   }
-  if (s * s + 8 <= tm.cap) {
-    const float* Ds = stage(tm, D, s * s, B.status);
+  if (s * ld + 8 <= tm.cap) {
+    const float* Ds = stage(tm, D, s * ld, B.status);
     tm.sync();
     sn_diag_bwd_smem(tm, S, Ds, Y);
   } else {
     // column chunks of D: x_c needs column c (rows c..s-1)
-    const uint32_t cw = max(1u, (tm.cap - 8) / s);
+    const uint32_t cw = max(1u, (tm.cap - 8) / ld);
     for (uint32_t c0 = 0; c0 < s; c0 += cw) {
       uint32_t c1 = min(s, c0 + cw);
-      const float* Dc = stage(tm, D + uint64_t(c0) * s, (c1 - c0) * s, B.status);
+      const float* Dc = stage(tm, D + uint64_t(c0) * ld, (c1 - c0) * ld, B.status);
       // a chunk can be wider than the team: columns in rounds of the team width
       const uint32_t w = team_width(tm, c1 - c0), np = tm.size / w;
       const uint32_t ccl = tm.rank % w, pp = tm.rank / w;
@@ -751,7 +754,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
         const uint32_t cc = cb + ccl;
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
         if (cc < c1 && pp < np)
-          for (uint32_t r = cc + pp; r < s; r += np) f4_fma(acc, Dc[(cc - c0) * s + r], tm.v0[r]);
+          for (uint32_t r = cc + pp; r < s; r += np) f4_fma(acc, Dc[(cc - c0) * ld + r], tm.v0[r]);
         team_column_sum(tm, acc, w, np, cb, c1, nullptr, Y + f, false);
       }
     }
@@ -771,7 +774,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
 template <int DIR>
 __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint32_t first, uint32_t last) {
   const SnDev F = B.sn[first], Lz = B.sn[last];
-  const uint64_t end = Lz.p_off + ((uint64_t(Lz.nrows) * Lz.ncols + Lz.nrows + 3) & ~3ull);
+  const uint64_t end = Lz.p_off + ((uint64_t(Lz.nrows) * sn_ld(Lz.ncols) + Lz.nrows + 3) & ~3ull);
   const float* src = B.vals + F.d_off;  // 16-byte aligned: d_off is a multiple of 4
   const uint32_t bytes = uint32_t(end - F.d_off) * 4u;
   tm.sync();  // previous readers of the buffer are done
@@ -794,15 +797,15 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
     const SnDev S = B.sn[k];
     const float* Ds = base + (S.d_off - F.d_off);
     const float* Ps = base + (S.p_off - F.d_off);
-    const uint32_t s = S.ncols, m = S.nrows, f = S.first - c0;
-    const uint32_t* Rr = reinterpret_cast<const uint32_t*>(Ps + m * s);  // staged with the panel
+    const uint32_t s = S.ncols, m = S.nrows, f = S.first - c0, ld = sn_ld(s);
+    const uint32_t* Rr = reinterpret_cast<const uint32_t*>(Ps + m * ld);  // staged with the panel
     if (DIR == 0) {
       // t = acc (all descendant updates are in); y = inv(L_kk) t into acc
       for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v0[c] = acc[f + c];
       tm.sync();
       for (uint32_t c = tm.rank; c < s; c += tm.size) {
         float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, Ds[c2 * s + c], tm.v0[c2]);
+        for (uint32_t c2 = 0; c2 <= c; ++c2) f4_fma(y, Ds[c2 * ld + c], tm.v0[c2]);
         acc[f + c] = y;
       }
       tm.sync();
@@ -811,7 +814,7 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
       for (uint32_t j = tm.rank; j < m; j += tm.size) {
         const uint32_t r = Rr[j];
         float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float* row = Ps + j * s;
+        const float* row = Ps + j * ld;
         for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], acc[f + c]);
         if (r < c1) acc[r - c0] = f4_sub(acc[r - c0], u);
         else B.U[S.rows_off + j] = u;
@@ -833,11 +836,11 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
         }
         tm.sync();
         if (part < parts) {
-          const float* P0 = Ps + size_t(j0) * s;
+          const float* P0 = Ps + size_t(j0) * ld;
           if (cl < s)
-            for (uint32_t j = part; j < nr; j += parts) f4_fma(sum0, P0[j * s + cl], tm.xg[j]);
+            for (uint32_t j = part; j < nr; j += parts) f4_fma(sum0, P0[j * ld + cl], tm.xg[j]);
           if (width + cl < s)
-            for (uint32_t j = part; j < nr; j += parts) f4_fma(sum1, P0[j * s + width + cl], tm.xg[j]);
+            for (uint32_t j = part; j < nr; j += parts) f4_fma(sum1, P0[j * ld + width + cl], tm.xg[j]);
         }
       }
       tm.sync();
@@ -846,7 +849,7 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
       // x = inv(L_kk)^T t into acc
       for (uint32_t c = tm.rank; c < s; c += tm.size) {
         float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Ds[c * s + c2], tm.v0[c2]);
+        for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Ds[c * ld + c2], tm.v0[c2]);
         acc[f + c] = x;
       }
       tm.sync();

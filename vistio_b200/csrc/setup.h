@@ -38,10 +38,21 @@ constexpr uint32_t kSubtreeFloats = 1024;
 // warp keeps the subtree's slice of the vector in shared memory.
 constexpr uint32_t kSubtreeCols = 32;
 constexpr uint32_t kBottomLevel = 0xffffffffu;
-// Floats of one supernode's packed region: inv(L_kk) (s x s), then the panel
-// (m x s) followed by its m row indices, each part padded to 4 floats.
+#if defined(__CUDACC__)
+#define VISTIO_HD __host__ __device__
+#else
+#define VISTIO_HD
+#endif
+// Leading dimension of a supernode's diagonal block (column-major) and panel
+// (row-major) as packed for the GPU: s rounded up to an odd number, so that
+// 32 lanes reading one column of 32 consecutive panel rows, or one row of 32
+// consecutive diagonal-block columns, hit 32 different shared-memory banks.
+VISTIO_HD constexpr uint32_t sn_ld(uint32_t s) { return s | 1u; }
+// Floats of one supernode's packed region: inv(L_kk) (s columns of sn_ld(s)),
+// then the panel (m rows of sn_ld(s)) followed by its m row indices, each
+// part padded to 4 floats.
 inline uint64_t sn_floats(uint32_t s, uint32_t m) {
-  return ((uint64_t(s) * s + 3) & ~3ull) + ((uint64_t(m) * s + m + 3) & ~3ull);
+  return ((uint64_t(s) * sn_ld(s) + 3) & ~3ull) + ((uint64_t(m) * sn_ld(s) + m + 3) & ~3ull);
 }
 
 // Supernodal factor of P A P^T = L L^T in the layout the GPU sweeps read.

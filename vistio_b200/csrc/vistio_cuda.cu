@@ -490,19 +490,22 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       const uint32_t sc = X.ncols, m = X.nrows;
       d.first = X.first; d.ncols = sc; d.nrows = m;
       d.rows_off = uint32_t(rowsb + X.rows_off);
-      d.d_off = valsb; valsb += pad4(uint64_t(sc) * sc);
-      d.p_off = valsb; valsb += pad4(uint64_t(m) * sc + m);  // panel, then its row indices
+      const uint32_t ld = sn_ld(sc);  // odd leading dimension of D and P (bank-conflict-free reads)
+      d.d_off = valsb; valsb += pad4(uint64_t(sc) * ld);
+      d.p_off = valsb; valsb += pad4(uint64_t(m) * ld + m);  // panel, then its row indices
       d.vbase = uint32_t(v0);
       d.inst = k;
       if (X.level != kBottomLevel) b->top.push_back({X.level, uint32_t(snb + q)});
       if (F.numeric) {  // else the device factorization writes D and P
         const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
         const double* Dn = F.vals.data() + X.diag_off;    // column-major s x s
-        for (uint64_t e = 0; e < uint64_t(m) * sc; ++e) vals[d.p_off + e] = float(Pn[e]);
-        for (uint64_t e = 0; e < uint64_t(sc) * sc; ++e) vals[d.d_off + e] = float(Dn[e]);
+        for (uint64_t j = 0; j < m; ++j)
+          for (uint32_t c = 0; c < sc; ++c) vals[d.p_off + j * ld + c] = float(Pn[j * sc + c]);
+        for (uint64_t c = 0; c < sc; ++c)
+          for (uint32_t i = 0; i < sc; ++i) vals[d.d_off + c * ld + i] = float(Dn[c * sc + i]);
       }
       // the panel's row indices (u32 bits), staged with the panel by the sweeps
-      std::memcpy(vals.data() + d.p_off + uint64_t(m) * sc, F.rows.data() + X.rows_off, size_t(m) * 4);
+      std::memcpy(vals.data() + d.p_off + uint64_t(m) * ld, F.rows.data() + X.rows_off, size_t(m) * 4);
     }
     rows.insert(rows.end(), F.rows.begin(), F.rows.end());
     for (size_t q = 0; q < F.sub_first.size(); ++q)
