@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--no-baselines", action="store_true", help="skip the CPU and plain-GPU side measurements")
+    ap.add_argument("--ipc-instances", type=int, default=64,
+                    help="sphere drapes of the contact measurement (0: skip it)")
+    ap.add_argument("--ipc-only", action="store_true", help="run only the contact measurement and print it")
     ap.add_argument("--serve-seconds", type=float, default=1.0,
                     help="arrival window of the served-stream measurement (0 skips it)")
     ap.add_argument("--refine", type=int, default=None,
@@ -197,6 +200,48 @@ def reference_arm(args):
 
 
 # ----------------------------------------------------------- served stream
+def ipc_batch(n, steps=10, warmup=5, threads=None):
+    """Batched contact drapes: `n` sphere drapes with the batched workload's grid
+    sides and materials, each starting 5 mm above a sphere of radius 0.3 m (so
+    the barriers are active from the first steps), ground and sphere barriers
+    and self-collision (thickness 1.5 d_hat), d_hat 1e-3, kappa 1e4, AL <= 5,
+    15 PD iterations per AL pass; `steps` step_with_ipc steps timed with CUDA
+    events after `warmup`."""
+    import torch
+    from vistio_b200 import api, scenarios
+    specs = workload(n, 0)
+    cfg = api.drape_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=1e-3, barrier_kappa=1e4)
+    contact = api.Contact(has_ground=True, ground_height=-0.3, has_sphere=True, sphere_center=(0.0, 0.0, 0.0),
+                          sphere_radius=0.3, self_collision=True, kappa=1e4, thickness=1.5e-3)
+
+    def make(sp):
+        m = scenarios.sphere_drape(side=sp.side, length=1.5, height=0.305)
+        setup = api.SetupDesc(stiffness=sp.stretch, bend_stiffness=sp.bending, density_gsm=sp.density_gsm)
+        return api.ProjectiveDynamicsSolver().init_explicit(m, cfg, setup)
+
+    with cf.ThreadPoolExecutor(threads or (os.cpu_count() or 4)) as ex:
+        solvers = list(ex.map(make, specs))
+    batch = api.Batch(solvers)
+    tune = batch.tune()
+    for _ in range(warmup):
+        batch.step(DT, 1, contact=contact)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(batch.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        batch.step(DT, steps, contact=contact)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    info = batch.info()
+    return {"value": n * steps / (ms / 1e3), "unit": UNIT, "instances": n, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms / steps, "vertices": info["vertices"], "triangles": info["triangles"],
+            "launches_per_step": batch.launches_per_step(), "sweep": tune["sweep_mode"],
+            "how": "sphere drapes with ground, sphere and self-contact barriers (IPC, AL <= 5 x 15 iterations), "
+                   "grid sides and materials of the batched workload, CUDA events over the timed steps"}
+
+
 def served_stream(window_s, rate=200.0, seed=20261203, threads=None):
     """The served drape stream: Poisson arrivals at `rate` req/s during
     `window_s` seconds, half sphere drapes (the sphere-drape geometry at the
@@ -327,6 +372,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from vistio_b200 import api
     api._default_ctx = api.Context(local)
+    if args.ipc_only:
+        if rank == 0:
+            print(json.dumps({"ipc": ipc_batch(args.ipc_instances, args.steps, args.warmup)}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     threads = max(1, (os.cpu_count() or 1) // max(1, world))
     specs = workload(args.instances, rank)
@@ -497,6 +548,8 @@ def main():
         # accuracy of the measured run: the metric is quoted at <= 1e-4 m against FP64
         out["error_vs_fp64"] = fp64_error(specs, order, batch, args.warmup + args.steps + e2e_steps,
                                           os.cpu_count() or 1)
+        if args.ipc_instances > 0:
+            out["ipc"] = ipc_batch(args.ipc_instances)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -533,7 +533,10 @@ __device__ __forceinline__ void add_grad(double4* G, uint32_t v, V3d<double> g, 
 // candidate pair: 3+3 vertex-triangle and 9 edge-edge tests. Each test is
 // screened in FP32; those with d^2 < 10 d_hat are decided and evaluated in
 // FP64 (distance, distance gradient, barrier) and rounded once.
-__global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactView S, int mode) {
+// Compiled for four blocks per SM (64 registers, a few spills in the FP64
+// branch) instead of the two that 124 registers allow: contact batch of 64
+// sphere drapes 93 -> 86 ms per step.
+__global__ void __launch_bounds__(256, 4) k_self_grad(BatchDev B, SelfContactView S, int mode) {
   const StepParams& P = *B.prm;
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   double4* G = B.gacc;
@@ -556,9 +559,11 @@ __global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactView S
       for (int q = 0; q < 3; ++q) {
         uint32_t v = X[q];
         if (v == Yt[0] || v == Yt[1] || v == Yt[2]) continue;
-        if (excluded(S, v, Yt[0]) || excluded(S, v, Yt[1]) || excluded(S, v, Yt[2])) continue;
+        // the FP32 screen first: it is cheaper than the exclusion lists, and
+        // the two filters commute
         V3d<float> p = ld3(B.pos, v);
         if (!(pt_d2<float>(p, ta, tb, tc) < screen)) continue;
+        if (excluded(S, v, Yt[0]) || excluded(S, v, Yt[1]) || excluded(S, v, Yt[2])) continue;
         const V3d<double> p8 = cvt<double>(p), a8 = cvt<double>(ta), b8 = cvt<double>(tb), c8 = cvt<double>(tc);
         double d = pt_d2<double>(p8, a8, b8, c8);
         if (!(d < dh && d > 0.0)) continue;
@@ -576,9 +581,9 @@ __global__ void __launch_bounds__(256) k_self_grad(BatchDev B, SelfContactView S
       for (int j = 0; j < 3; ++j) {
         uint32_t a0 = ae[i][0], a1 = ae[i][1], b0 = be[j][0], b1 = be[j][1];
         if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) continue;
-        if (excluded(S, a0, b0) && excluded(S, a0, b1) && excluded(S, a1, b0) && excluded(S, a1, b1)) continue;
         V3d<float> p0 = ld3(B.pos, a0), p1 = ld3(B.pos, a1), q0 = ld3(B.pos, b0), q1 = ld3(B.pos, b1);
         if (!(ee_d2<float>(p0, p1, q0, q1) < screen)) continue;
+        if (excluded(S, a0, b0) && excluded(S, a0, b1) && excluded(S, a1, b0) && excluded(S, a1, b1)) continue;
         const V3d<double> P0 = cvt<double>(p0), P1 = cvt<double>(p1), Q0 = cvt<double>(q0), Q1 = cvt<double>(q1);
         double d = ee_d2<double>(P0, P1, Q0, Q1);
         if (!(d < dh && d > 0.0)) continue;
