@@ -166,6 +166,15 @@ typedef struct vistio_contact_desc {
   int32_t self_collision;    /* triangle self contact, 1-ring exclusion */
   float kappa;               /* barrier stiffness; <= 0 estimates it from avg vertex mass */
   float thickness;           /* C-IPC thickness for self contacts (runner: 1.5 * d_hat) */
+  /* CylinderCollider (crates/vistio-contact/src/cylinder.rs:11-21): a vertical
+   * cylinder of the given radius around (center_x, center_z) with its top face
+   * at top_y, reaching down without end (the Cusick drape pedestal). */
+  int32_t has_cylinder;
+  float cylinder_center_x, cylinder_center_z, cylinder_top_y, cylinder_radius;
+  /* BoxCollider (crates/vistio-contact/src/box_collider.rs): an axis-aligned
+   * box [box_min, box_max] (the cantilever shelf). */
+  int32_t has_box;
+  float box_min[3], box_max[3];
 } vistio_contact_desc;
 
 /* StepResult (strategy.rs:15-24) plus contact diagnostics. */

@@ -825,6 +825,70 @@ template <class R> struct Sim : SimBase {
         }
       }
     }
+    if (c.has_cylinder) {  // cylinder.rs:121-198 (gradient only: collision_pipeline.rs:305-310)
+      const R cx = R(c.cylinder_center_x), cz = R(c.cylinder_center_z), top = R(c.cylinder_top_y);
+      const R rad = R(c.cylinder_radius);
+      for (uint32_t i = 0; i < n; ++i) {
+        R dx = P[i].x - cx, dy = P[i].y - top, dz = P[i].z - cz;
+        R r = std::sqrt(dx * dx + dz * dz);
+        R d_side = r - rad, d_top = dy;
+        R gx = 0, gy = 0, gz = 0, dist_sq;
+        if (d_top <= R(0) && d_side <= R(0)) {
+          F.max_violation = rmax(F.max_violation, -rmax(d_top, d_side));
+          if (d_top > d_side) gy = R(1);
+          else if (r > R(1e-6f)) { gx = dx / r; gz = dz / r; }
+          dist_sq = R(1e-12f);
+        } else if (d_top > R(0) && d_side <= R(0)) {
+          gy = R(1);
+          dist_sq = d_top * d_top;
+        } else if (d_top <= R(0) && d_side > R(0)) {
+          if (r > R(1e-6f)) { gx = dx / r; gz = dz / r; }
+          dist_sq = d_side * d_side;
+        } else {
+          if (r > R(1e-6f)) {
+            R d = std::sqrt(d_side * d_side + d_top * d_top);
+            gx = (d_side / d) * (dx / r); gy = d_top / d; gz = (d_side / d) * (dz / r);
+          }
+          dist_sq = d_side * d_side + d_top * d_top;
+        }
+        if (dist_sq < d_hat && dist_sq > R(0)) {
+          F.active++;
+          R factor = scaled_barrier_gradient(dist_sq, d_hat, kappa) * R(2) * std::sqrt(dist_sq);
+          F.grad[i].x += factor * gx; F.grad[i].y += factor * gy; F.grad[i].z += factor * gz;
+        }
+      }
+    }
+    if (c.has_box) {  // box_collider.rs:107-200 (gradient only: collision_pipeline.rs:312-317)
+      R ctr[3], ext[3];
+      for (int k = 0; k < 3; ++k) {
+        ctr[k] = (R(c.box_min[k]) + R(c.box_max[k])) * R(0.5);
+        ext[k] = (R(c.box_max[k]) - R(c.box_min[k])) * R(0.5);
+      }
+      for (uint32_t i = 0; i < n; ++i) {
+        R d[3] = {P[i].x - ctr[0], P[i].y - ctr[1], P[i].z - ctr[2]};
+        R q[3], g[3] = {0, 0, 0};
+        for (int k = 0; k < 3; ++k) q[k] = std::fabs(d[k]) - ext[k];
+        R max_q = rmax(rmax(q[0], q[1]), q[2]);
+        R dist_sq;
+        if (max_q <= R(0)) {
+          F.max_violation = rmax(F.max_violation, -max_q);
+          int k = max_q == q[0] ? 0 : max_q == q[1] ? 1 : 2;
+          g[k] = std::copysign(R(1), d[k]);
+          dist_sq = R(1e-12f);
+        } else {
+          dist_sq = R(0);
+          for (int k = 0; k < 3; ++k)
+            if (q[k] > R(0)) { dist_sq += q[k] * q[k]; g[k] = q[k] * std::copysign(R(1), d[k]); }
+          R dl = std::sqrt(dist_sq);
+          if (dl > R(1e-6f)) for (int k = 0; k < 3; ++k) g[k] /= dl;
+        }
+        if (dist_sq < d_hat && dist_sq > R(0)) {
+          F.active++;
+          R factor = scaled_barrier_gradient(dist_sq, d_hat, kappa) * R(2) * std::sqrt(dist_sq);
+          F.grad[i].x += factor * g[0]; F.grad[i].y += factor * g[1]; F.grad[i].z += factor * g[2];
+        }
+      }
+    }
     for (uint32_t i = 0; i < n; ++i) {  // collision_pipeline.rs:324-337
       if (!F.in_contact[i]) continue;
       V3<R>& nn = F.normal[i];
@@ -885,6 +949,54 @@ template <class R> struct Sim : SimBase {
             if (t >= R(0) && t <= R(1)) mt = rmin(mt, t * R(0.9f));
           }
         }
+      }
+      min_toi = rmin(min_toi, rmax(mt, R(1e-6f)));
+    }
+    if (c.has_cylinder) {  // cylinder.rs:201-262
+      const R cx = R(c.cylinder_center_x), cz = R(c.cylinder_center_z), top = R(c.cylinder_top_y);
+      const R rad = R(c.cylinder_radius), r2 = rad * rad;
+      R mt = R(1);
+      for (uint32_t i = 0; i < n; ++i) {
+        R px0 = P0[i].x - cx, py0 = P0[i].y - top, pz0 = P0[i].z - cz;
+        R vx = (P1[i].x - cx) - px0, vy = (P1[i].y - top) - py0, vz = (P1[i].z - cz) - pz0;
+        R a = vx * vx + vz * vz, b = R(2) * (px0 * vx + pz0 * vz), cc = px0 * px0 + pz0 * pz0 - r2;
+        if (a > R(1e-8f)) {
+          R disc = b * b - R(4) * a * cc;
+          if (disc >= R(0)) {
+            R t = (-b - std::sqrt(disc)) / (R(2) * a);
+            if (t >= R(0) && t <= R(1) && py0 + t * vy <= R(0)) mt = rmin(mt, t * R(0.9f));
+          }
+        }
+        if (vy < R(-1e-8f) && py0 > R(0)) {
+          R t = -py0 / vy;
+          if (t >= R(0) && t <= R(1)) {
+            R xh = px0 + t * vx, zh = pz0 + t * vz;
+            if (xh * xh + zh * zh <= r2) mt = rmin(mt, t * R(0.9f));
+          }
+        }
+      }
+      min_toi = rmin(min_toi, rmax(mt, R(1e-6f)));
+    }
+    if (c.has_box) {  // box_collider.rs:203-251
+      R mt = R(1);
+      for (uint32_t i = 0; i < n; ++i) {
+        R p0[3] = {P0[i].x, P0[i].y, P0[i].z};
+        R v[3] = {P1[i].x - P0[i].x, P1[i].y - P0[i].y, P1[i].z - P0[i].z};
+        R t_min = R(0), t_max = R(1);
+        bool hit = true;
+        for (int k = 0; k < 3 && hit; ++k) {
+          R lo = R(c.box_min[k]), hi = R(c.box_max[k]);
+          if (std::fabs(v[k]) < R(1e-8f)) {
+            hit = p0[k] >= lo && p0[k] <= hi;
+          } else {
+            R t1 = (lo - p0[k]) / v[k], t2 = (hi - p0[k]) / v[k];
+            if (t1 > t2) std::swap(t1, t2);
+            t_min = rmax(t_min, t1);
+            t_max = rmin(t_max, t2);
+            hit = t_min <= t_max && t_max >= R(0);
+          }
+        }
+        if (hit && t_min >= R(0) && t_min <= R(1)) mt = rmin(mt, t_min * R(0.9f));
       }
       min_toi = rmin(min_toi, rmax(mt, R(1e-6f)));
     }

@@ -63,6 +63,10 @@ typedef struct orc_contact {
   int32_t bvh_faithful;     // 1: reference median-split BVH incl. its pair drop; 0: complete set
   float kappa;              // barrier stiffness (already estimated)
   float thickness;          // C-IPC thickness for self contacts (1.5 * d_hat in the runner)
+  int32_t has_cylinder;     // CylinderCollider (cylinder.rs:11-21), endless downwards
+  float cylinder_center_x, cylinder_center_z, cylinder_top_y, cylinder_radius;
+  int32_t has_box;          // BoxCollider (box_collider.rs)
+  float box_min[3], box_max[3];
 } orc_contact;
 
 typedef struct orc_step_result {

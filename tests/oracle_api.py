@@ -40,7 +40,9 @@ class Contact(C.Structure):
     _fields_ = [("has_ground", C.c_int32), ("ground_height", C.c_float), ("has_sphere", C.c_int32),
                 ("sphere_center", C.c_float * 3), ("sphere_radius", C.c_float),
                 ("self_collision", C.c_int32), ("bvh_faithful", C.c_int32), ("kappa", C.c_float),
-                ("thickness", C.c_float)]
+                ("thickness", C.c_float), ("has_cylinder", C.c_int32), ("cylinder_center_x", C.c_float),
+                ("cylinder_center_z", C.c_float), ("cylinder_top_y", C.c_float), ("cylinder_radius", C.c_float),
+                ("has_box", C.c_int32), ("box_min", C.c_float * 3), ("box_max", C.c_float * 3)]
 
 
 class StepResult(C.Structure):

@@ -5,7 +5,7 @@
   computes on the same f32 positions (bit-exact);
 * CCD: the GPU vertex-triangle hit set over those pairs equals the oracle's,
   both evaluated in FP64 (bit-exact), with the same minimum TOI;
-* IPC step (ground, sphere): every step from an identical state within 1e-5
+* IPC step (ground, sphere, cylinder, box): every step from an identical state within 1e-5
   relative of the FP64 oracle, with the same AL pass count, active contacts
   and step size. The reference's own FP32 arithmetic (the oracle's ref32 mode)
   misses that bar on these steps (up to ~8e-4: the FP32 polar decomposition of
@@ -134,6 +134,11 @@ def ipc_pair(mesh, contact: api.Contact, d_hat=1e-3, kappa=1e4, iters=15, al=5, 
     c.sphere_radius = contact.sphere_radius
     c.self_collision, c.bvh_faithful = int(contact.self_collision), 0
     c.kappa, c.thickness = contact.kappa, contact.thickness
+    c.has_cylinder = int(contact.has_cylinder)
+    (c.cylinder_center_x, c.cylinder_center_z, c.cylinder_top_y, c.cylinder_radius) = contact.cylinder
+    c.has_box = int(contact.has_box)
+    c.box_min[:] = contact.box_min
+    c.box_max[:] = contact.box_max
     if contact.has_ground:
         ref.set_ground(1, contact.ground_height)
     return gpu, ref, c
@@ -178,6 +183,83 @@ def test_sphere_drape_run_within_1e4_m(refine):
     # non-penetration of the sphere within 2 cm (bench_tests.rs:138-225)
     r = np.linalg.norm(gpu.state()[0], axis=1)
     assert r.min() >= 0.3 - 0.02
+
+
+def estimated_kappa(mesh, d_hat=1e-3):
+    """estimate_initial_kappa (barrier.rs:97-116) from the garment's mean lumped
+    vertex mass, as the runner does from its vertex mass."""
+    sim = O.OracleSim(mesh, O.init_params(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0),
+                      O.default_config())
+    m = sim.masses()
+    return float(O.lib().orc_estimate_kappa(0.0, float(m[mesh.pinned == 0].mean()), 9.81, d_hat))
+
+
+def test_cusick_drape_steps_match_fp64():
+    """The Cusick drape disc (circular_grid(0.15, 64), 829 vertices) starting
+    3 cm above the pedestal cylinder of runner.rs:83-86 (top 0.3, radius 0.09,
+    ground -0.3; cylinder.rs: barrier off the top face, the wall and the rim,
+    CCD on the wall and the top face): every step from the oracle's state
+    within 1e-5 relative of FP64, with the same AL pass count, active contacts
+    and step size; the barrier becomes active and the line search engages."""
+    mesh = scenarios.cusick_drape(height=0.33)
+    pedestal = api.Contact(has_ground=True, ground_height=-0.3, has_cylinder=True, cylinder=(0.0, 0.0, 0.3, 0.09),
+                           kappa=estimated_kappa(mesh))
+    gpu, ref, c = ipc_pair(mesh, pedestal)
+    _, ref32, _ = ipc_pair(mesh, pedestal, precision=0)
+    active, backtracked = 0, 0
+    for s in range(40):
+        e, e32, rg, r64, r32 = step_errors(gpu, ref, ref32, c, pedestal)
+        print(f"step {s}: gpu {e:.2e} ref32 {e32:.2e} active {rg.active_contacts} alpha {rg.last_alpha}")
+        assert e <= 1e-5, (s, e, e32)
+        assert rg.al_iterations == r64.al_iterations
+        assert rg.active_contacts == r64.active_contacts
+        assert rg.last_alpha == r64.last_alpha
+        active = max(active, rg.active_contacts)
+        backtracked += rg.last_alpha < 1.0
+    assert active > 0, "the disc never reached the pedestal"
+    assert backtracked > 0
+
+
+def test_cusick_drape_no_penetration():
+    """bench_tests.rs:225-300: the Cusick drape for 1 s with the reference's
+    default configuration (IPC, d_hat 1e-3, kappa from the 2 g vertex mass)
+    over a cylinder of radius 0.18 with its top at 0.2 and the ground at
+    -0.3: no vertex below the top face comes within 2 cm inside the wall."""
+    mesh = scenarios.cusick_drape()
+    cfg = api.SolverConfig()
+    kappa = O.lib().orc_estimate_kappa(cfg.barrier_kappa, 0.002, abs(cfg.gravity[1]), cfg.barrier_d_hat)
+    contact = api.Contact(has_ground=True, ground_height=-0.3, has_cylinder=True, cylinder=(0.0, 0.0, 0.2, 0.18),
+                          kappa=kappa)
+    s = api.ProjectiveDynamicsSolver().init(mesh, cfg, pinned=mesh.pinned)
+    for _ in range(60):
+        s.step_with_ipc(DT, contact)
+        x = s.state()[0]
+        below = x[:, 1] < 0.2
+        if below.any():
+            r = np.sqrt(x[below, 0] ** 2 + x[below, 2] ** 2)
+            assert r.min() >= 0.18 - 0.02, r.min()
+
+
+def test_box_drape_steps_match_fp64():
+    """A 0.6 m sheet starting 3 cm above a 0.4 x 0.2 x 0.4 m box (box_collider.rs:
+    barrier off the faces, edges and corners; slab CCD): every step from the
+    oracle's state within 1e-5 relative of FP64, with the same AL pass count,
+    active contacts and step size."""
+    mesh = scenarios.sphere_drape(side=20, length=0.6, height=0.13)
+    box = api.Contact(has_ground=True, ground_height=-0.3, has_box=True, box_min=(-0.2, -0.1, -0.2),
+                      box_max=(0.2, 0.1, 0.2), kappa=estimated_kappa(mesh))
+    gpu, ref, c = ipc_pair(mesh, box)
+    _, ref32, _ = ipc_pair(mesh, box, precision=0)
+    active = 0
+    for s in range(30):
+        e, e32, rg, r64, r32 = step_errors(gpu, ref, ref32, c, box)
+        print(f"step {s}: gpu {e:.2e} ref32 {e32:.2e} active {rg.active_contacts} alpha {rg.last_alpha}")
+        assert e <= 1e-5, (s, e, e32)
+        assert rg.al_iterations == r64.al_iterations
+        assert rg.active_contacts == r64.active_contacts
+        assert rg.last_alpha == r64.last_alpha
+        active = max(active, rg.active_contacts)
+    assert active > 0, "the sheet never reached the box"
 
 
 def test_ground_contact_steps_match_fp64():

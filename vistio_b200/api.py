@@ -134,6 +134,13 @@ class Contact:
     self_collision: bool = False
     kappa: float = 0.0
     thickness: float = 0.0
+    # CylinderCollider (cylinder.rs): (center x, center z, top y, radius), endless downwards
+    has_cylinder: bool = False
+    cylinder: tuple = (0.0, 0.0, 0.0, 0.0)
+    # BoxCollider (box_collider.rs): axis-aligned [box_min, box_max]
+    has_box: bool = False
+    box_min: tuple = (0.0, 0.0, 0.0)
+    box_max: tuple = (0.0, 0.0, 0.0)
 
     def to_c(self) -> L.ContactDesc:
         c = L.ContactDesc()
@@ -145,6 +152,12 @@ class Contact:
         c.self_collision = int(self.self_collision)
         c.kappa = float(self.kappa)
         c.thickness = float(self.thickness)
+        c.has_cylinder = int(self.has_cylinder)
+        (c.cylinder_center_x, c.cylinder_center_z, c.cylinder_top_y,
+         c.cylinder_radius) = [float(v) for v in self.cylinder]
+        c.has_box = int(self.has_box)
+        c.box_min[:] = [float(v) for v in self.box_min]
+        c.box_max[:] = [float(v) for v in self.box_max]
         return c
 
 

@@ -111,6 +111,68 @@ __global__ void __launch_bounds__(256) k_detect(BatchDev B, int mode) {
         inc = true;
       }
     }
+    // The cylinder and the box contribute barrier gradients only: the
+    // reference's pipeline gives them no contact normal (collision_pipeline.rs
+    // :305-318), so they leave in_contact / friction / damping alone.
+    if (P.has_cyl) {  // CylinderCollider::detect_ipc_contacts (cylinder.rs:121-198)
+      const double dx = double(x.x) - double(P.cyl[0]), dz = double(x.z) - double(P.cyl[1]);
+      const double dt = double(x.y) - double(P.cyl[2]);  // above the top face when > 0
+      const double r = sqrt(dx * dx + dz * dz), ds = r - double(P.cyl[3]);  // outside the wall when > 0
+      const double rmin = double(1e-6f);
+      double ex = 0.0, ey = 0.0, ez = 0.0, dsq;
+      if (dt <= 0.0 && ds <= 0.0) {  // inside: the shorter way out, a tiny distance
+        vio = fmax(vio, -fmax(dt, ds));
+        if (dt > ds) ey = 1.0;
+        else if (r > rmin) { ex = dx / r; ez = dz / r; }
+        dsq = double(1e-12f);
+      } else if (dt > 0.0 && ds <= 0.0) {  // over the top face
+        ey = 1.0;
+        dsq = dt * dt;
+      } else if (dt <= 0.0) {  // beside the wall
+        if (r > rmin) { ex = dx / r; ez = dz / r; }
+        dsq = ds * ds;
+      } else {  // above and outside: the rim
+        if (r > rmin) {
+          const double d = sqrt(ds * ds + dt * dt);
+          ex = (ds / d) * (dx / r); ey = dt / d; ez = (ds / d) * (dz / r);
+        }
+        dsq = ds * ds + dt * dt;
+      }
+      if (dsq < dh && dsq > 0.0) {
+        active++;
+        const double f = scaled_barrier_grad64(dsq, dh, kap) * 2.0 * sqrt(dsq);
+        gx += f * ex; gy += f * ey; gz += f * ez;
+      }
+    }
+    if (P.has_box) {  // BoxCollider::detect_ipc_contacts (box_collider.rs:107-200)
+      const double px[3] = {double(x.x), double(x.y), double(x.z)};
+      double d[3], q[3], e[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < 3; ++k) {
+        const double c = (double(P.box_lo[k]) + double(P.box_hi[k])) * 0.5;
+        const double h = (double(P.box_hi[k]) - double(P.box_lo[k])) * 0.5;
+        d[k] = px[k] - c;
+        q[k] = fabs(d[k]) - h;  // > 0: outside the slab of axis k
+      }
+      const double mq = fmax(fmax(q[0], q[1]), q[2]);
+      double dsq;
+      if (mq <= 0.0) {  // inside: out through the nearest face, a tiny distance
+        vio = fmax(vio, -mq);
+        const int k = mq == q[0] ? 0 : mq == q[1] ? 1 : 2;
+        e[k] = copysign(1.0, d[k]);
+        dsq = double(1e-12f);
+      } else {
+        dsq = 0.0;
+        for (int k = 0; k < 3; ++k)
+          if (q[k] > 0.0) { dsq += q[k] * q[k]; e[k] = q[k] * copysign(1.0, d[k]); }
+        const double dl = sqrt(dsq);
+        if (dl > double(1e-6f)) { e[0] /= dl; e[1] /= dl; e[2] /= dl; }
+      }
+      if (dsq < dh && dsq > 0.0) {
+        active++;
+        const double f = scaled_barrier_grad64(dsq, dh, kap) * 2.0 * sqrt(dsq);
+        gx += f * e[0]; gy += f * e[1]; gz += f * e[2];
+      }
+    }
     if (inc) {
       const double ls = nx * nx + ny * ny + nz * nz;
       if (ls > double(1e-12f)) { const double il = 1.0 / sqrt(ls); nx *= il; ny *= il; nz *= il; }
@@ -141,7 +203,8 @@ __global__ void __launch_bounds__(256) k_detect(BatchDev B, int mode) {
   (void)I;
 }
 
-// CCD step bound for the colliders (ground_plane.rs:112-134, sphere.rs:178-224)
+// CCD step bound for the colliders (ground_plane.rs:112-134, sphere.rs:178-224,
+// cylinder.rs:201-262, box_collider.rs:203-251)
 // and the backtracking sum grad . d over free vertices (pd_solver.rs:915-925).
 __global__ void __launch_bounds__(256) k_ccd(BatchDev B) {
   int4 ch = B.vtx_chunks[blockIdx.x];
@@ -180,6 +243,45 @@ __global__ void __launch_bounds__(256) k_ccd(BatchDev B) {
           }
         }
       }
+    }
+    if (P.has_cyl) {
+      const float r2 = P.cyl[3] * P.cyl[3];
+      const float px0 = x0.x - P.cyl[0], py0 = x0.y - P.cyl[2], pz0 = x0.z - P.cyl[1];
+      const float vx = (x1.x - P.cyl[0]) - px0, vy = (x1.y - P.cyl[2]) - py0, vz = (x1.z - P.cyl[1]) - pz0;
+      // the endless wall: |(p0 + t v)_xz| = r, first root, hit below the top face
+      const float a = vx * vx + vz * vz, b = 2.f * (px0 * vx + pz0 * vz), c = px0 * px0 + pz0 * pz0 - r2;
+      if (a > 1e-8f) {
+        const float disc = b * b - 4.f * a * c;
+        if (disc >= 0.f) {
+          const float t = (-b - sqrtf(disc)) / (2.f * a);
+          if (t >= 0.f && t <= 1.f && py0 + t * vy <= 0.f) toi = fminf(toi, t * 0.9f);
+        }
+      }
+      // the top face: crossing y = top inside the radius
+      if (vy < -1e-8f && py0 > 0.f) {
+        const float t = -py0 / vy;
+        if (t >= 0.f && t <= 1.f) {
+          const float xh = px0 + t * vx, zh = pz0 + t * vz;
+          if (xh * xh + zh * zh <= r2) toi = fminf(toi, t * 0.9f);
+        }
+      }
+    }
+    if (P.has_box) {  // slab test: the entry time into the box during the step
+      const float p0[3] = {x0.x, x0.y, x0.z}, v[3] = {x1.x - x0.x, x1.y - x0.y, x1.z - x0.z};
+      float tmin = 0.f, tmax = 1.f;
+      bool hit = true;
+      for (int k = 0; k < 3 && hit; ++k) {
+        if (fabsf(v[k]) < 1e-8f) {
+          hit = p0[k] >= P.box_lo[k] && p0[k] <= P.box_hi[k];
+        } else {
+          float t1 = (P.box_lo[k] - p0[k]) / v[k], t2 = (P.box_hi[k] - p0[k]) / v[k];
+          if (t1 > t2) { const float tt = t1; t1 = t2; t2 = tt; }
+          tmin = fmaxf(tmin, t1);
+          tmax = fminf(tmax, t2);
+          hit = tmin <= tmax && tmax >= 0.f;
+        }
+      }
+      if (hit && tmin >= 0.f && tmin <= 1.f) toi = fminf(toi, tmin * 0.9f);
     }
     if (!B.pinned[g]) {
       float4 gr = B.grad[g];

@@ -67,6 +67,10 @@ struct StepParams {
   int32_t self_collision;
   float kappa;
   float thickness;
+  int32_t has_cyl;
+  float cyl[4];            // center x, center z, top y, radius
+  int32_t has_box;
+  float box_lo[3], box_hi[3];
   float d_hat;             // effective (compliant) d_hat
   float max_vel;           // velocity clamp (0 = off)
   float al_tolerance, al_mu_growth, al_mu_initial;

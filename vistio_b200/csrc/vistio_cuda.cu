@@ -690,6 +690,11 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
     p.sphere_r = ct->sphere_radius;
     p.self_collision = ct->self_collision;
     p.thickness = ct->thickness;
+    p.has_cyl = ct->has_cylinder;
+    p.cyl[0] = ct->cylinder_center_x; p.cyl[1] = ct->cylinder_center_z;
+    p.cyl[2] = ct->cylinder_top_y; p.cyl[3] = ct->cylinder_radius;
+    p.has_box = ct->has_box;
+    for (int k = 0; k < 3; ++k) { p.box_lo[k] = ct->box_min[k]; p.box_hi[k] = ct->box_max[k]; }
     // explicit stiffness, else 0: each garment uses its own estimate (InstDev::kappa)
     p.kappa = ct->kappa > 0.f ? ct->kappa : (c.barrier_kappa > 0.f ? c.barrier_kappa : 0.f);
   }

@@ -10,6 +10,8 @@ parameter mapping of the drape workloads:
   first 21 vertices pinned, no contact.
 * sphere_drape: 1.5 m x 1.5 m, 64x64 cells, sheet plane y = 0.5, sphere at the
   origin r = 0.3, ground y = -0.3 (runner.rs:77-81).
+* cusick_drape: a disc of radius 0.15 m (`circular_grid`, generators.rs:174)
+  at y = 0.5 over a pedestal cylinder (top y = 0.3, r = 0.09) and the ground.
 * self_fold: 0.2 m x 2.0 m, 40x400 cells, rotated 45 degrees about x with the
   lowest point at y = 0.5, ground y = 0, self contact.
 * batched sheets: hanging sheets of random side / size / material.
@@ -52,6 +54,39 @@ def quad_grid(cols: int, rows: int, width: float, height: float):
     return px, py, pz, tris
 
 
+def circular_grid(radius: float, segments: int):
+    """Disc in the XY plane (generators.rs:174-240): a (segments // 2)^2 grid of
+    side 2 radius keeps the vertices within 1.01 radius and the cells whose
+    four corners it kept, with the quad grid's checkerboard diagonals; float32
+    with the same operation order."""
+    f32 = np.float32
+    n = segments // 2
+    w = f32(radius) * f32(2.0)
+    hw = w / f32(2.0)
+    i = np.arange(n + 1, dtype=np.float32)
+    u = (i / f32(n)).astype(np.float32)
+    x = (-hw + u * w).astype(np.float32)  # along columns
+    y = (hw - u * w).astype(np.float32)   # along rows
+    gx = np.tile(x, n + 1).astype(np.float32)
+    gy = np.repeat(y, n + 1).astype(np.float32)
+    keep = np.sqrt((gx * gx + gy * gy).astype(np.float32)).astype(np.float32) <= f32(radius) * f32(1.01)
+    vmap = np.full((n + 1) * (n + 1), -1, dtype=np.int64)
+    vmap[keep] = np.arange(int(keep.sum()))
+    tris = []
+    for j in range(n):
+        for c in range(n):
+            tl = j * (n + 1) + c
+            tr, bl = tl + 1, tl + n + 1
+            br = bl + 1
+            q = [vmap[tl], vmap[tr], vmap[bl], vmap[br]]
+            if min(q) < 0:
+                continue
+            a, b, cc, d = q
+            tris += [a, cc, b, b, cc, d] if (c + j) % 2 == 0 else [a, cc, d, a, d, b]
+    return (gx[keep].copy(), gy[keep].copy(), np.zeros(int(keep.sum()), dtype=np.float32),
+            np.asarray(tris, dtype=np.uint32).reshape(-1, 3))
+
+
 @dataclasses.dataclass
 class Mesh:
     px: np.ndarray
@@ -82,6 +117,17 @@ def hanging_sheet(side: int = 20, length: float = 1.0, height: float = 1.0) -> M
 def sphere_drape(side: int = 64, length: float = 1.5, height: float = 0.5) -> Mesh:
     """scenarios.rs:120-147 with the sheet plane at y = 0.5; nothing pinned."""
     px, py, pz, tris = quad_grid(side, side, length, length)
+    pz = py.copy()
+    py = np.full_like(px, np.float32(height))
+    return Mesh(px, py, pz, tris, np.zeros(px.shape[0], dtype=np.uint8))
+
+
+def cusick_drape(height: float = 0.5, radius: float = 0.15, segments: int = 64) -> Mesh:
+    """scenarios.rs:151-174: a disc of radius 0.15 m (circular_grid(0.15, 64)),
+    turned into the XZ plane at y = `height` (0.5 in the reference), nothing
+    pinned; the runner adds a pedestal cylinder (axis at the origin, top y =
+    0.3, radius 0.09) and the ground at y = -0.3 (runner.rs:83-86)."""
+    px, py, pz, tris = circular_grid(radius, segments)
     pz = py.copy()
     py = np.full_like(px, np.float32(height))
     return Mesh(px, py, pz, tris, np.zeros(px.shape[0], dtype=np.uint8))
