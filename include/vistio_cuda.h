@@ -223,6 +223,12 @@ vistio_status vistio_solver_set_state(vistio_solver* s, const float* px, const f
                                       const float* vx, const float* vy, const float* vz);
 vistio_status vistio_solver_get_state(vistio_solver* s, float* px, float* py, float* pz, float* vx, float* vy,
                                       float* vz);
+/* Per vertex, the magnitude of the contact barrier gradient (colliders and
+ * self contact) of the last detect of the last step_with_ipc; zeros before
+ * any contact step. No counterpart in the reference's solver API: it fills
+ * the I/O contract's VertexMetadata::contact_force (crates/vistio-io/src/
+ * contract.rs:79-88). */
+vistio_status vistio_solver_contact_force(vistio_solver* s, float* out);
 vistio_status vistio_step(vistio_solver* s, float dt, vistio_step_result* res);
 vistio_status vistio_step_with_ipc(vistio_solver* s, float dt, const vistio_contact_desc* contact,
                                    vistio_step_result* res);

@@ -118,6 +118,7 @@ SIGNATURES = {
     "vistio_solver_set_ground": (C.c_int, [_vp, C.c_int32, C.c_float]),
     "vistio_solver_set_state": (C.c_int, [_vp, _fp, _fp, _fp, _fp, _fp, _fp]),
     "vistio_solver_get_state": (C.c_int, [_vp, _fp, _fp, _fp, _fp, _fp, _fp]),
+    "vistio_solver_contact_force": (C.c_int, [_vp, _fp]),
     "vistio_step": (C.c_int, [_vp, C.c_float, C.POINTER(StepResultC)]),
     "vistio_step_with_ipc": (C.c_int, [_vp, C.c_float, C.POINTER(ContactDesc), C.POINTER(StepResultC)]),
     "vistio_batch_create": (C.c_int, [_vp, C.POINTER(_vp), C.c_uint32, C.POINTER(_vp)]),

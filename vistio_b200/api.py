@@ -304,6 +304,12 @@ class ProjectiveDynamicsSolver:
         L.check(L.lib().vistio_solver_lumped_masses(self.h, _fp(out)), self.ctx.h)
         return out
 
+    def contact_force(self) -> np.ndarray:
+        """Per vertex |contact barrier gradient| of the last contact detect (vistio_solver_contact_force)."""
+        out = np.zeros(self.nv, np.float32)
+        L.check(L.lib().vistio_solver_contact_force(self.h, _fp(out)), self.ctx.h)
+        return out
+
     def set_ground(self, height: Optional[float]):
         L.check(L.lib().vistio_solver_set_ground(self.h, int(height is not None), float(height or 0.0)), self.ctx.h)
 

@@ -1170,6 +1170,22 @@ vistio_status vistio_solver_get_state(vistio_solver* s, float* px, float* py, fl
   return VISTIO_OK;
 }
 
+vistio_status vistio_solver_contact_force(vistio_solver* s, float* out) {
+  if (!s || !out) return fail(s ? s->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  const uint32_t nv = s->setup.nv;
+  if (!s->own) {
+    std::fill(out, out + nv, 0.f);
+    return VISTIO_OK;
+  }
+  vistio_batch* b = s->own;
+  vistio_ctx* ctx = b->ctx;
+  std::vector<float4> g(nv);
+  CU(cudaMemcpyAsync(g.data(), b->grad.p + b->vbase[0], nv * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  for (uint32_t i = 0; i < nv; ++i) out[i] = std::sqrt(g[i].x * g[i].x + g[i].y * g[i].y + g[i].z * g[i].z);
+  return VISTIO_OK;
+}
+
 vistio_status vistio_step(vistio_solver* s, float dt, vistio_step_result* res) {
   if (!s) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "Solver not initialized. Call init() first.");
   auto t0 = std::chrono::steady_clock::now();
