@@ -189,6 +189,18 @@ typedef struct vistio_step_result {
   int32_t status;
 } vistio_step_result;
 
+/* ContactResult (crates/vistio-contact/src/response.rs:13-20). */
+typedef struct vistio_contact_result {
+  uint32_t resolved_count;
+  float max_residual_penetration;
+  float total_force_magnitude;   /* the sum of the depths resolved */
+} vistio_contact_result;
+
+/* The collider rows of CollisionStepResult (collision_pipeline.rs:405-420). */
+typedef struct vistio_collider_results {
+  vistio_contact_result ground, sphere, cylinder, box;
+} vistio_collider_results;
+
 /* ---- context ---- */
 vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out);
 vistio_status vistio_ctx_destroy(vistio_ctx* ctx);
@@ -232,12 +244,26 @@ vistio_status vistio_solver_contact_force(vistio_solver* s, float* out);
 vistio_status vistio_step(vistio_solver* s, float dt, vistio_step_result* res);
 vistio_status vistio_step_with_ipc(vistio_solver* s, float dt, const vistio_contact_desc* contact,
                                    vistio_step_result* res);
+/* The runner's non-IPC branch after vistio_step (runner.rs:209-215 calling
+ * CollisionPipeline::step, collision_pipeline.rs:117-199, with the runner's
+ * thickness and stiffness of 0, which leave out the mesh contacts):
+ * GroundPlane::resolve twice, then SphereCollider, CylinderCollider and
+ * BoxCollider ::resolve, each on the colliders `contact` enables; the self
+ * collision and kappa fields are not read. Positions and velocities of the
+ * vertices inside a collider are projected onto its surface; `res` may be
+ * NULL. */
+vistio_status vistio_resolve_contacts(vistio_solver* s, const vistio_contact_desc* contact,
+                                      vistio_collider_results* res);
 
 /* ---- batches: many garments advanced together from HBM-resident ragged SoA ---- */
 vistio_status vistio_batch_create(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch** out);
 vistio_status vistio_batch_destroy(vistio_batch* b);
 /* Advances every instance `nsteps` steps of size dt; contact may be NULL. Asynchronous. */
 vistio_status vistio_batch_step(vistio_batch* b, float dt, uint32_t nsteps, const vistio_contact_desc* contact);
+/* vistio_resolve_contacts on every garment of the batch with the same
+ * colliders; res, when not NULL, holds one entry per garment. */
+vistio_status vistio_batch_resolve_contacts(vistio_batch* b, const vistio_contact_desc* contact,
+                                            vistio_collider_results* res);
 vistio_status vistio_batch_set_state(vistio_batch* b, uint32_t k, const float* px, const float* py, const float* pz,
                                      const float* vx, const float* vy, const float* vz);
 vistio_status vistio_batch_get_state(vistio_batch* b, uint32_t k, float* px, float* py, float* pz, float* vx,

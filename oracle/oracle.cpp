@@ -294,6 +294,7 @@ struct SimBase {
   virtual void assemble_rhs(float dt, float*, float*, float*) = 0;
   virtual void detect(const orc_contact* c, float d_hat, const float*, const float*, const float*,
                       float*, float*, float*, float*, float*, float*, uint8_t*, float*, uint32_t*) = 0;
+  virtual void resolve(const orc_contact* c, float* out) = 0;
   uint32_t n = 0, nt = 0;
   std::vector<uint32_t> tris;
   std::vector<HingeIdx> hidx;
@@ -305,6 +306,8 @@ struct SimBase {
   std::vector<float> hinge_rest, hinge_w, hinge_st;
   std::vector<uint32_t> hinge_v;
 };
+
+template <class R> V3<R> v3(const float* a) { return V3<R>(R(a[0]), R(a[1]), R(a[2])); }
 
 template <class R> struct Sim : SimBase {
   orc_params prm;
@@ -1160,6 +1163,112 @@ template <class R> struct Sim : SimBase {
     build_rhs(R(dtf), rhs);
     for (uint32_t i = 0; i < n; ++i) { rx[i] = float(rhs[i].x); ry[i] = float(rhs[i].y); rz[i] = float(rhs[i].z); }
   }
+  // CollisionPipeline::step with thickness 0 (collision_pipeline.rs:117-199):
+  // ground twice, sphere, cylinder, box; out[3c..3c+2] = resolved count,
+  // max penetration and depth sum of collider c (ground, sphere, cylinder,
+  // box), the first ground pass being the one reported.
+  void resolve(const orc_contact* c, float* out) override {
+    for (int k = 0; k < 12; ++k) out[k] = 0.f;
+    auto note = [&](int col, R depth) {
+      out[3 * col] += 1.f;
+      out[3 * col + 1] = std::max(out[3 * col + 1], float(depth));
+      out[3 * col + 2] += float(depth);
+    };
+    auto ground = [&](bool report) {  // ground_plane.rs:26-65
+      const R h = R(c->ground_height);
+      for (uint32_t i = 0; i < n; ++i) {
+        if (inv_mass[i] == R(0)) continue;
+        R depth = h - pos[i].y;
+        if (depth > R(0)) {
+          pos[i].y = h;
+          prev[i].y = h;
+          vel[i].x *= R(0.5);
+          vel[i].z *= R(0.5);
+          if (vel[i].y < R(0)) vel[i].y = R(0);
+          if (report) note(0, depth);
+        }
+      }
+    };
+    if (c->has_ground) { ground(true); ground(false); }
+    if (c->has_sphere) {  // sphere.rs:29-100
+      const V3<R> ctr = v3<R>(c->sphere_center);
+      const R rad = R(c->sphere_radius), r2 = rad * rad;
+      for (uint32_t i = 0; i < n; ++i) {
+        if (inv_mass[i] == R(0)) continue;
+        V3<R> d = pos[i] - ctr;
+        R dist2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        if (dist2 < r2 && dist2 > R(1e-12f)) {
+          R dist = std::sqrt(dist2), depth = rad - dist;
+          V3<R> nrm(d.x / dist, d.y / dist, d.z / dist);
+          pos[i] = pos[i] + nrm * depth;
+          R vn = vel[i].x * nrm.x + vel[i].y * nrm.y + vel[i].z * nrm.z;
+          if (vn < R(0)) vel[i] = (vel[i] - nrm * vn) * R(0.5);
+          note(1, depth);
+        } else if (dist2 <= R(1e-12f)) {
+          pos[i].y += rad;
+          vel[i] = V3<R>();
+          note(1, rad);
+        }
+      }
+    }
+    if (c->has_cylinder) {  // cylinder.rs:30-118
+      const R cx = R(c->cylinder_center_x), cz = R(c->cylinder_center_z), top = R(c->cylinder_top_y);
+      const R rad = R(c->cylinder_radius), r2 = rad * rad;
+      for (uint32_t i = 0; i < n; ++i) {
+        if (inv_mass[i] == R(0) || pos[i].y > top) continue;
+        R dx = pos[i].x - cx, dz = pos[i].z - cz;
+        R dist2 = dx * dx + dz * dz;
+        if (!(dist2 < r2)) continue;
+        R dist = std::sqrt(dist2), side = rad - dist, dtop = top - pos[i].y;
+        bool up = dtop < side || prev[i].y >= top || dist < R(1e-12f);
+        if (up) {
+          pos[i].y = top;
+          if (vel[i].y < R(0)) vel[i].y = R(0);
+          vel[i].x *= R(0.1f);
+          vel[i].z *= R(0.1f);
+          note(2, dtop);
+        } else {
+          if (dist > R(1e-12f)) {
+            R nx = dx / dist, nz = dz / dist;
+            pos[i].x += nx * side;
+            pos[i].z += nz * side;
+            R vn = vel[i].x * nx + vel[i].z * nz;
+            if (vn < R(0)) { vel[i].x -= vn * nx; vel[i].z -= vn * nz; }
+            vel[i].y *= R(0.7f);
+          }
+          note(2, side);
+        }
+      }
+    }
+    if (c->has_box) {  // box_collider.rs:26-99
+      const V3<R> lo = v3<R>(c->box_min), hi = v3<R>(c->box_max);
+      const R fr = R(0.7f);
+      for (uint32_t i = 0; i < n; ++i) {
+        if (inv_mass[i] == R(0)) continue;
+        V3<R>& p = pos[i];
+        V3<R>& v = vel[i];
+        if (!(p.x >= lo.x && p.x <= hi.x && p.y >= lo.y && p.y <= hi.y && p.z >= lo.z && p.z <= hi.z)) continue;
+        const R face[6] = {p.x - lo.x, hi.x - p.x, hi.y - p.y, p.y - lo.y, hi.z - p.z, p.z - lo.z};
+        R m = std::min(std::min(std::min(std::min(std::min(face[0], face[1]), face[3]), face[2]), face[5]), face[4]);
+        if (prev[i].y >= hi.y) m = face[2];
+        // the first face (in the order -x, +x, +y, -y, +z, -z) at the minimum
+        int k = 0;
+        while (k < 5 && face[k] != m) ++k;
+        R* axis[3] = {&v.x, &v.y, &v.z};
+        R* coord[3] = {&p.x, &p.y, &p.z};
+        const int ax[6] = {0, 0, 1, 1, 2, 2};
+        const R to[6] = {lo.x, hi.x, hi.y, lo.y, hi.z, lo.z};
+        const int outward[6] = {-1, 1, 1, -1, 1, -1};
+        *coord[ax[k]] = to[k];
+        R& vn = *axis[ax[k]];
+        if (R(outward[k]) * vn < R(0)) vn = R(0);
+        for (int a = 0; a < 3; ++a)
+          if (a != ax[k]) *axis[a] *= fr;
+        note(3, m);
+      }
+    }
+  }
+
   void detect(const orc_contact* c, float d_hat, const float* px, const float* py, const float* pz,
               float* gx, float* gy, float* gz, float* nx, float* ny, float* nz, uint8_t* inc,
               float* maxv, uint32_t* active) override {
@@ -1177,7 +1286,6 @@ template <class R> struct Sim : SimBase {
   }
 };
 
-template <class R> V3<R> v3(const float* a) { return V3<R>(R(a[0]), R(a[1]), R(a[2])); }
 
 }  // namespace
 
@@ -1208,6 +1316,7 @@ int orc_step(void* sim, float dt, orc_step_result* res) { return static_cast<Sim
 int orc_step_ipc(void* sim, float dt, const orc_contact* c, orc_step_result* res) {
   return static_cast<SimBase*>(sim)->step_ipc(dt, c, res);
 }
+void orc_resolve(void* sim, const orc_contact* c, float* out) { static_cast<SimBase*>(sim)->resolve(c, out); }
 void orc_set_ground(void* sim, int has, float h) { static_cast<SimBase*>(sim)->set_ground(has, h); }
 void orc_get_state(void* sim, float* px, float* py, float* pz, float* vx, float* vy, float* vz) {
   static_cast<SimBase*>(sim)->get_state(px, py, pz, vx, vy, vz);

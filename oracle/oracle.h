@@ -86,6 +86,10 @@ void* orc_create(int precision, uint32_t nv, const float* px, const float* py, c
 void orc_destroy(void* sim);
 int orc_step(void* sim, float dt, orc_step_result* res);
 int orc_step_ipc(void* sim, float dt, const orc_contact* contact, orc_step_result* res);
+// The colliders' resolve() after a plain step (CollisionPipeline::step with
+// thickness 0, collision_pipeline.rs:117-199). out[12]: per collider (ground,
+// sphere, cylinder, box) the resolved count, max penetration and depth sum.
+void orc_resolve(void* sim, const orc_contact* contact, float* out);
 void orc_set_ground(void* sim, int has_ground, float height);
 // Read/write state (SoA float arrays of length nv; NULL skips).
 void orc_get_state(void* sim, float* px, float* py, float* pz, float* vx, float* vy, float* vz);

@@ -106,6 +106,7 @@ def lib():
         L.orc_step.argtypes = [C.c_void_p, C.c_float, C.POINTER(StepResult)]
         L.orc_step_ipc.argtypes = [C.c_void_p, C.c_float, C.POINTER(Contact), C.POINTER(StepResult)]
         L.orc_set_ground.argtypes = [C.c_void_p, C.c_int, C.c_float]
+        L.orc_resolve.argtypes = [C.c_void_p, C.POINTER(Contact), C.POINTER(C.c_float)]
         L.orc_get_state.argtypes = [C.c_void_p] + [fp] * 6
         L.orc_set_state.argtypes = [C.c_void_p] + [fp] * 6
         dp = C.POINTER(C.c_double)
@@ -199,6 +200,13 @@ class OracleSim:
 
     def set_ground(self, has, h=0.0):
         lib().orc_set_ground(self.h, int(has), float(h))
+
+    def resolve(self, contact: Contact) -> np.ndarray:
+        """The colliders' resolve() after a plain step; rows ground, sphere, cylinder, box of
+        (resolved count, max penetration, depth sum)."""
+        out = np.zeros(12, np.float32)
+        lib().orc_resolve(self.h, C.byref(contact), out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out.reshape(4, 3)
 
     def state(self):
         out = [np.zeros(self.nv, np.float32) for _ in range(6)]

@@ -68,6 +68,16 @@ class StepResultC(C.Structure):
                 ("last_alpha", C.c_float), ("status", C.c_int32)]
 
 
+class ContactResultC(C.Structure):
+    _fields_ = [("resolved_count", C.c_uint32), ("max_residual_penetration", C.c_float),
+                ("total_force_magnitude", C.c_float)]
+
+
+class ColliderResultsC(C.Structure):
+    _fields_ = [("ground", ContactResultC), ("sphere", ContactResultC), ("cylinder", ContactResultC),
+                ("box", ContactResultC)]
+
+
 # Every entry point include/vistio_cuda.h declares, with its ctypes signature.
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("max_cohort", C.c_uint32),
@@ -121,6 +131,8 @@ SIGNATURES = {
     "vistio_solver_contact_force": (C.c_int, [_vp, _fp]),
     "vistio_step": (C.c_int, [_vp, C.c_float, C.POINTER(StepResultC)]),
     "vistio_step_with_ipc": (C.c_int, [_vp, C.c_float, C.POINTER(ContactDesc), C.POINTER(StepResultC)]),
+    "vistio_resolve_contacts": (C.c_int, [_vp, C.POINTER(ContactDesc), C.POINTER(ColliderResultsC)]),
+    "vistio_batch_resolve_contacts": (C.c_int, [_vp, C.POINTER(ContactDesc), C.POINTER(ColliderResultsC)]),
     "vistio_batch_create": (C.c_int, [_vp, C.POINTER(_vp), C.c_uint32, C.POINTER(_vp)]),
     "vistio_batch_destroy": (C.c_int, [_vp]),
     "vistio_batch_step": (C.c_int, [_vp, C.c_float, C.c_uint32, C.POINTER(ContactDesc)]),

@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
-from typing import Optional, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -178,6 +178,29 @@ class StepResult:
                    r.active_contacts, r.last_alpha)
 
 
+@dataclasses.dataclass
+class ContactResult:
+    """ContactResult (crates/vistio-contact/src/response.rs:13-20)."""
+    resolved_count: int
+    max_residual_penetration: float
+    total_force_magnitude: float
+
+
+@dataclasses.dataclass
+class ColliderResults:
+    """The collider rows of CollisionStepResult (collision_pipeline.rs:405-420)."""
+    ground: ContactResult
+    sphere: ContactResult
+    cylinder: ContactResult
+    box: ContactResult
+
+    @classmethod
+    def from_c(cls, r: L.ColliderResultsC) -> "ColliderResults":
+        def one(c):
+            return ContactResult(c.resolved_count, c.max_residual_penetration, c.total_force_magnitude)
+        return cls(one(r.ground), one(r.sphere), one(r.cylinder), one(r.box))
+
+
 def _fp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
@@ -335,6 +358,14 @@ class ProjectiveDynamicsSolver:
         L.check(L.lib().vistio_step_with_ipc(self.h, float(dt), C.byref(c), C.byref(r)), self.ctx.h)
         return StepResult.from_c(r)
 
+    def resolve_contacts(self, contact: Contact) -> ColliderResults:
+        """The runner's non-IPC collision step after step() (runner.rs:209-215): ground twice, then the
+        sphere, cylinder and box colliders project the vertices inside them onto their surfaces."""
+        r = L.ColliderResultsC()
+        c = contact.to_c()
+        L.check(L.lib().vistio_resolve_contacts(self.h, C.byref(c), C.byref(r)), self.ctx.h)
+        return ColliderResults.from_c(r)
+
 
 class Batch:
     """Many garments in one ragged SoA set of HBM buffers, stepped by one CUDA graph."""
@@ -360,6 +391,13 @@ class Batch:
         c = contact.to_c() if contact is not None else None
         L.check(L.lib().vistio_batch_step(self.h, float(dt), int(nsteps), C.byref(c) if c is not None else None),
                 self.ctx.h)
+
+    def resolve_contacts(self, contact: Contact) -> List[ColliderResults]:
+        """ProjectiveDynamicsSolver.resolve_contacts on every garment with the same colliders."""
+        r = (L.ColliderResultsC * len(self.solvers))()
+        c = contact.to_c()
+        L.check(L.lib().vistio_batch_resolve_contacts(self.h, C.byref(c), r), self.ctx.h)
+        return [ColliderResults.from_c(x) for x in r]
 
     def state(self, k: int):
         nv = self.nverts[k]

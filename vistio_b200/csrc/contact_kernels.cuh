@@ -298,6 +298,153 @@ __global__ void __launch_bounds__(256) k_ccd(BatchDev B) {
   }
 }
 
+// The colliders of the runner's non-IPC path (runner.rs:212-218 then
+// CollisionPipeline::step, collision_pipeline.rs:117-199, with no mesh or self
+// contact): after a plain step, GroundPlane, GroundPlane again, SphereCollider,
+// CylinderCollider and BoxCollider ::resolve, in that order, on every free
+// vertex (ground_plane.rs:26-65, sphere.rs:29-100, cylinder.rs:30-118,
+// box_collider.rs:26-99): a vertex inside is moved to the surface, its
+// velocity loses the inward part and is damped. FP32 like the reference.
+struct ColliderDev {
+  int32_t has_ground, has_sphere, has_cyl, has_box;
+  float ground_h, sc[3], sr, cyl[4], lo[3], hi[3];
+};
+
+// Separately rounded FP32 operations: the projections below are written
+// without fused multiply-adds, so each vertex lands on the same float the
+// reference's scalar Rust code computes.
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rdot3(float a, float b, float c, float x, float y, float z) {
+  return radd(radd(rmul(a, x), rmul(b, y)), rmul(c, z));
+}
+
+__device__ __forceinline__ void resolve_ground(const ColliderDev& C, float4& x, float4& v, float4& pv, uint32_t& n,
+                                               float& pen, float& f) {
+  const float depth = rsub(C.ground_h, x.y);
+  if (depth > 0.f) {
+    x.y = C.ground_h;
+    pv.y = C.ground_h;  // the velocity (x - prev) / dt is not to point down
+    v.x = rmul(v.x, 0.5f); v.z = rmul(v.z, 0.5f);
+    if (v.y < 0.f) v.y = 0.f;
+    ++n;
+    pen = fmaxf(pen, depth);
+    f = radd(f, depth);
+  }
+}
+
+// Per instance i and collider c (ground, sphere, cylinder, box), the
+// ContactResult fields of CollisionStepResult: out[8i+2c] += vertices
+// resolved, out[8i+2c+1] = max(itself, the float bits of the deepest
+// penetration) and force[4i+c] += the sum of the depths. The second ground
+// pass finds nothing the first left and is not counted, as in the reference.
+__global__ void __launch_bounds__(256) k_resolve(BatchDev B, ColliderDev C, uint32_t* out, double* force) {
+  int4 ch = B.vtx_chunks[blockIdx.x];
+  uint32_t n[4] = {0, 0, 0, 0};
+  float pen[4] = {0.f, 0.f, 0.f, 0.f}, f[4] = {0.f, 0.f, 0.f, 0.f};
+  if ((int)threadIdx.x < ch.z) {
+    const uint32_t g = uint32_t(ch.y) + threadIdx.x;
+    if (!B.pinned[g] && B.mass[g] > 1e-12f) {  // inv_mass != 0 (state.rs:108-116)
+      float4 x = B.pos[g], v = B.vel[g], pv = B.prev[g];
+      if (C.has_ground) {
+        resolve_ground(C, x, v, pv, n[0], pen[0], f[0]);
+        uint32_t n2 = 0;
+        float p2 = 0.f, f2 = 0.f;
+        resolve_ground(C, x, v, pv, n2, p2, f2);
+      }
+      if (C.has_sphere) {
+        const float r = C.sr, r2 = rmul(r, r);
+        const float dx = rsub(x.x, C.sc[0]), dy = rsub(x.y, C.sc[1]), dz = rsub(x.z, C.sc[2]);
+        const float d2 = rdot3(dx, dy, dz, dx, dy, dz);
+        if (d2 < r2 && d2 > 1e-12f) {
+          const float d = __fsqrt_rn(d2), depth = rsub(r, d);
+          const float nx = __fdiv_rn(dx, d), ny = __fdiv_rn(dy, d), nz = __fdiv_rn(dz, d);
+          x.x = radd(x.x, rmul(nx, depth)); x.y = radd(x.y, rmul(ny, depth)); x.z = radd(x.z, rmul(nz, depth));
+          const float vn = rdot3(v.x, v.y, v.z, nx, ny, nz);
+          if (vn < 0.f) {  // the normal part goes, the tangential part keeps half (friction 0.5)
+            v.x = rmul(rsub(v.x, rmul(nx, vn)), 0.5f);
+            v.y = rmul(rsub(v.y, rmul(ny, vn)), 0.5f);
+            v.z = rmul(rsub(v.z, rmul(nz, vn)), 0.5f);
+          }
+          ++n[1];
+          pen[1] = fmaxf(pen[1], depth);
+          f[1] = radd(f[1], depth);
+        } else if (d2 <= 1e-12f) {  // at the centre: straight up, at rest
+          x.y = radd(x.y, r);
+          v.x = 0.f; v.y = 0.f; v.z = 0.f;
+          ++n[1];
+          pen[1] = fmaxf(pen[1], r);
+          f[1] = radd(f[1], r);
+        }
+      }
+      if (C.has_cyl && !(x.y > C.cyl[2])) {  // only below the top face: the cylinder reaches down without end
+        const float r = C.cyl[3];
+        const float dx = rsub(x.x, C.cyl[0]), dz = rsub(x.z, C.cyl[1]);
+        const float d2 = radd(rmul(dx, dx), rmul(dz, dz));
+        if (d2 < rmul(r, r)) {
+          const float d = __fsqrt_rn(d2), side = rsub(r, d), top = rsub(C.cyl[2], x.y);
+          bool up = top < side;
+          if (pv.y >= C.cyl[2]) up = true;  // it was above the top a frame ago: it came through the top
+          if (d < 1e-12f) up = true;
+          if (up) {
+            x.y = C.cyl[2];
+            if (v.y < 0.f) v.y = 0.f;
+            v.x = rmul(v.x, 0.1f); v.z = rmul(v.z, 0.1f);
+            pen[2] = fmaxf(pen[2], top);
+            f[2] = radd(f[2], top);
+          } else {
+            if (d > 1e-12f) {
+              const float nx = __fdiv_rn(dx, d), nz = __fdiv_rn(dz, d);
+              x.x = radd(x.x, rmul(nx, side)); x.z = radd(x.z, rmul(nz, side));
+              const float vn = radd(rmul(v.x, nx), rmul(v.z, nz));
+              if (vn < 0.f) { v.x = rsub(v.x, rmul(vn, nx)); v.z = rsub(v.z, rmul(vn, nz)); }
+              v.y = rmul(v.y, 0.7f);
+            }
+            pen[2] = fmaxf(pen[2], side);
+            f[2] = radd(f[2], side);
+          }
+          ++n[2];
+        }
+      }
+      if (C.has_box && x.x >= C.lo[0] && x.x <= C.hi[0] && x.y >= C.lo[1] && x.y <= C.hi[1] && x.z >= C.lo[2] &&
+          x.z <= C.hi[2]) {
+        const float dnx = rsub(x.x, C.lo[0]), dpx = rsub(C.hi[0], x.x), dny = rsub(x.y, C.lo[1]);
+        const float dpy = rsub(C.hi[1], x.y), dnz = rsub(x.z, C.lo[2]), dpz = rsub(C.hi[2], x.z);
+        float md = fminf(fminf(fminf(fminf(fminf(dnx, dpx), dny), dpy), dnz), dpz);
+        if (pv.y >= C.hi[1]) md = dpy;  // it came through the top
+        const float fr = 0.7f;  // faces tried in the order -x, +x, +y, -y, +z, -z
+        if (md == dnx) { x.x = C.lo[0]; if (v.x > 0.f) v.x = 0.f; v.y = rmul(v.y, fr); v.z = rmul(v.z, fr); }
+        else if (md == dpx) { x.x = C.hi[0]; if (v.x < 0.f) v.x = 0.f; v.y = rmul(v.y, fr); v.z = rmul(v.z, fr); }
+        else if (md == dpy) { x.y = C.hi[1]; if (v.y < 0.f) v.y = 0.f; v.x = rmul(v.x, fr); v.z = rmul(v.z, fr); }
+        else if (md == dny) { x.y = C.lo[1]; if (v.y > 0.f) v.y = 0.f; v.x = rmul(v.x, fr); v.z = rmul(v.z, fr); }
+        else if (md == dpz) { x.z = C.hi[2]; if (v.z < 0.f) v.z = 0.f; v.x = rmul(v.x, fr); v.y = rmul(v.y, fr); }
+        else if (md == dnz) { x.z = C.lo[2]; if (v.z > 0.f) v.z = 0.f; v.x = rmul(v.x, fr); v.y = rmul(v.y, fr); }
+        ++n[3];
+        pen[3] = fmaxf(pen[3], md);
+        f[3] = radd(f[3], md);
+      }
+      B.pos[g] = x; B.vel[g] = v; B.prev[g] = pv;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    uint32_t k = n[c];
+    float p = pen[c];
+    double t = f[c];
+    warp_sum_u32(k);
+    for (int o = 16; o > 0; o >>= 1) {
+      p = fmaxf(p, __shfl_down_sync(0xffffffffu, p, o));
+      t += __shfl_down_sync(0xffffffffu, t, o);
+    }
+    if ((threadIdx.x & 31) == 0 && k) {
+      atomicAdd(out + 8 * ch.x + 2 * c, k);
+      atomicMax(out + 8 * ch.x + 2 * c + 1, __float_as_uint(p));  // non-negative floats order like their bits
+      atomicAdd(force + 4 * ch.x + c, t);
+    }
+  }
+}
+
 // Step-size selection (pd_solver.rs:896-932) and x <- x + alpha d on free vertices.
 __global__ void __launch_bounds__(256) k_ipc_update(BatchDev B) {
   int4 ch = B.vtx_chunks[blockIdx.x];

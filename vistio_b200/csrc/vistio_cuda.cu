@@ -175,6 +175,8 @@ struct vistio_batch {
   SelfContactDev self;       // self-contact buffers (allocated on first use)
   DevBuf<double4> gacc;      // FP64 self-contact gradient accumulator (first use)
   DevBuf<float> xyz_stage;   // interleaved positions for whole-batch copies (first use)
+  DevBuf<uint32_t> res_cnt;  // collider resolve counts and penetrations, 8 per garment (first use)
+  DevBuf<double> res_force;  // collider resolve depth sums, 4 per garment (first use)
   uint32_t n_tri_chunks = 0, n_hinge_chunks = 0, n_vtx_chunks = 0;
   uint64_t factor_bytes = 0, device_bytes = 0;
   BatchDev dev{};
@@ -1238,6 +1240,62 @@ vistio_status vistio_batch_destroy(vistio_batch* b) {
 vistio_status vistio_batch_step(vistio_batch* b, float dt, uint32_t nsteps, const vistio_contact_desc* contact) {
   if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
   return batch_run(b, dt, nsteps, contact);
+}
+
+vistio_status vistio_batch_resolve_contacts(vistio_batch* b, const vistio_contact_desc* ct,
+                                            vistio_collider_results* res) {
+  if (!b || !ct) return fail(b ? b->ctx : nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  vistio_ctx* ctx = b->ctx;
+  cudaStream_t st = ctx->stream;
+  CU(cudaSetDevice(ctx->device));
+  ColliderDev C{};
+  C.has_ground = ct->has_ground != 0;
+  C.ground_h = ct->ground_height;
+  C.has_sphere = ct->has_sphere != 0;
+  for (int k = 0; k < 3; ++k) C.sc[k] = ct->sphere_center[k];
+  C.sr = ct->sphere_radius;
+  C.has_cyl = ct->has_cylinder != 0;
+  C.cyl[0] = ct->cylinder_center_x; C.cyl[1] = ct->cylinder_center_z;
+  C.cyl[2] = ct->cylinder_top_y; C.cyl[3] = ct->cylinder_radius;
+  C.has_box = ct->has_box != 0;
+  for (int k = 0; k < 3; ++k) { C.lo[k] = ct->box_min[k]; C.hi[k] = ct->box_max[k]; }
+  if (!b->res_cnt.p) {
+    CU(b->res_cnt.alloc(8 * size_t(b->ninst), st));
+    CU(b->res_force.alloc(4 * size_t(b->ninst), st));
+  }
+  CU(cudaMemsetAsync(b->res_cnt.p, 0, 32 * size_t(b->ninst), st));
+  CU(cudaMemsetAsync(b->res_force.p, 0, 32 * size_t(b->ninst), st));
+  if (b->n_vtx_chunks) k_resolve<<<b->n_vtx_chunks, 256, 0, st>>>(b->dev, C, b->res_cnt.p, b->res_force.p);
+  CU(cudaGetLastError());
+  if (!res) return VISTIO_OK;
+  std::vector<uint32_t> cnt(8 * size_t(b->ninst));
+  std::vector<double> frc(4 * size_t(b->ninst));
+  CU(cudaMemcpyAsync(cnt.data(), b->res_cnt.p, cnt.size() * 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(frc.data(), b->res_force.p, frc.size() * 8, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  for (uint32_t i = 0; i < b->ninst; ++i) {
+    vistio_contact_result* r[4] = {&res[i].ground, &res[i].sphere, &res[i].cylinder, &res[i].box};
+    for (int c = 0; c < 4; ++c) {
+      r[c]->resolved_count = cnt[8 * i + 2 * c];
+      std::memcpy(&r[c]->max_residual_penetration, &cnt[8 * i + 2 * c + 1], 4);
+      r[c]->total_force_magnitude = float(frc[4 * i + c]);
+    }
+  }
+  return VISTIO_OK;
+}
+
+vistio_status vistio_resolve_contacts(vistio_solver* s, const vistio_contact_desc* contact,
+                                      vistio_collider_results* res) {
+  if (!s) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "Solver not initialized. Call init() first.");
+  if (!contact) return fail(s->ctx, VISTIO_ERR_INVALID_CONFIG, "null contact description");
+  vistio_status r = ensure_own(s);
+  if (r != VISTIO_OK) return r;
+  r = vistio_batch_resolve_contacts(s->own, contact, res);
+  if (r == VISTIO_OK && !res) {
+    vistio_ctx* ctx = s->own->ctx;
+    CU(cudaStreamSynchronize(ctx->stream));
+  }
+  return r;
 }
 
 // Whole-batch position copies: one contiguous copy of the interleaved xyz

@@ -12,6 +12,9 @@ parameter mapping of the drape workloads:
   origin r = 0.3, ground y = -0.3 (runner.rs:77-81).
 * cusick_drape: a disc of radius 0.15 m (`circular_grid`, generators.rs:174)
   at y = 0.5 over a pedestal cylinder (top y = 0.3, r = 0.09) and the ground.
+* cantilever_bending: a 0.1 m x 0.4 m strip at y = 0.5, three rows pinned, the
+  free end over a box shelf, stepped without IPC (scenarios.rs:176-201,
+  runner.rs:87-90).
 * self_fold: 0.2 m x 2.0 m, 40x400 cells, rotated 45 degrees about x with the
   lowest point at y = 0.5, ground y = 0, self contact.
 * batched sheets: hanging sheets of random side / size / material.
@@ -131,6 +134,23 @@ def cusick_drape(height: float = 0.5, radius: float = 0.15, segments: int = 64) 
     pz = py.copy()
     py = np.full_like(px, np.float32(height))
     return Mesh(px, py, pz, tris, np.zeros(px.shape[0], dtype=np.uint8))
+
+
+def cantilever_bending(cols: int = 10, rows: int = 40, width: float = 0.10, length: float = 0.40) -> Mesh:
+    """scenarios.rs:176-201: a 0.1 m x 0.4 m strip at y = 0.5, its first three
+    rows (z = 0.4 down to 0.38) pinned, its last row at z = 0 over the edge of
+    the box x in [-0.1, 0.1], y in [0, 0.499], z in [-0.2, 0] that the runner
+    adds (runner.rs:87-90); the runner steps it without IPC and resolves the
+    box after every step."""
+    px, py, pz, tris = quad_grid(cols, rows, width, length)
+    pz = (py + np.float32(0.20)).astype(np.float32)
+    py = np.full_like(px, np.float32(0.5))
+    pinned = np.zeros(px.shape[0], dtype=np.uint8)
+    pinned[: 3 * (cols + 1)] = 1
+    return Mesh(px, py, pz, tris, pinned)
+
+
+CANTILEVER_BOX = ((-0.1, 0.0, -0.2), (0.1, 0.499, 0.0))  # (min, max) of the shelf, runner.rs:87-90
 
 
 def self_fold(cols: int = 40, rows: int = 400, width: float = 0.2, height: float = 2.0,
