@@ -199,12 +199,16 @@ struct SparseChol {
     nd_order(verts, adj, xyz, side, perm);
     iperm.assign(n, 0);
     for (int k = 0; k < n; ++k) iperm[perm[k]] = k;
-    // Upper triangle of B = P A P^T, by columns.
+    // Upper triangle of B = P A P^T, by columns, from A's upper triangle in
+    // the original numbering: faer factors with Side::Upper
+    // (faer_solver.rs:84-88), and A[i][j], A[j][i] of the assembled matrix
+    // can differ in the last bit.
     std::vector<std::vector<std::pair<int, double>>> colsB(n);
     for (int i = 0; i < n; ++i)
       for (int p = Ap[i]; p < Ap[i + 1]; ++p) {
+        if (Aj[p] < i) continue;
         int r = iperm[i], c = iperm[Aj[p]];
-        if (r <= c) colsB[c].push_back({r, Ax[p]});
+        colsB[std::max(r, c)].push_back({std::min(r, c), Ax[p]});
       }
     // Elimination tree.
     std::vector<int> parent(n, -1), ancestor(n, -1);

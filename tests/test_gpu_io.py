@@ -52,3 +52,36 @@ def test_simulate_with_contact():
     assert f.shape == (mesh.nv,) and (f > 0).any()
     assert out.metrics.max_penetration <= 0.02
     assert out.metrics.timestep_count == 30
+
+
+def test_simulate_non_ipc_with_exporter(tmp_path):
+    """ipc=False: a plain step then the colliders' projections each step (the
+    runner's non-IPC branch), the same as driving the solver directly; the
+    exporter receives every step's positions."""
+    mesh = scenarios.sphere_drape(side=12, length=0.6, height=0.13)
+    box = api.Contact(has_ground=True, ground_height=-0.3, has_box=True, box_min=(-0.2, -0.1, -0.2),
+                      box_max=(0.2, 0.1, 0.2))
+    inp = vio.SimulationInput(vio.TriangleMesh.from_mesh(mesh), None, [False] * mesh.nv,
+                              vio.SimulationParams(duration=0.2, iterations=10, material_name="cotton_twill"))
+    e = vio.JsonFrameExporter(str(tmp_path / "frames.json"))
+    out = vio.simulate(inp, contact=box, ipc=False, exporter=e)
+    props = vio.MATERIALS["cotton_twill"]
+    s = api.ProjectiveDynamicsSolver().init_explicit(mesh, vio.solver_config(inp.params),
+                                                     vio.setup_for(props, inp.params.dt), pinned=mesh.pinned)
+    s.set_ground(-0.3)
+    boxed = 0
+    frames = []
+    for _ in range(12):
+        s.step(inp.params.dt)
+        boxed += s.resolve_contacts(box).box.resolved_count
+        frames.append(s.state()[0])
+    d = out.draped_mesh
+    assert np.array_equal(np.stack([d.pos_x, d.pos_y, d.pos_z], 1).astype(np.float32), frames[-1])
+    assert boxed > 0 and out.metrics.timestep_count == 12
+    assert not any(out.vertex_metadata.contact_force)
+    assert e.frame_count() == 12
+    e.finalize()
+    got = json.loads((tmp_path / "frames.json").read_text())
+    assert [f["timestep"] for f in got["frames"]] == list(range(12))
+    for f, x in zip(got["frames"], frames):
+        assert np.array_equal(np.array(f["positions"], np.float32), x.ravel())

@@ -89,3 +89,60 @@ def test_material_database_and_setup():
     with pytest.raises(L.VistioError) as e:
         vio.material("tweed")
     assert e.value.status == 2
+
+
+@pytest.mark.parametrize("value,text", [
+    (0.1, "0.1"), (1.0, "1.0"), (100.0, "100.0"), (1234.5, "1234.5"), (-2.5, "-2.5"), (0.0, "0.0"),
+    (-0.0, "-0.0"), (1e-7, "1e-7"), (1.5e20, "1.5e20"), (0.000123, "0.000123"), (1e-6, "0.000001"),
+    (1e13, "1e13"), (9999e9, "9999000000000.0"), (123456789.0, "123456790.0"), (float("nan"), "null"),
+    (float("inf"), "null"),
+])
+def test_json_f32_text(value, text):
+    """An f32 in JSON: the shortest decimal that reads back as the same f32."""
+    assert vio._json_f32(value) == text
+
+
+def test_json_f32_round_trips():
+    rng = np.random.default_rng(3)
+    a = (10 ** rng.uniform(-9, 20, 20000)).astype(np.float32) * np.where(rng.random(20000) < 0.5, -1, 1)
+    a = a.astype(np.float32)
+    text = vio._json_f32_array(a)
+    assert np.array_equal(np.array(json.loads(text), np.float32), a)
+    assert text == "[" + ",".join(vio._json_f32(x) for x in a) + "]"
+
+
+def test_json_frame_exporter(tmp_path):
+    """json_exporter.rs:39-104: init from the mesh, one frame per submit, the
+    whole animation written compactly on finalize, frames handed over."""
+    mesh = scenarios.hanging_sheet(3, 1.0)
+    path = tmp_path / "anim.json"
+    e = vio.JsonFrameExporter(str(path))
+    assert e.name() == "json_exporter" and e.frame_count() == 0
+    e.init(vio.TriangleMesh.from_mesh(mesh))
+    x = np.stack([mesh.px, mesh.py, mesh.pz], 1)
+    for t in range(3):
+        e.submit_frame(t, x + np.float32(0.1) * t)
+    assert e.frame_count() == 3
+    e.finalize()
+    assert e.frame_count() == 0
+    text = path.read_text()
+    assert " " not in text and text.startswith('{"vertex_count":16,"triangle_count":18,"indices":[')
+    d = json.loads(text)
+    assert list(d) == ["vertex_count", "triangle_count", "indices", "frames"]
+    assert d["indices"] == [int(i) for i in mesh.tris.ravel()]
+    assert [f["timestep"] for f in d["frames"]] == [0, 1, 2]
+    for t, f in enumerate(d["frames"]):
+        assert list(f) == ["timestep", "positions"]
+        np.testing.assert_array_equal(np.array(f["positions"], np.float32), (x + np.float32(0.1) * t).ravel())
+    # a scenarios.Mesh initialises the same way
+    e2 = vio.JsonFrameExporter(str(tmp_path / "b.json"))
+    e2.init(mesh)
+    assert (e2.vertex_count, e2.triangle_count, e2.indices) == (16, 18, d["indices"])
+
+
+def test_json_frame_exporter_write_error(tmp_path):
+    e = vio.JsonFrameExporter(str(tmp_path / "missing" / "a.json"))
+    e.init(scenarios.hanging_sheet(2, 1.0))
+    with pytest.raises(L.VistioError) as err:
+        e.finalize()
+    assert err.value.status == 4

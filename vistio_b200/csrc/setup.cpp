@@ -201,21 +201,31 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
   Graph g;
   g.n = n;
   {
-    std::vector<std::pair<uint32_t, uint32_t>> e;
-    e.reserve(size_t(row_ptr[n]) * 2);
+    // Bucket both directions of every off-diagonal entry by row (two counting
+    // passes), then sort and deduplicate each short row in place.
+    std::vector<uint32_t> deg(n + 1, 0);
     for (uint32_t i = 0; i < n; ++i)
       for (uint32_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p) {
         uint32_t j = col_idx[p];
         if (j >= n) { *status = 3; return "column index out of range"; }
-        if (j != i) { e.push_back({i, j}); e.push_back({j, i}); }
+        if (j != i) { deg[i + 1]++; deg[j + 1]++; }
       }
-    std::sort(e.begin(), e.end());
-    e.erase(std::unique(e.begin(), e.end()), e.end());
+    for (uint32_t i = 0; i < n; ++i) deg[i + 1] += deg[i];
+    std::vector<uint32_t> raw(deg[n]), fill(deg.begin(), deg.end() - 1);
+    for (uint32_t i = 0; i < n; ++i)
+      for (uint32_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p) {
+        uint32_t j = col_idx[p];
+        if (j != i) { raw[fill[i]++] = j; raw[fill[j]++] = i; }
+      }
     g.ptr.assign(n + 1, 0);
-    for (auto& x : e) g.ptr[x.first + 1]++;
-    for (uint32_t i = 0; i < n; ++i) g.ptr[i + 1] += g.ptr[i];
-    g.adj.resize(e.size());
-    for (size_t k = 0; k < e.size(); ++k) g.adj[k] = e[k].second;
+    g.adj.clear();
+    g.adj.reserve(raw.size());
+    for (uint32_t i = 0; i < n; ++i) {
+      auto b = raw.begin() + deg[i], e = raw.begin() + deg[i + 1];
+      std::sort(b, e);
+      g.adj.insert(g.adj.end(), b, std::unique(b, e));
+      g.ptr[i + 1] = uint32_t(g.adj.size());
+    }
   }
   std::vector<uint32_t> order;
   Dissector(g, coords).run(order);
@@ -273,25 +283,27 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
   std::vector<uint32_t> bp(n + 1, 0);
   std::vector<std::pair<uint32_t, double>> bent;
   {
-    std::vector<std::vector<std::pair<uint32_t, double>>> cols(n);
+    // Entries bucketed by permuted column (counting passes), each column then
+    // sorted by row; an entry given in both triangles counts once (the two
+    // copies of a symmetric matrix's entry hold the same value).
+    std::vector<uint32_t> cptr(n + 1, 0);
+    for (uint32_t i = 0; i < n; ++i)
+      for (uint32_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p) cptr[std::max(ip[i], ip[col_idx[p]]) + 1]++;
+    for (uint32_t c = 0; c < n; ++c) cptr[c + 1] += cptr[c];
+    std::vector<std::pair<uint32_t, double>> raw(cptr[n]);
+    std::vector<uint32_t> fill(cptr.begin(), cptr.end() - 1);
     for (uint32_t i = 0; i < n; ++i)
       for (uint32_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p) {
         uint32_t r = ip[i], c = ip[col_idx[p]];
-        if (r <= c) cols[c].push_back({r, vals[p]});
-        else cols[r].push_back({c, vals[p]});  // accept lower-triangle-only input as well
+        raw[fill[std::max(r, c)]++] = {std::min(r, c), vals[p]};  // accept lower-triangle-only input as well
       }
+    bent.reserve(raw.size());
     for (uint32_t c = 0; c < n; ++c) {
-      auto& v = cols[c];
-      std::sort(v.begin(), v.end(), [](auto& a, auto& b) { return a.first < b.first; });
-      // merge duplicates (an entry given in both triangles counts once)
-      std::vector<std::pair<uint32_t, double>> m;
-      for (auto& x : v) {
-        if (!m.empty() && m.back().first == x.first) continue;
-        m.push_back(x);
-      }
-      v.swap(m);
-      bp[c + 1] = bp[c] + uint32_t(v.size());
-      bent.insert(bent.end(), v.begin(), v.end());
+      auto b = raw.begin() + cptr[c], e = raw.begin() + cptr[c + 1];
+      std::stable_sort(b, e, [](const auto& x, const auto& y) { return x.first < y.first; });
+      for (auto it = b; it != e; ++it)
+        if (bent.size() == bp[c] || bent.back().first != it->first) bent.push_back(*it);
+      bp[c + 1] = uint32_t(bent.size());
     }
   }
   // Up-looking simplicial LL^T in FP64 (row k of L from the etree reach).
@@ -667,46 +679,90 @@ std::string build_instance(uint32_t nv, const float* px, const float* py, const 
   }
   I.nh = uint32_t(I.hinge_w.size());
   // assemble_system_matrix (assembly.rs:44-135): the f32 triplets in the
-  // reference's order, summed per (row, col) in f64 in that order.
-  struct Trip { uint32_t r, c; float v; };
-  std::vector<Trip> tr;
-  tr.reserve(nv + 9 * size_t(nt) + 16 * size_t(I.nh));
+  // reference's order (diagonal masses, then triangles, then hinges), summed
+  // per (row, col) in f64 in that order. Assembled row by row: a vertex's
+  // incidences (element, corner) are listed in increasing element order, so
+  // each (row, col) meets its triplets in the same order as the reference's
+  // single list; a column gets a slot on first sight and the slots are
+  // emitted by column.
   float h = prm.matrix_dt;
   float inv_h2 = 1.f / (h * h);
-  for (uint32_t i = 0; i < nv; ++i) tr.push_back({i, i, I.mass[i] * inv_h2});
-  for (uint32_t t = 0; t < nt; ++t) {
-    const float* d = &I.dm_inv[4 * size_t(t)];
-    float g[3][2] = {{-(d[0] + d[1]), -(d[2] + d[3])}, {d[0], d[2]}, {d[1], d[3]}};
-    for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) {
-        float dt_ = g[a][0] * g[b][0] + g[a][1] * g[b][1];
-        if (std::fabs(dt_) > 1e-12f) tr.push_back({tris[3 * t + a], tris[3 * t + b], I.tri_w[t] * dt_});
-      }
+  std::vector<uint32_t> tptr(nv + 1, 0), hptr(nv + 1, 0);
+  for (size_t q = 0; q < 3 * size_t(nt); ++q) tptr[tris[q] + 1]++;
+  for (size_t q = 0; q < 4 * size_t(I.nh); ++q) hptr[I.hinge_v[q] + 1]++;
+  for (uint32_t i = 0; i < nv; ++i) { tptr[i + 1] += tptr[i]; hptr[i + 1] += hptr[i]; }
+  std::vector<uint32_t> tinc(tptr[nv]), hinc(hptr[nv]);
+  {
+    std::vector<uint32_t> ft(tptr.begin(), tptr.end() - 1), fh(hptr.begin(), hptr.end() - 1);
+    for (size_t q = 0; q < 3 * size_t(nt); ++q) tinc[ft[tris[q]]++] = uint32_t(q);
+    for (size_t q = 0; q < 4 * size_t(I.nh); ++q) hinc[fh[I.hinge_v[q]]++] = uint32_t(q);
   }
-  for (uint32_t k = 0; k < I.nh; ++k) {
-    const float* s = &I.hinge_st[4 * size_t(k)];
-    for (int a = 0; a < 4; ++a)
-      for (int b = 0; b < 4; ++b) {
-        float v = I.hinge_w[k] * s[a] * s[b];
-        if (std::fabs(v) > 1e-12f) tr.push_back({I.hinge_v[4 * k + a], I.hinge_v[4 * k + b], v});
-      }
-  }
-  std::stable_sort(tr.begin(), tr.end(), [](const Trip& a, const Trip& b) { return a.r != b.r ? a.r < b.r : a.c < b.c; });
   I.A_ptr.assign(nv + 1, 0);
-  for (size_t k = 0; k < tr.size();) {
-    size_t j = k;
-    double s = 0.0;
-    while (j < tr.size() && tr[j].r == tr[k].r && tr[j].c == tr[k].c) { s += double(tr[j].v); ++j; }
-    I.A_col.push_back(tr[k].c);
-    I.A_val.push_back(s);
-    I.A_ptr[tr[k].r + 1]++;
-    k = j;
+  I.A_col.reserve(size_t(nv) * 16);
+  I.A_val.reserve(size_t(nv) * 16);
+  std::vector<int32_t> slot_of(nv, -1);
+  std::vector<std::pair<uint32_t, double>> slots;
+  auto add = [&](uint32_t c, float v) {
+    int32_t& sl = slot_of[c];
+    if (sl < 0) { sl = int32_t(slots.size()); slots.push_back({c, 0.0}); }
+    slots[size_t(sl)].second += double(v);
+  };
+  for (uint32_t r = 0; r < nv; ++r) {
+    slots.clear();
+    add(r, I.mass[r] * inv_h2);
+    for (uint32_t e = tptr[r]; e < tptr[r + 1]; ++e) {
+      const uint32_t t = tinc[e] / 3, a = tinc[e] % 3;
+      const float* d = &I.dm_inv[4 * size_t(t)];
+      float g[3][2] = {{-(d[0] + d[1]), -(d[2] + d[3])}, {d[0], d[2]}, {d[1], d[3]}};
+      for (int b2 = 0; b2 < 3; ++b2) {
+        float dt_ = g[a][0] * g[b2][0] + g[a][1] * g[b2][1];
+        if (std::fabs(dt_) > 1e-12f) add(tris[3 * size_t(t) + b2], I.tri_w[t] * dt_);
+      }
+    }
+    for (uint32_t e = hptr[r]; e < hptr[r + 1]; ++e) {
+      const uint32_t k = hinc[e] / 4, a = hinc[e] % 4;
+      const float* st = &I.hinge_st[4 * size_t(k)];
+      for (int b2 = 0; b2 < 4; ++b2) {
+        float v = I.hinge_w[k] * st[a] * st[b2];
+        if (std::fabs(v) > 1e-12f) add(I.hinge_v[4 * size_t(k) + b2], v);
+      }
+    }
+    for (auto& x : slots) slot_of[x.first] = -1;
+    std::sort(slots.begin(), slots.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    for (auto& x : slots) { I.A_col.push_back(x.first); I.A_val.push_back(x.second); }
+    I.A_ptr[r + 1] = uint32_t(I.A_col.size());
   }
-  for (uint32_t i = 0; i < nv; ++i) I.A_ptr[i + 1] += I.A_ptr[i];
+  mirror_upper(nv, I.A_ptr, I.A_col, I.A_val);
   std::string err = factorize_csr(nv, I.A_ptr.data(), I.A_col.data(), I.A_val.data(), I.rest.data(), I.factor, status,
                                   prm.numeric);
   if (!err.empty()) return "Cholesky factorization failed: " + err;
   return "";
+}
+
+void mirror_upper(uint32_t n, std::vector<uint32_t>& ptr, std::vector<uint32_t>& col, std::vector<double>& val) {
+  std::vector<uint32_t> P(n + 1, 0);
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t q = ptr[i]; q < ptr[i + 1]; ++q) {
+      const uint32_t j = col[q];
+      if (j < i) continue;
+      P[i + 1]++;
+      if (j != i) P[j + 1]++;
+    }
+  for (uint32_t i = 0; i < n; ++i) P[i + 1] += P[i];
+  std::vector<uint32_t> C(P[n]), cur(P.begin(), P.end() - 1);
+  std::vector<double> V(P[n]);
+  // row i receives its lower entries while the rows j < i are visited, before
+  // its own upper ones: every row comes out sorted
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t q = ptr[i]; q < ptr[i + 1]; ++q) {
+      const uint32_t j = col[q];
+      if (j < i) continue;
+      C[cur[i]] = j; V[cur[i]++] = val[q];
+      if (j != i) { C[cur[j]] = i; V[cur[j]++] = val[q]; }
+    }
+  ptr.swap(P);
+  col.swap(C);
+  val.swap(V);
 }
 
 void append_permuted_matrix(const InstanceSetup& I, uint32_t base, std::vector<uint32_t>& ptr,

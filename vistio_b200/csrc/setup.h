@@ -120,6 +120,12 @@ std::string build_instance(uint32_t nv, const float* px, const float* py, const 
                            uint32_t nt, const uint32_t* tris, const uint8_t* pinned,
                            const SetupParams& prm, InstanceSetup& out, int* status);
 
+// Replaces a CSR matrix (rows sorted) by the symmetric matrix its upper
+// triangle (column >= row) defines, rows sorted: what faer factors with
+// Side::Upper (crates/vistio-math/src/faer_solver.rs:84-88). Mirrored pairs of
+// a PD system matrix can differ in the last bit (w s_a s_b against w s_b s_a).
+void mirror_upper(uint32_t n, std::vector<uint32_t>& ptr, std::vector<uint32_t>& col, std::vector<double>& val);
+
 // Appends I's system matrix with rows and columns in solve (permuted) order:
 // for each permuted row r the end offset to ptr, and its entries (column
 // base + iperm[col], f64 value) to col / val. ptr starts as {0} (or the end of

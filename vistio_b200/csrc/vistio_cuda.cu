@@ -1507,18 +1507,14 @@ vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_
     k = j;
   }
   for (uint32_t i = 0; i < n; ++i) f->A_ptr[i + 1] += f->A_ptr[i];
-  // faer reads the upper triangle (Side::Upper): mirror A's upper part.
-  std::vector<uint32_t> up_ptr(n + 1, 0), up_col;
-  std::vector<double> up_val;
-  for (uint32_t i = 0; i < n; ++i) {
-    for (uint32_t p = f->A_ptr[i]; p < f->A_ptr[i + 1]; ++p)
-      if (f->A_col[p] >= i) { up_col.push_back(f->A_col[p]); up_val.push_back(f->A_val[p]); }
-    up_ptr[i + 1] = uint32_t(up_col.size());
-  }
+  // faer reads the upper triangle (Side::Upper): the symmetric matrix it defines
+  std::vector<uint32_t> sym_ptr = f->A_ptr, sym_col = f->A_col;
+  std::vector<double> sym_val = f->A_val;
+  mirror_upper(n, sym_ptr, sym_col, sym_val);
   // the host finds the ordering and the symbolic structure; the numeric
   // factorization runs on the device (k_front) when the batch is packed
   int st = 0;
-  std::string err = factorize_csr(n, up_ptr.data(), up_col.data(), up_val.data(), nullptr, f->f, &st, false);
+  std::string err = factorize_csr(n, sym_ptr.data(), sym_col.data(), sym_val.data(), nullptr, f->f, &st, false);
   if (!err.empty()) return fail(ctx, st == 11 ? VISTIO_ERR_NOT_SPD : VISTIO_ERR_INVALID_CONFIG, err);
   // Device layout: a one-instance batch with no elements.
   auto* s = new vistio_solver();
@@ -1526,25 +1522,10 @@ vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_
   s->cfg.max_iterations = 1;
   s->setup.nv = n;
   s->setup.factor = f->f;
-  {  // the symmetric matrix the upper triangle defines, rows in original order
-    std::vector<uint32_t>& P = s->setup.A_ptr;
-    P.assign(n + 1, 0);
-    for (uint32_t i = 0; i < n; ++i)
-      for (uint32_t q = up_ptr[i]; q < up_ptr[i + 1]; ++q) {
-        P[i + 1]++;
-        if (up_col[q] != i) P[up_col[q] + 1]++;
-      }
-    for (uint32_t i = 0; i < n; ++i) P[i + 1] += P[i];
-    s->setup.A_col.resize(P[n]);
-    s->setup.A_val.resize(P[n]);
-    std::vector<uint32_t> cur(P.begin(), P.end() - 1);
-    for (uint32_t i = 0; i < n; ++i)
-      for (uint32_t q = up_ptr[i]; q < up_ptr[i + 1]; ++q) {
-        const uint32_t j = up_col[q];
-        s->setup.A_col[cur[i]] = j; s->setup.A_val[cur[i]++] = up_val[q];
-        if (j != i) { s->setup.A_col[cur[j]] = i; s->setup.A_val[cur[j]++] = up_val[q]; }
-      }
-  }
+  // the symmetric matrix the upper triangle defines, rows in original order
+  s->setup.A_ptr.swap(sym_ptr);
+  s->setup.A_col.swap(sym_col);
+  s->setup.A_val.swap(sym_val);
   s->setup.mass.assign(n, 0.f);
   s->setup.pinned.assign(n, 0);
   s->setup.prm.matrix_dt = 1.f;

@@ -19,6 +19,11 @@ definitions are therefore this module's and are stated at each field.
 
 A body mesh is not simulated: the solver's obstacles are the analytical
 colliders of `api.Contact` (ground, sphere, cylinder, box).
+
+`JsonFrameExporter` writes an animation in the layout of the reference's
+JSON frame exporter (crates/vistio-render/src/json_exporter.rs:14-104), with
+every position printed as the shortest decimal that reads back as the same
+f32, the form serde_json gives an f32.
 """
 from __future__ import annotations
 
@@ -209,6 +214,89 @@ class SimulationOutput:
                                 SimulationMetrics(**d["metrics"]))
 
 
+def _json_f32(v) -> str:
+    """The JSON text of an f32: the shortest decimal that reads back as the same
+    float, positional for 1e-6 <= |v| < 1e13 ("0.1", "100.0", "0.000123"),
+    else d.ddde<k> ("1e-7", "1.5e20"); a non-finite value is null."""
+    f = np.float32(v)
+    if not np.isfinite(f):
+        return "null"
+    if f == 0:
+        return "-0.0" if np.signbit(f) else "0.0"
+    mant, exp = np.format_float_scientific(f, unique=True, trim="-").split("e")
+    neg = mant.startswith("-")
+    digits = mant.lstrip("-").replace(".", "")
+    n = len(digits)
+    kk = int(exp) + 1  # 10^(kk-1) <= |v| < 10^kk
+    k = kk - n         # the power of ten of the last digit
+    if 0 <= k and kk <= 13:
+        out = digits + "0" * k + ".0"
+    elif 0 < kk <= 13:
+        out = digits[:kk] + "." + digits[kk:]
+    elif -6 < kk <= 0:
+        out = "0." + "0" * (-kk) + digits
+    elif n == 1:
+        out = f"{digits}e{kk - 1}"
+    else:
+        out = f"{digits[0]}.{digits[1:]}e{kk - 1}"
+    return "-" + out if neg else out
+
+
+def _json_f32_array(a) -> str:
+    out = []
+    for x in np.asarray(a, np.float32).ravel():
+        t = str(x)  # numpy's shortest text: the same where it is positional
+        out.append(t if np.isfinite(x) and "e" not in t else _json_f32(x))
+    return "[" + ",".join(out) + "]"
+
+
+class JsonFrameExporter:
+    """JsonFrameExporter (json_exporter.rs:39-104): collects the positions of
+    every submitted frame and writes the whole animation to one JSON file on
+    finalize(): {"vertex_count", "triangle_count", "indices", "frames":
+    [{"timestep", "positions": [x0, y0, z0, x1, ...]}]}, compact as
+    serde_json::to_string writes it. The frames are handed over on finalize()
+    (frame_count() is 0 afterwards)."""
+
+    def __init__(self, output_path: str):
+        self.output_path = str(output_path)
+        self.indices: List[int] = []
+        self.vertex_count = 0
+        self.triangle_count = 0
+        self.frames: List[tuple] = []
+
+    def init(self, mesh):
+        """From a TriangleMesh of the contract or a scenarios.Mesh."""
+        if isinstance(mesh, TriangleMesh):
+            self.vertex_count, self.triangle_count = mesh.vertex_count(), mesh.triangle_count()
+            self.indices = [int(i) for i in mesh.indices]
+        else:
+            self.vertex_count, self.triangle_count = mesh.nv, mesh.nt
+            self.indices = [int(i) for i in np.asarray(mesh.tris).ravel()]
+
+    def submit_frame(self, timestep: int, positions):
+        """positions: (V, 3) (or the three coordinate arrays stacked that way)."""
+        self.frames.append((int(timestep), np.array(positions, np.float32).reshape(-1, 3)))
+
+    def finalize(self):
+        frames, self.frames = self.frames, []
+        parts = [f'{{"vertex_count":{self.vertex_count},"triangle_count":{self.triangle_count},"indices":[',
+                 ",".join(str(i) for i in self.indices), '],"frames":[']
+        parts.append(",".join(f'{{"timestep":{t},"positions":{_json_f32_array(x)}}}' for t, x in frames))
+        parts.append("]}")
+        try:
+            with open(self.output_path, "w") as f:
+                f.write("".join(parts))
+        except OSError as e:
+            raise L.VistioError(4, f"{self.output_path}: {e}") from None
+
+    def name(self) -> str:
+        return "json_exporter"
+
+    def frame_count(self) -> int:
+        return len(self.frames)
+
+
 def validate_input(inp: SimulationInput):
     """validate_input (validator.rs:17-90): raises VistioError with the
     reference's messages."""
@@ -314,10 +402,16 @@ def _membrane(rest: np.ndarray, x: np.ndarray, tris: np.ndarray, stiffness: floa
     return strain, energy
 
 
-def simulate(inp: SimulationInput, contact: Optional[api.Contact] = None, ctx=None) -> SimulationOutput:
+def simulate(inp: SimulationInput, contact: Optional[api.Contact] = None, ctx=None, ipc: bool = True,
+             exporter: Optional[JsonFrameExporter] = None) -> SimulationOutput:
     """Runs `inp` on the GPU solver: round(duration / dt) steps, each a plain
     PD step, or a step with IPC contact against `contact`'s colliders (its
-    self-contact thickness defaults to the input's contact_thickness)."""
+    self-contact thickness defaults to the input's contact_thickness). With
+    ipc=False the colliders act as the runner's non-IPC branch has them: a
+    plain step, then their resolve() projections (runner.rs:209-215).
+    `exporter`, when given, is initialised with the garment and receives the
+    positions after every step (timestep 0, 1, ...); finalize() is the
+    caller's."""
     validate_input(inp)
     if inp.body is not None:
         raise L.VistioError(3, "A body mesh is not simulated: pass the obstacles as analytical colliders (Contact)")
@@ -329,12 +423,23 @@ def simulate(inp: SimulationInput, contact: Optional[api.Contact] = None, ctx=No
     if contact is not None and contact.self_collision and contact.thickness == 0.0:
         contact = dataclasses.replace(contact, thickness=p.contact_thickness)
     s = api.ProjectiveDynamicsSolver(ctx).init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
+    if contact is not None and not ipc and contact.has_ground:
+        s.set_ground(contact.ground_height)  # runner.rs:152-157
     steps = max(1, int(round(p.duration / p.dt)))
+    if exporter is not None:
+        exporter.init(inp.garment)
     t0 = time.perf_counter()
     iters = 0
-    for _ in range(steps):
-        r = s.step_with_ipc(p.dt, contact) if contact is not None else s.step(p.dt)
+    for k in range(steps):
+        if contact is not None and ipc:
+            r = s.step_with_ipc(p.dt, contact)
+        else:
+            r = s.step(p.dt)
+            if contact is not None:
+                s.resolve_contacts(contact)
         iters += r.iterations
+        if exporter is not None:
+            exporter.submit_frame(k, s.state()[0])
     wall = time.perf_counter() - t0
     x, v = s.state()
     rest = np.stack([mesh.px, mesh.py, mesh.pz], 1)
@@ -345,7 +450,7 @@ def simulate(inp: SimulationInput, contact: Optional[api.Contact] = None, ctx=No
     gdir = np.asarray(p.gravity_direction, np.float64)
     kinetic = 0.5 * float(np.sum(m[free] * np.sum(v[free].astype(np.float64) ** 2, 1)))
     potential = float(np.sum(m[free] * p.gravity * -(x[free].astype(np.float64) @ gdir)))
-    force = s.contact_force() if contact is not None else np.zeros(mesh.nv, np.float32)
+    force = s.contact_force() if contact is not None and ipc else np.zeros(mesh.nv, np.float32)
     nrm = _vertex_normals(x, mesh.tris)
     g = inp.garment
     draped = TriangleMesh(_f32(x[:, 0]), _f32(x[:, 1]), _f32(x[:, 2]), _f32(nrm[:, 0]), _f32(nrm[:, 1]),
