@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--ipc-instances", type=int, default=64,
                     help="sphere drapes of the contact measurement (0: skip it)")
     ap.add_argument("--ipc-only", action="store_true", help="run only the contact measurement and print it")
+    ap.add_argument("--serve-only", action="store_true", help="run only the served stream and print it")
+    ap.add_argument("--serve-gpu-factorization", action="store_true",
+                    help="served stream: factorize each set-up on the GPU at cohort start (host threads otherwise)")
     ap.add_argument("--serve-seconds", type=float, default=1.0,
                     help="arrival window of the served-stream measurement (0 skips it)")
     ap.add_argument("--refine", type=int, default=None,
@@ -242,7 +245,7 @@ def ipc_batch(n, steps=10, warmup=5, threads=None):
                    "grid sides and materials of the batched workload, CUDA events over the timed steps"}
 
 
-def served_stream(window_s, rate=200.0, seed=20261203, threads=None):
+def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factorization=False):
     """The served drape stream: Poisson arrivals at `rate` req/s during
     `window_s` seconds, half sphere drapes (the sphere-drape geometry at the
     drawn side, IPC d_hat 1e-3, kappa 1e4, AL <= 5, 15 iterations) and half
@@ -266,7 +269,8 @@ def served_stream(window_s, rate=200.0, seed=20261203, threads=None):
     cfg_s = api.drape_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=1e-3, barrier_kappa=1e4)
     cfg_p = api.drape_config(max_iterations=ITERS)
     srv = api.Server(hbm_budget_bytes=120 << 30, max_cohort=64, setup_threads=threads or (os.cpu_count() or 4),
-                     steps_per_slice=10, cache_bytes=2 << 30)
+                     steps_per_slice=10, cache_bytes=2 << 30, gpu_factorization=gpu_factorization)
+    sym0 = api.symbolic_cache_info()
     t0 = time.perf_counter()
     k = 0
     while k < len(arrivals):
@@ -286,6 +290,7 @@ def served_stream(window_s, rate=200.0, seed=20261203, threads=None):
     srv.drain(3600)
     st = srv.stats()
     srv.close()
+    sym1 = api.symbolic_cache_info()
     return {"window_s": window_s, "rate_per_s": rate, "requests": len(arrivals),
             "sphere_requests": sum(a["sphere"] for a in arrivals),
             "completed": st["completed"], "failed": st["failed"],
@@ -293,6 +298,8 @@ def served_stream(window_s, rate=200.0, seed=20261203, threads=None):
             "latency_s": {"p50": st["p50_latency_s"], "p99": st["p99_latency_s"], "mean": st["mean_latency_s"]},
             "max_cohorts_active": st["max_cohorts_active"], "peak_device_bytes": st["max_bytes_in_use"],
             "setup_cache": {"hits": st["cache_hits"], "misses": st["cache_misses"]},
+            "factorization": "GPU (cohort start)" if gpu_factorization else "host (set-up threads)",
+            "symbolic_cache": {"hits": sym1["hits"] - sym0["hits"], "misses": sym1["misses"] - sym0["misses"]},
             "how": "Poisson arrivals at the stated rate during the window, then drained; each request 300 steps"}
 
 
@@ -378,12 +385,24 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return
+    if args.serve_only:
+        if rank == 0:
+            print(json.dumps({"serving": served_stream(args.serve_seconds,
+                                                       gpu_factorization=args.serve_gpu_factorization)}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     threads = max(1, (os.cpu_count() or 1) // max(1, world))
     specs = workload(args.instances, rank)
+    from vistio_b200 import api as _api
+    sym0 = _api.symbolic_cache_info()
     t0 = time.time()
     batch, solvers, order = build_batch(specs, threads, args.refine)
     setup_s = time.time() - t0
+    sym1 = _api.symbolic_cache_info()
+    symbolic = {"hits": sym1["hits"] - sym0["hits"], "misses": sym1["misses"] - sym0["misses"],
+                "host_threads": threads}
     tune = batch.tune()  # level schedule picked by timing this batch's sweeps
     info = batch.info()
     V = info["vertices"]
@@ -496,7 +515,7 @@ def main():
            "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
            "clocks": clocks, "roofline": roofline,
            "batch": {"vertices": V, "triangles": T, "hinges": H, "factor_bytes": info["factor_bytes"],
-                     "setup_s": setup_s,
+                     "setup_s": setup_s, "symbolic_cache": symbolic,
                      "factorization": dict(batch.factor_stats(), where="GPU, multifrontal FP64, every garment")}}
 
     if rank == 0 and not args.no_baselines:
@@ -544,7 +563,7 @@ def main():
                                "sample": f"one instance of each of the {len(sample)} topologies x {cpu_steps} steps "
                                          f"({secs:.1f} s); each topology is 1/8 of the workload"}
         if args.serve_seconds > 0:
-            out["serving"] = served_stream(args.serve_seconds)
+            out["serving"] = served_stream(args.serve_seconds, gpu_factorization=args.serve_gpu_factorization)
         # accuracy of the measured run: the metric is quoted at <= 1e-4 m against FP64
         out["error_vs_fp64"] = fp64_error(specs, order, batch, args.warmup + args.steps + e2e_steps,
                                           os.cpu_count() or 1)

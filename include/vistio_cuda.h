@@ -410,6 +410,19 @@ vistio_status vistio_server_get_stats(vistio_server* s, vistio_server_stats* st)
  * fault. */
 vistio_status vistio_diag_wait_timeout(vistio_ctx* ctx, uint32_t polls);
 
+/* ---- symbolic analysis cache ---- */
+/* The host keeps the symbolic factorizations it computes (ordering,
+ * supernodes, row structures, sweep schedules) in a process-wide cache keyed
+ * by the exact matrix pattern and dissection order; a hit returns what a new
+ * analysis would compute. Garments that share a mesh topology, at any uniform
+ * scale, then pay for the analysis once. It serves the set-ups whose numbers
+ * are factorized on the GPU (host_factorization = 0, the default) and
+ * vistio_sparse_factorize. No counterpart in the reference. */
+vistio_status vistio_symbolic_cache_info(uint64_t* hits, uint64_t* misses, uint64_t* bytes, uint64_t* entries);
+/* Bound on the bytes it holds (default 1 GiB), least recently used out
+ * first; 0 empties and disables it. */
+vistio_status vistio_symbolic_cache_set_limit(uint64_t bytes);
+
 /* ---- SparseSolver mirror ---- */
 vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
                                       const float* values, vistio_factor** out);

@@ -108,3 +108,27 @@ def test_quad_grid_matches_reference_generator():
                               t.ctypes.data_as(C.POINTER(C.c_uint32)))
         assert np.array_equal(px, a[0]) and np.array_equal(py, a[1]) and np.array_equal(pz, a[2])
         assert np.array_equal(tris.reshape(-1), t)
+
+
+def test_symbolic_cache_hits_equal_fresh_analyses(tmp_path):
+    """The host's symbolic-analysis cache (factorize_csr, numeric = false): a hit
+    is the Factor a fresh analysis gives, field for field (grids with pins, DS
+    bending, perturbed geometry); uniformly scaled copies of a grid share one
+    entry; concurrent set-ups of one mesh run one analysis; the byte bound
+    evicts, and 0 empties it."""
+    out = str(tmp_path / "scc")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-o", out,
+                           os.path.join(ROOT, "tests", "cpp", "symbolic_cache_check.cpp"),
+                           os.path.join(ROOT, "vistio_b200", "csrc", "setup.cpp"), "-lpthread"])
+    r = json.loads(subprocess.check_output([out]))
+    assert r["identical"] == r["cases"] and r["scaled_same"] == r["scales"], r
+    assert r["scaled_ok"] and r["concurrent_ok"] and r["evict_ok"] and r["zero_ok"], r
+
+
+def test_symbolic_cache_entry_points_without_a_device():
+    from vistio_b200 import api
+    info = api.symbolic_cache_info()
+    assert set(info) == {"hits", "misses", "bytes", "entries"}
+    api.set_symbolic_cache_limit(0)
+    assert api.symbolic_cache_info()["entries"] == 0
+    api.set_symbolic_cache_limit(1 << 30)

@@ -164,6 +164,8 @@ SIGNATURES = {
     "vistio_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
     "vistio_solver_device_bytes": (C.c_int, [_vp, C.c_int32, _u64p]),
     "vistio_sparse_factorize": (C.c_int, [_vp, C.c_uint32, _u32p, _u32p, _fp, C.POINTER(_vp)]),
+    "vistio_symbolic_cache_info": (C.c_int, [C.POINTER(C.c_uint64)] * 4),
+    "vistio_symbolic_cache_set_limit": (C.c_int, [C.c_uint64]),
     "vistio_sparse_solve": (C.c_int, [_vp, _fp, _fp]),
     "vistio_sparse_destroy": (C.c_int, [_vp]),
     "vistio_broadphase_pairs": (C.c_int, [_vp, C.c_uint32, _fp, _fp, _fp, C.c_uint32, _u32p, C.c_float, _u32p,

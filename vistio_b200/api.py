@@ -483,6 +483,18 @@ class Batch:
         return v.value
 
 
+def symbolic_cache_info() -> dict:
+    """The host's cache of symbolic factorizations (vistio_symbolic_cache_info)."""
+    vals = [C.c_uint64() for _ in range(4)]
+    L.check(L.lib().vistio_symbolic_cache_info(*[C.byref(v) for v in vals]))
+    return dict(zip(("hits", "misses", "bytes", "entries"), (v.value for v in vals)))
+
+
+def set_symbolic_cache_limit(nbytes: int):
+    """Bound the symbolic cache's bytes (0 empties and disables it)."""
+    L.check(L.lib().vistio_symbolic_cache_set_limit(int(nbytes)))
+
+
 class SparseSolver:
     """SparseSolver / FaerSolver mirror (crates/vistio-math/src/sparse.rs:110-120)."""
 

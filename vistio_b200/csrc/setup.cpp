@@ -5,10 +5,63 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <condition_variable>
+#include <memory>
+#include <mutex>
 #include <numeric>
+#include <unordered_map>
 
 namespace vistio {
 namespace {
+
+// Symbolic factors (numeric == false) keyed by the exact adjacency and
+// dissection order they were computed from. Everything factorize_csr derives
+// after the dissection (postorder, supernodes, row structures, schedules)
+// depends on nothing else, so a hit returns the Factor a fresh analysis would
+// build: garments that share a mesh pay for the analysis once. Entries hold
+// their key arrays and are compared in full; the cache is bounded in bytes and
+// evicts the least recently used entry first. An analysis in progress is
+// listed as pending: a thread that needs the same one waits for it instead of
+// repeating it (set-up threads tend to start on the same mesh together).
+struct SymEntry {
+  std::vector<uint32_t> ptr, adj, order;
+  std::shared_ptr<const Factor> factor;
+  uint64_t bytes = 0, used = 0;
+  bool same(const std::vector<uint32_t>& p, const std::vector<uint32_t>& a, const std::vector<uint32_t>& o) const {
+    return order == o && ptr == p && adj == a;
+  }
+};
+struct SymPending {
+  uint64_t key = 0;
+  SymEntry entry;     // the key arrays; `factor` is set when done
+  bool done = false;  // done without a factor: the analysis was abandoned
+};
+struct SymCache {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::unordered_multimap<uint64_t, SymEntry> map;
+  std::vector<std::shared_ptr<SymPending>> pending;
+  uint64_t bytes = 0, clock = 0, hits = 0, misses = 0, limit = uint64_t(1) << 30;
+};
+SymCache& sym_cache() {
+  static SymCache c;
+  return c;
+}
+
+uint64_t fnv_words(uint64_t h, const std::vector<uint32_t>& v) {
+  for (uint32_t w : v)
+    for (int b = 0; b < 4; ++b) { h ^= (w >> (8 * b)) & 0xffu; h *= 1099511628211ull; }
+  return h;
+}
+
+template <class T> uint64_t vec_bytes(const std::vector<T>& v) { return v.size() * sizeof(T); }
+
+uint64_t factor_bytes(const Factor& f) {
+  return vec_bytes(f.perm) + vec_bytes(f.iperm) + vec_bytes(f.sn) + vec_bytes(f.rows) + vec_bytes(f.row_sn) +
+         vec_bytes(f.level_ptr) + vec_bytes(f.level_rows) + vec_bytes(f.level_sn_ptr) + vec_bytes(f.level_sn) +
+         vec_bytes(f.sub_first) + vec_bytes(f.sub_last) + vec_bytes(f.fwd_ptr) + vec_bytes(f.fwd_sn) +
+         vec_bytes(f.fwd_pos);
+}
 
 struct F3 {
   float x, y, z;
@@ -122,9 +175,13 @@ class Dissector {
         lo[k] = std::min(lo[k], xyz_[3 * v + k]);
         hi[k] = std::max(hi[k], xyz_[3 * v + k]);
       }
+    // The longest axis, a later one only when clearly longer: extents equal up
+    // to rounding (a square sheet) give the same axis at every scale, so a
+    // uniformly scaled mesh gets the same ordering (and its symbolic factor
+    // comes from the cache).
     int ax = 0;
     for (int k = 1; k < 3; ++k)
-      if (hi[k] - lo[k] > hi[ax] - lo[ax]) ax = k;
+      if (hi[k] - lo[k] > (hi[ax] - lo[ax]) * (1.f + 1e-4f)) ax = k;
     std::stable_sort(verts.begin(), verts.end(),
                      [&](uint32_t a, uint32_t b) { return xyz_[3 * a + ax] < xyz_[3 * b + ax]; });
     size_t mid = verts.size() / 2;
@@ -229,6 +286,52 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
   }
   std::vector<uint32_t> order;
   Dissector(g, coords).run(order);
+  std::shared_ptr<SymPending> mine;  // this call's analysis, while pending
+  if (!numeric) {
+    const uint64_t key = fnv_words(fnv_words(fnv_words(14695981039346656037ull, g.ptr), g.adj), order);
+    SymCache& C = sym_cache();
+    std::unique_lock<std::mutex> lk(C.mu);
+    for (;;) {
+      auto range = C.map.equal_range(key);
+      for (auto it = range.first; it != range.second; ++it)
+        if (it->second.same(g.ptr, g.adj, order)) {
+          it->second.used = ++C.clock;
+          C.hits++;
+          f = *it->second.factor;
+          return "";
+        }
+      std::shared_ptr<SymPending> other;
+      for (auto& p : C.pending)
+        if (p->key == key && p->entry.same(g.ptr, g.adj, order)) { other = p; break; }
+      if (!other) break;
+      C.cv.wait(lk, [&] { return other->done; });
+      if (other->entry.factor) {
+        C.hits++;
+        f = *other->entry.factor;
+        return "";
+      }  // abandoned: look again
+    }
+    C.misses++;
+    mine = std::make_shared<SymPending>();
+    mine->key = key;
+    mine->entry.ptr = g.ptr;
+    mine->entry.adj = g.adj;
+    mine->entry.order = order;
+    C.pending.push_back(mine);
+  }
+  // An early return leaves the pending analysis abandoned, and its waiters
+  // compute their own.
+  struct Abandon {
+    std::shared_ptr<SymPending>& p;
+    ~Abandon() {
+      if (!p) return;
+      SymCache& C = sym_cache();
+      std::lock_guard<std::mutex> lk(C.mu);
+      p->done = true;
+      C.pending.erase(std::find(C.pending.begin(), C.pending.end(), p));
+      C.cv.notify_all();
+    }
+  } abandon{mine};
   // Elimination tree of the permuted matrix, then a postorder so every
   // subtree is a contiguous column range.
   auto etree_of = [&](const std::vector<uint32_t>& perm, std::vector<uint32_t>& ip, std::vector<int>& parent) {
@@ -552,7 +655,52 @@ std::string factorize_csr(uint32_t n, const uint32_t* row_ptr, const uint32_t* c
       f.fwd_sn[q] = k;
       f.fwd_pos[q] = r;
     }
+  if (mine) {
+    SymCache& C = sym_cache();
+    std::lock_guard<std::mutex> lk(C.mu);
+    SymEntry& e = mine->entry;
+    e.factor = std::make_shared<const Factor>(f);
+    e.bytes = factor_bytes(f) + vec_bytes(e.ptr) + vec_bytes(e.adj) + vec_bytes(e.order);
+    if (e.bytes <= C.limit) {
+      while (C.bytes + e.bytes > C.limit && !C.map.empty()) {
+        auto victim = C.map.begin();
+        for (auto it = C.map.begin(); it != C.map.end(); ++it)
+          if (it->second.used < victim->second.used) victim = it;
+        C.bytes -= victim->second.bytes;
+        C.map.erase(victim);
+      }
+      e.used = ++C.clock;
+      C.bytes += e.bytes;
+      C.map.emplace(mine->key, e);
+    }
+    mine->done = true;  // waiters take the factor from the pending record
+    C.pending.erase(std::find(C.pending.begin(), C.pending.end(), mine));
+    C.cv.notify_all();
+    mine.reset();
+  }
   return "";
+}
+
+void symbolic_cache_info(uint64_t* hits, uint64_t* misses, uint64_t* bytes, uint64_t* entries) {
+  SymCache& C = sym_cache();
+  std::lock_guard<std::mutex> lk(C.mu);
+  if (hits) *hits = C.hits;
+  if (misses) *misses = C.misses;
+  if (bytes) *bytes = C.bytes;
+  if (entries) *entries = C.map.size();
+}
+
+void symbolic_cache_set_limit(uint64_t limit_bytes) {
+  SymCache& C = sym_cache();
+  std::lock_guard<std::mutex> lk(C.mu);
+  C.limit = limit_bytes;
+  while (C.bytes > C.limit && !C.map.empty()) {
+    auto victim = C.map.begin();
+    for (auto it = C.map.begin(); it != C.map.end(); ++it)
+      if (it->second.used < victim->second.used) victim = it;
+    C.bytes -= victim->second.bytes;
+    C.map.erase(victim);
+  }
 }
 
 // ----------------------------------------------------------- instance
@@ -603,17 +751,34 @@ std::string build_instance(uint32_t nv, const float* px, const float* py, const 
   // Interior edges (topology.rs:58-121), kept sorted by (v0, v1). The wing of
   // tri_a comes from the lower-indexed triangle.
   if (prm.bending != BEND_NONE) {
-    std::vector<std::pair<uint64_t, uint32_t>> he;  // (edge key, triangle)
-    he.reserve(3 * size_t(nt));
-    for (uint32_t t = 0; t < nt; ++t) {
-      uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
-      uint32_t e[3][2] = {{a, b}, {b, c}, {c, a}};
-      for (auto& x : e) {
-        uint32_t lo = std::min(x[0], x[1]), hi = std::max(x[0], x[1]);
-        he.push_back({(uint64_t(lo) << 32) | hi, t});
+    // Half-edges (edge key, triangle) in stable (lo, hi) order: bucketed by the
+    // lower vertex in triangle order, then each short bucket insertion-sorted
+    // by the higher one.
+    std::vector<uint32_t> lo_ptr(nv + 1, 0);
+    for (size_t q = 0; q < 3 * size_t(nt); ++q) {
+      uint32_t x = tris[q], y = tris[q % 3 == 2 ? q - 2 : q + 1];
+      lo_ptr[std::min(x, y) + 1]++;
+    }
+    for (uint32_t i = 0; i < nv; ++i) lo_ptr[i + 1] += lo_ptr[i];
+    std::vector<std::pair<uint64_t, uint32_t>> he(3 * size_t(nt));
+    {
+      std::vector<uint32_t> fill(lo_ptr.begin(), lo_ptr.end() - 1);
+      for (uint32_t t = 0; t < nt; ++t) {
+        uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
+        uint32_t e[3][2] = {{a, b}, {b, c}, {c, a}};
+        for (auto& x : e) {
+          uint32_t lo = std::min(x[0], x[1]), hi = std::max(x[0], x[1]);
+          he[fill[lo]++] = {(uint64_t(lo) << 32) | hi, t};
+        }
       }
     }
-    std::stable_sort(he.begin(), he.end(), [](auto& x, auto& y) { return x.first < y.first; });
+    for (uint32_t v = 0; v < nv; ++v)
+      for (uint32_t i = lo_ptr[v] + 1; i < lo_ptr[v + 1]; ++i) {
+        auto x = he[i];
+        uint32_t j = i;
+        for (; j > lo_ptr[v] && he[j - 1].first > x.first; --j) he[j] = he[j - 1];
+        he[j] = x;
+      }
     auto wing = [&](uint32_t t, uint32_t v0, uint32_t v1) {
       uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
       if (a != v0 && a != v1) return a;

@@ -120,6 +120,13 @@ std::string build_instance(uint32_t nv, const float* px, const float* py, const 
                            uint32_t nt, const uint32_t* tris, const uint8_t* pinned,
                            const SetupParams& prm, InstanceSetup& out, int* status);
 
+// The process-wide cache of symbolic factors (factorize_csr with numeric ==
+// false), keyed by the exact adjacency and dissection order: counters, bytes
+// held and entries; and its byte bound (default 1 GiB; 0 disables it and
+// empties it).
+void symbolic_cache_info(uint64_t* hits, uint64_t* misses, uint64_t* bytes, uint64_t* entries);
+void symbolic_cache_set_limit(uint64_t limit_bytes);
+
 // Replaces a CSR matrix (rows sorted) by the symmetric matrix its upper
 // triangle (column >= row) defines, rows sorted: what faer factors with
 // Side::Upper (crates/vistio-math/src/faer_solver.rs:84-88). Mirrored pairs of

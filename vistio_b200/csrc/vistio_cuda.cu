@@ -1480,6 +1480,16 @@ vistio_status vistio_batch_phase_bytes(const vistio_batch* b, int32_t phase, uin
 }
 
 // ---- SparseSolver mirror (sparse.rs:110-120, faer_solver.rs:67-129) ----
+vistio_status vistio_symbolic_cache_info(uint64_t* hits, uint64_t* misses, uint64_t* bytes, uint64_t* entries) {
+  symbolic_cache_info(hits, misses, bytes, entries);
+  return VISTIO_OK;
+}
+
+vistio_status vistio_symbolic_cache_set_limit(uint64_t bytes) {
+  symbolic_cache_set_limit(bytes);
+  return VISTIO_OK;
+}
+
 vistio_status vistio_sparse_factorize(vistio_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
                                       const float* values, vistio_factor** out) {
   if (!ctx || !row_ptr || !col_idx || !values || !out) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null argument");
