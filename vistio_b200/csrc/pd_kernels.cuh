@@ -136,7 +136,9 @@ struct BatchDev {
   // dependency-driven sweeps (k_sweep): work units in forward order (see
   // SweepUnit), the supernodal tree, per-supernode counters (zero between
   // sweeps) and the two work queues
-  const uint2* df_units;
+  const uint2* df_units;       // backward sweep, taken from the end
+  const uint2* df_units_fwd;   // forward sweep: top supernodes deepest first
+  const uint32_t* df_items_fwd;  // warp supernodes of the forward units
   const uint32_t* df_parent;   // parent supernode (global id) or kNoParent
   const uint32_t* df_nkids;
   const uint32_t* df_kid_ptr;
@@ -1014,7 +1016,7 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_sweep(Bat
     __syncthreads();
     const uint32_t q = s_unit;
     if (q >= nunits) break;
-    const uint2 u = B.df_units[DIR == 0 ? q : nunits - 1 - q];
+    const uint2 u = DIR == 0 ? B.df_units_fwd[q] : B.df_units[nunits - 1 - q];
     const uint32_t kind = u.x & 3u, count = u.x >> 2;
     if (kind == 1) {
       const uint32_t k = u.y;
@@ -1038,7 +1040,7 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_sweep(Bat
         __syncwarp();
         if (DIR == 0) dep_leave<0>(B, it.y, lane, 32);
       } else {
-        const uint32_t k = B.lvl_items[u.y + warp];
+        const uint32_t k = (DIR == 0 ? B.df_items_fwd : B.lvl_items)[u.y + warp];
         const SnDev S = B.sn[k];
         if (ipc && B.red[S.inst].al_done) continue;
         if (lane == 0) dep_enter<DIR>(B, k);

@@ -165,7 +165,12 @@ struct vistio_batch {
   // sweeps: 0 = one launch per level (k_level), 1 = dependency-driven (k_sweep)
   uint32_t sweep_mode = 1;
   std::vector<uint2> units_host;                    // k_sweep work units in forward order
-  uint32_t n_units = 0;
+  uint32_t n_units = 0, n_units_fwd = 0;
+  std::vector<uint2> units_fwd_host;                // k_sweep<0> units: top supernodes deepest first
+  std::vector<uint32_t> items_fwd_host;             // their warp supernodes, bundled by depth
+  std::vector<uint32_t> sn_depth;                   // ancestors of each supernode in its tree
+  DevBuf<uint2> df_units_fwd;
+  DevBuf<uint32_t> df_items_fwd;
   DevBuf<uint2> df_units;
   DevBuf<uint32_t> df_parent, df_nkids, df_kid_ptr, df_kids, df_cnt, df_flag, df_queue;
   DevBuf<SnDev> sn;
@@ -238,6 +243,37 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
       b->units_host.push_back(make_uint2(2u | (std::min(kSolveWarps, nw - i) << 2), off + nb + i));
   }
   b->n_units = uint32_t(b->units_host.size());
+  // The forward sweep's critical path runs from the deepest supernodes of the
+  // tallest trees to their roots. Its units: the bottom subtrees as above,
+  // then the top supernodes by depth below their root, deepest first (blocks,
+  // then warp supernodes by eight of one depth), so the tall trees' chains
+  // start while the short trees' supernodes fill the GPU. Children are deeper
+  // than their parent: the order stays topological.
+  {
+    uint32_t D = 0;
+    for (auto& t : b->top) D = std::max(D, b->sn_depth[t.second] + 1);
+    std::vector<std::vector<uint32_t>> dblk(D), dwrp(D);
+    for (auto& t : b->top) {
+      const SnDev& S = b->sn_host[t.second];
+      (warp_item(S.ncols, S.nrows, limit) ? dwrp : dblk)[b->sn_depth[t.second]].push_back(t.second);
+    }
+    b->units_fwd_host.clear();
+    b->items_fwd_host.clear();
+    for (uint32_t q = 0; q < b->n_sub; q += kSolveWarps)
+      b->units_fwd_host.push_back(make_uint2(0u | (std::min(kSolveWarps, b->n_sub - q) << 2), q));
+    for (uint32_t d = D; d-- > 0;) {
+      std::stable_sort(dblk[d].begin(), dblk[d].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
+      std::stable_sort(dwrp[d].begin(), dwrp[d].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
+      for (uint32_t k : dblk[d]) b->units_fwd_host.push_back(make_uint2(1u | (1u << 2), k));
+      for (size_t i = 0; i < dwrp[d].size(); i += kSolveWarps) {
+        const uint32_t off = uint32_t(b->items_fwd_host.size());
+        const uint32_t cnt = uint32_t(std::min<size_t>(kSolveWarps, dwrp[d].size() - i));
+        b->items_fwd_host.insert(b->items_fwd_host.end(), dwrp[d].begin() + i, dwrp[d].begin() + i + cnt);
+        b->units_fwd_host.push_back(make_uint2(2u | (cnt << 2), off));
+      }
+    }
+    b->n_units_fwd = uint32_t(b->units_fwd_host.size());
+  }
   return items;
 }
 
@@ -248,6 +284,12 @@ cudaError_t upload_schedule(vistio_batch* b, const std::vector<uint32_t>& items,
   if (!items.empty()) e = cudaMemcpyAsync(b->lvl_items.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && !b->units_host.empty())
     e = cudaMemcpyAsync(b->df_units.p, b->units_host.data(), b->units_host.size() * sizeof(uint2),
+                        cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !b->units_fwd_host.empty())
+    e = cudaMemcpyAsync(b->df_units_fwd.p, b->units_fwd_host.data(), b->units_fwd_host.size() * sizeof(uint2),
+                        cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !b->items_fwd_host.empty())
+    e = cudaMemcpyAsync(b->df_items_fwd.p, b->items_fwd_host.data(), b->items_fwd_host.size() * 4,
                         cudaMemcpyHostToDevice, st);
   return e;
 }
@@ -539,7 +581,6 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   }
   b->sn_host = sn;
   b->n_sub = uint32_t(subs.size());
-  std::vector<uint32_t> items = schedule_levels(b, b->warp_limit);
   // the supernodal tree for the dependency-driven sweeps (global ids)
   std::vector<uint32_t> df_parent(NSN, kNoParent), df_nkids(NSN, 0), df_kid_ptr(NSN + 1, 0), df_kids;
   for (uint32_t k = 0; k < n; ++k) {
@@ -551,6 +592,11 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
         df_nkids[base + F.sn[q].parent]++;
       }
   }
+  // depth below the root: parents come after their children (postorder)
+  b->sn_depth.assign(NSN, 0);
+  for (uint64_t g = NSN; g-- > 0;)
+    if (df_parent[g] != kNoParent) b->sn_depth[g] = b->sn_depth[df_parent[g]] + 1;
+  std::vector<uint32_t> items = schedule_levels(b, b->warp_limit);
   for (uint64_t g = 0; g < NSN; ++g) df_kid_ptr[g + 1] = df_kid_ptr[g] + df_nkids[g];
   df_kids.resize(df_kid_ptr[NSN]);
   {
@@ -596,6 +642,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->lvl_items.upload(items, st));
   CU(b->sub_items.upload(subs, st));
   CU(b->df_units.alloc((b->n_sub + kSolveWarps - 1) / kSolveWarps + b->top.size() + 1, st));
+  CU(b->df_units_fwd.alloc((b->n_sub + kSolveWarps - 1) / kSolveWarps + b->top.size() + 1, st));
+  CU(b->df_items_fwd.alloc(b->top.size() + 1, st));
   CU(upload_schedule(b, items, st));
   CU(b->df_parent.upload(df_parent, st)); CU(b->df_nkids.upload(df_nkids, st));
   CU(b->df_kid_ptr.upload(df_kid_ptr, st)); CU(b->df_kids.upload(df_kids, st));
@@ -635,6 +683,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   d.sn = b->sn.p; d.rows = b->rows.p; d.vals = b->vals.p; d.lvl_items = b->lvl_items.p; d.sub_items = b->sub_items.p;
   d.fwd_ptr = b->fwd_ptr.p; d.fwd = b->fwd.p; d.U = b->U.p;
   d.df_units = b->df_units.p; d.df_parent = b->df_parent.p; d.df_nkids = b->df_nkids.p;
+  d.df_units_fwd = b->df_units_fwd.p; d.df_items_fwd = b->df_items_fwd.p;
   d.df_kid_ptr = b->df_kid_ptr.p; d.df_kids = b->df_kids.p; d.df_cnt = b->df_cnt.p; d.df_flag = b->df_flag.p;
   d.df_queue = b->df_queue.p;
   d.a_ptr = b->a_ptr.p; d.a_col = b->a_col.p; d.a_val = b->a_val.p; d.R0 = b->R0.p; d.W = b->W.p;
@@ -708,7 +757,7 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
 uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
   if (b->sweep_mode == 1 && b->n_units) {
     const uint32_t grid = std::min(b->n_units, b->ctx->sweep_blocks);
-    k_sweep<0><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units);
+    k_sweep<0><<<std::min(b->n_units_fwd, b->ctx->sweep_blocks), kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd);
     k_sweep<1><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units);
     return 2;
   }
