@@ -474,6 +474,9 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     d.has_ground = solvers[k]->has_ground; d.ground_h = solvers[k]->ground_h;
     d.sn_base = uint32_t(NSN); d.nsn = uint32_t(I.factor.sn.size());
     d.kappa = estimate_kappa(solvers[k]->cfg, I);
+    d.unit_stencils = 1;
+    for (size_t q = 0; q < I.hinge_st.size() && d.unit_stencils; ++q)
+      if (I.hinge_st[q] != ((q & 3u) < 2u ? -1.f : 1.f)) d.unit_stencils = 0;
     V += I.nv; T += I.nt; H += I.nh; NSN += I.factor.sn.size(); NROWS += I.factor.rows.size();
     for (const Supernode& X : I.factor.sn) NVALS += sn_floats(X.ncols, X.nrows);
     NLVL += I.factor.nlevels + 1; NFWD += I.factor.fwd_sn.size();
