@@ -313,12 +313,11 @@ __global__ void __launch_bounds__(256, 5) k_tri(BatchDev B) {
   o[6] = float(c2.x); o[7] = float(c2.y); o[8] = float(c2.z);
 }
 
-// Rotation of v = p - centre about `axis` by angle minus v itself:
-// (axis (axis . v) - v)(1 - cos) + (axis x v) sin (bending.rs:231-239).
-__device__ __forceinline__ float3 rot_delta(float3 v, float3 axis, float ang) {
-  float s = sinf(ang);
-  float h = sinf(0.5f * ang);
-  float omc = 2.f * h * h;  // 1 - cos, without cancellation
+// Rotation of v = p - centre about `axis` by an angle minus v itself:
+// (axis (axis . v) - v)(1 - cos) + (axis x v) sin (bending.rs:231-239), given
+// sin and 1 - cos. The two wings turn by +half and -half: the same 1 - cos and
+// opposite sines, so one pair of sines serves both.
+__device__ __forceinline__ float3 rot_delta(float3 v, float3 axis, float s, float omc) {
   float dt = dot3(axis, v);
   return (axis * dt - v) * omc + cross3(axis, v) * s;
 }
@@ -355,8 +354,10 @@ __global__ void __launch_bounds__(256) k_hinge(BatchDev B) {
       float sign = dot3(cross3(qa, qb), ed) >= 0.f ? 1.f : -1.f;
       float half = diff * 0.5f * sign;
       float3 mid = (p0 + p1) * 0.5f;
-      float3 da = rot_delta(pa - mid, ed, half);
-      float3 db = rot_delta(pb - mid, ed, -half);
+      const float s = sinf(half), hq = sinf(0.5f * half);
+      const float omc = 2.f * hq * hq;  // 1 - cos, without cancellation
+      float3 da = rot_delta(pa - mid, ed, s, omc);
+      float3 db = rot_delta(pb - mid, ed, -s, omc);
       out = (da * st.z + db * st.w) * wr.x;
     }
   }
