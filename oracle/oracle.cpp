@@ -1321,6 +1321,41 @@ int orc_step_ipc(void* sim, float dt, const orc_contact* c, orc_step_result* res
   return static_cast<SimBase*>(sim)->step_ipc(dt, c, res);
 }
 void orc_resolve(void* sim, const orc_contact* c, float* out) { static_cast<SimBase*>(sim)->resolve(c, out); }
+
+int orc_sparse_solve(uint32_t rows, uint32_t cols, const uint32_t* row_ptr, const uint32_t* col_idx,
+                     const float* vals, const float* rhs, float* sol) {
+  if (rows != cols) return 1;  // "Matrix must be square"
+  if (rows == 0) return 2;     // "Cannot factorize empty matrix"
+  const int n = int(rows);
+  // upper-triangle entries summed per (row, col) in f64, then mirrored
+  std::vector<std::map<int, double>> up(n);
+  for (int i = 0; i < n; ++i)
+    for (uint32_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p) {
+      const int j = int(col_idx[p]);
+      if (j >= i) up[i][j] += double(vals[p]);
+    }
+  std::vector<std::map<int, double>> full(n);
+  for (int i = 0; i < n; ++i)
+    for (auto& e : up[i]) {
+      full[i][e.first] = e.second;
+      full[e.first][i] = e.second;
+    }
+  std::vector<int> Ap(n + 1, 0), Aj;
+  std::vector<double> Ax;
+  for (int i = 0; i < n; ++i) {
+    for (auto& e : full[i]) { Aj.push_back(e.first); Ax.push_back(e.second); }
+    Ap[i + 1] = int(Aj.size());
+  }
+  std::vector<double> xyz(3 * size_t(n), 0.0);
+  for (int i = 0; i < n; ++i) xyz[3 * size_t(i)] = double(i);
+  SparseChol chol;
+  if (!chol.factor(n, Ap, Aj, Ax, xyz)) return 3;
+  std::vector<double> b(n), x(n);
+  for (int i = 0; i < n; ++i) b[i] = double(rhs[i]);
+  chol.solve(b.data(), x.data());
+  for (int i = 0; i < n; ++i) sol[i] = float(x[i]);
+  return 0;
+}
 void orc_set_ground(void* sim, int has, float h) { static_cast<SimBase*>(sim)->set_ground(has, h); }
 void orc_get_state(void* sim, float* px, float* py, float* pz, float* vx, float* vy, float* vz) {
   static_cast<SimBase*>(sim)->get_state(px, py, pz, vx, vy, vz);

@@ -114,6 +114,12 @@ void orc_quad_grid(uint32_t cols, uint32_t rows, float width, float height,
                    float* px, float* py, float* pz, uint32_t* tris);
 
 // ---- known-answer kernels for the contact primitives ----
+// SparseSolver::factorize + solve (crates/vistio-math/src/faer_solver.rs:67-125)
+// on a general CSR with f32 values: duplicates summed in f64, the upper
+// triangle read (Side::Upper), the oracle's FP64 LL^T. Returns 0 ok, 1 not
+// square, 2 empty, 3 not SPD.
+int orc_sparse_solve(uint32_t rows, uint32_t cols, const uint32_t* row_ptr, const uint32_t* col_idx,
+                     const float* vals, const float* rhs, float* sol);
 float orc_pt_dist2(const float p[3], const float a[3], const float b[3], const float c[3], int* dtype);
 float orc_ee_dist2(const float a0[3], const float a1[3], const float b0[3], const float b1[3], int* dtype);
 void orc_pt_grad(const float p[3], const float a[3], const float b[3], const float c[3], float out[12]);

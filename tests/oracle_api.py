@@ -107,6 +107,8 @@ def lib():
         L.orc_step_ipc.argtypes = [C.c_void_p, C.c_float, C.POINTER(Contact), C.POINTER(StepResult)]
         L.orc_set_ground.argtypes = [C.c_void_p, C.c_int, C.c_float]
         L.orc_resolve.argtypes = [C.c_void_p, C.POINTER(Contact), C.POINTER(C.c_float)]
+        L.orc_sparse_solve.argtypes = [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                       C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.orc_get_state.argtypes = [C.c_void_p] + [fp] * 6
         L.orc_set_state.argtypes = [C.c_void_p] + [fp] * 6
         dp = C.POINTER(C.c_double)
@@ -296,3 +298,27 @@ def ccd_hits(p0, p1, tris, pairs):
                         tris.ctypes.data_as(u32p), len(pairs), pairs.ctypes.data_as(u32p),
                         hits.ctypes.data_as(u32p), cap, C.byref(nh))
     return hits[: nh.value], mt
+
+
+def sparse_solve(rows, cols, triplets, rhs):
+    """orc_sparse_solve on a CSR built from (row, col, value) triplets, rows
+    sorted by column (CsrMatrix::from_triplets, crates/vistio-math/src/sparse.rs).
+    Returns (status, solution)."""
+    by_row = [[] for _ in range(rows)]
+    for r, c, v in triplets:
+        by_row[r].append((c, v))
+    ptr, col, val = [0], [], []
+    for r in range(rows):
+        for c, v in sorted(by_row[r], key=lambda e: e[0]):
+            col.append(c)
+            val.append(v)
+        ptr.append(len(col))
+    ptr = np.asarray(ptr, np.uint32)
+    col = np.asarray(col if col else [0], np.uint32)
+    val = np.asarray(val if val else [0.0], np.float32)
+    b = np.ascontiguousarray(rhs, np.float32)
+    x = np.zeros(max(rows, 1), np.float32)
+    st = lib().orc_sparse_solve(rows, cols, ptr.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                col.ctypes.data_as(C.POINTER(C.c_uint32)), val.ctypes.data_as(C.POINTER(C.c_float)),
+                                b.ctypes.data_as(C.POINTER(C.c_float)), x.ctypes.data_as(C.POINTER(C.c_float)))
+    return st, x[:rows]
