@@ -465,6 +465,13 @@ vistio_status vistio_broadphase_pairs_noalloc(vistio_ctx* ctx, uint32_t nv, cons
 vistio_status vistio_ccd_hits(vistio_ctx* ctx, uint32_t nv, const float* p0, const float* p1, uint32_t nt,
                               const uint32_t* tris, uint64_t npairs, const uint32_t* pairs, uint32_t* hits,
                               uint64_t cap, uint64_t* nhits, float* min_toi);
+/* The device's barrier gradient for n squared distances d2: kappa b'(d2)
+ * (crates/vistio-contact/src/barrier.rs:35-46 and the scaled form's clamp of
+ * non-finite values, :78-87), or with thickness > 0 the C-IPC form
+ * b'(d2 - thickness^2) (:138-163), in FP64 as the contact kernels evaluate
+ * it. Test-only. */
+vistio_status vistio_barrier_grad(vistio_ctx* ctx, uint32_t n, const double* d2, double d_hat, double kappa,
+                                  double thickness, double* out);
 
 #ifdef __cplusplus
 }

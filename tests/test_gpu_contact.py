@@ -371,3 +371,30 @@ def test_self_fold_configuration():
     print(f"self_fold 40x400: kappa {kappa:.4g}, worst step error {worst:.2e}, active contacts {active}")
     assert worst <= 1e-5, worst
     assert active > 0
+
+
+def test_device_barrier_gradient_matches_oracle():
+    """vistio_barrier_grad: the device's FP64 barrier gradient (barrier.rs:35-46,
+    78-87, and the C-IPC form 138-163) against the oracle's FP32 restatement
+    over six decades of squared distance, within 1e-4 relative (the oracle
+    rounds its inputs and result to f32), zero at and beyond d_hat, and the
+    known answers of barrier_tests.rs."""
+    d_hat, kappa = 1e-3, 1e4
+    d2 = np.concatenate([np.geomspace(1e-9, 2e-3, 400), [0.0, d_hat, 2 * d_hat]])
+    g = api.barrier_grad(d2, d_hat, kappa)
+    L = O.lib()
+    ref = np.array([L.orc_scaled_barrier_gradient(float(x), d_hat, kappa) for x in d2], np.float64)
+    inside = (d2 > 0) & (d2 < d_hat * (1 - 1e-6))
+    assert np.all(np.abs(g[inside] - ref[inside]) <= 1e-4 * np.abs(ref[inside]) + 1e-6)
+    assert np.all(g[d2 >= d_hat] == 0.0) and np.all(g[inside] < 0.0)
+    # thickness form: d_eff = d2 - t^2; at or below the thickness the clamped maximum
+    t = 1.5e-3
+    gt = api.barrier_grad(d2, d_hat, kappa, thickness=t)
+    reft = np.array([kappa * L.orc_barrier_gradient_thick(float(x), d_hat, t) for x in d2], np.float64)
+    deff = d2 - t * t
+    ins = (deff > 1e-12) & (deff < d_hat * (1 - 1e-6))
+    assert np.all(np.abs(gt[ins] - reft[ins]) <= 1e-4 * np.abs(reft[ins]) + 1e-6)
+    assert np.all(gt[deff <= 0] == gt[deff <= 0][0]) and gt[deff <= 0][0] < 0
+    # barrier_tests.rs: repulsive inside, massive at d <= 0 (unscaled < -5)
+    assert api.barrier_grad([0.005], 0.01, 1.0)[0] < 0.0
+    assert api.barrier_grad([0.0], 0.01, 1.0)[0] < -5.0

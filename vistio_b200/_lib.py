@@ -170,6 +170,8 @@ SIGNATURES = {
     "vistio_sparse_destroy": (C.c_int, [_vp]),
     "vistio_broadphase_pairs": (C.c_int, [_vp, C.c_uint32, _fp, _fp, _fp, C.c_uint32, _u32p, C.c_float, _u32p,
                                           C.c_uint64, _u64p]),
+    "vistio_barrier_grad": (C.c_int, [_vp, C.c_uint32, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double,
+                                       C.POINTER(C.c_double)]),
     "vistio_ccd_hits": (C.c_int, [_vp, C.c_uint32, _fp, _fp, C.c_uint32, _u32p, C.c_uint64, _u32p, _u32p,
                                   C.c_uint64, _u64p, _fp]),
     "vistio_broadphase_pairs_noalloc": (C.c_int, [_vp, C.c_uint32, _fp, _fp, _fp, C.c_uint32, _u32p, C.c_float,

@@ -589,6 +589,17 @@ def ccd_hits(p0: np.ndarray, p1: np.ndarray, tris: np.ndarray, pairs: np.ndarray
     return hits[: nh.value], mt.value
 
 
+def barrier_grad(d2, d_hat: float, kappa: float, thickness: float = 0.0, ctx: Optional[Context] = None) -> np.ndarray:
+    """The device's kappa-scaled barrier gradient at squared distances d2 (FP64; C-IPC form when thickness > 0)."""
+    ctx = ctx or default_context()
+    d = np.ascontiguousarray(d2, np.float64).reshape(-1)
+    out = np.zeros_like(d)
+    dp = C.POINTER(C.c_double)
+    L.check(L.lib().vistio_barrier_grad(ctx.h, d.shape[0], d.ctypes.data_as(dp), float(d_hat), float(kappa),
+                                        float(thickness), out.ctypes.data_as(dp)), ctx.h)
+    return out
+
+
 REQUEST_STATES = {0: "queued", 1: "setup", 2: "ready", 3: "running", 4: "done", 5: "failed"}
 
 

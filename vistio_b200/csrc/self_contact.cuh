@@ -510,6 +510,14 @@ __device__ __forceinline__ double scaled_barrier_grad_thick64(double d, double d
   return signbit(r) ? -1e6 : 1e6;
 }
 
+// The two barrier gradients above over an array (the test-only entry point).
+__global__ void __launch_bounds__(256) k_barrier_grad(const double* d2, uint32_t n, double d_hat, double kappa,
+                                                      double th, double* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = th > 0.0 ? scaled_barrier_grad_thick64(d2[i], d_hat, kappa, th) : scaled_barrier_grad64(d2[i], d_hat, kappa);
+}
+
 __device__ __forceinline__ bool excluded(const SelfContactView& S, uint32_t i, uint32_t j) {
   for (uint32_t p = S.adj_ptr[i], e = S.adj_ptr[i + 1]; p < e; ++p) {
     uint32_t a = S.adj[p];

@@ -1672,6 +1672,23 @@ vistio_status vistio_ccd_hits(vistio_ctx* ctx, uint32_t nv, const float* p0, con
   return ccd_hits_impl(ctx, nv, p0, p1, nt, tris, npairs, pairs, hits, cap, nhits, min_toi);
 }
 
+vistio_status vistio_barrier_grad(vistio_ctx* ctx, uint32_t n, const double* d2, double d_hat, double kappa,
+                                  double thickness, double* out) {
+  if (!ctx || (n && (!d2 || !out))) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  if (n == 0) return VISTIO_OK;
+  cudaStream_t st = ctx->stream;
+  CU(cudaSetDevice(ctx->device));
+  DevBuf<double> din, dout;
+  CU(din.alloc(n, st));
+  CU(dout.alloc(n, st));
+  CU(cudaMemcpyAsync(din.p, d2, 8 * size_t(n), cudaMemcpyHostToDevice, st));
+  k_barrier_grad<<<(n + 255) / 256, 256, 0, st>>>(din.p, n, d_hat, kappa, thickness, dout.p);
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(out, dout.p, 8 * size_t(n), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return VISTIO_OK;
+}
+
 }  // extern "C"
 
 // ======================================================= self-contact host
