@@ -486,7 +486,7 @@ def main():
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     achieved = alg[dom] / (kern_ms[dom] * 1e-3) / 1e9
-    solve_kernels = ("k_red_reset + k_sweep<0> + k_sweep<1> + k_update" if batch.sweep_mode()[0] == "dataflow" else
+    solve_kernels = ("k_red_reset + k_sweep + k_update" if batch.sweep_mode()[0] == "dataflow" else
                      "k_red_reset + k_subtree<0> + k_level<0> x L + k_level<1> x L + k_subtree<1> + k_update")
     roofline = {"bound": "hbm", "kernel": {"solve": solve_kernels, "membrane": "k_tri", "bending": "k_hinge",
                                           "gather": "k_gather"}[dom],

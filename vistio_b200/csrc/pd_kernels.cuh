@@ -146,7 +146,7 @@ struct BatchDev {
   const uint32_t* df_kids;
   uint32_t* df_cnt;            // forward: children finished
   uint32_t* df_flag;           // backward: parent finished
-  uint32_t* df_queue;          // next unit: [0] forward, [1] backward
+  uint32_t* df_queue;          // [0] next unit, [1] blocks done (k_sweep resets both)
   // FP64 refinement: the factored matrix A (f64, rows and columns in each
   // instance's solve order, global row ids), the right-hand side the first
   // sweep solved (R0) and the correction vector the refinement sweeps solve in
@@ -702,7 +702,9 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
     // chunk of x[R] are gathered; columns in at most two rounds of the team
     // width (warp items have s <= kWarpVec, block items s <= 256 <= the block width)
     stage_issue(tm, D, whole);
-    for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
+    // own columns through L2: the forward sweep may have written them in
+    // this launch, on another SM
+    for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = __ldcg(Y + f + c);
     const uint32_t width = team_width(tm, s), parts = tm.size / width;
     const uint32_t cl = tm.rank % width, part = tm.rank / width;
     float4 sum0 = make_float4(0.f, 0.f, 0.f, 0.f), sum1 = sum0;
@@ -729,7 +731,7 @@ __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const S
     tm.sync();
     return;
   }
-  for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = Y[f + c];
+  for (uint32_t c = tm.rank; c < s; c += tm.size) tm.v1[c] = __ldcg(Y + f + c);
   const uint32_t width = team_width(tm, s);
   const uint32_t parts = tm.size / width;
   const uint32_t cl = tm.rank % width, part = tm.rank / width;
@@ -795,7 +797,7 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
   const uint32_t c0 = F.first, c1 = Lz.first + Lz.ncols, nc = c1 - c0;
   float4* Yg = B.Y + F.vbase;
   float4* acc = tm.v1;  // rows c0 .. c1 of this instance (nc <= vcap, enforced by the set-up)
-  for (uint32_t c = tm.rank; c < nc; c += tm.size) acc[c] = Yg[c0 + c];
+  for (uint32_t c = tm.rank; c < nc; c += tm.size) acc[c] = __ldcg(Yg + c0 + c);  // possibly written this launch
   const bool ok = mbar_wait(tm.bar, tm.parity);
   tm.parity ^= 1u;
   if (!ok) {
@@ -982,81 +984,103 @@ __device__ __forceinline__ bool dep_wait(const BatchDev& B, const uint32_t* word
   return false;
 }
 
-// Forward: wait for the children of supernode k; backward: for its parent.
+// Forward: wait for the children of supernode k; backward: for its parent's
+// backward, or for a root its own forward (both sweeps share one launch).
 template <int DIR>
 __device__ __forceinline__ void dep_enter(const BatchDev& B, uint32_t k) {
   if (DIR == 0) {
     const uint32_t need = B.df_nkids[k];
     if (need && dep_wait(B, B.df_cnt + k, need)) B.df_cnt[k] = 0u;
-  } else if (B.df_parent[k] != kNoParent) {
-    if (dep_wait(B, B.df_flag + k, 1u)) B.df_flag[k] = 0u;
+  } else if (dep_wait(B, B.df_flag + k, 1u)) {
+    B.df_flag[k] = 0u;
   }
 }
 
-// Forward: count k in at its parent; backward: release k's children (lanes
-// `rank` of `size` share the children).
+// Forward: count k in at its parent (a root releases its own backward);
+// backward: release k's children (lanes `rank` of `size` share the children).
 template <int DIR>
 __device__ __forceinline__ void dep_leave(const BatchDev& B, uint32_t k, uint32_t rank, uint32_t size) {
   if (DIR == 0) {
     const uint32_t p = B.df_parent[k];
-    if (rank == 0 && p != kNoParent) atomicAdd(B.df_cnt + p, 1u);
+    if (rank == 0) {
+      if (p != kNoParent) atomicAdd(B.df_cnt + p, 1u);
+      else atomicExch(B.df_flag + k, 1u);
+    }
   } else {
     for (uint32_t q = B.df_kid_ptr[k] + rank, qe = B.df_kid_ptr[k + 1]; q < qe; q += size)
       atomicExch(B.df_flag + B.df_kids[q], 1u);
   }
 }
 
+// One work unit of the dependency-driven sweeps (the whole block runs it).
 template <int DIR>
-__global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_sweep(BatchDev B, uint32_t nunits) {
+__device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uint2 u, bool ipc) {
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t kind = u.x & 3u, count = u.x >> 2;
+  if (kind == 1) {
+    const uint32_t k = u.y;
+    const SnDev S = B.sn[k];
+    if (ipc && B.red[S.inst].al_done) return;
+    if (tid == 0) dep_enter<DIR>(B, k);
+    __syncthreads();
+    if (DIR == 0) sn_forward(B, t.bt, S);
+    else sn_backward(B, t.bt, S);
+    __threadfence();
+    __syncthreads();
+    dep_leave<DIR>(B, k, tid, 32 * kSolveWarps);
+  } else if (warp < count) {
+    if (kind == 0) {
+      const uint2 it = B.sub_items[u.y + warp];
+      if (ipc && B.red[B.sn[it.x].inst].al_done) return;
+      if (DIR == 1 && lane == 0) dep_enter<1>(B, it.y);
+      __syncwarp();
+      subtree_sweep<DIR>(B, t.wt, it.x, it.y);
+      __threadfence();
+      __syncwarp();
+      if (DIR == 0) dep_leave<0>(B, it.y, lane, 32);
+    } else {
+      const uint32_t k = (DIR == 0 ? B.df_items_fwd : B.lvl_items)[u.y + warp];
+      const SnDev S = B.sn[k];
+      if (ipc && B.red[S.inst].al_done) return;
+      if (lane == 0) dep_enter<DIR>(B, k);
+      __syncwarp();
+      if (DIR == 0) sn_forward(B, t.wt, S);
+      else sn_backward(B, t.wt, S);
+      __threadfence();
+      __syncwarp();
+      dep_leave<DIR>(B, k, lane, 32);
+    }
+  }
+}
+
+// Both dependency-driven sweeps in one launch: resident blocks take the
+// forward units (top supernodes deepest first), then the backward units (the
+// level order from the top). A unit waits only for units handed out before
+// it: in the forward sweep for its children, in the backward sweep for its
+// parent's backward or, at a root, for its own forward. So a garment's
+// backward sweep starts as soon as its own forward sweep ends, beside the
+// forward tail of the others. The last block out resets the queue.
+__global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_sweep(BatchDev B, uint32_t nfwd, uint32_t nbwd) {
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
   __shared__ uint32_t s_abort, s_unit;
   SweepTeams t = make_teams(smem4, s_bar, &s_abort);
-  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // the other direction's queue restarts for its next launch (it is not running)
-  if (blockIdx.x == 0 && tid == 0) B.df_queue[DIR ^ 1] = 0u;
+  const uint32_t tid = threadIdx.x;
   const bool ipc = B.prm->ipc != 0;
   for (;;) {
     __syncthreads();  // every warp is done with the previous unit
-    if (tid == 0) s_unit = atomicAdd(B.df_queue + DIR, 1u);
+    if (tid == 0) s_unit = atomicAdd(B.df_queue, 1u);
     __syncthreads();
     const uint32_t q = s_unit;
-    if (q >= nunits) break;
-    const uint2 u = DIR == 0 ? B.df_units_fwd[q] : B.df_units[nunits - 1 - q];
-    const uint32_t kind = u.x & 3u, count = u.x >> 2;
-    if (kind == 1) {
-      const uint32_t k = u.y;
-      const SnDev S = B.sn[k];
-      if (ipc && B.red[S.inst].al_done) continue;
-      if (tid == 0) dep_enter<DIR>(B, k);
-      __syncthreads();
-      if (DIR == 0) sn_forward(B, t.bt, S);
-      else sn_backward(B, t.bt, S);
-      __threadfence();
-      __syncthreads();
-      dep_leave<DIR>(B, k, tid, 32 * kSolveWarps);
-    } else if (warp < count) {
-      if (kind == 0) {
-        const uint2 it = B.sub_items[u.y + warp];
-        if (ipc && B.red[B.sn[it.x].inst].al_done) continue;
-        if (DIR == 1 && lane == 0) dep_enter<1>(B, it.y);
-        __syncwarp();
-        subtree_sweep<DIR>(B, t.wt, it.x, it.y);
-        __threadfence();
-        __syncwarp();
-        if (DIR == 0) dep_leave<0>(B, it.y, lane, 32);
-      } else {
-        const uint32_t k = (DIR == 0 ? B.df_items_fwd : B.lvl_items)[u.y + warp];
-        const SnDev S = B.sn[k];
-        if (ipc && B.red[S.inst].al_done) continue;
-        if (lane == 0) dep_enter<DIR>(B, k);
-        __syncwarp();
-        if (DIR == 0) sn_forward(B, t.wt, S);
-        else sn_backward(B, t.wt, S);
-        __threadfence();
-        __syncwarp();
-        dep_leave<DIR>(B, k, lane, 32);
-      }
+    if (q >= nfwd + nbwd) break;
+    if (q < nfwd) sweep_unit<0>(B, t, B.df_units_fwd[q], ipc);
+    else sweep_unit<1>(B, t, B.df_units[nbwd - 1 - (q - nfwd)], ipc);
+  }
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(B.df_queue + 1, 1u) == gridDim.x - 1) {  // every block has taken its last unit
+      B.df_queue[0] = 0u;
+      B.df_queue[1] = 0u;
     }
   }
 }

@@ -166,7 +166,7 @@ struct vistio_batch {
   uint32_t sweep_mode = 1;
   std::vector<uint2> units_host;                    // k_sweep work units in forward order
   uint32_t n_units = 0, n_units_fwd = 0;
-  std::vector<uint2> units_fwd_host;                // k_sweep<0> units: top supernodes deepest first
+  std::vector<uint2> units_fwd_host;                // k_sweep forward units: top supernodes deepest first
   std::vector<uint32_t> items_fwd_host;             // their warp supernodes, bundled by depth
   std::vector<uint32_t> sn_depth;                   // ancestors of each supernode in its tree
   DevBuf<uint2> df_units_fwd;
@@ -759,10 +759,9 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
 // on dv.Y (right-hand side in, solution out). Returns the launches.
 uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
   if (b->sweep_mode == 1 && b->n_units) {
-    const uint32_t grid = std::min(b->n_units, b->ctx->sweep_blocks);
-    k_sweep<0><<<std::min(b->n_units_fwd, b->ctx->sweep_blocks), kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd);
-    k_sweep<1><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units);
-    return 2;
+    const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks);
+    k_sweep<<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
+    return 1;
   }
   uint32_t L = uint32_t(b->lvl_off.size()), n = 0;
   const uint32_t sub_grid = (b->n_sub + kSolveWarps - 1) / kSolveWarps;
@@ -990,11 +989,10 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   CU(cudaFuncSetAttribute(k_level<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_subtree<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_subtree<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
-  CU(cudaFuncSetAttribute(k_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
-  CU(cudaFuncSetAttribute(k_sweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   {
     int per_sm = 0, sms = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<0>, kSolveThreads, kSolveSmem));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep, kSolveThreads, kSolveSmem));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     c->sweep_blocks = uint32_t(std::max(1, per_sm) * std::max(1, sms));
   }
