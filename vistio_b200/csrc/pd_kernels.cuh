@@ -276,23 +276,12 @@ __device__ __forceinline__ M32 model_target(int model, const M32& F, float warp_
 }
 
 // ------------------------------------------------------------- kernels
-// Local membrane step: per triangle, w * g_k . (F_target - F) for k = 0..2.
-// Compiled for five blocks per SM (48 registers; the FP64 projection spills a
-// little): 0.31 -> 0.215 ms per iteration on 7.9 M triangles against the 68
-// registers and three blocks the compiler picks unbounded. The loads of the
-// vertex positions are latency-bound, so warps in flight matter more.
-__global__ void __launch_bounds__(256, 5) k_tri(BatchDev B) {
-  int4 ch = B.tri_chunks[blockIdx.x];
-  if ((int)threadIdx.x >= ch.z) return;
-  if (B.prm->ipc && B.red[ch.x].al_done) return;
-  uint32_t t = uint32_t(ch.y) + threadIdx.x;
-  const InstDev I = B.inst[ch.x];
-  uint4 id = B.tri_idx[t];
-  float4 dm = B.tri_dm[t];
-  float w = B.tri_w[t];
+// Local membrane step of one triangle: w * g_k . (F_target - F) for k = 0..2.
+__device__ __forceinline__ void tri_project(const BatchDev& B, const InstDev& I, uint32_t t, float4 dm, float w,
+                                            float4 q0, float4 q1, float4 q2) {
   // FP64 from the FP32 positions on (the projection is the ill-conditioned
   // part; the outputs are rounded once).
-  const double3 p0 = d3(B.pos[id.x]), p1 = d3(B.pos[id.y]), p2 = d3(B.pos[id.z]);
+  const double3 p0 = d3(q0), p1 = d3(q1), p2 = d3(q2);
   M32 ds; ds.c0 = p1 - p0; ds.c1 = p2 - p0;
   M32 F = mul2(ds, dm.x, dm.y, dm.z, dm.w);
   float det = dm.x * dm.w - dm.y * dm.z;
@@ -311,6 +300,31 @@ __global__ void __launch_bounds__(256, 5) k_tri(BatchDev B) {
   o[0] = float(c0.x); o[1] = float(c0.y); o[2] = float(c0.z);
   o[3] = float(c1.x); o[4] = float(c1.y); o[5] = float(c1.z);
   o[6] = float(c2.x); o[7] = float(c2.y); o[8] = float(c2.z);
+}
+
+// The membrane step over a chunk of up to 256 triangles with 128 threads:
+// each thread loads both of its triangles (indices, rest data, the six
+// vertex positions) before it projects either, so twice the loads are in
+// flight per warp; eight blocks per SM (64 registers). The loads are
+// latency-bound: 0.216 -> 0.176 ms per iteration on 7.9 M triangles against
+// one triangle per thread at five 256-thread blocks per SM.
+constexpr int kTriThreads = 128;
+__global__ void __launch_bounds__(kTriThreads, 8) k_tri(BatchDev B) {
+  int4 ch = B.tri_chunks[blockIdx.x];
+  const uint32_t i0 = threadIdx.x, i1 = threadIdx.x + kTriThreads;
+  if ((int)i0 >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  const bool two = (int)i1 < ch.z;
+  const uint32_t t0 = uint32_t(ch.y) + i0, t1 = uint32_t(ch.y) + i1;
+  const InstDev I = B.inst[ch.x];
+  const uint4 a = B.tri_idx[t0], b = two ? B.tri_idx[t1] : a;
+  const float4 dma = B.tri_dm[t0], dmb = two ? B.tri_dm[t1] : dma;
+  const float wa = B.tri_w[t0], wb = two ? B.tri_w[t1] : wa;
+  const float4 qa0 = B.pos[a.x], qa1 = B.pos[a.y], qa2 = B.pos[a.z];
+  float4 qb0 = qa0, qb1 = qa1, qb2 = qa2;
+  if (two) { qb0 = B.pos[b.x]; qb1 = B.pos[b.y]; qb2 = B.pos[b.z]; }
+  tri_project(B, I, t0, dma, wa, qa0, qa1, qa2);
+  if (two) tri_project(B, I, t1, dmb, wb, qb0, qb1, qb2);
 }
 
 // Rotation of v = p - centre about `axis` by an angle minus v itself:

@@ -800,7 +800,7 @@ uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update, uint32_t 
 
 uint32_t launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update, uint32_t refine) {
   uint32_t n = 1;
-  if (b->n_tri_chunks) { k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
+  if (b->n_tri_chunks) { k_tri<<<b->n_tri_chunks, kTriThreads, 0, st>>>(b->dev); ++n; }
   if (b->n_hinge_chunks) { k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
   k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, refine > 0);
   return n + launch_solve(b, st, do_update, refine);
@@ -1487,7 +1487,7 @@ vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase) {
   cudaStream_t st = ctx->stream;
   switch (phase) {
     case 0: k_predict<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
-    case 1: if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev); break;
+    case 1: if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kTriThreads, 0, st>>>(b->dev); break;
     case 2: if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); break;
     case 3: k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, b->refine > 0); break;
     case 4: launch_solve(b, st, 0, 0); break;
