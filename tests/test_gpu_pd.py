@@ -273,8 +273,11 @@ def test_level_schedules_and_autotuner():
 def test_dataflow_sweeps_match_levels_on_a_mixed_batch():
     """A batch of many garments of different sizes (so that the dependency-
     driven sweeps interleave supernodes of different levels and garments)
-    steps bit-identically with both sweep kinds, plain and with IPC."""
-    sides = [12, 37, 20, 64, 9, 48, 31, 25] * 3
+    steps bit-identically with both sweep kinds, plain and with IPC. Sides 2
+    and 3 are garments whose whole elimination tree is one bottom subtree: in
+    the single dependency-driven launch their backward unit waits on their own
+    forward."""
+    sides = [12, 37, 20, 64, 9, 48, 31, 25, 2, 3] * 3
     cfg = api.drape_config(max_iterations=10, al_max_iterations=3, barrier_d_hat=1e-3, barrier_kappa=1e4)
     contact = api.Contact(has_ground=True, ground_height=0.6, kappa=1e4)
     res = {}
