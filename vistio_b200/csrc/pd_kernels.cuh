@@ -1142,34 +1142,46 @@ __global__ void __launch_bounds__(256) k_accum(BatchDev B) {
 // step, x <- x + d, the pin reset (:429-435) and the ground clamp (:438).
 // add_w folds the last refinement correction into d (and into Y, where the
 // IPC kernels read d).
-__global__ void __launch_bounds__(256) k_update(BatchDev B, int do_update, int add_w) {
+__device__ __forceinline__ void update_one(const BatchDev& B, const InstDev& I, uint32_t g, float4 d, float4 x,
+                                           int do_update, int add_w, uint32_t row, double& dsq, double& nsq,
+                                           bool& bad) {
+  if (add_w) {
+    d = f4_add(d, B.W[row]);
+    B.Y[row] = d;
+  }
+  dsq += double(d.x) * d.x + double(d.y) * d.y + double(d.z) * d.z;
+  nsq += double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z;
+  bad = bad || !(isfinite(d.x) && isfinite(d.y) && isfinite(d.z));
+  if (do_update) {
+    float4 nx;
+    if (B.pinned[g]) nx = B.prev[g];
+    else {
+      nx = make_float4(x.x + d.x, x.y + d.y, x.z + d.z, 0.f);
+      if (I.has_ground && nx.y < I.ground_h) nx.y = I.ground_h;  // state.rs:180-189
+    }
+    B.pos[g] = nx;
+  }
+}
+
+// Two vertices per thread (128 threads over a chunk of up to 256), both
+// vertices' loads issued before either update: 0.063 -> about 0.043 ms per
+// iteration on 4.05 M vertices (the solve phase 1.315 -> 1.295 ms).
+__global__ void __launch_bounds__(128) k_update(BatchDev B, int do_update, int add_w) {
   int4 ch = B.vtx_chunks[blockIdx.x];
   const InstDev I = B.inst[ch.x];
   InstRed& R = B.red[ch.x];
   if (B.prm->ipc && R.al_done) return;
   double dsq = 0.0, nsq = 0.0;
   bool bad = false;
-  if ((int)threadIdx.x < ch.z) {
-    uint32_t g = uint32_t(ch.y) + threadIdx.x;
-    const uint32_t row = I.vbase + B.perm_local[g];
-    float4 d = B.Y[row];
-    if (add_w) {
-      d = f4_add(d, B.W[row]);
-      B.Y[row] = d;
-    }
-    float4 x = B.pos[g];
-    dsq = double(d.x) * d.x + double(d.y) * d.y + double(d.z) * d.z;
-    nsq = double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z;
-    bad = !(isfinite(d.x) && isfinite(d.y) && isfinite(d.z));
-    if (do_update) {
-      float4 nx;
-      if (B.pinned[g]) nx = B.prev[g];
-      else {
-        nx = make_float4(x.x + d.x, x.y + d.y, x.z + d.z, 0.f);
-        if (I.has_ground && nx.y < I.ground_h) nx.y = I.ground_h;  // state.rs:180-189
-      }
-      B.pos[g] = nx;
-    }
+  const uint32_t i0 = threadIdx.x, i1 = threadIdx.x + 128;
+  if ((int)i0 < ch.z) {
+    const bool two = (int)i1 < ch.z;
+    const uint32_t g0 = uint32_t(ch.y) + i0, g1 = uint32_t(ch.y) + i1;
+    const uint32_t r0 = I.vbase + B.perm_local[g0], r1 = two ? I.vbase + B.perm_local[g1] : r0;
+    const float4 d0 = B.Y[r0], d1 = two ? B.Y[r1] : d0;
+    const float4 x0 = B.pos[g0], x1 = two ? B.pos[g1] : x0;
+    update_one(B, I, g0, d0, x0, do_update, add_w, r0, dsq, nsq, bad);
+    if (two) update_one(B, I, g1, d1, x1, do_update, add_w, r1, dsq, nsq, bad);
   }
   for (int o = 16; o > 0; o >>= 1) {
     dsq += __shfl_down_sync(0xffffffffu, dsq, o);

@@ -794,7 +794,7 @@ uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update, uint32_t 
     if (k) { k_accum<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
     n += launch_refinement(b, st);
   }
-  k_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, do_update, refine > 0);
+  k_update<<<b->n_vtx_chunks, 128, 0, st>>>(b->dev, do_update, refine > 0);  // two vertices per thread
   return n;
 }
 
