@@ -23,6 +23,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -93,10 +94,9 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"vistio_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -476,7 +476,8 @@ def main():
     torch.cuda.synchronize()
     dom = max(kern_ms, key=kern_ms.get)
 
-    # algorithmic bytes per launch (per-unit figures x units)
+    # algorithmic bytes per launch: per-unit figures (V vertices, T triangles, H hinges,
+    # nnz(L) of the oracle's ordering) times the units of the launch
     nnz_ref = oracle_nnz_by_side(specs)
     nnz_total = sum(nnz_ref[s.side] for s in specs)
     T, H = info["triangles"], info["hinges"]

@@ -448,9 +448,12 @@ vistio_status vistio_broadphase_pairs(vistio_ctx* ctx, uint32_t nv, const float*
  * device work), and at most VISTIO_NOALLOC_MAX_PAIRS candidate pairs (else
  * VISTIO_ERR_CAPACITY with *count set). pairs == NULL queries the count;
  * cap < *count returns VISTIO_ERR_CAPACITY and writes nothing.
- * The context's device must be current on the calling thread. The first call
- * on each device looks up the region's address (cudaGetSymbolAddress), so make
- * that first call before any stream capture. The region is shared by every
+ * The call makes the context's device current, looks up the region's address
+ * (cudaGetSymbolAddress) and is synchronous: it returns with the pairs on the
+ * host, so it cannot be captured into a CUDA graph. The triangles are not
+ * reordered by Morton code first (vistio_broadphase_pairs does that): the tree
+ * is built over mesh order, which finds the same pairs at a traversal cost that
+ * depends on how spatially ordered the mesh is. The region is shared by every
  * call on the device: calls on one device must not overlap (two threads or two
  * contexts with calls in flight at once race on it). Each call clears the
  * counters it needs; nothing has to be zeroed by the caller. */

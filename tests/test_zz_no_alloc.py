@@ -2,8 +2,12 @@
 no device memory on the call (its buffers live in a fixed region built into
 the library). Its pair lists must equal those of vistio_broadphase_pairs on
 the same inputs, call after call: the second and third calls reuse the region
-a previous, differently sized call left behind. The module sorts last so it
-also runs after every other GPU test in the same process."""
+a previous, differently sized call left behind. The cases include a mesh whose
+triangles are stored in random order (this entry point builds its tree over
+mesh order, without the Morton sort) and one of 64,800 triangles, near the
+65,536-triangle limit. Across several calls the device's free memory and the
+default memory pool's reserved and used bytes must not change. The module
+sorts last so it also runs after every other GPU test in the same process."""
 import numpy as np
 import pytest
 
@@ -29,10 +33,26 @@ def folded_sheet(cols, rows, width, height, gap, seed):
     return np.stack([px, y + 0.5, z], 1).astype(np.float32), tris
 
 
+def permuted(pos, tris, seed):
+    """The same surface with its triangles stored in a random order."""
+    order = np.random.default_rng(seed).permutation(len(tris))
+    return pos, np.ascontiguousarray(tris[order])
+
+
+def flat_sheet(side, length, seed):
+    """A jittered flat quad-grid sheet (2 side^2 triangles)."""
+    px, py, pz, tris = scenarios.quad_grid(side, side, length, length)
+    rng = np.random.default_rng(seed)
+    pos = np.stack([px, rng.uniform(-2e-4, 2e-4, px.shape).astype(np.float32) + 0.5, py], 1)
+    return pos.astype(np.float32), tris
+
+
 CASES = [
     folded_sheet(8, 60, 0.1, 0.6, 0.004, 0) + (7.5e-4,),
     folded_sheet(20, 140, 0.2, 1.4, 0.003, 1) + (1.5e-3,),  # 5600 triangles, a larger tree
     folded_sheet(3, 5, 0.05, 0.1, 0.002, 2) + (1e-3,),
+    permuted(*folded_sheet(20, 140, 0.2, 1.4, 0.003, 1), 4) + (1.5e-3,),  # triangles out of spatial order
+    flat_sheet(180, 1.8, 3) + (1e-3,),  # 64,800 triangles, about 546k pairs
 ]
 
 
@@ -71,3 +91,32 @@ def test_noalloc_empty_and_limits():
                                                     len(tris), np.ascontiguousarray(tris, np.uint32).ctypes.data_as(u32),
                                                     margin, out.ctypes.data_as(u32), n - 1, C.byref(cnt))
     assert st == CAPACITY and cnt.value == n
+
+
+def _device_memory():
+    """(free bytes of the device, reserved and used bytes of its default pool)."""
+    import torch
+    from cuda.bindings import runtime as rt
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info()
+    err, pool = rt.cudaDeviceGetDefaultMemPool(torch.cuda.current_device())
+    assert err == rt.cudaError_t.cudaSuccess
+    out = [free]
+    for attr in (rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent):
+        err, v = rt.cudaMemPoolGetAttribute(pool, attr)
+        assert err == rt.cudaError_t.cudaSuccess
+        out.append(int(v))
+    return tuple(out)
+
+
+def test_noalloc_calls_allocate_no_device_memory():
+    """After one warm-up call (which may load the library's module), calls of
+    four different sizes leave the device's free memory and the default pool's
+    reserved and used bytes exactly as they were."""
+    got = [len(api.broadphase_pairs_noalloc(p, t, m)) for p, t, m in CASES[:1]]
+    before = _device_memory()
+    for p, t, m in (CASES[4], CASES[1], CASES[2], CASES[3]):
+        got.append(len(api.broadphase_pairs_noalloc(p, t, m)))
+    after = _device_memory()
+    assert before == after, (before, after)
+    assert min(got[1:]) > 0

@@ -550,25 +550,32 @@ def broadphase_pairs(pos: np.ndarray, tris: np.ndarray, margin: float, ctx: Opti
     return out[: cnt.value]
 
 
+NOALLOC_MAX_PAIRS = 1 << 20  # VISTIO_NOALLOC_MAX_PAIRS
+_noalloc_host = None  # one reusable host buffer of NOALLOC_MAX_PAIRS pairs
+
+
 def broadphase_pairs_noalloc(pos: np.ndarray, tris: np.ndarray, margin: float,
                              ctx: Optional[Context] = None) -> np.ndarray:
     """broadphase_pairs through the allocation-free entry point: the library
     allocates no device memory for the call (meshes up to 65536 triangles and
     65536 vertices, up to 1048576 pairs; larger inputs raise VistioError with
-    status CAPACITY). Calls on one device must not overlap."""
+    status CAPACITY). Calls on one device must not overlap. One call per
+    query: the pairs land in a host buffer sized for the maximum pair count,
+    allocated once and reused, and the result is a copy of its first rows."""
+    global _noalloc_host
     ctx = ctx or default_context()
     pos = _f32(pos)
     tris = np.ascontiguousarray(tris, np.uint32)
     cols = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+    if _noalloc_host is None:
+        _noalloc_host = np.zeros((NOALLOC_MAX_PAIRS, 2), np.uint32)
     cnt = C.c_uint64()
     u32 = C.POINTER(C.c_uint32)
-    fn = L.lib().vistio_broadphase_pairs_noalloc
-    L.check(fn(ctx.h, pos.shape[0], *[_fp(c) for c in cols], tris.shape[0], tris.ctypes.data_as(u32), float(margin),
-               None, 0, C.byref(cnt)), ctx.h)
-    out = np.zeros((max(cnt.value, 1), 2), np.uint32)
-    L.check(fn(ctx.h, pos.shape[0], *[_fp(c) for c in cols], tris.shape[0], tris.ctypes.data_as(u32), float(margin),
-               out.ctypes.data_as(u32), cnt.value, C.byref(cnt)), ctx.h)
-    return out[: cnt.value]
+    L.check(L.lib().vistio_broadphase_pairs_noalloc(ctx.h, pos.shape[0], *[_fp(c) for c in cols], tris.shape[0],
+                                                    tris.ctypes.data_as(u32), float(margin),
+                                                    _noalloc_host.ctypes.data_as(u32), NOALLOC_MAX_PAIRS,
+                                                    C.byref(cnt)), ctx.h)
+    return _noalloc_host[: cnt.value].copy()
 
 
 def ccd_hits(p0: np.ndarray, p1: np.ndarray, tris: np.ndarray, pairs: np.ndarray, ctx: Optional[Context] = None):

@@ -1934,21 +1934,29 @@ vistio_status ccd_hits_impl(vistio_ctx* ctx, uint32_t nv, const float* p0, const
 }  // namespace vistio
 
 // ================================================ allocation-free broad phase
-// vistio_broadphase_pairs_noalloc runs the kernels of vistio_broadphase_pairs
-// with every device buffer carved out of one fixed region that is part of the
-// library image, so the call itself allocates and frees no device memory.
-// It is meant for callers that cannot allocate on the call: a server whose
-// HBM is fully committed to resident garments and factors (a cudaMalloc there
-// can fail, or push out memory it has promised elsewhere), and per-frame
-// collision queries on a latency-critical thread, where cudaFree's implicit
-// device-wide synchronisation would stall all other work on the GPU.
+// vistio_broadphase_pairs_noalloc finds the same candidate pairs as
+// vistio_broadphase_pairs with every device buffer carved out of one fixed
+// region that is part of the library image, so the call itself allocates and
+// frees no device memory. It is meant for callers that cannot allocate on the
+// call: a server whose HBM is fully committed to resident garments and
+// factors (a cudaMalloc there can fail, or push out memory it has promised
+// elsewhere), and per-frame collision queries on a latency-critical thread,
+// where cudaFree's implicit device-wide synchronisation would stall all other
+// work on the GPU.
+//
+// Unlike vistio_broadphase_pairs it does not reorder the triangles by Morton
+// code first: the implicit balanced tree is built over the triangles in mesh
+// order. The pair set is the same (every overlapping pair is found whatever the
+// leaf order); only the traversal cost differs on meshes whose triangles are
+// not stored in spatial order.
 //
 // The region is sized for meshes of up to kNaMaxTris triangles and kNaMaxVerts
 // vertices and for up to kNaMaxPairs candidate pairs (about 16 MB); larger
 // inputs are rejected with VISTIO_ERR_CAPACITY before any device work. There
 // is one region per device, so calls on the same device must not overlap:
 // two of them in flight at once (two threads, or two contexts' streams)
-// race on it.
+// race on it. The call is synchronous (it reads the pair count back) and so
+// cannot be captured into a CUDA graph.
 namespace vistio_na {
 constexpr uint32_t kNaMaxTris = 65536;
 constexpr uint32_t kNaMaxVerts = 65536;
@@ -1956,7 +1964,6 @@ constexpr uint32_t kNaMaxPairs = 1u << 20;
 constexpr uint32_t kNaMaxBoxes = 2 * kNaMaxTris + 32;  // every tree level of kNaMaxTris leaves
 constexpr uint32_t kNaChunks = (kNaMaxTris + kElemThreads - 1) / kElemThreads;
 constexpr uint32_t kNaScanBlocks = (kNaMaxTris + vistio::kScanBlock - 1) / vistio::kScanBlock;
-constexpr int kNaMaxDevices = 64;
 
 constexpr uint64_t na_up(uint64_t x) { return (x + 255) & ~uint64_t(255); }
 
@@ -1990,26 +1997,18 @@ using namespace vistio_na;
 static __device__ __align__(256) unsigned char g_na_scratch[NaLayout::bytes];
 
 namespace vistio_na {
-std::mutex g_na_mu;
-unsigned char* g_na_base[kNaMaxDevices] = {};
-
-// Device address of the region on the context's device, looked up once per
-// device (the first call on each device does it, with that device current).
+// Device address of the region on the context's device. Host code cannot use
+// g_na_scratch itself (on the host it names a stand-in, not device memory), so
+// every call makes the context's device current and asks the runtime for the
+// address: a cheap lookup, and never stale after the device's context has been
+// reset and the module reloaded.
 vistio_status na_region(vistio_ctx* ctx, unsigned char** out) {
-  int cur = -1;
-  CU(cudaGetDevice(&cur));
-  if (cur != ctx->device)
-    return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "the context's device must be current on the calling thread");
-  if (cur < 0 || cur >= kNaMaxDevices) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "device index out of range");
-  std::lock_guard<std::mutex> lock(g_na_mu);
-  if (!g_na_base[cur]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(ctx, VISTIO_ERR_GPU, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_na_base[cur] = static_cast<unsigned char*>(p);
-  }
-  *out = g_na_base[cur];
+  CU(cudaSetDevice(ctx->device));
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(ctx, VISTIO_ERR_GPU, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  *out = static_cast<unsigned char*>(p);
   return VISTIO_OK;
 }
 
