@@ -277,19 +277,25 @@ vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, ui
 /* Autotuner of the sweeps (no counterpart in the reference). Two things are
  * chosen by timing this batch's forward and backward sweeps:
  * - the sweep kind: 0 = one kernel launch per level of the supernodal trees;
- *   1 = one dependency-driven launch per direction, in which each supernode
- *   waits only for its own children (forward) or parent (backward);
+ *   1 = one dependency-driven launch for both directions, in which each
+ *   supernode waits only for its own children (forward) or parent (backward);
+ *   2 (batches with garment groups: at least 8 garments of one mesh topology)
+ *   = the bottom of the groups' trees swept one lane per garment, before and
+ *   after kind 1 sweeps the rest; the same results, bit for bit, as kind 1 at
+ *   the limit 6144;
  * - which top-level supernodes a single warp takes and which a whole block,
  *   by a limit on s (s + m): 0, 1024, 2048, 4096, 6144, 12288 and 2^30.
- * candidate_ms (14 entries, may be NULL) receives the time of each limit for
- * kind 0 (entries 0-6), then for kind 1 (entries 7-13); the fastest pair is
- * kept (*chosen_limit; the kind from vistio_batch_get_sweep_mode). Without
- * tuning: kind 1 with the limit 6144. Captured step graphs are rebuilt on the
- * next step. Synchronises the batch's stream. */
+ * candidate_ms (21 entries, may be NULL) receives the time of each limit for
+ * kind 0 (entries 0-6), kind 1 (entries 7-13) and kind 2 (entries 14-20; -1
+ * without garment groups); the fastest pair is kept (*chosen_limit; the kind
+ * from vistio_batch_get_sweep_mode). Without tuning: kind 2 if the batch has
+ * garment groups, else kind 1, with the limit 6144. Captured step graphs are
+ * rebuilt on the next step. Synchronises the batch's stream. */
 vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms);
 /* Sets the warp-item limit directly (any value; see vistio_batch_tune). */
 vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit);
-/* Sets the sweep kind (0 or 1; see vistio_batch_tune). */
+/* Sets the sweep kind (0, 1, or 2 for a batch with garment groups; see
+ * vistio_batch_tune). */
 vistio_status vistio_batch_set_sweep_mode(vistio_batch* b, uint32_t mode);
 /* The sweep kind and warp-item limit in use. */
 vistio_status vistio_batch_get_sweep_mode(const vistio_batch* b, uint32_t* mode, uint32_t* warp_limit);

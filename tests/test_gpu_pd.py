@@ -243,7 +243,7 @@ def test_level_schedules_and_autotuner():
         for mesh, h in meshes:
             setup = api.SetupDesc(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0, matrix_dt=h)
             out = {}
-            for mode in api.Batch.SWEEP_MODES:
+            for mode in ("levels", "dataflow"):  # one garment: no garment groups
                 s = api.ProjectiveDynamicsSolver().init_explicit(mesh, cfg, setup, pinned=mesh.pinned)
                 batch = api.Batch([s])
                 batch.set_warp_limit(lim)
@@ -281,7 +281,7 @@ def test_dataflow_sweeps_match_levels_on_a_mixed_batch():
     cfg = api.drape_config(max_iterations=10, al_max_iterations=3, barrier_d_hat=1e-3, barrier_kappa=1e4)
     contact = api.Contact(has_ground=True, ground_height=0.6, kappa=1e4)
     res = {}
-    for mode in api.Batch.SWEEP_MODES:
+    for mode in ("levels", "dataflow"):  # at most 3 garments per topology: no garment groups
         solvers = []
         for k, sd in enumerate(sides):
             m = scenarios.hanging_sheet(sd, 0.5 + 0.03 * k)
@@ -294,6 +294,73 @@ def test_dataflow_sweeps_match_levels_on_a_mixed_batch():
         res[mode] = [batch.state(k)[0] for k in range(len(sides))]
     for a, b in zip(res["levels"], res["dataflow"]):
         assert np.array_equal(a, b)
+
+
+def grouped_batch_solvers(cfg, sides):
+    """Hanging sheets of the given grid sides, each with its own length and
+    material (same topology per side, different numbers)."""
+    solvers = []
+    for k, sd in enumerate(sides):
+        m = scenarios.hanging_sheet(sd, 0.5 + 0.011 * k)
+        setup = api.SetupDesc(stiffness=300.0 + 37.0 * k, bend_stiffness=1e-5 * (1 + k % 7), density_gsm=90.0 + 3 * k)
+        solvers.append(api.ProjectiveDynamicsSolver().init_explicit(m, cfg, setup, pinned=m.pinned))
+    return solvers
+
+
+# 20 garments of side 12 (one group of 20 lanes), 40 of side 9 (a group of 32
+# and one of 8), 35 of side 16 (a group of 32, 3 left per garment), singles
+# (among them sides 2 and 3, whose whole tree is one bottom subtree), all
+# interleaved in batch order
+GROUPED_SIDES = ([12] * 20 + [9] * 40 + [16] * 35 + [31, 2, 3, 24])
+GROUPED_SIDES = [GROUPED_SIDES[(k * 37) % len(GROUPED_SIDES)] for k in range(len(GROUPED_SIDES))]
+
+
+@pytest.mark.parametrize("refine", [0, 1])
+def test_grouped_sweeps_bit_identical_to_dataflow_and_to_solo(refine):
+    """Garment groups (8 or more garments of one mesh topology, swept one
+    lane per garment at the bottom of their trees) give exactly the results
+    of the per-garment dependency-driven sweeps, plain and with IPC, with and
+    without a refinement sweep, and exactly what the garments give stepped
+    alone. A batch with groups starts in the grouped kind."""
+    assert len(set(GROUPED_SIDES)) == 7 and len(GROUPED_SIDES) == 99
+    cfg = api.drape_config(max_iterations=8, al_max_iterations=3, barrier_d_hat=1e-3, barrier_kappa=1e4,
+                           refinement_sweeps=refine)
+    contact = api.Contact(has_ground=True, ground_height=0.3, kappa=1e4)
+    res = {}
+    for mode in ("dataflow", "grouped"):
+        batch = api.Batch(grouped_batch_solvers(cfg, GROUPED_SIDES))
+        assert batch.sweep_mode()[0] == "grouped"
+        batch.set_sweep_mode(mode)
+        batch.step(DT, 3)
+        batch.step(DT, 3, contact=contact)
+        res[mode] = [batch.state(k)[0] for k in range(len(GROUPED_SIDES))]
+        batch.close()
+    for k, (a, b) in enumerate(zip(res["dataflow"], res["grouped"])):
+        assert np.array_equal(a, b), (k, GROUPED_SIDES[k], float(np.abs(a - b).max()))
+    # garments of each group, stepped alone
+    solo = grouped_batch_solvers(cfg, GROUPED_SIDES)
+    for k in (0, 1, 2, 5, 7, 11):
+        for _ in range(3):
+            solo[k].step(DT)
+        for _ in range(3):
+            solo[k].step_with_ipc(DT, contact)
+        assert np.array_equal(solo[k].state()[0], res["grouped"][k]), (k, GROUPED_SIDES[k])
+
+
+def test_grouped_kind_needs_groups_and_tunes():
+    """The grouped kind is refused for a batch without garment groups; with
+    groups the autotuner times it beside the other two kinds."""
+    cfg = api.drape_config(max_iterations=6)
+    few = api.Batch(grouped_batch_solvers(cfg, [12, 12, 9]))
+    assert few.sweep_mode()[0] == "dataflow"
+    with pytest.raises(Exception):
+        few.set_sweep_mode("grouped")
+    batch = api.Batch(grouped_batch_solvers(cfg, [12] * 16 + [20] * 9))
+    t = batch.tune()
+    print(t)
+    assert set(t["sweep_ms"]) == {"levels", "dataflow", "grouped"}
+    assert all(v > 0 for m in t["sweep_ms"].values() for v in m.values())
+    batch.step(DT, 2)
 
 
 @pytest.mark.parametrize("side,length", [(20, 1.0), (48, 1.5)])

@@ -447,25 +447,27 @@ class Batch:
 
     TUNE_LIMITS = (0, 1024, 2048, 4096, 6144, 12288, 1 << 30)
 
-    SWEEP_MODES = ("levels", "dataflow")
+    SWEEP_MODES = ("levels", "dataflow", "grouped")
 
     def tune(self) -> dict:
         """Autotunes the sweeps on this batch (vistio_batch_tune): returns the
         chosen sweep kind and warp-item limit, and the sweep time of every
         candidate (per kind, per limit)."""
         chosen = C.c_uint32()
-        ms = (C.c_float * 14)()
+        ms = (C.c_float * 21)()
         L.check(L.lib().vistio_batch_tune(self.h, C.byref(chosen), ms), self.ctx.h)
         return {"sweep_mode": self.sweep_mode()[0], "warp_item_limit": chosen.value,
                 "sweep_ms": {mode: {str(lim): float(ms[7 * m + i]) for i, lim in enumerate(self.TUNE_LIMITS)}
-                             for m, mode in enumerate(self.SWEEP_MODES)}}
+                             for m, mode in enumerate(self.SWEEP_MODES) if ms[7 * m] >= 0}}
 
     def set_warp_limit(self, limit: int):
         L.check(L.lib().vistio_batch_set_warp_limit(self.h, int(limit)), self.ctx.h)
 
     def set_sweep_mode(self, mode: str):
         """"levels": one launch per level; "dataflow": one dependency-driven
-        launch per direction."""
+        launch for both directions; "grouped" (batches with garment groups:
+        8 or more garments of one mesh topology): the groups' tree bottoms
+        one lane per garment, the rest dependency-driven."""
         L.check(L.lib().vistio_batch_set_sweep_mode(self.h, self.SWEEP_MODES.index(mode)), self.ctx.h)
 
     def sweep_mode(self) -> tuple:

@@ -49,6 +49,41 @@ struct SnDev {
   uint64_t p_off;    // P (float offset)
   uint32_t vbase;    // first vertex (row) of the owning instance
   uint32_t inst;     // owning instance
+  uint32_t u_off;    // U slot of panel row 0; row j's slot is u_off + j * u_stride
+  uint32_t u_stride; // 1, or the lanes of a garment group (U interleaved by garment)
+};
+
+// Garment groups. Garments of a batch whose factors share one symbolic
+// structure (the same mesh topology: the same supernodes, row structures and
+// elimination tree; only the numbers differ) are swept together at the bottom
+// of their trees, one lane per garment: every lane runs the same loops over
+// the same row indices, and a factor entry of the whole group is one 128-byte
+// line (the group's values are interleaved, entry-major and garment-minor).
+constexpr uint32_t kGroupLanes = 32;
+// A group of fewer garments would read less than one 32-byte sector per entry.
+constexpr uint32_t kGroupMinLanes = 8;
+
+// One supernode of a group topology. Ids of GsnDev entries are global (every
+// topology's supernodes concatenated); parent and kids are local to the
+// topology, like the per-garment supernode ids minus the garment's base.
+struct GsnDev {
+  uint32_t first, ncols, nrows;
+  uint32_t rows_off;  // first of its nrows row indices in g_rows
+  uint32_t u_local;   // per-garment U slot of panel row 0 (local slot numbering)
+  uint32_t parent;    // local parent, or 0xffffffff for a root
+  uint32_t kid_off;   // its children in g_kids[kid_off, kid_off + nkids)
+  uint32_t nkids;
+  uint64_t g_off;     // entries before it in a group's value block: the triangle of
+                      // inv(L_kk) (s (s + 1) / 2 entries, row by row), then the
+                      // panel (m rows of s entries)
+};
+
+struct GroupDev {
+  uint32_t sn_off;    // global GsnDev id of the topology's local supernode 0
+  uint32_t lanes;     // garments in the group (kGroupMinLanes .. kGroupLanes)
+  uint64_t base;      // first entry of the group's value block in g_vals
+  uint32_t u_base;    // U slot of local slot 0 of lane 0: slot i of lane l is u_base + i * 32 + l
+  uint32_t row_base;  // the topology's rows in g_fwd_ptr start here
 };
 
 // Per-step constants read from device memory so a captured graph stays valid
@@ -147,6 +182,21 @@ struct BatchDev {
   uint32_t* df_cnt;            // forward: children finished
   uint32_t* df_flag;           // backward: parent finished
   uint32_t* df_queue;          // [0] next unit, [1] blocks done (k_sweep resets both)
+  // garment-grouped sweeps (k_gsweep)
+  const GroupDev* grp;
+  const GsnDev* gsn;
+  const uint32_t* g_rows;      // topology-local row indices of the panels
+  const uint32_t* g_fwd_ptr;   // per topology row (row_base + r): its pull list in g_fwd
+  const uint32_t* g_fwd;       // local U slots a row pulls in the forward sweep
+  const uint32_t* g_kids;      // local children
+  const uint2* g_subs;         // bottom subtrees: (first, last) global GsnDev ids
+  const uint32_t* gl_vbase;    // per group lane (group * 32 + lane): the garment's first row
+  const uint32_t* gl_snbase;   // ... its first global supernode id
+  const uint32_t* gl_inst;     // ... its instance
+  const float* g_vals;         // interleaved factor values: entry e of a group at (base + e) * 32 + lane
+  const uint2* g_items_fwd;    // work items, forward order: (group, kind | local id << 1)
+  const uint2* g_items_bwd;    // backward order
+  uint32_t* g_queue;           // [0] next item, [1] warps done (k_gsweep resets both)
   // FP64 refinement: the factored matrix A (f64, rows and columns in each
   // instance's solve order, global row ids), the right-hand side the first
   // sweep solved (R0) and the correction vector the refinement sweeps solve in
@@ -602,7 +652,7 @@ __device__ __forceinline__ void sn_push_rows(const BatchDev& B, const Team& tm, 
     float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
     const float* row = Ps + j * ld;
     for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], tm.v1[c]);
-    B.U[S.rows_off + j0 + j] = u;
+    B.U[S.u_off + (j0 + j) * S.u_stride] = u;
   }
 }
 
@@ -703,8 +753,90 @@ __device__ __forceinline__ void sn_diag_bwd_smem(const Team& tm, const SnDev& S,
   }
 }
 
-// Backward step of one supernode: t = y - P^T x[R]; x = inv(L_kk)^T t.
+// Backward step of one supernode with a warp team: t = y - P^T x[R];
+// x = inv(L_kk)^T t. Lane c < s owns column c and forms its sum over the panel
+// rows j in ascending order (one FMA chain from zero), then x_c = sum over
+// c2 = c .. s-1 of inv(L_kk)(c2, c) t_c2, again ascending: the same order the
+// garment-grouped sweep (one lane per garment) uses, so the two give the same
+// bits. Rows arrive in chunks (their x gathered into xg, the panel staged
+// whole or by row chunks); the order of the sums does not depend on the chunks.
+__device__ __forceinline__ void sn_backward_warp(const BatchDev& B, Team& tm, const SnDev& S) {
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first, ld = sn_ld(s);
+  float4* Y = B.Y + S.vbase;
+  const float* D = B.vals + S.d_off;
+  const float* Pp = B.vals + S.p_off;
+  const uint32_t* Rr = B.rows + S.rows_off;
+  const uint32_t c = tm.rank;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  // own columns through L2: the forward sweep may have written them in this
+  // launch, on another SM
+  const float4 yc = c < s ? __ldcg(Y + f + c) : acc;
+  const uint32_t whole = uint32_t(S.p_off - S.d_off) + m * ld + m;  // [D | P | rows] is one contiguous region
+  const float* Ds = nullptr;
+  if (whole + 8 <= tm.cap) {
+    // the whole supernode in one copy, in flight while the first chunk of
+    // x[R] is gathered
+    stage_issue(tm, D, whole);
+    for (uint32_t j0 = 0; j0 < m; j0 += tm.xcap) {
+      const uint32_t nr = min(tm.xcap, m - j0);
+      __syncwarp();
+      for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = __ldcg(Y + Rr[j0 + j]);
+      if (!Ds) Ds = stage_wait(tm, D, B.status);
+      __syncwarp();
+      if (c < s) {
+        const float* P0 = Ds + (S.p_off - S.d_off) + size_t(j0) * ld + c;
+        for (uint32_t j = 0; j < nr; ++j) f4_fma(acc, P0[j * ld], tm.xg[j]);
+      }
+    }
+    if (!Ds) Ds = stage_wait(tm, D, B.status);
+    __syncwarp();
+    if (c < s) tm.v0[c] = f4_sub(yc, acc);
+    __syncwarp();
+    sn_diag_bwd_smem(tm, S, Ds, Y);
+    __syncwarp();
+    return;
+  }
+  const uint32_t rc = max(1u, min((tm.cap - 8) / ld, tm.xcap));
+  for (uint32_t j0 = 0; j0 < m; j0 += rc) {
+    const uint32_t nr = min(rc, m - j0);
+    __syncwarp();  // previous readers of xg are done
+    for (uint32_t j = tm.rank; j < nr; j += tm.size) tm.xg[j] = __ldcg(Y + Rr[j0 + j]);
+    const float* Ps = stage(tm, Pp + uint64_t(j0) * ld, nr * ld, B.status);
+    __syncwarp();
+    if (c < s)
+      for (uint32_t j = 0; j < nr; ++j) f4_fma(acc, Ps[j * ld + c], tm.xg[j]);
+  }
+  __syncwarp();
+  if (c < s) tm.v0[c] = f4_sub(yc, acc);
+  __syncwarp();
+  if (s * ld + 8 <= tm.cap) {
+    Ds = stage(tm, D, s * ld, B.status);
+    __syncwarp();
+    sn_diag_bwd_smem(tm, S, Ds, Y);
+  } else {
+    // column chunks of D: x_c needs only column c (rows c .. s-1)
+    const uint32_t cw = max(1u, (tm.cap - 8) / ld);
+    for (uint32_t c0 = 0; c0 < s; c0 += cw) {
+      const uint32_t c1 = min(s, c0 + cw);
+      const float* Dc = stage(tm, D + uint64_t(c0) * ld, (c1 - c0) * ld, B.status);
+      if (c >= c0 && c < c1) {
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, Dc[(c - c0) * ld + c2], tm.v0[c2]);
+        Y[f + c] = x;
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Backward step of one supernode: t = y - P^T x[R]; x = inv(L_kk)^T t. A
+// block team splits each column's sum over parts of the rows and adds the
+// parts in a fixed order.
 __device__ __forceinline__ void sn_backward(const BatchDev& B, Team& tm, const SnDev& S) {
+  if (!tm.block) {
+    sn_backward_warp(B, tm, S);
+    return;
+  }
   const uint32_t s = S.ncols, m = S.nrows, f = S.first, ld = sn_ld(s);
   float4* Y = B.Y + S.vbase;
   const float* D = B.vals + S.d_off;
@@ -845,16 +977,15 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
         const float* row = Ps + j * ld;
         for (uint32_t c = 0; c < s; ++c) f4_fma(u, row[c], acc[f + c]);
         if (r < c1) acc[r - c0] = f4_sub(acc[r - c0], u);
-        else B.U[S.rows_off + j] = u;
+        else B.U[S.u_off + j * S.u_stride] = u;
       }
       tm.sync();
     } else {
       // t = y - P^T x[R] (x of rows in the subtree from acc, above it from Y),
-      // the gathered x in chunks of xcap rows; s <= 64 needs at most two
-      // column rounds of width 32
-      const uint32_t width = team_width(tm, s), parts = tm.size / width;
-      const uint32_t cl = tm.rank % width, part = tm.rank / width;
-      float4 sum0 = make_float4(0.f, 0.f, 0.f, 0.f), sum1 = sum0;
+      // the gathered x in chunks of xcap rows; lane c < s sums column c over
+      // the rows in ascending order
+      float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+      const uint32_t c = tm.rank;
       for (uint32_t j0 = 0; j0 < m; j0 += tm.xcap) {
         const uint32_t nr = min(tm.xcap, m - j0);
         tm.sync();
@@ -863,17 +994,14 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
           tm.xg[j] = r < c1 ? acc[r - c0] : __ldcg(Yg + r);
         }
         tm.sync();
-        if (part < parts) {
-          const float* P0 = Ps + size_t(j0) * ld;
-          if (cl < s)
-            for (uint32_t j = part; j < nr; j += parts) f4_fma(sum0, P0[j * ld + cl], tm.xg[j]);
-          if (width + cl < s)
-            for (uint32_t j = part; j < nr; j += parts) f4_fma(sum1, P0[j * ld + width + cl], tm.xg[j]);
+        if (c < s) {
+          const float* P0 = Ps + size_t(j0) * ld + c;
+          for (uint32_t j = 0; j < nr; ++j) f4_fma(sum, P0[j * ld], tm.xg[j]);
         }
       }
       tm.sync();
-      team_column_sum(tm, sum0, width, parts, 0, s, acc + f, tm.v0, true);
-      if (width < s) team_column_sum(tm, sum1, width, parts, width, s, acc + f, tm.v0, true);
+      if (c < s) tm.v0[c] = f4_sub(acc[f + c], sum);
+      tm.sync();
       // x = inv(L_kk)^T t into acc
       for (uint32_t c = tm.rank; c < s; c += tm.size) {
         float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1096,6 +1224,275 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_sweep(Bat
       B.df_queue[0] = 0u;
       B.df_queue[1] = 0u;
     }
+  }
+}
+
+// ------------------------------------------------ garment-grouped sweeps
+// k_gsweep sweeps the bottom of the supernodal trees of every garment group:
+// the bottom subtrees, then the supernodes above them that a warp would take
+// (at most 32 columns, s (s + m) within the default warp-item limit) as long
+// as all their descendants are swept here too. Each warp takes work items from
+// a queue (no block-wide barrier): one bottom subtree or one such supernode of
+// a topology, for every garment of one group at once, lane l for the group's
+// garment l. The lanes never exchange data: each runs, for its own garment,
+// the per-garment warp sweep's arithmetic in the same order
+//   forward   t = y - the pulled U slots in list order; y_c = sum over
+//             c2 <= c ascending of inv(L_kk)(c, c2) t_c2; u_j = sum over c
+//             ascending of P(j, c) y_c;
+//   backward  each column's sum over the panel rows ascending, t_c = y_c -
+//             that sum; x_c = sum over c2 >= c ascending of inv(L_kk)(c2, c) t_c2,
+// so a garment's solution is bit-identical to the per-garment sweeps'. Each
+// lane keeps its vector (a supernode's columns, or a subtree's slice of at
+// most 32 columns) in shared memory, component k of column c of lane l at
+// [(3 c + k) * 32 + l]: a warp's accesses hit 32 banks. Factor entries come
+// straight from HBM: one entry of a whole group is one coalesced 128-byte
+// line, and a topology's row indices and pull lists are read once for all
+// its garments. Dependencies are per garment, as in k_sweep: each lane waits
+// on, and signals, its own garment's counters. Waits are bounded (status bit 4).
+constexpr uint32_t kGWarps = 8;
+constexpr uint32_t kGThreads = 32 * kGWarps;
+constexpr uint32_t kGCols = 32;
+constexpr uint32_t kGSmem = kGWarps * kGCols * 3 * 32 * 4;  // 96 KB: two blocks per SM
+constexpr uint32_t kGColBlock = 8;                          // backward: columns summed side by side
+constexpr uint32_t kGNone = 0xffffffffu;
+
+struct GLane {
+  float* v;  // component x of column 0 of this lane
+  __device__ __forceinline__ float4 get(uint32_t c) const {
+    return make_float4(v[(3 * c) * 32], v[(3 * c + 1) * 32], v[(3 * c + 2) * 32], 0.f);
+  }
+  __device__ __forceinline__ void set(uint32_t c, float4 a) const {
+    v[(3 * c) * 32] = a.x;
+    v[(3 * c + 1) * 32] = a.y;
+    v[(3 * c + 2) * 32] = a.z;
+  }
+};
+
+// Streamed factor entry (read once per sweep).
+__device__ __forceinline__ float gval(const float* p) { return __ldcs(p); }
+
+// y = inv(L_kk) t in place on columns f .. f + s of L, the triangle's rows at
+// D (entry (c, c2) at D[(c (c + 1) / 2 + c2) * 32]); descending c, so every
+// y_c reads only t values.
+__device__ __forceinline__ void g_diag_fwd(const GLane& L, uint32_t f, uint32_t s, const float* D) {
+  for (int c = int(s) - 1; c >= 0; --c) {
+    float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float* row = D + size_t(uint32_t(c) * uint32_t(c + 1) / 2) * 32;
+#pragma unroll 8
+    for (uint32_t c2 = 0; c2 <= uint32_t(c); ++c2) f4_fma(y, gval(row + c2 * 32), L.get(f + c2));
+    L.set(f + uint32_t(c), y);
+  }
+}
+
+// x = inv(L_kk)^T t in place on columns f .. f + s of L; ascending c, so every
+// x_c reads only t values.
+__device__ __forceinline__ void g_diag_bwd(const GLane& L, uint32_t f, uint32_t s, const float* D) {
+  for (uint32_t c = 0; c < s; ++c) {
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 8
+    for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, gval(D + size_t(c2 * (c2 + 1) / 2 + c) * 32), L.get(f + c2));
+    L.set(f + c, x);
+  }
+}
+
+// u_j = P(j, :) . y for the m panel rows (P row-major, y in columns f .. f + s
+// of L), four rows at a time so that each y_c is read once per four rows;
+// emit(j, u) takes each row's update.
+template <class Emit>
+__device__ __forceinline__ void g_push(const GLane& L, uint32_t f, uint32_t s, uint32_t m, const float* P, Emit emit) {
+  for (uint32_t j0 = 0; j0 < m; j0 += 4) {
+    const uint32_t nr = min(4u, m - j0);
+    float4 u[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) u[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float* P0 = P + size_t(j0) * s * 32;
+    // unrolled so that the loads of several columns are in flight before the
+    // first multiply waits on one
+#pragma unroll 8
+    for (uint32_t c = 0; c < s; ++c) {
+      const float4 y = L.get(f + c);
+#pragma unroll
+      for (uint32_t r = 0; r < 4; ++r)
+        if (r < nr) f4_fma(u[r], gval(P0 + size_t(r * s + c) * 32), y);
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < 4; ++r)
+      if (r < nr) emit(j0 + r, u[r]);
+  }
+}
+
+// t_c = L_c - sum over panel rows j of P(j, c) x(R_j) for the s columns at f,
+// kGColBlock columns side by side, each column's sum in ascending j; xget(r)
+// gives x of row r.
+template <class XGet>
+__device__ __forceinline__ void g_bwd_panel(const GLane& L, uint32_t f, uint32_t s, uint32_t m, const float* P,
+                                            const uint32_t* R, XGet xget) {
+  for (uint32_t cb = 0; cb < s; cb += kGColBlock) {
+    float4 acc[kGColBlock];
+#pragma unroll
+    for (uint32_t k = 0; k < kGColBlock; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (uint32_t j = 0; j < m; ++j) {
+      const float4 x = xget(__ldg(R + j));
+      const float* Pj = P + (size_t(j) * s + cb) * 32;
+#pragma unroll
+      for (uint32_t k = 0; k < kGColBlock; ++k)
+        if (cb + k < s) f4_fma(acc[k], gval(Pj + k * 32), x);
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < kGColBlock; ++k)
+      if (cb + k < s) L.set(f + cb + k, f4_sub(L.get(f + cb + k), acc[k]));
+  }
+}
+
+// One work item for one lane (its group's garment `lane`).
+template <int DIR>
+__device__ __forceinline__ void g_item(const BatchDev& B, uint2 it, const GLane& L, uint32_t lane, bool ipc) {
+  const GroupDev G = B.grp[it.x];
+  if (lane >= G.lanes) return;
+  const uint32_t gl = it.x * kGroupLanes + lane;
+  if (ipc && B.red[B.gl_inst[gl]].al_done) return;
+  const uint32_t snb = B.gl_snbase[gl];
+  float4* Y = B.Y + B.gl_vbase[gl];
+  const float* vals = B.g_vals + G.base * 32 + lane;
+  float4* U = B.U + G.u_base + lane;  // the garment's U slot i at U[i * 32]
+  const uint32_t id = it.y >> 1;
+  if ((it.y & 1u) == 0) {
+    // one bottom subtree: the warp keeps its slice of the vector (columns
+    // c0 .. c1) for the whole sweep, as the per-garment subtree sweep does
+    const uint2 st = B.g_subs[id];
+    const GsnDev A = B.gsn[st.x], Z = B.gsn[st.y];
+    const uint32_t c0 = A.first, c1 = Z.first + Z.ncols, nc = c1 - c0;
+    const uint32_t root = snb + (st.y - G.sn_off);
+    if (DIR == 1 && dep_wait(B, B.df_flag + root, 1u)) B.df_flag[root] = 0u;
+    for (uint32_t c = 0; c < nc; ++c) L.set(c, __ldcg(Y + c0 + c));
+    if (DIR == 0) {
+      for (uint32_t q = st.x; q <= st.y; ++q) {
+        const GsnDev S = B.gsn[q];
+        const uint32_t s = S.ncols, m = S.nrows, f = S.first - c0;
+        const float* D = vals + S.g_off * 32;
+        g_diag_fwd(L, f, s, D);
+        const uint32_t* R = B.g_rows + S.rows_off;
+        g_push(L, f, s, m, D + size_t(s * (s + 1) / 2) * 32, [&](uint32_t j, float4 u) {
+          const uint32_t r = __ldg(R + j);
+          if (r < c1) L.set(r - c0, f4_sub(L.get(r - c0), u));
+          else U[size_t(S.u_local + j) * 32] = u;
+        });
+      }
+    } else {
+      for (uint32_t q = st.y + 1; q-- > st.x;) {
+        const GsnDev S = B.gsn[q];
+        const uint32_t s = S.ncols, m = S.nrows, f = S.first - c0;
+        const float* D = vals + S.g_off * 32;
+        g_bwd_panel(L, f, s, m, D + size_t(s * (s + 1) / 2) * 32, B.g_rows + S.rows_off,
+                    [&](uint32_t r) { return r < c1 ? L.get(r - c0) : __ldcg(Y + r); });
+        g_diag_bwd(L, f, s, D);
+      }
+    }
+    for (uint32_t c = 0; c < nc; ++c) Y[c0 + c] = L.get(c);
+    __threadfence();
+    if (DIR == 0) {
+      if (Z.parent != kGNone) atomicAdd(B.df_cnt + snb + Z.parent, 1u);
+      else atomicExch(B.df_flag + root, 1u);
+    }
+    return;
+  }
+  // one supernode above the subtrees
+  const GsnDev S = B.gsn[id];
+  const uint32_t s = S.ncols, m = S.nrows, f = S.first;
+  const uint32_t me = snb + (id - G.sn_off);
+  const float* D = vals + S.g_off * 32;
+  const float* P = D + size_t(s * (s + 1) / 2) * 32;
+  if (DIR == 0) {
+    if (S.nkids && dep_wait(B, B.df_cnt + me, S.nkids)) B.df_cnt[me] = 0u;
+    const uint32_t* fp = B.g_fwd_ptr + G.row_base + f;
+    for (uint32_t c = 0; c < s; ++c) {
+      float4 t = Y[f + c];
+      for (uint32_t q = __ldg(fp + c), qe = __ldg(fp + c + 1); q < qe; ++q)
+        t = f4_sub(t, __ldcg(U + size_t(__ldg(B.g_fwd + q)) * 32));
+      L.set(c, t);
+    }
+    g_diag_fwd(L, 0, s, D);
+    for (uint32_t c = 0; c < s; ++c) Y[f + c] = L.get(c);
+    g_push(L, 0, s, m, P, [&](uint32_t j, float4 u) { U[size_t(S.u_local + j) * 32] = u; });
+    __threadfence();
+    if (S.parent != kGNone) atomicAdd(B.df_cnt + snb + S.parent, 1u);
+    else atomicExch(B.df_flag + me, 1u);
+  } else {
+    if (dep_wait(B, B.df_flag + me, 1u)) B.df_flag[me] = 0u;
+    for (uint32_t c = 0; c < s; ++c) L.set(c, __ldcg(Y + f + c));
+    g_bwd_panel(L, 0, s, m, P, B.g_rows + S.rows_off, [&](uint32_t r) { return __ldcg(Y + r); });
+    g_diag_bwd(L, 0, s, D);
+    for (uint32_t c = 0; c < s; ++c) Y[f + c] = L.get(c);
+    __threadfence();
+    for (uint32_t k = 0; k < S.nkids; ++k) atomicExch(B.df_flag + snb + __ldg(B.g_kids + S.kid_off + k), 1u);
+  }
+}
+
+// The forward (DIR = 0) or backward (DIR = 1) grouped sweep over `nitems`
+// work items in topological order. Each warp takes items until the queue is
+// empty; an item only waits for items handed out before it, whose warps are
+// running, so there is no deadlock whatever the number of resident warps. The
+// last warp out resets the queue.
+template <int DIR>
+__global__ void __launch_bounds__(kGThreads, 2) k_gsweep(BatchDev B, uint32_t nitems) {
+  extern __shared__ float gsm[];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const GLane L{gsm + warp * (kGCols * 3 * 32) + lane};
+  const bool ipc = B.prm->ipc != 0;
+  const uint2* items = DIR == 0 ? B.g_items_fwd : B.g_items_bwd;
+  for (;;) {
+    uint32_t q = 0;
+    if (lane == 0) q = atomicAdd(B.g_queue, 1u);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= nitems) break;
+    g_item<DIR>(B, items[q], L, lane, ipc);
+    __syncwarp();
+  }
+  if (lane == 0) {
+    __threadfence();
+    if (atomicAdd(B.g_queue + 1, 1u) == gridDim.x * kGWarps - 1) {
+      B.g_queue[0] = 0u;
+      B.g_queue[1] = 0u;
+    }
+  }
+}
+
+// Largest c with c (c + 1) / 2 <= e.
+__device__ __forceinline__ uint32_t tri_row(uint32_t e) {
+  uint32_t c = uint32_t((sqrtf(8.f * float(e) + 1.f) - 1.f) * 0.5f);
+  while ((c + 1) * (c + 2) / 2 <= e) ++c;
+  while (c * (c + 1) / 2 > e) --c;
+  return c;
+}
+
+// Copies the grouped supernodes' factor values from the per-garment regions
+// (D column-major, P row-major, leading dimension sn_ld(s)) into the groups'
+// interleaved blocks; one block per (group, global GsnDev id) of `work`.
+// Lanes beyond a group's garments get zeros.
+__global__ void __launch_bounds__(256) k_gpack(BatchDev B, float* g_vals, const uint2* work) {
+  const uint2 w = work[blockIdx.x];
+  const GroupDev G = B.grp[w.x];
+  const GsnDev S = B.gsn[w.y];
+  const uint32_t lane = threadIdx.x & 31, row = threadIdx.x >> 5, rows = blockDim.x >> 5;
+  const uint32_t s = S.ncols, m = S.nrows, nd = s * (s + 1) / 2, ne = nd + m * s;
+  float* out = g_vals + (G.base + S.g_off) * 32 + lane;
+  if (lane >= G.lanes) {
+    for (uint32_t e = row; e < ne; e += rows) out[size_t(e) * 32] = 0.f;
+    return;
+  }
+  const SnDev P = B.sn[B.gl_snbase[w.x * kGroupLanes + lane] + (w.y - G.sn_off)];
+  const uint32_t ld = sn_ld(s);
+  for (uint32_t e = row; e < ne; e += rows) {
+    float v;
+    if (e < nd) {
+      const uint32_t c = tri_row(e), c2 = e - c * (c + 1) / 2;
+      v = B.vals[P.d_off + uint64_t(c2) * ld + c];
+    } else {
+      const uint32_t j = (e - nd) / s, c = (e - nd) % s;
+      v = B.vals[P.p_off + uint64_t(j) * ld + c];
+    }
+    out[size_t(e) * 32] = v;
   }
 }
 

@@ -35,7 +35,8 @@ struct vistio_ctx {
   std::mutex mu;
   int refs = 0;
   bool closed = false;
-  uint32_t sweep_blocks = 0;  // resident k_sweep blocks on this device (SMs x blocks per SM)
+  uint32_t sweep_blocks = 0;   // resident k_sweep blocks on this device (SMs x blocks per SM)
+  uint32_t gsweep_blocks = 0;  // resident k_gsweep blocks
 };
 
 namespace {
@@ -162,7 +163,8 @@ struct vistio_batch {
   std::vector<SnDev> sn_host;                       // supernode table, for re-scheduling
   uint32_t warp_limit = kWarpItemLimit;             // s (s + m) limit of a warp item
   float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
-  // sweeps: 0 = one launch per level (k_level), 1 = dependency-driven (k_sweep)
+  // sweeps: 0 = one launch per level (k_level), 1 = dependency-driven (k_sweep),
+  // 2 = garment groups' tree bottoms by k_gsweep, the rest by k_sweep
   uint32_t sweep_mode = 1;
   std::vector<uint2> units_host;                    // k_sweep work units in forward order
   uint32_t n_units = 0, n_units_fwd = 0;
@@ -175,6 +177,16 @@ struct vistio_batch {
   DevBuf<uint32_t> df_parent, df_nkids, df_kid_ptr, df_kids, df_cnt, df_flag, df_queue;
   DevBuf<SnDev> sn;
   DevBuf<float4> U;
+  // garment groups (k_gsweep, sweep mode 2): the bottom of the trees of
+  // garments that share a symbolic structure, swept one lane per garment
+  uint32_t n_groups = 0, n_gitems_fwd = 0, n_gitems_bwd = 0, n_gpack = 0, n_sub_plain = 0;
+  std::vector<uint8_t> sn_grouped;  // per global supernode: swept by k_gsweep in mode 2
+  DevBuf<GroupDev> grp;
+  DevBuf<GsnDev> gsn;
+  DevBuf<uint32_t> g_rows, g_fwd_ptr, g_fwd, g_kids, gl_vbase, gl_snbase, gl_inst, g_queue;
+  DevBuf<uint2> g_subs, g_items_fwd, g_items_bwd, g_pack;
+  DevBuf<float> g_vals;
+  uint64_t g_bytes = 0;
   DevBuf<InstRed> red;
   DevBuf<StepParams> prm;
   SelfContactDev self;       // self-contact buffers (allocated on first use)
@@ -211,10 +223,15 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
 // supernodes for a whole block (heaviest first), then those for one warp
 // (heaviest first). Fills lvl_off / lvl_nb / lvl_nw and returns the items.
 std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
+  // in sweep mode 2 the garment groups' tree bottoms belong to k_gsweep
+  const bool grouped = b->sweep_mode == 2;
+  auto skip = [&](uint32_t g) { return grouped && b->sn_grouped[g]; };
+  const uint32_t nsub = grouped ? b->n_sub_plain : b->n_sub;
   uint32_t L = 0;
   for (auto& t : b->top) L = std::max(L, t.first + 1);
   std::vector<std::vector<uint32_t>> blk(L), wrp(L);
   for (auto& t : b->top) {
+    if (skip(t.second)) continue;
     const SnDev& S = b->sn_host[t.second];
     (warp_item(S.ncols, S.nrows, limit) ? wrp : blk)[t.first].push_back(t.second);
   }
@@ -234,8 +251,8 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
   // k_sweep units in forward order: bottom subtrees by eight, then each level's
   // block supernodes one by one and its warp supernodes by eight
   b->units_host.clear();
-  for (uint32_t q = 0; q < b->n_sub; q += kSolveWarps)
-    b->units_host.push_back(make_uint2(0u | (std::min(kSolveWarps, b->n_sub - q) << 2), q));
+  for (uint32_t q = 0; q < nsub; q += kSolveWarps)
+    b->units_host.push_back(make_uint2(0u | (std::min(kSolveWarps, nsub - q) << 2), q));
   for (uint32_t l = 0; l < L; ++l) {
     const uint32_t off = b->lvl_off[l], nb = b->lvl_nb[l], nw = b->lvl_nw[l];
     for (uint32_t i = 0; i < nb; ++i) b->units_host.push_back(make_uint2(1u | (1u << 2), items[off + i]));
@@ -254,13 +271,14 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
     for (auto& t : b->top) D = std::max(D, b->sn_depth[t.second] + 1);
     std::vector<std::vector<uint32_t>> dblk(D), dwrp(D);
     for (auto& t : b->top) {
+      if (skip(t.second)) continue;
       const SnDev& S = b->sn_host[t.second];
       (warp_item(S.ncols, S.nrows, limit) ? dwrp : dblk)[b->sn_depth[t.second]].push_back(t.second);
     }
     b->units_fwd_host.clear();
     b->items_fwd_host.clear();
-    for (uint32_t q = 0; q < b->n_sub; q += kSolveWarps)
-      b->units_fwd_host.push_back(make_uint2(0u | (std::min(kSolveWarps, b->n_sub - q) << 2), q));
+    for (uint32_t q = 0; q < nsub; q += kSolveWarps)
+      b->units_fwd_host.push_back(make_uint2(0u | (std::min(kSolveWarps, nsub - q) << 2), q));
     for (uint32_t d = D; d-- > 0;) {
       std::stable_sort(dblk[d].begin(), dblk[d].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
       std::stable_sort(dwrp[d].begin(), dwrp[d].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
@@ -453,6 +471,100 @@ vistio_status factor_on_device(vistio_ctx* ctx, vistio_batch* b, vistio_solver* 
   return VISTIO_OK;
 }
 
+// True if two factors have one symbolic structure: the same ordering
+// outcome, supernodes, row structures, elimination tree, bottom subtrees and
+// pull lists (only the numbers may differ).
+bool same_structure(const Factor& a, const Factor& b) {
+  if (a.n != b.n || a.sn.size() != b.sn.size() || a.rows.size() != b.rows.size() || a.nlevels != b.nlevels ||
+      a.sub_first.size() != b.sub_first.size() || a.fwd_sn.size() != b.fwd_sn.size())
+    return false;
+  auto eq = [](const std::vector<uint32_t>& x, const std::vector<uint32_t>& y) {
+    return x.size() == y.size() && (x.empty() || std::memcmp(x.data(), y.data(), x.size() * 4) == 0);
+  };
+  for (size_t q = 0; q < a.sn.size(); ++q) {
+    const Supernode &x = a.sn[q], &y = b.sn[q];
+    if (x.first != y.first || x.ncols != y.ncols || x.nrows != y.nrows || x.rows_off != y.rows_off ||
+        x.parent != y.parent || x.level != y.level)
+      return false;
+  }
+  return eq(a.rows, b.rows) && eq(a.sub_first, b.sub_first) && eq(a.sub_last, b.sub_last) && eq(a.fwd_ptr, b.fwd_ptr) &&
+         eq(a.fwd_sn, b.fwd_sn) && eq(a.fwd_pos, b.fwd_pos);
+}
+
+// The garment groups of a batch: garments of one symbolic structure (a
+// topology), in batch order, kGroupLanes per group; a remainder of fewer
+// than kGroupMinLanes garments stays ungrouped. Per topology, the supernodes
+// k_gsweep takes: every bottom-subtree supernode, and every supernode of at
+// most kWarpVec columns within the default warp-item limit all of whose
+// children are taken (so the taken set is closed downwards).
+struct GroupPlan {
+  struct Topo {
+    uint32_t leader = 0;
+    std::vector<uint32_t> members;
+    std::vector<uint8_t> taken, insub;
+    std::vector<uint32_t> depth;  // supernodes above each one
+    uint64_t entries = 0;         // interleaved entries of one group's value block
+    uint32_t sn_off = 0, row_base = 0, sub_base = 0, rows_base = 0, fwd_base = 0;
+  };
+  std::vector<Topo> topos;
+  std::vector<int32_t> group;  // per garment: its group, or -1
+  std::vector<uint32_t> lane;  // per garment: its lane in the group
+  std::vector<uint32_t> gtopo; // per group: its topology
+  std::vector<std::vector<uint32_t>> gmembers;
+};
+
+GroupPlan plan_groups(vistio_solver* const* solvers, uint32_t n) {
+  GroupPlan G;
+  G.group.assign(n, -1);
+  G.lane.assign(n, 0);
+  std::vector<GroupPlan::Topo> all;
+  for (uint32_t k = 0; k < n; ++k) {
+    const Factor& F = solvers[k]->setup.factor;
+    size_t t = 0;
+    for (; t < all.size(); ++t)
+      if (same_structure(solvers[all[t].leader]->setup.factor, F)) break;
+    if (t == all.size()) {
+      all.emplace_back();
+      all.back().leader = k;
+    }
+    all[t].members.push_back(k);
+  }
+  for (auto& T : all) {
+    if (T.members.size() < kGroupMinLanes) continue;
+    const Factor& F = solvers[T.leader]->setup.factor;
+    const uint32_t ns = uint32_t(F.sn.size());
+    T.insub.assign(ns, 0);
+    for (size_t q = 0; q < F.sub_first.size(); ++q)
+      for (uint32_t k = F.sub_first[q]; k <= F.sub_last[q]; ++k) T.insub[k] = 1;
+    T.taken.assign(ns, 0);
+    std::vector<uint8_t> kids_taken(ns, 1);
+    for (uint32_t q = 0; q < ns; ++q) {  // children precede their parents
+      const Supernode& X = F.sn[q];
+      T.taken[q] = T.insub[q] ||
+                   (kids_taken[q] && X.ncols <= kWarpVec && uint64_t(X.ncols) * (X.ncols + X.nrows) <= kWarpItemLimit);
+      if (X.parent != UINT32_MAX && !T.taken[q]) kids_taken[X.parent] = 0;
+      if (T.taken[q]) T.entries += uint64_t(X.ncols) * (X.ncols + 1) / 2 + uint64_t(X.nrows) * X.ncols;
+    }
+    T.depth.assign(ns, 0);
+    for (uint32_t q = ns; q-- > 0;)
+      if (F.sn[q].parent != UINT32_MAX) T.depth[q] = T.depth[F.sn[q].parent] + 1;
+    const uint32_t ti = uint32_t(G.topos.size());
+    for (size_t i = 0; i < T.members.size(); i += kGroupLanes) {
+      const uint32_t cnt = uint32_t(std::min<size_t>(kGroupLanes, T.members.size() - i));
+      if (cnt < kGroupMinLanes) break;
+      const uint32_t g = uint32_t(G.gmembers.size());
+      G.gmembers.emplace_back(T.members.begin() + i, T.members.begin() + i + cnt);
+      G.gtopo.push_back(ti);
+      for (uint32_t l = 0; l < cnt; ++l) {
+        G.group[T.members[i + l]] = int32_t(g);
+        G.lane[T.members[i + l]] = l;
+      }
+    }
+    G.topos.push_back(std::move(T));
+  }
+  return G;
+}
+
 vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_t n, vistio_batch* b) {
   cudaStream_t st = ctx->stream;
   b->ctx = ctx;
@@ -504,13 +616,29 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   uint32_t LMAX = 0;
   for (uint32_t k = 0; k < n; ++k) LMAX = std::max(LMAX, solvers[k]->setup.factor.nlevels);
   (void)LMAX;
-  std::vector<uint2> subs;
+  std::vector<uint2> subs, subs_grouped;
+  // Garment groups, and the U slots of every garment: ungrouped garments
+  // first, one contiguous run each; then per group 32 slots per local slot,
+  // lane-minor (slot i of lane l at u_base + i * 32 + l)
+  GroupPlan gp = plan_groups(solvers, n);
+  std::vector<uint64_t> ubase(n, 0), g_ubase(gp.gmembers.size(), 0);
+  uint64_t NU = 0;
+  for (uint32_t k = 0; k < n; ++k)
+    if (gp.group[k] < 0) { ubase[k] = NU; NU += solvers[k]->setup.factor.rows.size(); }
+  for (size_t g = 0; g < gp.gmembers.size(); ++g) {
+    g_ubase[g] = NU;
+    NU += uint64_t(kGroupLanes) * solvers[gp.gmembers[g][0]]->setup.factor.rows.size();
+  }
+  if (NU >= (1ull << 32)) return fail(ctx, VISTIO_ERR_CAPACITY, "batch too large for 32-bit U slot indices");
   uint64_t snb = 0, rowsb = 0, valsb = 0, fwdb = 0;
   for (uint32_t k = 0; k < n; ++k) {
     vistio_solver* S = solvers[k];
     const InstanceSetup& I = S->setup;
     const Factor& F = I.factor;
     uint64_t v0 = vb[k], t0 = tb[k], h0 = hb[k];
+    const bool grouped = gp.group[k] >= 0;
+    const uint64_t ub = grouped ? g_ubase[gp.group[k]] + gp.lane[k] : ubase[k];
+    const uint32_t us = grouped ? kGroupLanes : 1u;  // U slot of local slot i: ub + i * us
     for (uint32_t i = 0; i < I.nv; ++i) {
       pos[v0 + i] = make_float4(S->host_pos[3 * i], S->host_pos[3 * i + 1], S->host_pos[3 * i + 2], 0.f);
       vel[v0 + i] = make_float4(S->host_vel[3 * i], S->host_vel[3 * i + 1], S->host_vel[3 * i + 2], 0.f);
@@ -542,6 +670,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       d.p_off = valsb; valsb += pad4(uint64_t(m) * ld + m);  // panel, then its row indices
       d.vbase = uint32_t(v0);
       d.inst = k;
+      d.u_off = uint32_t(ub + uint64_t(X.rows_off) * us);
+      d.u_stride = us;
       if (X.level != kBottomLevel) b->top.push_back({X.level, uint32_t(snb + q)});
       if (F.numeric) {  // else the device factorization writes D and P
         const double* Pn = F.vals.data() + X.panel_off;   // row-major m x s
@@ -556,10 +686,10 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     }
     rows.insert(rows.end(), F.rows.begin(), F.rows.end());
     for (size_t q = 0; q < F.sub_first.size(); ++q)
-      subs.push_back(make_uint2(uint32_t(snb + F.sub_first[q]), uint32_t(snb + F.sub_last[q])));
+      (grouped ? subs_grouped : subs).push_back(make_uint2(uint32_t(snb + F.sub_first[q]), uint32_t(snb + F.sub_last[q])));
     for (uint32_t r = 0; r < I.nv; ++r) fwd_ptr[v0 + r] = uint32_t(fwdb + F.fwd_ptr[r]);
     for (size_t q = 0; q < F.fwd_sn.size(); ++q)
-      fwd[fwdb + q] = uint32_t(rowsb + F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]);
+      fwd[fwdb + q] = uint32_t(ub + uint64_t(F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]) * us);
     snb += F.sn.size(); rowsb += F.rows.size(); fwdb += F.fwd_sn.size();
   }
   fwd_ptr[V] = uint32_t(fwdb);
@@ -583,6 +713,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     b->refine = b->cfg.refinement_sweeps;
   }
   b->sn_host = sn;
+  b->n_sub_plain = uint32_t(subs.size());
+  subs.insert(subs.end(), subs_grouped.begin(), subs_grouped.end());
   b->n_sub = uint32_t(subs.size());
   // the supernodal tree for the dependency-driven sweeps (global ids)
   std::vector<uint32_t> df_parent(NSN, kNoParent), df_nkids(NSN, 0), df_kid_ptr(NSN + 1, 0), df_kids;
@@ -654,7 +786,7 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   CU(b->df_flag.alloc(NSN, st)); CU(cudaMemsetAsync(b->df_flag.p, 0, NSN * 4, st));
   CU(b->df_queue.alloc(2, st)); CU(cudaMemsetAsync(b->df_queue.p, 0, 8, st));
   CU(b->fwd_ptr.upload(fwd_ptr, st)); CU(b->fwd.upload(fwd, st));
-  CU(b->U.alloc(rows.size(), st));
+  CU(b->U.alloc(NU, st));
   if (have_a) { CU(b->a_ptr.upload(a_ptr, st)); CU(b->a_col.upload(a_col, st)); CU(b->a_val.upload(a_val, st)); }
   if (b->refine) { CU(b->R0.alloc(V, st)); CU(b->W.alloc(V, st)); }
   if (on_device) {
@@ -693,6 +825,114 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   d.grad = b->grad.p; d.grad_up = b->grad_up.p; d.lam = b->lam.p; d.fin_n = b->fin_n.p;
   d.in_contact = b->in_contact.p; d.in_contact_up = b->in_contact_up.p; d.ever = b->ever.p;
   d.red = b->red.p; d.prm = b->prm.p; d.status = b->status.p;
+  // ---- garment groups: topology tables, lanes, interleaved values, work items
+  b->n_groups = uint32_t(gp.gmembers.size());
+  b->sn_grouped.assign(NSN, 0);
+  if (b->n_groups) {
+    std::vector<GsnDev> gsn;
+    std::vector<uint32_t> g_rows, g_fwd_ptr, g_fwd, g_kids;
+    std::vector<uint2> g_subs;
+    for (auto& T : gp.topos) {
+      const Factor& F = solvers[T.leader]->setup.factor;
+      const uint32_t ns = uint32_t(F.sn.size());
+      T.sn_off = uint32_t(gsn.size());
+      T.rows_base = uint32_t(g_rows.size());
+      T.row_base = uint32_t(g_fwd_ptr.size());
+      T.fwd_base = uint32_t(g_fwd.size());
+      T.sub_base = uint32_t(g_subs.size());
+      std::vector<std::vector<uint32_t>> kids(ns);
+      for (uint32_t q = 0; q < ns; ++q)
+        if (F.sn[q].parent != UINT32_MAX) kids[F.sn[q].parent].push_back(q);
+      uint64_t goff = 0;
+      for (uint32_t q = 0; q < ns; ++q) {
+        const Supernode& X = F.sn[q];
+        GsnDev g{};
+        g.first = X.first; g.ncols = X.ncols; g.nrows = X.nrows;
+        g.rows_off = T.rows_base + X.rows_off;
+        g.u_local = X.rows_off;
+        g.parent = X.parent == UINT32_MAX ? kGNone : X.parent;
+        g.kid_off = uint32_t(g_kids.size());
+        g.nkids = uint32_t(kids[q].size());
+        g_kids.insert(g_kids.end(), kids[q].begin(), kids[q].end());
+        g.g_off = goff;
+        if (T.taken[q]) goff += uint64_t(X.ncols) * (X.ncols + 1) / 2 + uint64_t(X.nrows) * X.ncols;
+        gsn.push_back(g);
+      }
+      g_rows.insert(g_rows.end(), F.rows.begin(), F.rows.end());
+      for (uint32_t r = 0; r <= F.n; ++r) g_fwd_ptr.push_back(T.fwd_base + F.fwd_ptr[r]);
+      for (size_t q = 0; q < F.fwd_sn.size(); ++q) g_fwd.push_back(F.sn[F.fwd_sn[q]].rows_off + F.fwd_pos[q]);
+      for (size_t q = 0; q < F.sub_first.size(); ++q)
+        g_subs.push_back(make_uint2(T.sn_off + F.sub_first[q], T.sn_off + F.sub_last[q]));
+    }
+    const uint32_t NG = b->n_groups;
+    std::vector<GroupDev> grp(NG);
+    std::vector<uint32_t> gl_vbase(kGroupLanes * NG, 0), gl_snbase(kGroupLanes * NG, 0), gl_inst(kGroupLanes * NG, 0);
+    std::vector<uint2> pack, items_fwd, items_bwd;
+    uint64_t gbase = 0;
+    struct TopItem { uint32_t depth, q, g; };
+    std::vector<TopItem> tops;
+    for (uint32_t g = 0; g < NG; ++g) {
+      const auto& T = gp.topos[gp.gtopo[g]];
+      const auto& mem = gp.gmembers[g];
+      grp[g] = GroupDev{T.sn_off, uint32_t(mem.size()), gbase, uint32_t(g_ubase[g]), T.row_base};
+      gbase += T.entries;
+      for (uint32_t l = 0; l < mem.size(); ++l) {
+        const uint32_t k = mem[l];
+        gl_vbase[kGroupLanes * g + l] = uint32_t(vb[k]);
+        gl_snbase[kGroupLanes * g + l] = hi[k].sn_base;
+        gl_inst[kGroupLanes * g + l] = k;
+        for (uint32_t q = 0; q < T.taken.size(); ++q)
+          if (T.taken[q]) b->sn_grouped[hi[k].sn_base + q] = 1;
+      }
+      for (uint32_t q = 0; q < T.taken.size(); ++q) {
+        if (!T.taken[q]) continue;
+        pack.push_back(make_uint2(g, T.sn_off + q));
+        if (!T.insub[q]) tops.push_back(TopItem{T.depth[q], q, g});
+      }
+      const uint32_t nsub = uint32_t(solvers[T.leader]->setup.factor.sub_first.size());
+      for (uint32_t i = 0; i < nsub; ++i) items_fwd.push_back(make_uint2(g, (T.sub_base + i) << 1));
+    }
+    // forward: the subtrees, then the supernodes above them deepest first;
+    // backward: those shallowest first, then the subtrees. Within a depth the
+    // same supernode of every group is adjacent (its row indices are shared).
+    std::stable_sort(tops.begin(), tops.end(), [](const TopItem& a, const TopItem& c) {
+      return a.depth != c.depth ? a.depth > c.depth : a.q != c.q ? a.q < c.q : a.g < c.g;
+    });
+    for (const TopItem& t : tops)
+      items_fwd.push_back(make_uint2(t.g, ((gp.topos[gp.gtopo[t.g]].sn_off + t.q) << 1) | 1u));
+    for (size_t i = tops.size(); i-- > 0;)
+      items_bwd.push_back(make_uint2(tops[i].g, ((gp.topos[gp.gtopo[tops[i].g]].sn_off + tops[i].q) << 1) | 1u));
+    for (const uint2& it : items_fwd)
+      if ((it.y & 1u) == 0) items_bwd.push_back(it);
+    b->n_gitems_fwd = uint32_t(items_fwd.size());
+    b->n_gitems_bwd = uint32_t(items_bwd.size());
+    b->n_gpack = uint32_t(pack.size());
+    CU(b->grp.upload(grp, st)); CU(b->gsn.upload(gsn, st));
+    CU(b->g_rows.upload(g_rows, st)); CU(b->g_fwd_ptr.upload(g_fwd_ptr, st)); CU(b->g_kids.upload(g_kids, st));
+    CU(b->g_fwd.upload(g_fwd, st));
+    CU(b->g_subs.upload(g_subs, st));
+    CU(b->gl_vbase.upload(gl_vbase, st)); CU(b->gl_snbase.upload(gl_snbase, st)); CU(b->gl_inst.upload(gl_inst, st));
+    CU(b->g_items_fwd.upload(items_fwd, st)); CU(b->g_items_bwd.upload(items_bwd, st));
+    CU(b->g_pack.upload(pack, st));
+    CU(b->g_queue.alloc(2, st)); CU(cudaMemsetAsync(b->g_queue.p, 0, 8, st));
+    CU(b->g_vals.alloc(gbase * kGroupLanes, st));
+    d.grp = b->grp.p; d.gsn = b->gsn.p; d.g_rows = b->g_rows.p; d.g_fwd_ptr = b->g_fwd_ptr.p; d.g_fwd = b->g_fwd.p;
+    d.g_kids = b->g_kids.p; d.g_subs = b->g_subs.p; d.gl_vbase = b->gl_vbase.p; d.gl_snbase = b->gl_snbase.p;
+    d.gl_inst = b->gl_inst.p; d.g_vals = b->g_vals.p; d.g_items_fwd = b->g_items_fwd.p;
+    d.g_items_bwd = b->g_items_bwd.p; d.g_queue = b->g_queue.p;
+    // the groups' factor values, interleaved from the per-garment regions
+    if (!pack.empty()) k_gpack<<<uint32_t(pack.size()), 256, 0, st>>>(d, b->g_vals.p, b->g_pack.p);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(st));
+    b->g_bytes = gbase * kGroupLanes * 4 + gsn.size() * sizeof(GsnDev) + (g_rows.size() + g_fwd_ptr.size() +
+                 g_fwd.size() + g_kids.size()) * 4 + (items_fwd.size() + items_bwd.size() + pack.size()) * 8;
+    b->device_bytes += b->g_bytes;
+    b->g_pack.reset();
+    b->sweep_mode = 2;
+    std::vector<uint32_t> items2 = schedule_levels(b, b->warp_limit);
+    CU(upload_schedule(b, items2, st));
+    CU(cudaStreamSynchronize(st));
+  }
   b->dev_w = d;
   b->dev_w.Y = b->W.p;
   return VISTIO_OK;
@@ -758,6 +998,21 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
 // Forward then backward sweep, level by level over the whole batch, in place
 // on dv.Y (right-hand side in, solution out). Returns the launches.
 uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
+  if (b->sweep_mode == 2 && b->n_groups) {
+    // the groups' tree bottoms forward, everything above them (and the
+    // ungrouped garments) both ways, then the groups' tree bottoms backward
+    const uint32_t gf = std::min((b->n_gitems_fwd + kGWarps - 1) / kGWarps, b->ctx->gsweep_blocks);
+    const uint32_t gb = std::min((b->n_gitems_bwd + kGWarps - 1) / kGWarps, b->ctx->gsweep_blocks);
+    uint32_t n = 0;
+    if (gf) { k_gsweep<0><<<gf, kGThreads, kGSmem, st>>>(dv, b->n_gitems_fwd); ++n; }
+    if (b->n_units_fwd + b->n_units) {
+      const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks);
+      k_sweep<<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
+      ++n;
+    }
+    if (gb) { k_gsweep<1><<<gb, kGThreads, kGSmem, st>>>(dv, b->n_gitems_bwd); ++n; }
+    return n;
+  }
   if (b->sweep_mode == 1 && b->n_units) {
     const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks);
     k_sweep<<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
@@ -990,11 +1245,15 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   CU(cudaFuncSetAttribute(k_subtree<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_subtree<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_gsweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+  CU(cudaFuncSetAttribute(k_gsweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
   {
     int per_sm = 0, sms = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep, kSolveThreads, kSolveSmem));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     c->sweep_blocks = uint32_t(std::max(1, per_sm) * std::max(1, sms));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gsweep<0>, kGThreads, kGSmem));
+    c->gsweep_blocks = uint32_t(std::max(1, per_sm) * std::max(1, sms));
   }
   *out = c.release();
   return VISTIO_OK;
@@ -1427,7 +1686,11 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
   CU(cudaEventCreate(&e1));
   float best = 0.f;
   uint32_t best_limit = b->warp_limit, best_mode = b->sweep_mode;
-  for (int c = 0; c < 14; ++c) {
+  for (int c = 0; c < 21; ++c) {
+    if (c >= 14 && !b->n_groups) {  // no garment groups: no grouped candidates
+      if (candidate_ms) candidate_ms[c] = -1.f;
+      continue;
+    }
     b->sweep_mode = uint32_t(c / 7);
     std::vector<uint32_t> items = schedule_levels(b, kTuneLimits[c % 7]);
     CU(upload_schedule(b, items, st));
@@ -1469,8 +1732,14 @@ vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit) {
 
 vistio_status vistio_batch_set_sweep_mode(vistio_batch* b, uint32_t mode) {
   if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
-  if (mode > 1) return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "sweep mode must be 0 or 1");
+  if (mode > 2) return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "sweep mode must be 0, 1 or 2");
+  if (mode == 2 && !b->n_groups)
+    return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "sweep mode 2 needs garment groups (none in this batch)");
+  vistio_ctx* ctx = b->ctx;
   b->sweep_mode = mode;
+  std::vector<uint32_t> items = schedule_levels(b, b->warp_limit);  // mode 2 leaves the groups' supernodes out
+  CU(upload_schedule(b, items, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
   return drop_graphs(b);
 }
 
