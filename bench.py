@@ -55,6 +55,9 @@ def parse():
                     help="served stream: factorize each set-up on the GPU at cohort start (host threads otherwise)")
     ap.add_argument("--serve-seconds", type=float, default=1.0,
                     help="arrival window of the served-stream measurement (0 skips it)")
+    ap.add_argument("--sustain-rate", type=float, default=16.0,
+                    help="arrival rate (req/s) of the second served stream, one that one GPU sustains")
+    ap.add_argument("--sustain-seconds", type=float, default=10.0, help="its arrival window")
     ap.add_argument("--refine", type=int, default=None,
                     help="FP64 refinement sweeps of the global solve (default: the solver's default)")
     return ap.parse_args()
@@ -289,14 +292,10 @@ def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
     return out
 
 
-def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factorization=False):
-    """The served drape stream: Poisson arrivals at `rate` req/s during
-    `window_s` seconds, half sphere drapes (the sphere-drape geometry at the
-    drawn side, IPC d_hat 1e-3, kappa 1e4, AL <= 5, 15 iterations) and half
-    hanging sheets (10 iterations); grid side log-uniform in [20, 192],
-    materials as in the batched workload, 300 steps each, 120 GB admission
-    budget. Latency runs from a request's arrival to its completion."""
-    from vistio_b200 import api, scenarios
+def stream_arrivals(window_s, rate=200.0, seed=20261203):
+    """Poisson arrivals at `rate` req/s during `window_s` seconds: half sphere
+    drapes, half hanging sheets, grid side log-uniform in [20, 192], materials
+    as in the batched workload."""
     rng = np.random.default_rng(seed)
     t, arrivals = 0.0, []
     while True:
@@ -308,10 +307,29 @@ def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factori
                              stretch=float(math.exp(rng.uniform(math.log(2e2), math.log(5e3)))),
                              bending=float(math.exp(rng.uniform(math.log(1e-5), math.log(1e-3)))),
                              density=float(rng.uniform(0.08, 0.30) * 1000.0)))
-    sphere = api.Contact(has_ground=True, ground_height=-0.3, has_sphere=True, sphere_center=(0.0, 0.0, 0.0),
-                         sphere_radius=0.3, kappa=1e4)
-    cfg_s = api.drape_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=1e-3, barrier_kappa=1e4)
-    cfg_p = api.drape_config(max_iterations=ITERS)
+    return arrivals
+
+
+def _request(a):
+    """(mesh, config, set-up, contact or None) of one arrival: sphere drapes at
+    the drawn side (IPC d_hat 1e-3, kappa 1e4, AL <= 5, 15 iterations), hanging
+    sheets with 10 iterations."""
+    from vistio_b200 import api, scenarios
+    setup = api.SetupDesc(stiffness=a["stretch"], bend_stiffness=a["bending"], density_gsm=a["density"])
+    if a["sphere"]:
+        sphere = api.Contact(has_ground=True, ground_height=-0.3, has_sphere=True, sphere_center=(0.0, 0.0, 0.0),
+                             sphere_radius=0.3, kappa=1e4)
+        cfg = api.drape_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=1e-3, barrier_kappa=1e4)
+        return scenarios.sphere_drape(side=a["side"], length=1.5, height=0.5), cfg, setup, sphere
+    return scenarios.hanging_sheet(a["side"], 1.0), api.drape_config(max_iterations=ITERS), setup, None
+
+
+def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factorization=False):
+    """The served drape stream: the arrivals of stream_arrivals, 300 steps
+    each, 120 GB admission budget. Latency runs from a request's arrival to
+    its completion."""
+    from vistio_b200 import api
+    arrivals = stream_arrivals(window_s, rate, seed)
     srv = api.Server(hbm_budget_bytes=120 << 30, max_cohort=64, setup_threads=threads or (os.cpu_count() or 4),
                      steps_per_slice=10, cache_bytes=2 << 30, gpu_factorization=gpu_factorization)
     sym0 = api.symbolic_cache_info()
@@ -320,14 +338,11 @@ def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factori
     while k < len(arrivals):
         now = time.perf_counter() - t0
         while k < len(arrivals) and arrivals[k]["t"] <= now:
-            a = arrivals[k]
-            setup = api.SetupDesc(stiffness=a["stretch"], bend_stiffness=a["bending"], density_gsm=a["density"])
-            if a["sphere"]:
-                m = scenarios.sphere_drape(side=a["side"], length=1.5, height=0.5)
-                srv.submit(m, cfg_s, setup, 300, DT, contact=sphere, ipc=True)
+            m, cfg, setup, contact = _request(arrivals[k])
+            if contact is not None:
+                srv.submit(m, cfg, setup, 300, DT, contact=contact, ipc=True)
             else:
-                m = scenarios.hanging_sheet(a["side"], 1.0)
-                srv.submit(m, cfg_p, setup, 300, DT, pinned=m.pinned)
+                srv.submit(m, cfg, setup, 300, DT, pinned=m.pinned)
             k += 1
         srv.tick()
         time.sleep(0.0005)
@@ -345,6 +360,48 @@ def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factori
             "factorization": "GPU (cohort start)" if gpu_factorization else "host (set-up threads)",
             "symbolic_cache": {"hits": sym1["hits"] - sym0["hits"], "misses": sym1["misses"] - sym0["misses"]},
             "how": "Poisson arrivals at the stated rate during the window, then drained; each request 300 steps"}
+
+
+def batched_same_mix(window_s, rate=200.0, seed=20261203, threads=None):
+    """The served stream's requests run offline as two batches (the sphere
+    drapes, the hanging sheets), all present from the start, 300 steps each:
+    the batched rate on the same mix, device-timed with CUDA events."""
+    import torch
+    from vistio_b200 import api
+    arrivals = stream_arrivals(window_s, rate, seed)
+    total_ms, units = 0.0, 0
+    for sphere in (True, False):
+        reqs = [_request(a) for a in arrivals if a["sphere"] == sphere]
+        if not reqs:
+            continue
+
+        def make(r):
+            m, cfg, setup, _ = r
+            return api.ProjectiveDynamicsSolver().init_explicit(m, cfg, setup,
+                                                                pinned=None if sphere else m.pinned)
+
+        with cf.ThreadPoolExecutor(threads or (os.cpu_count() or 4)) as ex:
+            solvers = list(ex.map(make, reqs))
+        batch = api.Batch(solvers)
+        batch.tune()
+        contact = reqs[0][3]
+        batch.step(DT, 1, contact=contact)
+        torch.cuda.synchronize()
+        stream = torch.cuda.ExternalStream(batch.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            batch.step(DT, 299, contact=contact)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1) * 300.0 / 299.0
+        units += 300 * len(reqs)
+        batch.close()
+        for sv in solvers:
+            sv.close()
+    return {"value": units / (total_ms / 1e3), "unit": UNIT, "requests": len(arrivals),
+            "how": "the same requests as two batches (sphere drapes with IPC, hanging sheets), 300 steps each, "
+                   "one batch after the other, CUDA events"}
 
 
 # ------------------------------------------------- single-garment configs
@@ -614,8 +671,10 @@ def main():
         return
     if args.serve_only:
         if rank == 0:
-            print(json.dumps({"serving": served_stream(args.serve_seconds,
-                                                       gpu_factorization=args.serve_gpu_factorization)}), flush=True)
+            srv = served_stream(args.serve_seconds, gpu_factorization=args.serve_gpu_factorization)
+            srv["batched_same_mix"] = batched_same_mix(args.serve_seconds)
+            srv["served_over_batched_same_mix"] = srv["throughput_instance_steps_per_s"] / srv["batched_same_mix"]["value"]
+            print(json.dumps({"serving": srv}), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -834,6 +893,13 @@ def main():
             out["configs"][name]["gpu_over_cpu"] = out["configs"][name]["gpu"]["value"] / cpu["value"]
         if args.serve_seconds > 0:
             out["serving"] = served_stream(args.serve_seconds, gpu_factorization=args.serve_gpu_factorization)
+            mix = batched_same_mix(args.serve_seconds)
+            out["serving"]["batched_same_mix"] = mix
+            out["serving"]["served_over_batched_same_mix"] = \
+                out["serving"]["throughput_instance_steps_per_s"] / mix["value"]
+            # a stream at a rate one GPU sustains, beside the specified burst
+            out["serving_sustained"] = served_stream(args.sustain_seconds, rate=args.sustain_rate, seed=20261204,
+                                                     gpu_factorization=args.serve_gpu_factorization)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
