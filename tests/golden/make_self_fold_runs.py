@@ -22,7 +22,14 @@ Output: self_fold_<name>.npz with the FP64 positions (float32) after steps
 100, 200 and 300, and per step the max |x_ref32 - x_fp64| (the reference's
 own FP32 spread) and the FP64 run's active-contact count.
 
+With --literal N it instead steps the reference's literal wiring of the
+configuration for N steps and prints each step's lowest point, highest
+point, largest displacement and active contacts (no fixture): the system
+matrix assembled with dt = 1/60 while the steps use 1/120, and d_hat = 5e-4
+passed as barrier_d_hat (a squared distance), thickness 1.5 d_hat.
+
 Usage: python tests/golden/make_self_fold_runs.py [drop|near ...]
+       python tests/golden/make_self_fold_runs.py --literal N [precision]
 """
 from __future__ import annotations
 
@@ -94,6 +101,33 @@ def run(name):
     print("wrote", out)
 
 
+def literal(nsteps, precision=1):
+    mesh = scenarios.self_fold(40, 400, 0.2, 2.0, lowest=0.5)
+    prm = O.init_params(model=O.MODEL_ORTHO, stiffness=1e3, warp=1e3, weft=6e2, bend_stiffness=1e-4,
+                        density_gsm=150.0, matrix_dt=1.0 / 60.0)
+    cfg = O.default_config(max_iterations=10, al_max_iterations=5, barrier_d_hat=D_HAT)
+    sim = O.OracleSim(mesh, prm, cfg, precision=precision)
+    sim.set_ground(1, 0.0)
+    c = O.Contact()
+    c.has_ground, c.ground_height = 1, 0.0
+    c.self_collision, c.bvh_faithful = 1, 0
+    c.thickness = 1.5 * D_HAT
+    c.kappa = float(O.lib().orc_estimate_kappa(0.0, float(sim.masses().mean()), 9.81, D_HAT))
+    prev = sim.state()[0]
+    for n in range(1, nsteps + 1):
+        r = sim.step_ipc(DT, c)
+        p = sim.state()[0]
+        print(f"literal step {n}: lowest {p[:, 1].min():.4f} highest {p[:, 1].max():.4f} "
+              f"max displacement {np.abs(p - prev).max():.4f} active {r.active_contacts} finite {np.isfinite(p).all()}",
+              flush=True)
+        if not np.isfinite(p).all():
+            break
+        prev = p
+
+
 if __name__ == "__main__":
-    for nm in sys.argv[1:] or list(LOWEST):
-        run(nm)
+    if sys.argv[1:2] == ["--literal"]:
+        literal(int(sys.argv[2]), int(sys.argv[3]) if len(sys.argv) > 3 else 1)
+    else:
+        for nm in sys.argv[1:] or list(LOWEST):
+            run(nm)
