@@ -292,6 +292,18 @@ vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, ui
  * garment groups, else kind 1, with the limit 6144. Captured step graphs are
  * rebuilt on the next step. Synchronises the batch's stream. */
 vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms);
+/* Autotunes the shapes of the local steps on this batch (no reference
+ * counterpart): triangles per thread of the membrane step (1: 256 threads
+ * per chunk of 256 triangles; 2: 128 threads, both triangles' loads issued
+ * first) and hinges per thread of the bending step (the same two shapes),
+ * each timed over five launches; the faster of each pair is kept. The shapes
+ * compute the same arithmetic per element: results are bit-identical.
+ * candidate_ms (4 entries, may be NULL): membrane 1, 2, bending 1, 2. Without
+ * tuning: 2 triangles and 1 hinge per thread. Synchronises the stream. */
+vistio_status vistio_batch_tune_local(vistio_batch* b, uint32_t* tri_per_thread, uint32_t* hinge_per_thread,
+                                      float* candidate_ms);
+/* Sets the local steps' elements per thread directly (1 or 2 each). */
+vistio_status vistio_batch_set_local_shape(vistio_batch* b, uint32_t tri_per_thread, uint32_t hinge_per_thread);
 /* Sets the warp-item limit directly (any value; see vistio_batch_tune). */
 vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit);
 /* Sets the sweep kind (0, 1, or 2 for a batch with garment groups; see

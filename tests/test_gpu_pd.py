@@ -347,6 +347,26 @@ def test_grouped_sweeps_bit_identical_to_dataflow_and_to_solo(refine):
         assert np.array_equal(solo[k].state()[0], res["grouped"][k]), (k, GROUPED_SIDES[k])
 
 
+def test_local_step_shapes_bit_identical_and_tuned():
+    """The membrane and bending steps with one or two elements per thread give
+    bit-identical trajectories; the autotuner times both shapes of each."""
+    cfg = api.drape_config(max_iterations=6)
+    out = {}
+    for shape in ((1, 1), (2, 2), (1, 2), (2, 1)):
+        batch = api.Batch(grouped_batch_solvers(cfg, [12, 31, 9, 47, 20]))
+        batch.set_local_shape(*shape)
+        batch.step(DT, 3)
+        out[shape] = [batch.state(k)[0] for k in range(5)]
+        batch.close()
+    for shape in out:
+        for a, b in zip(out[shape], out[(2, 1)]):
+            assert np.array_equal(a, b), shape
+    batch = api.Batch(grouped_batch_solvers(cfg, [12, 31, 9, 47, 20]))
+    t = batch.tune()
+    assert t["triangles_per_thread"] in (1, 2) and t["hinges_per_thread"] in (1, 2)
+    assert all(v > 0 for m in t["local_ms"].values() for v in m.values())
+
+
 def test_grouped_kind_needs_groups_and_tunes():
     """The grouped kind is refused for a batch without garment groups; with
     groups the autotuner times it beside the other two kinds."""

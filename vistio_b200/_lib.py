@@ -148,6 +148,8 @@ SIGNATURES = {
     "vistio_batch_phase_bytes": (C.c_int, [_vp, C.c_int32, _u64p]),
     "vistio_diag_wait_timeout": (C.c_int, [_vp, C.c_uint32]),
     "vistio_batch_tune": (C.c_int, [_vp, _u32p, _fp]),
+    "vistio_batch_tune_local": (C.c_int, [_vp, _u32p, _u32p, _fp]),
+    "vistio_batch_set_local_shape": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
     "vistio_batch_set_warp_limit": (C.c_int, [_vp, C.c_uint32]),
     "vistio_batch_set_sweep_mode": (C.c_int, [_vp, C.c_uint32]),
     "vistio_batch_get_sweep_mode": (C.c_int, [_vp, _u32p, _u32p]),

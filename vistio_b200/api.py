@@ -456,9 +456,20 @@ class Batch:
         chosen = C.c_uint32()
         ms = (C.c_float * 21)()
         L.check(L.lib().vistio_batch_tune(self.h, C.byref(chosen), ms), self.ctx.h)
+        tri, hinge = C.c_uint32(), C.c_uint32()
+        lms = (C.c_float * 4)()
+        L.check(L.lib().vistio_batch_tune_local(self.h, C.byref(tri), C.byref(hinge), lms), self.ctx.h)
         return {"sweep_mode": self.sweep_mode()[0], "warp_item_limit": chosen.value,
                 "sweep_ms": {mode: {str(lim): float(ms[7 * m + i]) for i, lim in enumerate(self.TUNE_LIMITS)}
-                             for m, mode in enumerate(self.SWEEP_MODES) if ms[7 * m] >= 0}}
+                             for m, mode in enumerate(self.SWEEP_MODES) if ms[7 * m] >= 0},
+                "triangles_per_thread": tri.value, "hinges_per_thread": hinge.value,
+                "local_ms": {"membrane": {"1": float(lms[0]), "2": float(lms[1])},
+                             "bending": {"1": float(lms[2]), "2": float(lms[3])}}}
+
+    def set_local_shape(self, triangles_per_thread: int, hinges_per_thread: int):
+        """Elements per thread of the membrane and bending steps (1 or 2 each)."""
+        L.check(L.lib().vistio_batch_set_local_shape(self.h, int(triangles_per_thread), int(hinges_per_thread)),
+                self.ctx.h)
 
     def set_warp_limit(self, limit: int):
         L.check(L.lib().vistio_batch_set_warp_limit(self.h, int(limit)), self.ctx.h)

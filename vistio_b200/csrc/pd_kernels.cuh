@@ -377,6 +377,18 @@ __global__ void __launch_bounds__(kTriThreads, 8) k_tri(BatchDev B) {
   if (two) tri_project(B, I, t1, dmb, wb, qb0, qb1, qb2);
 }
 
+// The same membrane step with one triangle per thread (a chunk of up to 256
+// triangles on 256 threads, four blocks per SM): the autotuner's other shape.
+__global__ void __launch_bounds__(256, 4) k_tri1(BatchDev B) {
+  int4 ch = B.tri_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  const uint32_t t = uint32_t(ch.y) + threadIdx.x;
+  const InstDev I = B.inst[ch.x];
+  const uint4 a = B.tri_idx[t];
+  tri_project(B, I, t, B.tri_dm[t], B.tri_w[t], B.pos[a.x], B.pos[a.y], B.pos[a.z]);
+}
+
 // Rotation of v = p - centre about `axis` by an angle minus v itself:
 // (axis (axis . v) - v)(1 - cos) + (axis x v) sin (bending.rs:231-239), given
 // sin and 1 - cos. The two wings turn by +half and -half: the same 1 - cos and
@@ -386,19 +398,9 @@ __device__ __forceinline__ float3 rot_delta(float3 v, float3 axis, float s, floa
   return (axis * dt - v) * omc + cross3(axis, v) * s;
 }
 
-// Local bending step: per hinge, w * s . (target - x); only the wings move
+// Local bending step of one hinge: w * s . (target - x); only the wings move
 // (bending.rs:182-227, discrete_shells.rs:285-337).
-__global__ void __launch_bounds__(256) k_hinge(BatchDev B) {
-  int4 ch = B.hinge_chunks[blockIdx.x];
-  if ((int)threadIdx.x >= ch.z) return;
-  if (B.prm->ipc && B.red[ch.x].al_done) return;
-  uint32_t h = uint32_t(ch.y) + threadIdx.x;
-  uint4 id = B.hinge_idx[h];
-  // the wings' stencil weights; a garment whose stencils are all (-1, -1, 1, 1)
-  // skips their load (16 B per hinge), with the same products
-  const float4 st = B.inst[ch.x].unit_stencils ? make_float4(-1.f, -1.f, 1.f, 1.f) : B.hinge_st[h];
-  float2 wr = B.hinge_wr[h];
-  float3 p0 = f3(B.pos[id.x]), p1 = f3(B.pos[id.y]), pa = f3(B.pos[id.z]), pb = f3(B.pos[id.w]);
+__device__ __forceinline__ float4 hinge_project(float4 st, float2 wr, float3 p0, float3 p1, float3 pa, float3 pb) {
   float3 out = make_float3(0.f, 0.f, 0.f);
   float3 e = p1 - p0;
   float el = len3(e);
@@ -425,7 +427,41 @@ __global__ void __launch_bounds__(256) k_hinge(BatchDev B) {
       out = (da * st.z + db * st.w) * wr.x;
     }
   }
-  B.hinge_out[h] = make_float4(out.x, out.y, out.z, 0.f);
+  return make_float4(out.x, out.y, out.z, 0.f);
+}
+
+// One hinge per thread over a chunk of up to 256 hinges. A garment whose
+// stencils are all (-1, -1, 1, 1) skips their load (16 B per hinge), with the
+// same products.
+__global__ void __launch_bounds__(256) k_hinge(BatchDev B) {
+  int4 ch = B.hinge_chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  uint32_t h = uint32_t(ch.y) + threadIdx.x;
+  uint4 id = B.hinge_idx[h];
+  const float4 st = B.inst[ch.x].unit_stencils ? make_float4(-1.f, -1.f, 1.f, 1.f) : B.hinge_st[h];
+  float2 wr = B.hinge_wr[h];
+  B.hinge_out[h] = hinge_project(st, wr, f3(B.pos[id.x]), f3(B.pos[id.y]), f3(B.pos[id.z]), f3(B.pos[id.w]));
+}
+
+// Two hinges per thread (128 threads over a chunk of up to 256), both hinges'
+// loads issued before either projection: the autotuner's other shape.
+__global__ void __launch_bounds__(128, 8) k_hinge2(BatchDev B) {
+  int4 ch = B.hinge_chunks[blockIdx.x];
+  const uint32_t i0 = threadIdx.x, i1 = threadIdx.x + 128;
+  if ((int)i0 >= ch.z) return;
+  if (B.prm->ipc && B.red[ch.x].al_done) return;
+  const bool two = (int)i1 < ch.z;
+  const uint32_t h0 = uint32_t(ch.y) + i0, h1 = two ? uint32_t(ch.y) + i1 : h0;
+  const bool unit = B.inst[ch.x].unit_stencils != 0;
+  const uint4 a = B.hinge_idx[h0], b = B.hinge_idx[h1];
+  const float4 sa = unit ? make_float4(-1.f, -1.f, 1.f, 1.f) : B.hinge_st[h0];
+  const float4 sb = unit ? make_float4(-1.f, -1.f, 1.f, 1.f) : B.hinge_st[h1];
+  const float2 wa = B.hinge_wr[h0], wb = B.hinge_wr[h1];
+  const float3 a0 = f3(B.pos[a.x]), a1 = f3(B.pos[a.y]), a2 = f3(B.pos[a.z]), a3 = f3(B.pos[a.w]);
+  const float3 b0 = f3(B.pos[b.x]), b1 = f3(B.pos[b.y]), b2 = f3(B.pos[b.z]), b3 = f3(B.pos[b.w]);
+  B.hinge_out[h0] = hinge_project(sa, wa, a0, a1, a2, a3);
+  if (two) B.hinge_out[h1] = hinge_project(sb, wb, b0, b1, b2, b3);
 }
 
 // Residual gather: r_i = m_i (pred_i / dt^2 - x_i / h^2) + sum of element

@@ -162,6 +162,7 @@ struct vistio_batch {
   std::vector<std::pair<uint32_t, uint32_t>> top;  // (level, supernode) of every top-level supernode
   std::vector<SnDev> sn_host;                       // supernode table, for re-scheduling
   uint32_t warp_limit = kWarpItemLimit;             // s (s + m) limit of a warp item
+  uint32_t tri_per = 2, hinge_per = 1;              // elements per thread of k_tri / k_hinge (autotuned)
   float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
   // sweeps: 0 = one launch per level (k_level), 1 = dependency-driven (k_sweep),
   // 2 = garment groups' tree bottoms by k_gsweep, the rest by k_sweep
@@ -1053,10 +1054,22 @@ uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update, uint32_t 
   return n;
 }
 
+// The local steps in the shapes the autotuner chose (elements per thread).
+void launch_membrane(vistio_batch* b, cudaStream_t st) {
+  if (!b->n_tri_chunks) return;
+  if (b->tri_per == 2) k_tri<<<b->n_tri_chunks, kTriThreads, 0, st>>>(b->dev);
+  else k_tri1<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev);
+}
+void launch_bending(vistio_batch* b, cudaStream_t st) {
+  if (!b->n_hinge_chunks) return;
+  if (b->hinge_per == 2) k_hinge2<<<b->n_hinge_chunks, kElemThreads / 2, 0, st>>>(b->dev);
+  else k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev);
+}
+
 uint32_t launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update, uint32_t refine) {
   uint32_t n = 1;
-  if (b->n_tri_chunks) { k_tri<<<b->n_tri_chunks, kTriThreads, 0, st>>>(b->dev); ++n; }
-  if (b->n_hinge_chunks) { k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
+  if (b->n_tri_chunks) { launch_membrane(b, st); ++n; }
+  if (b->n_hinge_chunks) { launch_bending(b, st); ++n; }
   k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, refine > 0);
   return n + launch_solve(b, st, do_update, refine);
 }
@@ -1721,6 +1734,50 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
   return VISTIO_OK;
 }
 
+vistio_status vistio_batch_tune_local(vistio_batch* b, uint32_t* tri_per_thread, uint32_t* hinge_per_thread,
+                                      float* candidate_ms) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  vistio_ctx* ctx = b->ctx;
+  cudaStream_t st = ctx->stream;
+  StepParams p{};
+  p.dt = 1.f / 60.f;
+  CU(cudaMemcpyAsync(b->prm.p, &p, sizeof(p), cudaMemcpyHostToDevice, st));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  float ms[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int c = 0; c < 4; ++c) {
+    const uint32_t per = 1u + uint32_t(c & 1);
+    if (c < 2) b->tri_per = per; else b->hinge_per = per;
+    for (int r = 0; r < 6; ++r) {  // one warm-up, five timed
+      if (r == 1) CU(cudaEventRecord(e0, st));
+      if (c < 2) launch_membrane(b, st); else launch_bending(b, st);
+    }
+    CU(cudaEventRecord(e1, st));
+    CU(cudaEventSynchronize(e1));
+    CU(cudaEventElapsedTime(&ms[c], e0, e1));
+    ms[c] /= 5.f;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CU(cudaGetLastError());
+  b->tri_per = ms[1] <= ms[0] ? 2u : 1u;
+  b->hinge_per = ms[3] < ms[2] ? 2u : 1u;
+  if (tri_per_thread) *tri_per_thread = b->tri_per;
+  if (hinge_per_thread) *hinge_per_thread = b->hinge_per;
+  if (candidate_ms) std::memcpy(candidate_ms, ms, sizeof(ms));
+  return drop_graphs(b);
+}
+
+vistio_status vistio_batch_set_local_shape(vistio_batch* b, uint32_t tri_per_thread, uint32_t hinge_per_thread) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  if (tri_per_thread < 1 || tri_per_thread > 2 || hinge_per_thread < 1 || hinge_per_thread > 2)
+    return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "elements per thread must be 1 or 2");
+  b->tri_per = tri_per_thread;
+  b->hinge_per = hinge_per_thread;
+  return drop_graphs(b);
+}
+
 vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit) {
   if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
   vistio_ctx* ctx = b->ctx;
@@ -1756,8 +1813,8 @@ vistio_status vistio_batch_launch_phase(vistio_batch* b, int32_t phase) {
   cudaStream_t st = ctx->stream;
   switch (phase) {
     case 0: k_predict<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
-    case 1: if (b->n_tri_chunks) k_tri<<<b->n_tri_chunks, kTriThreads, 0, st>>>(b->dev); break;
-    case 2: if (b->n_hinge_chunks) k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev); break;
+    case 1: launch_membrane(b, st); break;
+    case 2: launch_bending(b, st); break;
     case 3: k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, b->refine > 0); break;
     case 4: launch_solve(b, st, 0, 0); break;
     case 5: k_finalize<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); break;
