@@ -529,12 +529,37 @@ __device__ __forceinline__ bool excluded(const SelfContactView& S, uint32_t i, u
 
 // Contributions are summed in FP64: at a vertex between two layers they are
 // large and of opposite sign, and an FP32 sum would keep mostly rounding.
-__device__ __forceinline__ void add_grad(double4* G, uint32_t v, V3d<double> g, double bg) {
-  double* p = reinterpret_cast<double*>(G + v);
-  atomicAdd(p + 0, bg * g.x);
-  atomicAdd(p + 1, bg * g.y);
-  atomicAdd(p + 2, bg * g.z);
-}
+// A candidate pair touches at most six vertices (its two triangles'); the
+// contributions of its 15 tests are first summed per vertex slot (slots 0-2:
+// triangle a's corners, 3-5: triangle b's) in this thread's column of a
+// shared-memory array, then added to the accumulator with at most 18 atomics
+// instead of up to 180. The column of thread t holds value i at [i][t]:
+// consecutive threads, consecutive doubles.
+constexpr int kGradThreads = 256;
+struct PairGrad {
+  double* g;  // this thread's column: value i (slot i / 3, component i % 3) at g[i * kGradThreads]
+  __device__ __forceinline__ void clear() const {
+#pragma unroll
+    for (int i = 0; i < 18; ++i) g[i * kGradThreads] = 0.0;
+  }
+  __device__ __forceinline__ void add(int slot, V3d<double> v, double bg) const {
+    double* q = g + 3 * slot * kGradThreads;
+    q[0] += bg * v.x;
+    q[kGradThreads] += bg * v.y;
+    q[2 * kGradThreads] += bg * v.z;
+  }
+  __device__ __forceinline__ void flush(double4* G, const uint32_t* av, const uint32_t* bv) const {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      const double x = g[(3 * i) * kGradThreads], y = g[(3 * i + 1) * kGradThreads], z = g[(3 * i + 2) * kGradThreads];
+      if (x == 0.0 && y == 0.0 && z == 0.0) continue;
+      double* p = reinterpret_cast<double*>(G + (i < 3 ? av[i] : bv[i - 3]));
+      atomicAdd(p + 0, x);
+      atomicAdd(p + 1, y);
+      atomicAdd(p + 2, z);
+    }
+  }
+};
 
 // SelfCollisionSystem::detect_ipc_contacts (self_collision.rs:199-276) and
 // IpcContactSet::compute_barrier_gradient (ipc_response.rs:170-219), per
@@ -543,8 +568,9 @@ __device__ __forceinline__ void add_grad(double4* G, uint32_t v, V3d<double> g, 
 // FP64 (distance, distance gradient, barrier) and rounded once.
 // Compiled for four blocks per SM (64 registers, a few spills in the FP64
 // branch) instead of the two that 124 registers allow: contact batch of 64
-// sphere drapes 93 -> 86 ms per step.
-__global__ void __launch_bounds__(256, 4) k_self_grad(BatchDev B, SelfContactView S, int mode) {
+// sphere drapes 93 -> 86 ms per step (before the per-pair sums).
+__global__ void __launch_bounds__(kGradThreads, 4) k_self_grad(BatchDev B, SelfContactView S, int mode) {
+  __shared__ double acc_s[18 * kGradThreads];  // 36 KB: four blocks per SM
   const StepParams& P = *B.prm;
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   double4* G = B.gacc;
@@ -560,9 +586,12 @@ __global__ void __launch_bounds__(256, 4) k_self_grad(BatchDev B, SelfContactVie
     uint32_t av[3] = {A.x, A.y, A.z}, bv[3] = {Bt.x, Bt.y, Bt.z};
     uint32_t nact = 0;
     bool viol = false;
+    const PairGrad acc{acc_s + threadIdx.x};
+    acc.clear();
     for (int side = 0; side < 2; ++side) {
       const uint32_t* X = side == 0 ? av : bv;
       const uint32_t* Yt = side == 0 ? bv : av;
+      const int xs = side == 0 ? 0 : 3, ys = side == 0 ? 3 : 0;  // slots of X's and Yt's corners
       V3d<float> ta = ld3(B.pos, Yt[0]), tb = ld3(B.pos, Yt[1]), tc = ld3(B.pos, Yt[2]);
       for (int q = 0; q < 3; ++q) {
         uint32_t v = X[q];
@@ -580,14 +609,14 @@ __global__ void __launch_bounds__(256, 4) k_self_grad(BatchDev B, SelfContactVie
         double bg = th > 0.0 ? scaled_barrier_grad_thick64(d, dh, kap, th) : scaled_barrier_grad64(d, dh, kap);
         V3d<double> g[4];
         pt_grad<double>(p8, a8, b8, c8, g);
-        add_grad(G, v, g[0], bg); add_grad(G, Yt[0], g[1], bg); add_grad(G, Yt[1], g[2], bg); add_grad(G, Yt[2], g[3], bg);
+        acc.add(xs + q, g[0], bg); acc.add(ys + 0, g[1], bg); acc.add(ys + 1, g[2], bg); acc.add(ys + 2, g[3], bg);
       }
     }
-    uint32_t ae[3][2] = {{av[0], av[1]}, {av[1], av[2]}, {av[2], av[0]}};
-    uint32_t be[3][2] = {{bv[0], bv[1]}, {bv[1], bv[2]}, {bv[2], bv[0]}};
+    // edges (0,1), (1,2), (2,0) of each triangle, as corner slots
+    const int ea[3][2] = {{0, 1}, {1, 2}, {2, 0}};
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) {
-        uint32_t a0 = ae[i][0], a1 = ae[i][1], b0 = be[j][0], b1 = be[j][1];
+        uint32_t a0 = av[ea[i][0]], a1 = av[ea[i][1]], b0 = bv[ea[j][0]], b1 = bv[ea[j][1]];
         if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) continue;
         V3d<float> p0 = ld3(B.pos, a0), p1 = ld3(B.pos, a1), q0 = ld3(B.pos, b0), q1 = ld3(B.pos, b1);
         if (!(ee_d2<float>(p0, p1, q0, q1) < screen)) continue;
@@ -600,8 +629,10 @@ __global__ void __launch_bounds__(256, 4) k_self_grad(BatchDev B, SelfContactVie
         double bg = th > 0.0 ? scaled_barrier_grad_thick64(d, dh, kap, th) : scaled_barrier_grad64(d, dh, kap);
         V3d<double> g[4];
         ee_grad<double>(P0, P1, Q0, Q1, g);
-        add_grad(G, a0, g[0], bg); add_grad(G, a1, g[1], bg); add_grad(G, b0, g[2], bg); add_grad(G, b1, g[3], bg);
+        acc.add(ea[i][0], g[0], bg); acc.add(ea[i][1], g[1], bg);
+        acc.add(3 + ea[j][0], g[2], bg); acc.add(3 + ea[j][1], g[3], bg);
       }
+    if (nact) acc.flush(G, av, bv);
     if (mode == 1 && nact) {
       atomicAdd(&R.active, nact);
       if (viol) atomicMax(&R.maxviol_bits, __float_as_uint(1e-3f));
@@ -761,7 +792,7 @@ inline uint32_t launch_self_detect(const BatchDev& d, const SelfContactView& S, 
   k_scan_sums<<<1, kScanBlock, 0, st>>>(S.block_sums, S.scan_blocks, S.npairs);
   k_scan_add<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);
   k_self_write<<<n_tri_chunks, 256, 0, st>>>(d, S);
-  k_self_grad<<<4 * 148, 256, 0, st>>>(d, S, mode);
+  k_self_grad<<<4 * 148, kGradThreads, 0, st>>>(d, S, mode);
   return 8 + ns;
 }
 
