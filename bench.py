@@ -221,24 +221,30 @@ def reference_arm(args):
 
 
 # ----------------------------------------------------------- served stream
+D_HAT_IPC = 1e-3  # m, a distance: barrier_d_hat = D_HAT_IPC^2, self-contact thickness 1.5 D_HAT_IPC
+
+
 def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
     """Batched contact drapes: `n` sphere drapes with the batched workload's grid
-    sides and materials, each starting 5 mm above a sphere of radius 0.3 m (so
-    the barriers are active from the first steps), ground and sphere barriers
-    and self-collision (thickness 1.5 d_hat), d_hat 1e-3, kappa 1e4, AL <= 5,
-    15 PD iterations per AL pass; `steps` step_with_ipc steps timed with CUDA
-    events after `warmup`. With a `pool`, the first drape of each grid side is
-    also run by the oracle in FP64 over the same warmup + steps steps (the
-    error), and stepped alone on the GPU (the plain one-garment-per-launch
-    rate)."""
+    sides and materials, each starting 1 mm above a sphere of radius 0.3 m (so
+    the barriers are active from the first step), ground and sphere barriers
+    and self-collision, d_hat = 1e-3 m read as a distance (barrier_d_hat =
+    1e-6 m^2, self-contact thickness 1.5e-3 m; read as a squared distance, a
+    3.2 cm zone on a 1.2-9 cm mesh puts every non-adjacent neighbour in
+    contact and the sheets explode), kappa 1e4, AL <= 5, 15 PD iterations per
+    AL pass; `steps` step_with_ipc steps timed with CUDA events after
+    `warmup`. With a `pool`, the first drape of each grid side is also run by
+    the oracle in FP64 over the same warmup + steps steps (the error), and
+    stepped alone on the GPU (the plain one-garment-per-launch rate)."""
     from vistio_b200 import api, scenarios
     specs = workload(n, 0)
-    cfg = api.drape_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=1e-3, barrier_kappa=1e4)
+    dh2 = D_HAT_IPC * D_HAT_IPC
+    cfg = api.drape_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=dh2, barrier_kappa=1e4)
     contact = api.Contact(has_ground=True, ground_height=-0.3, has_sphere=True, sphere_center=(0.0, 0.0, 0.0),
-                          sphere_radius=0.3, self_collision=True, kappa=1e4, thickness=1.5e-3)
+                          sphere_radius=0.3, self_collision=True, kappa=1e4, thickness=1.5 * D_HAT_IPC)
 
     def mesh(sp):
-        return scenarios.sphere_drape(side=sp.side, length=1.5, height=0.305)
+        return scenarios.sphere_drape(side=sp.side, length=1.5, height=0.301)
 
     def make(sp):
         setup = api.SetupDesc(stiffness=sp.stretch, bend_stiffness=sp.bending, density_gsm=sp.density_gsm)
@@ -251,8 +257,9 @@ def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
     if pool is not None:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_api as O
-        oc = O.default_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=1e-3)
-        c = _oracle_contact(True, -0.3, ((0.0, 0.0, 0.0), 0.3), self_collision=True, kappa=1e4, thickness=1.5e-3)
+        oc = O.default_config(max_iterations=15, al_max_iterations=5, barrier_d_hat=dh2)
+        c = _oracle_contact(True, -0.3, ((0.0, 0.0, 0.0), 0.3), self_collision=True, kappa=1e4,
+                            thickness=1.5 * D_HAT_IPC)
         for side, k in first.items():
             sp = specs[k]
             prm = O.init_params(stiffness=sp.stretch, bend_stiffness=sp.bending, density_gsm=sp.density_gsm)
@@ -268,8 +275,9 @@ def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
     out = {"value": value, "unit": UNIT, "instances": n, "steps": steps, "warmup": warmup,
            "ms_per_step": ms / steps, "vertices": info["vertices"], "triangles": info["triangles"],
            "launches_per_step": batch.launches_per_step(), "sweep": tune["sweep_mode"],
-           "how": "sphere drapes with ground, sphere and self-contact barriers (IPC, AL <= 5 x 15 iterations), "
-                  "grid sides and materials of the batched workload, CUDA events over the timed steps"}
+           "how": "sphere drapes with ground, sphere and self-contact barriers (IPC, AL <= 5 x 15 iterations, "
+                  "d_hat 1 mm as a distance), grid sides and materials of the batched workload, CUDA events over "
+                  "the timed steps"}
     if pool is not None:
         errs = {str(specs[k].side): float(np.abs(batch.state(k)[0] - refs[k].result()).max()) for k in refs}
         out["error_vs_fp64"] = {"max_m": max(errs.values()), "per_side_m": errs, "steps": warmup + steps,

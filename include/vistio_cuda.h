@@ -286,10 +286,14 @@ vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, ui
  * - which top-level supernodes a single warp takes and which a whole block,
  *   by a limit on s (s + m): 0, 1024, 2048, 4096, 6144, 12288 and 2^30.
  * candidate_ms (21 entries, may be NULL) receives the time of each limit for
- * kind 0 (entries 0-6), kind 1 (entries 7-13) and kind 2 (entries 14-20; -1
- * without garment groups); the fastest pair is kept (*chosen_limit; the kind
- * from vistio_batch_get_sweep_mode). Without tuning: kind 2 if the batch has
- * garment groups, else kind 1, with the limit 6144. Captured step graphs are
+ * kind 0 (entries 0-6) and kind 1 (entries 7-13); entries 14-20 time kind 2 at
+ * kind 1's fastest limit with the group limits 0, 64, 128, 256, 512, 1024 and
+ * 6144 (the largest s (s + m) of a supernode above the bottom subtrees that
+ * the groups sweep one lane per garment; -1 without garment groups or above
+ * that warp-item limit). The fastest candidate is kept (*chosen_limit; the
+ * kind from vistio_batch_get_sweep_mode, the group limit from
+ * vistio_batch_get_group_limit). Without tuning: kind 2 if the batch has
+ * garment groups, else kind 1, with the limits 6144. Captured step graphs are
  * rebuilt on the next step. Synchronises the batch's stream. */
 vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms);
 /* Autotunes the shapes of the local steps on this batch (no reference
@@ -304,6 +308,10 @@ vistio_status vistio_batch_tune_local(vistio_batch* b, uint32_t* tri_per_thread,
                                       float* candidate_ms);
 /* Sets the local steps' elements per thread directly (1 or 2 each). */
 vistio_status vistio_batch_set_local_shape(vistio_batch* b, uint32_t tri_per_thread, uint32_t hinge_per_thread);
+/* Sets / reads the group limit of sweep kind 2 (see vistio_batch_tune; at
+ * most 6144; the batch must have garment groups). No reference counterpart. */
+vistio_status vistio_batch_set_group_limit(vistio_batch* b, uint32_t limit);
+vistio_status vistio_batch_get_group_limit(const vistio_batch* b, uint32_t* limit);
 /* Sets the warp-item limit directly (any value; see vistio_batch_tune). */
 vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit);
 /* Sets the sweep kind (0, 1, or 2 for a batch with garment groups; see

@@ -327,16 +327,21 @@ def test_grouped_sweeps_bit_identical_to_dataflow_and_to_solo(refine):
                            refinement_sweeps=refine)
     contact = api.Contact(has_ground=True, ground_height=0.3, kappa=1e4)
     res = {}
-    for mode in ("dataflow", "grouped"):
+    for mode, glimit in (("dataflow", None), ("grouped", 0), ("grouped", 256), ("grouped", 6144)):
         batch = api.Batch(grouped_batch_solvers(cfg, GROUPED_SIDES))
         assert batch.sweep_mode()[0] == "grouped"
         batch.set_sweep_mode(mode)
+        if glimit is not None:
+            batch.set_group_limit(glimit)
+            assert batch.group_limit() == glimit
         batch.step(DT, 3)
         batch.step(DT, 3, contact=contact)
-        res[mode] = [batch.state(k)[0] for k in range(len(GROUPED_SIDES))]
+        res[(mode, glimit)] = [batch.state(k)[0] for k in range(len(GROUPED_SIDES))]
         batch.close()
-    for k, (a, b) in enumerate(zip(res["dataflow"], res["grouped"])):
-        assert np.array_equal(a, b), (k, GROUPED_SIDES[k], float(np.abs(a - b).max()))
+    for key in res:
+        for k, (a, b) in enumerate(zip(res[("dataflow", None)], res[key])):
+            assert np.array_equal(a, b), (key, k, GROUPED_SIDES[k], float(np.abs(a - b).max()))
+    res["grouped"] = res[("grouped", 6144)]
     # garments of each group, stepped alone
     solo = grouped_batch_solvers(cfg, GROUPED_SIDES)
     for k in (0, 1, 2, 5, 7, 11):

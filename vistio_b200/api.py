@@ -449,6 +449,8 @@ class Batch:
 
     SWEEP_MODES = ("levels", "dataflow", "grouped")
 
+    GROUP_LIMITS = (0, 64, 128, 256, 512, 1024, 6144)
+
     def tune(self) -> dict:
         """Autotunes the sweeps on this batch (vistio_batch_tune): returns the
         chosen sweep kind and warp-item limit, and the sweep time of every
@@ -459,12 +461,27 @@ class Batch:
         tri, hinge = C.c_uint32(), C.c_uint32()
         lms = (C.c_float * 4)()
         L.check(L.lib().vistio_batch_tune_local(self.h, C.byref(tri), C.byref(hinge), lms), self.ctx.h)
+        sweep_ms = {mode: {str(lim): float(ms[7 * m + i]) for i, lim in enumerate(self.TUNE_LIMITS)}
+                    for m, mode in enumerate(self.SWEEP_MODES[:2])}
+        grouped = {str(lim): float(ms[14 + i]) for i, lim in enumerate(self.GROUP_LIMITS) if ms[14 + i] >= 0}
+        if grouped:
+            sweep_ms["grouped"] = grouped
         return {"sweep_mode": self.sweep_mode()[0], "warp_item_limit": chosen.value,
-                "sweep_ms": {mode: {str(lim): float(ms[7 * m + i]) for i, lim in enumerate(self.TUNE_LIMITS)}
-                             for m, mode in enumerate(self.SWEEP_MODES) if ms[7 * m] >= 0},
+                "group_limit": self.group_limit() if grouped else None,
+                "sweep_ms": sweep_ms,
                 "triangles_per_thread": tri.value, "hinges_per_thread": hinge.value,
                 "local_ms": {"membrane": {"1": float(lms[0]), "2": float(lms[1])},
                              "bending": {"1": float(lms[2]), "2": float(lms[3])}}}
+
+    def set_group_limit(self, limit: int):
+        """Largest s (s + m) of a supernode above the bottom subtrees that the
+        garment groups sweep one lane per garment (sweep kind "grouped")."""
+        L.check(L.lib().vistio_batch_set_group_limit(self.h, int(limit)), self.ctx.h)
+
+    def group_limit(self) -> int:
+        v = C.c_uint32()
+        L.check(L.lib().vistio_batch_get_group_limit(self.h, C.byref(v)), self.ctx.h)
+        return v.value
 
     def set_local_shape(self, triangles_per_thread: int, hinges_per_thread: int):
         """Elements per thread of the membrane and bending steps (1 or 2 each)."""

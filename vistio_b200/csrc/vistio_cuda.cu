@@ -188,6 +188,16 @@ struct vistio_batch {
   DevBuf<uint2> g_subs, g_items_fwd, g_items_bwd, g_pack;
   DevBuf<float> g_vals;
   uint64_t g_bytes = 0;
+  // per topology with groups: what decides which supernodes k_gsweep takes
+  struct GTopoHost {
+    std::vector<uint8_t> taken, insub;     // laid out for the groups; bottom-subtree supernode
+    std::vector<uint32_t> depth, parent, cost;  // cost = s (s + m)
+    uint32_t sn_off = 0, sub_base = 0, nsub = 0;
+  };
+  std::vector<GTopoHost> gtopo_host;
+  std::vector<uint32_t> group_topo;                 // per group
+  std::vector<std::vector<uint32_t>> group_snbase;  // per group, per lane: the garment's first supernode
+  uint32_t group_limit = kWarpItemLimit;            // largest s (s + m) of a supernode above the subtrees in k_gsweep
   DevBuf<InstRed> red;
   DevBuf<StepParams> prm;
   SelfContactDev self;       // self-contact buffers (allocated on first use)
@@ -312,6 +322,57 @@ cudaError_t upload_schedule(vistio_batch* b, const std::vector<uint32_t>& items,
                         cudaMemcpyHostToDevice, st);
   return e;
 }
+// The supernodes k_gsweep takes at a limit: every bottom-subtree supernode,
+// and every laid-out supernode above them whose s (s + m) is at most `limit`
+// and all of whose children are taken (closed downwards). Sets the
+// per-supernode flags that keep them out of k_sweep's schedule and uploads
+// k_gsweep's work items: forward, the subtrees, then the supernodes above them
+// deepest first; backward, those shallowest first, then the subtrees. Within
+// a depth the same supernode of every group is adjacent (shared row indices).
+cudaError_t schedule_groups(vistio_batch* b, uint32_t limit, cudaStream_t st) {
+  std::fill(b->sn_grouped.begin(), b->sn_grouped.end(), uint8_t(0));
+  std::vector<std::vector<uint8_t>> act(b->gtopo_host.size());
+  for (size_t t = 0; t < b->gtopo_host.size(); ++t) {
+    const auto& T = b->gtopo_host[t];
+    const uint32_t ns = uint32_t(T.taken.size());
+    std::vector<uint8_t> kids_ok(ns, 1);
+    act[t].assign(ns, 0);
+    for (uint32_t q = 0; q < ns; ++q) {  // children precede their parents
+      act[t][q] = T.insub[q] || (T.taken[q] && kids_ok[q] && T.cost[q] <= limit);
+      if (!act[t][q] && T.parent[q] != UINT32_MAX) kids_ok[T.parent[q]] = 0;
+    }
+  }
+  struct TopItem { uint32_t depth, q, g; };
+  std::vector<TopItem> tops;
+  std::vector<uint2> fwd, bwd;
+  for (uint32_t g = 0; g < b->group_topo.size(); ++g) {
+    const uint32_t t = b->group_topo[g];
+    const auto& T = b->gtopo_host[t];
+    for (uint32_t base : b->group_snbase[g])
+      for (uint32_t q = 0; q < act[t].size(); ++q)
+        if (act[t][q]) b->sn_grouped[base + q] = 1;
+    for (uint32_t q = 0; q < act[t].size(); ++q)
+      if (act[t][q] && !T.insub[q]) tops.push_back(TopItem{T.depth[q], q, g});
+    for (uint32_t i = 0; i < T.nsub; ++i) fwd.push_back(make_uint2(g, (T.sub_base + i) << 1));
+  }
+  std::stable_sort(tops.begin(), tops.end(), [](const TopItem& a, const TopItem& c) {
+    return a.depth != c.depth ? a.depth > c.depth : a.q != c.q ? a.q < c.q : a.g < c.g;
+  });
+  const size_t nsub_items = fwd.size();
+  for (const TopItem& x : tops) fwd.push_back(make_uint2(x.g, ((b->gtopo_host[b->group_topo[x.g]].sn_off + x.q) << 1) | 1u));
+  for (size_t i = tops.size(); i-- > 0;)
+    bwd.push_back(make_uint2(tops[i].g, ((b->gtopo_host[b->group_topo[tops[i].g]].sn_off + tops[i].q) << 1) | 1u));
+  bwd.insert(bwd.end(), fwd.begin(), fwd.begin() + nsub_items);
+  b->n_gitems_fwd = uint32_t(fwd.size());
+  b->n_gitems_bwd = uint32_t(bwd.size());
+  b->group_limit = limit;
+  cudaError_t e = cudaSuccess;
+  if (!fwd.empty()) e = cudaMemcpyAsync(b->g_items_fwd.p, fwd.data(), fwd.size() * sizeof(uint2), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !bwd.empty())
+    e = cudaMemcpyAsync(b->g_items_bwd.p, bwd.data(), bwd.size() * sizeof(uint2), cudaMemcpyHostToDevice, st);
+  return e;
+}
+
 inline uint64_t pad4(uint64_t n) { return (n + 3) & ~3ull; }
 float estimate_kappa(const vistio_solver_config& c, const InstanceSetup& I);
 
@@ -868,52 +929,46 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     const uint32_t NG = b->n_groups;
     std::vector<GroupDev> grp(NG);
     std::vector<uint32_t> gl_vbase(kGroupLanes * NG, 0), gl_snbase(kGroupLanes * NG, 0), gl_inst(kGroupLanes * NG, 0);
-    std::vector<uint2> pack, items_fwd, items_bwd;
-    uint64_t gbase = 0;
-    struct TopItem { uint32_t depth, q, g; };
-    std::vector<TopItem> tops;
+    std::vector<uint2> pack;
+    uint64_t gbase = 0, max_items = 0;
+    for (const auto& T : gp.topos) {
+      vistio_batch::GTopoHost h;
+      const Factor& F = solvers[T.leader]->setup.factor;
+      h.taken = T.taken; h.insub = T.insub; h.depth = T.depth;
+      h.sn_off = T.sn_off; h.sub_base = T.sub_base; h.nsub = uint32_t(F.sub_first.size());
+      for (const Supernode& X : F.sn) {
+        h.parent.push_back(X.parent);
+        h.cost.push_back(X.ncols * (X.ncols + X.nrows));
+      }
+      b->gtopo_host.push_back(std::move(h));
+    }
     for (uint32_t g = 0; g < NG; ++g) {
       const auto& T = gp.topos[gp.gtopo[g]];
       const auto& mem = gp.gmembers[g];
       grp[g] = GroupDev{T.sn_off, uint32_t(mem.size()), gbase, uint32_t(g_ubase[g]), T.row_base};
       gbase += T.entries;
+      b->group_topo.push_back(gp.gtopo[g]);
+      b->group_snbase.emplace_back();
       for (uint32_t l = 0; l < mem.size(); ++l) {
         const uint32_t k = mem[l];
         gl_vbase[kGroupLanes * g + l] = uint32_t(vb[k]);
         gl_snbase[kGroupLanes * g + l] = hi[k].sn_base;
         gl_inst[kGroupLanes * g + l] = k;
-        for (uint32_t q = 0; q < T.taken.size(); ++q)
-          if (T.taken[q]) b->sn_grouped[hi[k].sn_base + q] = 1;
+        b->group_snbase.back().push_back(hi[k].sn_base);
       }
       for (uint32_t q = 0; q < T.taken.size(); ++q) {
         if (!T.taken[q]) continue;
         pack.push_back(make_uint2(g, T.sn_off + q));
-        if (!T.insub[q]) tops.push_back(TopItem{T.depth[q], q, g});
+        ++max_items;  // a supernode above the subtrees, or part of one subtree item
       }
-      const uint32_t nsub = uint32_t(solvers[T.leader]->setup.factor.sub_first.size());
-      for (uint32_t i = 0; i < nsub; ++i) items_fwd.push_back(make_uint2(g, (T.sub_base + i) << 1));
     }
-    // forward: the subtrees, then the supernodes above them deepest first;
-    // backward: those shallowest first, then the subtrees. Within a depth the
-    // same supernode of every group is adjacent (its row indices are shared).
-    std::stable_sort(tops.begin(), tops.end(), [](const TopItem& a, const TopItem& c) {
-      return a.depth != c.depth ? a.depth > c.depth : a.q != c.q ? a.q < c.q : a.g < c.g;
-    });
-    for (const TopItem& t : tops)
-      items_fwd.push_back(make_uint2(t.g, ((gp.topos[gp.gtopo[t.g]].sn_off + t.q) << 1) | 1u));
-    for (size_t i = tops.size(); i-- > 0;)
-      items_bwd.push_back(make_uint2(tops[i].g, ((gp.topos[gp.gtopo[tops[i].g]].sn_off + tops[i].q) << 1) | 1u));
-    for (const uint2& it : items_fwd)
-      if ((it.y & 1u) == 0) items_bwd.push_back(it);
-    b->n_gitems_fwd = uint32_t(items_fwd.size());
-    b->n_gitems_bwd = uint32_t(items_bwd.size());
     b->n_gpack = uint32_t(pack.size());
     CU(b->grp.upload(grp, st)); CU(b->gsn.upload(gsn, st));
     CU(b->g_rows.upload(g_rows, st)); CU(b->g_fwd_ptr.upload(g_fwd_ptr, st)); CU(b->g_kids.upload(g_kids, st));
     CU(b->g_fwd.upload(g_fwd, st));
     CU(b->g_subs.upload(g_subs, st));
     CU(b->gl_vbase.upload(gl_vbase, st)); CU(b->gl_snbase.upload(gl_snbase, st)); CU(b->gl_inst.upload(gl_inst, st));
-    CU(b->g_items_fwd.upload(items_fwd, st)); CU(b->g_items_bwd.upload(items_bwd, st));
+    CU(b->g_items_fwd.alloc(max_items + 1, st)); CU(b->g_items_bwd.alloc(max_items + 1, st));
     CU(b->g_pack.upload(pack, st));
     CU(b->g_queue.alloc(2, st)); CU(cudaMemsetAsync(b->g_queue.p, 0, 8, st));
     CU(b->g_vals.alloc(gbase * kGroupLanes, st));
@@ -926,10 +981,11 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(st));
     b->g_bytes = gbase * kGroupLanes * 4 + gsn.size() * sizeof(GsnDev) + (g_rows.size() + g_fwd_ptr.size() +
-                 g_fwd.size() + g_kids.size()) * 4 + (items_fwd.size() + items_bwd.size() + pack.size()) * 8;
+                 g_fwd.size() + g_kids.size()) * 4 + (2 * max_items + pack.size()) * 8;
     b->device_bytes += b->g_bytes;
     b->g_pack.reset();
     b->sweep_mode = 2;
+    CU(schedule_groups(b, b->group_limit, st));
     std::vector<uint32_t> items2 = schedule_levels(b, b->warp_limit);
     CU(upload_schedule(b, items2, st));
     CU(cudaStreamSynchronize(st));
@@ -1678,6 +1734,8 @@ void* vistio_batch_stream(vistio_batch* b) { return b ? (void*)b->ctx->stream : 
 // top supernode for a block) ... 2^30 (every one of at most kWarpVec columns
 // for a warp).
 static const uint32_t kTuneLimits[7] = {0u, 1024u, 2048u, 4096u, 6144u, 12288u, 1u << 30};
+// Group limits of the grouped kind's candidates: 0 takes the bottom subtrees only.
+static const uint32_t kGroupTuneLimits[7] = {0u, 64u, 128u, 256u, 512u, 1024u, 6144u};
 
 namespace {
 vistio_status drop_graphs(vistio_batch* b) {  // captured steps bake the schedule into their launches
@@ -1697,15 +1755,19 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
-  float best = 0.f;
-  uint32_t best_limit = b->warp_limit, best_mode = b->sweep_mode;
+  float best = 0.f, best1 = 0.f;
+  uint32_t best_limit = b->warp_limit, best_mode = b->sweep_mode, best_glimit = b->group_limit;
+  uint32_t best1_limit = kWarpItemLimit;  // the fastest limit of kind 1: kind 2 runs its rest at it
   for (int c = 0; c < 21; ++c) {
-    if (c >= 14 && !b->n_groups) {  // no garment groups: no grouped candidates
+    const uint32_t glimit = c >= 14 ? kGroupTuneLimits[c - 14] : b->group_limit;
+    if (c >= 14 && (!b->n_groups || glimit > best1_limit)) {  // no groups, or a limit kind 1's rest could not match
       if (candidate_ms) candidate_ms[c] = -1.f;
       continue;
     }
     b->sweep_mode = uint32_t(c / 7);
-    std::vector<uint32_t> items = schedule_levels(b, kTuneLimits[c % 7]);
+    const uint32_t limit = c >= 14 ? best1_limit : kTuneLimits[c % 7];
+    if (c >= 14) CU(schedule_groups(b, glimit, st));
+    std::vector<uint32_t> items = schedule_levels(b, limit);
     CU(upload_schedule(b, items, st));
     CU(cudaMemsetAsync(b->Y.p, 0, b->V * sizeof(float4), st));
     launch_sweeps(b, b->dev, st);  // warm-up
@@ -1717,13 +1779,15 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
     CU(cudaEventElapsedTime(&ms, e0, e1));
     ms /= 3.f;
     if (candidate_ms) candidate_ms[c] = ms;
-    if (c == 0 || ms < best) { best = ms; best_limit = kTuneLimits[c % 7]; best_mode = b->sweep_mode; }
+    if (c >= 7 && c < 14 && (c == 7 || ms < best1)) { best1 = ms; best1_limit = limit; }
+    if (c == 0 || ms < best) { best = ms; best_limit = limit; best_mode = b->sweep_mode; best_glimit = glimit; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   uint32_t status = 0;
   CU(cudaMemcpyAsync(&status, b->status.p, sizeof(status), cudaMemcpyDeviceToHost, st));
   b->sweep_mode = best_mode;
+  if (b->n_groups) CU(schedule_groups(b, best_glimit, st));
   std::vector<uint32_t> items = schedule_levels(b, best_limit);
   CU(upload_schedule(b, items, st));
   CU(cudaStreamSynchronize(st));
@@ -1731,6 +1795,23 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
   b->tuned_ms = best;
   drop_graphs(b);
   if (chosen_limit) *chosen_limit = best_limit;
+  return VISTIO_OK;
+}
+
+vistio_status vistio_batch_set_group_limit(vistio_batch* b, uint32_t limit) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  vistio_ctx* ctx = b->ctx;
+  if (!b->n_groups) return fail(ctx, VISTIO_ERR_INVALID_CONFIG, "the batch has no garment groups");
+  CU(schedule_groups(b, std::min(limit, kWarpItemLimit), ctx->stream));
+  std::vector<uint32_t> items = schedule_levels(b, b->warp_limit);
+  CU(upload_schedule(b, items, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return drop_graphs(b);
+}
+
+vistio_status vistio_batch_get_group_limit(const vistio_batch* b, uint32_t* limit) {
+  if (!b || !limit) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null argument");
+  *limit = b->group_limit;
   return VISTIO_OK;
 }
 
