@@ -1307,52 +1307,89 @@ struct GLane {
 // Streamed factor entry (read once per sweep).
 __device__ __forceinline__ float gval(const float* p) { return __ldcs(p); }
 
-// y = inv(L_kk) t in place on columns f .. f + s of L, the triangle's rows at
-// D (entry (c, c2) at D[(c (c + 1) / 2 + c2) * 32]); descending c, so every
-// y_c reads only t values.
-__device__ __forceinline__ void g_diag_fwd(const GLane& L, uint32_t f, uint32_t s, const float* D) {
-  for (int c = int(s) - 1; c >= 0; --c) {
-    float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float* row = D + size_t(uint32_t(c) * uint32_t(c + 1) / 2) * 32;
-#pragma unroll 8
-    for (uint32_t c2 = 0; c2 <= uint32_t(c); ++c2) f4_fma(y, gval(row + c2 * 32), L.get(f + c2));
-    L.set(f + uint32_t(c), y);
+// Brings [p, p + bytes) into L2 ahead of its use (a bulk prefetch, no
+// shared memory involved); p 16-byte aligned, bytes rounded down to 16.
+__device__ __forceinline__ void l2_prefetch(const void* p, uint64_t bytes) {
+  for (uint64_t o = 0; o + 16 <= bytes; o += 32768) {
+    const uint64_t left = bytes - o;
+    const uint32_t n = uint32_t(left < 32768 ? left : 32768) & ~15u;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(static_cast<const char*>(p) + o), "r"(n)
+                 : "memory");
   }
 }
 
-// x = inv(L_kk)^T t in place on columns f .. f + s of L; ascending c, so every
-// x_c reads only t values.
-__device__ __forceinline__ void g_diag_bwd(const GLane& L, uint32_t f, uint32_t s, const float* D) {
-  for (uint32_t c = 0; c < s; ++c) {
-    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+// y = inv(L_kk) t in place on columns f .. f + s of L, the triangle's rows at
+// D (entry (c, c2) at D[(c (c + 1) / 2 + c2) * 32]); descending c, two rows
+// per pass (each y_c reads only t values, so the rows are independent and
+// their loads overlap), each row summed over c2 ascending.
+__device__ __forceinline__ void g_diag_fwd(const GLane& L, uint32_t f, uint32_t s, const float* D) {
+  int c = int(s) - 1;
+  for (; c >= 1; c -= 2) {
+    float4 y0 = make_float4(0.f, 0.f, 0.f, 0.f), y1 = y0;
+    const float* r0 = D + size_t(uint32_t(c) * uint32_t(c + 1) / 2) * 32;
+    const float* r1 = D + size_t(uint32_t(c - 1) * uint32_t(c) / 2) * 32;
 #pragma unroll 8
-    for (uint32_t c2 = c; c2 < s; ++c2) f4_fma(x, gval(D + size_t(c2 * (c2 + 1) / 2 + c) * 32), L.get(f + c2));
+    for (uint32_t c2 = 0; c2 < uint32_t(c); ++c2) {
+      const float4 t = L.get(f + c2);
+      f4_fma(y0, gval(r0 + c2 * 32), t);
+      f4_fma(y1, gval(r1 + c2 * 32), t);
+    }
+    f4_fma(y0, gval(r0 + uint32_t(c) * 32), L.get(f + uint32_t(c)));
+    L.set(f + uint32_t(c), y0);
+    L.set(f + uint32_t(c) - 1, y1);
+  }
+  if (c == 0) {
+    float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+    f4_fma(y, gval(D), L.get(f));
+    L.set(f, y);
+  }
+}
+
+// x = inv(L_kk)^T t in place on columns f .. f + s of L; ascending c, two
+// rows per pass (each x_c reads only t values), each summed over c2 ascending.
+__device__ __forceinline__ void g_diag_bwd(const GLane& L, uint32_t f, uint32_t s, const float* D) {
+  uint32_t c = 0;
+  for (; c + 1 < s; c += 2) {
+    float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
+    f4_fma(x0, gval(D + size_t(c * (c + 1) / 2 + c) * 32), L.get(f + c));
+#pragma unroll 8
+    for (uint32_t c2 = c + 1; c2 < s; ++c2) {
+      const float4 t = L.get(f + c2);
+      const float* row = D + size_t(c2 * (c2 + 1) / 2 + c) * 32;
+      f4_fma(x0, gval(row), t);
+      f4_fma(x1, gval(row + 32), t);
+    }
+    L.set(f + c, x0);
+    L.set(f + c + 1, x1);
+  }
+  if (c < s) {
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+    f4_fma(x, gval(D + size_t(c * (c + 1) / 2 + c) * 32), L.get(f + c));
     L.set(f + c, x);
   }
 }
 
 // u_j = P(j, :) . y for the m panel rows (P row-major, y in columns f .. f + s
-// of L), four rows at a time so that each y_c is read once per four rows;
-// emit(j, u) takes each row's update.
+// of L), eight rows at a time so that each y_c is read once per eight rows and
+// the rows' loads overlap; emit(j, u) takes each row's update.
+constexpr uint32_t kGPushRows = 8;
 template <class Emit>
 __device__ __forceinline__ void g_push(const GLane& L, uint32_t f, uint32_t s, uint32_t m, const float* P, Emit emit) {
-  for (uint32_t j0 = 0; j0 < m; j0 += 4) {
-    const uint32_t nr = min(4u, m - j0);
-    float4 u[4];
+  for (uint32_t j0 = 0; j0 < m; j0 += kGPushRows) {
+    const uint32_t nr = min(kGPushRows, m - j0);
+    float4 u[kGPushRows];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) u[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t r = 0; r < kGPushRows; ++r) u[r] = make_float4(0.f, 0.f, 0.f, 0.f);
     const float* P0 = P + size_t(j0) * s * 32;
-    // unrolled so that the loads of several columns are in flight before the
-    // first multiply waits on one
-#pragma unroll 8
+#pragma unroll 4
     for (uint32_t c = 0; c < s; ++c) {
       const float4 y = L.get(f + c);
 #pragma unroll
-      for (uint32_t r = 0; r < 4; ++r)
+      for (uint32_t r = 0; r < kGPushRows; ++r)
         if (r < nr) f4_fma(u[r], gval(P0 + size_t(r * s + c) * 32), y);
     }
 #pragma unroll
-    for (uint32_t r = 0; r < 4; ++r)
+    for (uint32_t r = 0; r < kGPushRows; ++r)
       if (r < nr) emit(j0 + r, u[r]);
   }
 }
@@ -1400,6 +1437,12 @@ __device__ __forceinline__ void g_item(const BatchDev& B, uint2 it, const GLane&
     const GsnDev A = B.gsn[st.x], Z = B.gsn[st.y];
     const uint32_t c0 = A.first, c1 = Z.first + Z.ncols, nc = c1 - c0;
     const uint32_t root = snb + (st.y - G.sn_off);
+    const GsnDev Zn = B.gsn[st.y];  // the item's data: [A.g_off, end of Z) is contiguous
+    if (lane == 0) {
+      const uint64_t e0 = A.g_off, e1 = Zn.g_off + uint64_t(Zn.ncols) * (Zn.ncols + 1) / 2 + uint64_t(Zn.nrows) * Zn.ncols;
+      const uint64_t nb = (e1 - e0) * 128;
+      l2_prefetch(B.g_vals + (G.base + e0) * 32, nb < 65536 ? nb : 65536);
+    }
     if (DIR == 1 && dep_wait(B, B.df_flag + root, 1u)) B.df_flag[root] = 0u;
     for (uint32_t c = 0; c < nc; ++c) L.set(c, __ldcg(Y + c0 + c));
     if (DIR == 0) {
@@ -1439,6 +1482,8 @@ __device__ __forceinline__ void g_item(const BatchDev& B, uint2 it, const GLane&
   const uint32_t me = snb + (id - G.sn_off);
   const float* D = vals + S.g_off * 32;
   const float* P = D + size_t(s * (s + 1) / 2) * 32;
+  if (lane == 0)  // in flight while the dependency wait runs
+    l2_prefetch(B.g_vals + (G.base + S.g_off) * 32, (uint64_t(s) * (s + 1) / 2 + uint64_t(m) * s) * 128);
   if (DIR == 0) {
     if (S.nkids && dep_wait(B, B.df_cnt + me, S.nkids)) B.df_cnt[me] = 0u;
     const uint32_t* fp = B.g_fwd_ptr + G.row_base + f;
