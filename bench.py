@@ -332,14 +332,20 @@ def _request(a):
     return scenarios.hanging_sheet(a["side"], 1.0), api.drape_config(max_iterations=ITERS), setup, None
 
 
-def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factorization=False):
+ADMIT_WAIT_MS = 250
+
+
+def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factorization=False,
+                  admit_wait_ms=ADMIT_WAIT_MS):
     """The served drape stream: the arrivals of stream_arrivals, 300 steps
-    each, 120 GB admission budget. Latency runs from a request's arrival to
-    its completion."""
+    each, 120 GB admission budget, cohorts of up to 64 requests formed with an
+    admission window of `admit_wait_ms`. Latency runs from a request's arrival
+    to its completion."""
     from vistio_b200 import api
     arrivals = stream_arrivals(window_s, rate, seed)
     srv = api.Server(hbm_budget_bytes=120 << 30, max_cohort=64, setup_threads=threads or (os.cpu_count() or 4),
-                     steps_per_slice=10, cache_bytes=2 << 30, gpu_factorization=gpu_factorization)
+                     steps_per_slice=10, cache_bytes=2 << 30, gpu_factorization=gpu_factorization,
+                     admit_wait_ms=admit_wait_ms)
     sym0 = api.symbolic_cache_info()
     t0 = time.perf_counter()
     k = 0
@@ -367,6 +373,7 @@ def served_stream(window_s, rate=200.0, seed=20261203, threads=None, gpu_factori
             "setup_cache": {"hits": st["cache_hits"], "misses": st["cache_misses"]},
             "factorization": "GPU (cohort start)" if gpu_factorization else "host (set-up threads)",
             "symbolic_cache": {"hits": sym1["hits"] - sym0["hits"], "misses": sym1["misses"] - sym0["misses"]},
+            "admit_wait_ms": admit_wait_ms, "cohorts_started": st["cohorts_started"],
             "how": "Poisson arrivals at the stated rate during the window, then drained; each request 300 steps"}
 
 

@@ -368,6 +368,12 @@ typedef struct vistio_server_config {
    * streams, and the dependency-driven sweeps keep blocks resident that wait
    * for one another, so 0 suits a busy server. */
   uint32_t sweep_mode;
+  /* Admission window: while any cohort is running, ready requests of one step
+   * configuration wait up to this long (from the first one's readiness) for
+   * others to form a larger cohort, unless max_cohort of them are ready.
+   * Fewer, larger cohorts keep the GPU's work in fewer, wider launches. 0:
+   * every tick starts a cohort with whatever is ready. */
+  uint32_t admit_wait_ms;
 } vistio_server_config;
 
 typedef struct vistio_request {

@@ -121,3 +121,29 @@ def test_memory_budget_admission_and_oversize_request():
         pos, _ = srv.result(rid)
         assert np.abs(pos - run_alone(req)[0]).max() <= 1e-6
     srv.close()
+
+
+def test_admission_window_forms_larger_cohorts():
+    """With an admission window, requests of one step configuration that
+    become ready while a cohort runs wait (bounded) for company: the second
+    wave's five requests start as one cohort instead of trickling into
+    several, and every result still equals the request run alone."""
+    blocker = plain_request(32, 1.0, 1000.0, 1e-4, 150.0, 300)
+    wave = [plain_request(8 + k, 0.5 + 0.1 * k, 500.0 + 100 * k, 1e-4, 120.0, 30) for k in range(5)]
+    srv = api.Server(hbm_budget_bytes=4 << 30, max_cohort=16, setup_threads=1, steps_per_slice=5, admit_wait_ms=400)
+    b_id = submit(srv, blocker)
+    t0 = time.time()
+    while srv.query(b_id)["state"] != "running":
+        srv.tick()
+        assert time.time() - t0 < 120
+    ids = [submit(srv, r) for r in wave]  # one set-up thread: they become ready one by one
+    srv.drain(600)
+    info = [srv.query(i) for i in ids]
+    assert all(q["state"] == "done" for q in info), info
+    assert len({q["cohort"] for q in info}) == 1, info  # one cohort for the whole wave
+    st = srv.stats()
+    assert st["cohorts_started"] == 2, st
+    for rid, req in zip(ids, wave):
+        pos, _ = srv.result(rid)
+        assert np.abs(pos - run_alone(req)[0]).max() <= 1e-6
+    srv.close()

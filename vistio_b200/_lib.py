@@ -82,7 +82,7 @@ class ColliderResultsC(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("max_cohort", C.c_uint32),
                 ("setup_threads", C.c_uint32), ("steps_per_slice", C.c_uint32), ("cache_bytes", C.c_uint64),
-                ("gpu_factorization", C.c_uint32), ("sweep_mode", C.c_uint32)]
+                ("gpu_factorization", C.c_uint32), ("sweep_mode", C.c_uint32), ("admit_wait_ms", C.c_uint32)]
 
 
 class RequestC(C.Structure):

@@ -648,12 +648,15 @@ class Server:
 
     def __init__(self, hbm_budget_bytes: int = 8 << 30, max_cohort: int = 64, setup_threads: int = 4,
                  steps_per_slice: int = 10, cache_bytes: int = 1 << 30, device: int = 0,
-                 gpu_factorization: bool = False, sweep_mode: str = "levels"):
+                 gpu_factorization: bool = False, sweep_mode: str = "levels", admit_wait_ms: int = 0):
         """gpu_factorization False: the set-up threads factorize on the host,
         beside the GPU's work; True: each request's own host_factorization.
-        sweep_mode: the sweep kind of every cohort (Batch.SWEEP_MODES)."""
+        sweep_mode: the sweep kind of every cohort (Batch.SWEEP_MODES).
+        admit_wait_ms: while cohorts run, how long ready requests of one step
+        configuration may wait for others to form a larger cohort."""
         cfg = L.ServerConfig(device, int(hbm_budget_bytes), int(max_cohort), int(setup_threads), int(steps_per_slice),
-                             int(cache_bytes), int(bool(gpu_factorization)), Batch.SWEEP_MODES.index(sweep_mode))
+                             int(cache_bytes), int(bool(gpu_factorization)), Batch.SWEEP_MODES.index(sweep_mode),
+                             int(admit_wait_ms))
         h = C.c_void_p()
         st = L.lib().vistio_server_create(C.byref(cfg), C.byref(h))
         if st != L.OK:

@@ -362,9 +362,20 @@ void admit(vistio_server* S) {
   }
   std::vector<Request*> left;
   bool full = false;
+  const double now = seconds_since(S->t0);
   for (uint64_t key : order) {
     std::vector<Request*>& g = groups[key];
     size_t i = 0;
+    // the admission window: while the GPU has work, let a small set wait
+    // for company (bounded by admit_wait_ms from its first readiness)
+    if (S->cfg.admit_wait_ms && !S->cohorts.empty() && g.size() < S->cfg.max_cohort) {
+      double first = g[0]->t_ready;
+      for (Request* r : g) first = std::min(first, r->t_ready);
+      if (now - first < 1e-3 * double(S->cfg.admit_wait_ms)) {
+        left.insert(left.end(), g.begin(), g.end());
+        continue;
+      }
+    }
     while (i < g.size() && !full) {
       std::vector<Request*> take;
       uint64_t sum = 0;
