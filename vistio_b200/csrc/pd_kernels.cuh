@@ -327,8 +327,11 @@ __device__ __forceinline__ M32 model_target(int model, const M32& F, float warp_
 
 // ------------------------------------------------------------- kernels
 // Local membrane step of one triangle: w * g_k . (F_target - F) for k = 0..2.
-__device__ __forceinline__ void tri_project(const BatchDev& B, const InstDev& I, uint32_t t, float4 dm, float w,
-                                            float4 q0, float4 q1, float4 q2) {
+// Compiled once (not inlined): the membrane kernels of both shapes run the
+// same instructions, so the compiler's multiply-add contraction cannot differ
+// between them and their results are bit-identical.
+__device__ __noinline__ void tri_project_one(float* __restrict__ tri_out, int32_t model, float warp, float weft,
+                                             uint32_t t, float4 dm, float w, float4 q0, float4 q1, float4 q2) {
   // FP64 from the FP32 positions on (the projection is the ill-conditioned
   // part; the outputs are rounded once).
   const double3 p0 = d3(q0), p1 = d3(q1), p2 = d3(q2);
@@ -337,7 +340,7 @@ __device__ __forceinline__ void tri_project(const BatchDev& B, const InstDev& I,
   float det = dm.x * dm.w - dm.y * dm.z;
   double3 d0 = make_double3(0.0, 0.0, 0.0), d1 = d0;
   if (fabsf(det) > 1e-12f) {  // element.rs:192-202: degenerate rest shape keeps p
-    M32 Ft = model_target(I.model, F, I.warp, I.weft);
+    M32 Ft = model_target(model, F, warp, weft);
     d0 = (Ft.c0 - F.c0) * double(w);
     d1 = (Ft.c1 - F.c1) * double(w);
   }
@@ -346,10 +349,14 @@ __device__ __forceinline__ void tri_project(const BatchDev& B, const InstDev& I,
   const double3 c0 = d0 * g00 + d1 * g01;
   const double3 c1 = d0 * double(dm.x) + d1 * double(dm.z);
   const double3 c2 = d0 * double(dm.y) + d1 * double(dm.w);
-  float* o = B.tri_out + 9ull * t;
+  float* o = tri_out + 9ull * t;
   o[0] = float(c0.x); o[1] = float(c0.y); o[2] = float(c0.z);
   o[3] = float(c1.x); o[4] = float(c1.y); o[5] = float(c1.z);
   o[6] = float(c2.x); o[7] = float(c2.y); o[8] = float(c2.z);
+}
+__device__ __forceinline__ void tri_project(const BatchDev& B, const InstDev& I, uint32_t t, float4 dm, float w,
+                                            float4 q0, float4 q1, float4 q2) {
+  tri_project_one(B.tri_out, I.model, I.warp, I.weft, t, dm, w, q0, q1, q2);
 }
 
 // The membrane step over a chunk of up to 256 triangles with 128 threads:
@@ -399,8 +406,9 @@ __device__ __forceinline__ float3 rot_delta(float3 v, float3 axis, float s, floa
 }
 
 // Local bending step of one hinge: w * s . (target - x); only the wings move
-// (bending.rs:182-227, discrete_shells.rs:285-337).
-__device__ __forceinline__ float4 hinge_project(float4 st, float2 wr, float3 p0, float3 p1, float3 pa, float3 pb) {
+// (bending.rs:182-227, discrete_shells.rs:285-337). Compiled once (not
+// inlined), so both bending kernels' shapes give bit-identical results.
+__device__ __noinline__ float4 hinge_project(float4 st, float2 wr, float3 p0, float3 p1, float3 pa, float3 pb) {
   float3 out = make_float3(0.f, 0.f, 0.f);
   float3 e = p1 - p0;
   float el = len3(e);

@@ -569,6 +569,26 @@ struct PairGrad {
 // Compiled for four blocks per SM (64 registers, a few spills in the FP64
 // branch) instead of the two that 124 registers allow: contact batch of 64
 // sphere drapes 93 -> 86 ms per step (before the per-pair sums).
+// Lower bounds of the tests' distances, cheaper than the tests: a
+// vertex-triangle distance is at least the vertex's distance to the
+// triangle's plane, an edge-edge distance at least the distance between the
+// two segments' boxes. A test whose bound reaches the FP32 screen (10 d_hat)
+// is skipped without the full test; it could not have been active (d < d_hat)
+// in any precision, so the contact set and gradient are unchanged.
+__device__ __forceinline__ bool vt_far(V3d<float> p, V3d<float> a, V3d<float> n, float nn, float screen) {
+  const float h = vdot(n, vsub(p, a));
+  return nn > 1e-30f && h * h >= screen * nn;
+}
+__device__ __forceinline__ bool ee_far(V3d<float> p0, V3d<float> p1, V3d<float> q0, V3d<float> q1, float screen) {
+  auto gap = [](float alo, float ahi, float blo, float bhi) {
+    return fmaxf(fmaxf(blo - ahi, alo - bhi), 0.f);
+  };
+  const float gx = gap(fminf(p0.x, p1.x), fmaxf(p0.x, p1.x), fminf(q0.x, q1.x), fmaxf(q0.x, q1.x));
+  const float gy = gap(fminf(p0.y, p1.y), fmaxf(p0.y, p1.y), fminf(q0.y, q1.y), fmaxf(q0.y, q1.y));
+  const float gz = gap(fminf(p0.z, p1.z), fmaxf(p0.z, p1.z), fminf(q0.z, q1.z), fmaxf(q0.z, q1.z));
+  return gx * gx + gy * gy + gz * gz >= screen;
+}
+
 __global__ void __launch_bounds__(kGradThreads, 4) k_self_grad(BatchDev B, SelfContactView S, int mode) {
   __shared__ double acc_s[18 * kGradThreads];  // 36 KB: four blocks per SM
   const StepParams& P = *B.prm;
@@ -592,13 +612,16 @@ __global__ void __launch_bounds__(kGradThreads, 4) k_self_grad(BatchDev B, SelfC
       const uint32_t* X = side == 0 ? av : bv;
       const uint32_t* Yt = side == 0 ? bv : av;
       const int xs = side == 0 ? 0 : 3, ys = side == 0 ? 3 : 0;  // slots of X's and Yt's corners
-      V3d<float> ta = ld3(B.pos, Yt[0]), tb = ld3(B.pos, Yt[1]), tc = ld3(B.pos, Yt[2]);
+      const V3d<float> ta = ld3(B.pos, Yt[0]), tb = ld3(B.pos, Yt[1]), tc = ld3(B.pos, Yt[2]);
+      const V3d<float> n = vcross(vsub(tb, ta), vsub(tc, ta));
+      const float nn = vdot(n, n);
       for (int q = 0; q < 3; ++q) {
         uint32_t v = X[q];
         if (v == Yt[0] || v == Yt[1] || v == Yt[2]) continue;
+        const V3d<float> p = ld3(B.pos, v);
+        if (vt_far(p, ta, n, nn, screen)) continue;
         // the FP32 screen first: it is cheaper than the exclusion lists, and
         // the two filters commute
-        V3d<float> p = ld3(B.pos, v);
         if (!(pt_d2<float>(p, ta, tb, tc) < screen)) continue;
         if (excluded(S, v, Yt[0]) || excluded(S, v, Yt[1]) || excluded(S, v, Yt[2])) continue;
         const V3d<double> p8 = cvt<double>(p), a8 = cvt<double>(ta), b8 = cvt<double>(tb), c8 = cvt<double>(tc);
@@ -618,7 +641,8 @@ __global__ void __launch_bounds__(kGradThreads, 4) k_self_grad(BatchDev B, SelfC
       for (int j = 0; j < 3; ++j) {
         uint32_t a0 = av[ea[i][0]], a1 = av[ea[i][1]], b0 = bv[ea[j][0]], b1 = bv[ea[j][1]];
         if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) continue;
-        V3d<float> p0 = ld3(B.pos, a0), p1 = ld3(B.pos, a1), q0 = ld3(B.pos, b0), q1 = ld3(B.pos, b1);
+        const V3d<float> p0 = ld3(B.pos, a0), p1 = ld3(B.pos, a1), q0 = ld3(B.pos, b0), q1 = ld3(B.pos, b1);
+        if (ee_far(p0, p1, q0, q1, screen)) continue;
         if (!(ee_d2<float>(p0, p1, q0, q1) < screen)) continue;
         if (excluded(S, a0, b0) && excluded(S, a0, b1) && excluded(S, a1, b0) && excluded(S, a1, b1)) continue;
         const V3d<double> P0 = cvt<double>(p0), P1 = cvt<double>(p1), Q0 = cvt<double>(q0), Q1 = cvt<double>(q1);
