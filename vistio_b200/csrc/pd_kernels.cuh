@@ -32,6 +32,9 @@ struct InstDev {
   float ground_h;
   uint32_t sn_base, nsn;
   int32_t unit_stencils;       // every hinge stencil is (-1, -1, 1, 1) (dihedral bending): not loaded
+  uint32_t tbase, hbase;       // first triangle and hinge of the garment
+  uint32_t inc_ptr;            // its connectivity class's per-vertex offsets in vtri_ptr / vhinge_ptr
+  uint32_t tinc_off, hinc_off; // its class's codes in vtri / vhinge
 };
 
 // One supernode in HBM: one contiguous, 16-byte aligned region holding
@@ -151,11 +154,12 @@ struct BatchDev {
   const float4* hinge_st;
   const float2* hinge_wr;  // (weight, rest angle)
   float4* hinge_out;       // w * s . (target - x)
-  // vertex incidence (CSR over global vertex ids)
+  // vertex incidence, one CSR per connectivity class over the garment's local
+  // vertex ids (InstDev::inc_ptr, tinc_off, hinc_off)
   const uint32_t* vtri_ptr;
-  const uint32_t* vtri;    // (triangle << 2) | slot
+  const uint32_t* vtri;    // (local triangle << 2) | slot
   const uint32_t* vhinge_ptr;
-  const uint32_t* vhinge;  // (hinge << 2) | slot
+  const uint32_t* vhinge;  // (local hinge << 2) | slot
   // solve
   const uint32_t* perm_local;  // vertex -> instance-local permuted row
   const uint32_t* row_vertex;  // global row -> instance-local vertex
@@ -491,16 +495,21 @@ __global__ void __launch_bounds__(256) k_gather(BatchDev B, int keep_rhs) {
   // stencil only this vertex's weight (gather 0.313 -> 0.278 ms per iteration),
   // none where every stencil is (-1, -1, 1, 1): -1 for the edge's ends, 1 for
   // the wings, the same products as the loaded weights
+  // the garment's connectivity class's lists (shared by the garments of one
+  // mesh topology: read once for all of them, from L2 after the first)
+  const uint32_t l = g - I.vbase;
+  const uint32_t* tcode = B.vtri + I.tinc_off;
+  const uint32_t* hcode = B.vhinge + I.hinc_off;
 #pragma unroll 4
-  for (uint32_t e = B.vtri_ptr[g], ee = B.vtri_ptr[g + 1]; e < ee; ++e) {
-    uint32_t code = __ldg(B.vtri + e);
-    const float* o = B.tri_out + 9ull * (code >> 2) + 3 * (code & 3u);
+  for (uint32_t e = __ldg(B.vtri_ptr + I.inc_ptr + l), ee = __ldg(B.vtri_ptr + I.inc_ptr + l + 1); e < ee; ++e) {
+    uint32_t code = __ldg(tcode + e);
+    const float* o = B.tri_out + 9ull * (I.tbase + (code >> 2)) + 3 * (code & 3u);
     r.x += __ldg(o); r.y += __ldg(o + 1); r.z += __ldg(o + 2);
   }
 #pragma unroll 4
-  for (uint32_t e = B.vhinge_ptr[g], ee = B.vhinge_ptr[g + 1]; e < ee; ++e) {
-    uint32_t code = __ldg(B.vhinge + e);
-    uint32_t h = code >> 2, k = code & 3u;
+  for (uint32_t e = __ldg(B.vhinge_ptr + I.inc_ptr + l), ee = __ldg(B.vhinge_ptr + I.inc_ptr + l + 1); e < ee; ++e) {
+    uint32_t code = __ldg(hcode + e);
+    uint32_t h = I.hbase + (code >> 2), k = code & 3u;
     float s = I.unit_stencils ? (k < 2u ? -1.f : 1.f) : __ldg(reinterpret_cast<const float*>(B.hinge_st + h) + k);
     float4 o = __ldg(B.hinge_out + h);
     r.x += s * o.x; r.y += s * o.y; r.z += s * o.z;

@@ -668,9 +668,8 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   std::vector<uint4> hinge_idx(H);
   std::vector<float4> hinge_st(H);
   std::vector<float2> hinge_wr(H);
-  std::vector<uint32_t> vtri_ptr(V + 1, 0), vhinge_ptr(V + 1, 0), perm_local(V), fwd_ptr(V + 1, 0),
-      rows;
-  std::vector<uint32_t> vtri(3 * T), vhinge(4 * H);
+  std::vector<uint32_t> vtri_ptr, vhinge_ptr, perm_local(V), fwd_ptr(V + 1, 0), rows;
+  std::vector<uint32_t> vtri, vhinge;  // incidence, per connectivity class
   std::vector<SnDev> sn(NSN);
   std::vector<float> vals(NVALS + 4, 0.f);  // +16 bytes: staging windows round up to 16 bytes
   std::vector<uint32_t> fwd(NFWD);
@@ -801,22 +800,46 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     for (uint64_t g = 0; g < NSN; ++g)
       if (df_parent[g] != kNoParent) df_kids[cur[df_parent[g]]++] = uint32_t(g);
   }
-  // vertex incidence
-  for (uint64_t t = 0; t < T; ++t) { vtri_ptr[tri_idx[t].x + 1]++; vtri_ptr[tri_idx[t].y + 1]++; vtri_ptr[tri_idx[t].z + 1]++; }
-  for (uint64_t h = 0; h < H; ++h) {
-    vhinge_ptr[hinge_idx[h].x + 1]++; vhinge_ptr[hinge_idx[h].y + 1]++;
-    vhinge_ptr[hinge_idx[h].z + 1]++; vhinge_ptr[hinge_idx[h].w + 1]++;
-  }
-  for (uint64_t i = 0; i < V; ++i) { vtri_ptr[i + 1] += vtri_ptr[i]; vhinge_ptr[i + 1] += vhinge_ptr[i]; }
+  // Vertex incidence, once per connectivity class: garments with the same
+  // triangles and hinges (the batched workload's garments of one grid side)
+  // share one list of (local element << 2 | slot) codes and one array of
+  // local offsets per vertex; each garment adds its own element bases.
   {
-    std::vector<uint32_t> c1(vtri_ptr.begin(), vtri_ptr.end() - 1), c2(vhinge_ptr.begin(), vhinge_ptr.end() - 1);
-    for (uint64_t t = 0; t < T; ++t) {
-      uint32_t ids[3] = {tri_idx[t].x, tri_idx[t].y, tri_idx[t].z};
-      for (uint32_t s = 0; s < 3; ++s) vtri[c1[ids[s]]++] = uint32_t(t << 2) | s;
-    }
-    for (uint64_t h = 0; h < H; ++h) {
-      uint32_t ids[4] = {hinge_idx[h].x, hinge_idx[h].y, hinge_idx[h].z, hinge_idx[h].w};
-      for (uint32_t s = 0; s < 4; ++s) vhinge[c2[ids[s]]++] = uint32_t(h << 2) | s;
+    std::vector<uint32_t> leader;  // first garment of each class
+    for (uint32_t k = 0; k < n; ++k) {
+      const InstanceSetup& I = solvers[k]->setup;
+      uint32_t c = 0;
+      for (; c < leader.size(); ++c) {
+        const InstanceSetup& J = solvers[leader[c]]->setup;
+        if (J.nv == I.nv && J.nt == I.nt && J.nh == I.nh && J.tris == I.tris && J.hinge_v == I.hinge_v) break;
+      }
+      if (c == leader.size()) {
+        leader.push_back(k);
+        const uint32_t pbase = uint32_t(vtri_ptr.size()), tbase = uint32_t(vtri.size()), hbase = uint32_t(vhinge.size());
+        std::vector<uint32_t> pt(I.nv + 1, 0), ph(I.nv + 1, 0);
+        for (uint32_t t = 0; t < I.nt; ++t)
+          for (uint32_t q = 0; q < 3; ++q) pt[I.tris[3 * t + q] + 1]++;
+        for (uint32_t h = 0; h < I.nh; ++h)
+          for (uint32_t q = 0; q < 4; ++q) ph[I.hinge_v[4 * h + q] + 1]++;
+        for (uint32_t i = 0; i < I.nv; ++i) { pt[i + 1] += pt[i]; ph[i + 1] += ph[i]; }
+        std::vector<uint32_t> ct(3ull * I.nt), cn(4ull * I.nh);
+        std::vector<uint32_t> c1(pt.begin(), pt.end() - 1), c2(ph.begin(), ph.end() - 1);
+        for (uint32_t t = 0; t < I.nt; ++t)
+          for (uint32_t q = 0; q < 3; ++q) ct[c1[I.tris[3 * t + q]]++] = (t << 2) | q;
+        for (uint32_t h = 0; h < I.nh; ++h)
+          for (uint32_t q = 0; q < 4; ++q) cn[c2[I.hinge_v[4 * h + q]]++] = (h << 2) | q;
+        vtri_ptr.insert(vtri_ptr.end(), pt.begin(), pt.end());
+        vhinge_ptr.insert(vhinge_ptr.end(), ph.begin(), ph.end());
+        vtri.insert(vtri.end(), ct.begin(), ct.end());
+        vhinge.insert(vhinge.end(), cn.begin(), cn.end());
+        hi[k].inc_ptr = pbase; hi[k].tinc_off = tbase; hi[k].hinc_off = hbase;
+      } else {
+        hi[k].inc_ptr = hi[leader[c]].inc_ptr;
+        hi[k].tinc_off = hi[leader[c]].tinc_off;
+        hi[k].hinc_off = hi[leader[c]].hinc_off;
+      }
+      hi[k].tbase = uint32_t(tb[k]);
+      hi[k].hbase = uint32_t(hb[k]);
     }
   }
   auto tch = make_chunks(tb, tc), hch = make_chunks(hb, hc), vch = make_chunks(vb, vc);
