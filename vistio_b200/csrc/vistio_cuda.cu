@@ -161,6 +161,10 @@ struct vistio_batch {
   std::vector<uint32_t> lvl_off, lvl_nb, lvl_nw;
   std::vector<std::pair<uint32_t, uint32_t>> top;  // (level, supernode) of every top-level supernode
   std::vector<SnDev> sn_host;                       // supernode table, for re-scheduling
+  // per global supernode: (structure class << 32) | local id. Work units of
+  // the per-garment sweeps take equal keys side by side (the same supernode
+  // of garments that share a topology: equal work for the block's warps).
+  std::vector<uint64_t> sn_key;
   uint32_t warp_limit = kWarpItemLimit;             // s (s + m) limit of a warp item
   uint32_t tri_per = 2, hinge_per = 1;              // elements per thread of k_tri / k_hinge (autotuned)
   float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
@@ -247,11 +251,18 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
     (warp_item(S.ncols, S.nrows, limit) ? wrp : blk)[t.first].push_back(t.second);
   }
   auto weight = [&](uint32_t q) { return uint64_t(b->sn_host[q].ncols) * (b->sn_host[q].ncols + b->sn_host[q].nrows); };
+  // heaviest first; equal supernodes of garments of one topology side by side
+  auto heavier = [&](uint32_t a, uint32_t c) {
+    const uint64_t wa = weight(a), wc = weight(c);
+    if (wa != wc) return wa > wc;
+    if (!b->sn_key.empty() && b->sn_key[a] != b->sn_key[c]) return b->sn_key[a] < b->sn_key[c];
+    return a < c;
+  };
   std::vector<uint32_t> items;
   b->lvl_off.clear(); b->lvl_nb.clear(); b->lvl_nw.clear();
   for (uint32_t l = 0; l < L; ++l) {
-    std::stable_sort(blk[l].begin(), blk[l].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
-    std::stable_sort(wrp[l].begin(), wrp[l].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
+    std::stable_sort(blk[l].begin(), blk[l].end(), heavier);
+    std::stable_sort(wrp[l].begin(), wrp[l].end(), heavier);
     b->lvl_off.push_back(uint32_t(items.size()));
     b->lvl_nb.push_back(uint32_t(blk[l].size()));
     b->lvl_nw.push_back(uint32_t(wrp[l].size()));
@@ -291,8 +302,8 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
     for (uint32_t q = 0; q < nsub; q += kSolveWarps)
       b->units_fwd_host.push_back(make_uint2(0u | (std::min(kSolveWarps, nsub - q) << 2), q));
     for (uint32_t d = D; d-- > 0;) {
-      std::stable_sort(dblk[d].begin(), dblk[d].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
-      std::stable_sort(dwrp[d].begin(), dwrp[d].end(), [&](uint32_t a, uint32_t c) { return weight(a) > weight(c); });
+      std::stable_sort(dblk[d].begin(), dblk[d].end(), heavier);
+      std::stable_sort(dwrp[d].begin(), dwrp[d].end(), heavier);
       for (uint32_t k : dblk[d]) b->units_fwd_host.push_back(make_uint2(1u | (1u << 2), k));
       for (size_t i = 0; i < dwrp[d].size(); i += kSolveWarps) {
         const uint32_t off = uint32_t(b->items_fwd_host.size());
@@ -571,6 +582,7 @@ struct GroupPlan {
   std::vector<Topo> topos;
   std::vector<int32_t> group;  // per garment: its group, or -1
   std::vector<uint32_t> lane;  // per garment: its lane in the group
+  std::vector<uint32_t> sclass;  // per garment: its symbolic structure class (any size)
   std::vector<uint32_t> gtopo; // per group: its topology
   std::vector<std::vector<uint32_t>> gmembers;
 };
@@ -579,6 +591,7 @@ GroupPlan plan_groups(vistio_solver* const* solvers, uint32_t n) {
   GroupPlan G;
   G.group.assign(n, -1);
   G.lane.assign(n, 0);
+  G.sclass.assign(n, 0);
   std::vector<GroupPlan::Topo> all;
   for (uint32_t k = 0; k < n; ++k) {
     const Factor& F = solvers[k]->setup.factor;
@@ -590,6 +603,7 @@ GroupPlan plan_groups(vistio_solver* const* solvers, uint32_t n) {
       all.back().leader = k;
     }
     all[t].members.push_back(k);
+    G.sclass[k] = uint32_t(t);
   }
   for (auto& T : all) {
     if (T.members.size() < kGroupMinLanes) continue;
@@ -774,6 +788,16 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
     b->refine = b->cfg.refinement_sweeps;
   }
   b->sn_host = sn;
+  b->sn_key.assign(NSN, 0);
+  for (uint32_t k = 0; k < n; ++k)
+    for (uint32_t q = 0; q < hi[k].nsn; ++q) b->sn_key[hi[k].sn_base + q] = (uint64_t(gp.sclass[k]) << 32) | q;
+  // subtree units take eight consecutive subtrees: the same subtree of
+  // garments of one topology side by side (equal work for the block's warps)
+  auto by_key = [&](const uint2& a, const uint2& c) {
+    return b->sn_key[a.x] != b->sn_key[c.x] ? b->sn_key[a.x] < b->sn_key[c.x] : a.x < c.x;
+  };
+  std::sort(subs.begin(), subs.end(), by_key);
+  std::sort(subs_grouped.begin(), subs_grouped.end(), by_key);
   b->n_sub_plain = uint32_t(subs.size());
   subs.insert(subs.end(), subs_grouped.begin(), subs_grouped.end());
   b->n_sub = uint32_t(subs.size());
