@@ -1220,9 +1220,13 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
     __syncthreads();
     if (DIR == 0) sn_forward(B, t.bt, S);
     else sn_backward(B, t.bt, S);
-    __threadfence();
+    // one fence after the barrier covers the whole block's writes (the fence
+    // is cumulative over what the barrier ordered before it); then signal
     __syncthreads();
-    dep_leave<DIR>(B, k, tid, 32 * kSolveWarps);
+    if (tid == 0) {
+      __threadfence();
+      dep_leave<DIR>(B, k, 0, 1);
+    }
   } else if (warp < count) {
     if (kind == 0) {
       const uint2 it = B.sub_items[u.y + warp];
@@ -1230,9 +1234,11 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
       if (DIR == 1 && lane == 0) dep_enter<1>(B, it.y);
       __syncwarp();
       subtree_sweep<DIR>(B, t.wt, it.x, it.y);
-      __threadfence();
       __syncwarp();
-      if (DIR == 0) dep_leave<0>(B, it.y, lane, 32);
+      if (DIR == 0 && lane == 0) {
+        __threadfence();
+        dep_leave<0>(B, it.y, 0, 1);
+      }
     } else {
       const uint32_t k = (DIR == 0 ? B.df_items_fwd : B.lvl_items)[u.y + warp];
       const SnDev S = B.sn[k];
@@ -1241,9 +1247,11 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
       __syncwarp();
       if (DIR == 0) sn_forward(B, t.wt, S);
       else sn_backward(B, t.wt, S);
-      __threadfence();
       __syncwarp();
-      dep_leave<DIR>(B, k, lane, 32);
+      if (lane == 0) {
+        __threadfence();
+        dep_leave<DIR>(B, k, 0, 1);
+      }
     }
   }
 }
@@ -1258,18 +1266,25 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
 __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_sweep(BatchDev B, uint32_t nfwd, uint32_t nbwd) {
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
-  __shared__ uint32_t s_abort, s_unit;
+  __shared__ uint32_t s_abort, s_unit[2];
   SweepTeams t = make_teams(smem4, s_bar, &s_abort);
   const uint32_t tid = threadIdx.x;
   const bool ipc = B.prm->ipc != 0;
-  for (;;) {
-    __syncthreads();  // every warp is done with the previous unit
-    if (tid == 0) s_unit = atomicAdd(B.df_queue, 1u);
-    __syncthreads();
-    const uint32_t q = s_unit;
+  // Thread 0 takes the next unit from the queue while the block works on the
+  // current one (the atomic's latency hides behind the unit). A block then
+  // holds one unit it has not started, which cannot deadlock: the smallest
+  // unfinished unit is always one that a block is working on (a block takes
+  // its next unit after its current one), and it waits only for smaller ones.
+  if (tid == 0) s_unit[0] = atomicAdd(B.df_queue, 1u);
+  for (uint32_t it = 0;; ++it) {
+    __syncthreads();  // every warp is done with the previous unit; s_unit[it & 1] is written
+    const uint32_t q = s_unit[it & 1];
     if (q >= nfwd + nbwd) break;
+    uint32_t next = 0;
+    if (tid == 0) next = atomicAdd(B.df_queue, 1u);
     if (q < nfwd) sweep_unit<0>(B, t, B.df_units_fwd[q], ipc);
     else sweep_unit<1>(B, t, B.df_units[nbwd - 1 - (q - nfwd)], ipc);
+    if (tid == 0) s_unit[(it + 1) & 1] = next;  // read by all after the next barrier
   }
   if (tid == 0) {
     __threadfence();
@@ -1539,13 +1554,17 @@ __global__ void __launch_bounds__(kGThreads, 2) k_gsweep(BatchDev B, uint32_t ni
   const GLane L{gsm + warp * (kGCols * 3 * 32) + lane};
   const bool ipc = B.prm->ipc != 0;
   const uint2* items = DIR == 0 ? B.g_items_fwd : B.g_items_bwd;
-  for (;;) {
-    uint32_t q = 0;
-    if (lane == 0) q = atomicAdd(B.g_queue, 1u);
-    q = __shfl_sync(0xffffffffu, q, 0);
-    if (q >= nitems) break;
+  // lane 0 takes the next item while the warp works on the current one (see
+  // k_sweep: the smallest unfinished item is always one a warp is working on)
+  uint32_t q = 0;
+  if (lane == 0) q = atomicAdd(B.g_queue, 1u);
+  q = __shfl_sync(0xffffffffu, q, 0);
+  while (q < nitems) {
+    uint32_t next = 0;
+    if (lane == 0) next = atomicAdd(B.g_queue, 1u);
     g_item<DIR>(B, items[q], L, lane, ipc);
     __syncwarp();
+    q = __shfl_sync(0xffffffffu, next, 0);
   }
   if (lane == 0) {
     __threadfence();
