@@ -607,9 +607,10 @@ def first_of_each_topology(specs, order):
     return sorted(first.values())
 
 
-def fp64_runs(specs, order, nsteps, pool):
-    """Starts the oracle's FP64 runs of the first instance of each topology
-    over nsteps steps on `pool`; returns {batch index: future of positions}."""
+def fp64_runs(specs, order, nsteps, pool, precision=1):
+    """Starts the oracle's runs (precision 1: FP64; 0: the reference's FP32
+    arithmetic) of the first instance of each topology over nsteps steps on
+    `pool`; returns {batch index: future of positions}."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_api as O
     from vistio_b200 import scenarios
@@ -618,7 +619,7 @@ def fp64_runs(specs, order, nsteps, pool):
         s = specs[order[k]]
         m = scenarios.hanging_sheet(s.side, s.length)
         p = O.init_params(stiffness=s.stretch, bend_stiffness=s.bending, density_gsm=s.density_gsm)
-        sim = O.OracleSim(m, p, O.default_config(max_iterations=ITERS), precision=1)
+        sim = O.OracleSim(m, p, O.default_config(max_iterations=ITERS), precision=precision)
         for _ in range(nsteps):
             sim.step(DT)
         return sim.state()[0]
@@ -626,12 +627,16 @@ def fp64_runs(specs, order, nsteps, pool):
     return {k: pool.submit(run, k) for k in first_of_each_topology(specs, order)}
 
 
-def fp64_error(specs, order, states, refs, nsteps):
+def fp64_error(specs, order, states, refs, nsteps, refs32=None):
     """Max |x_gpu - x_fp64| (m) after nsteps steps on the first instance of
-    each topology (states: batch index -> GPU positions)."""
+    each topology (states: batch index -> GPU positions); with refs32, also
+    the reference FP32 restatement's own distance from FP64."""
     res = [(specs[order[k]].side, float(np.abs(states[k] - refs[k].result()).max())) for k in sorted(states)]
-    return {"max_m": max(e for _, e in res), "per_side_m": {str(side): e for side, e in res}, "steps": nsteps,
-            "how": "first instance of each topology vs the FP64 oracle run of the same steps"}
+    out = {"max_m": max(e for _, e in res), "per_side_m": {str(side): e for side, e in res}, "steps": nsteps,
+           "how": "first instance of each topology vs the FP64 oracle run of the same steps"}
+    if refs32 is not None:
+        out["ref32_max_m"] = max(float(np.abs(refs32[k].result() - refs[k].result()).max()) for k in refs)
+    return out
 
 
 def timed_steps(batch, steps, warmup, contact=None):
@@ -703,6 +708,7 @@ def main():
     # the host beside the GPU work (rank 0, full runs only)
     pool = cf.ThreadPoolExecutor(max(1, os.cpu_count() or 1)) if rank == 0 and not args.no_baselines else None
     refs = fp64_runs(specs, order, err_steps, pool) if pool else None
+    refs32 = fp64_runs(specs, order, err_steps, pool, precision=0) if pool else None
     from vistio_b200 import api as _api
     sym0 = _api.symbolic_cache_info()
     t0 = time.time()
@@ -843,7 +849,7 @@ def main():
         batch2.step(DT, err_steps - args.warmup - args.steps)
         states2 = {k: batch2.state(k)[0] for k in refs}
         batch2.close()
-        out["error_vs_fp64"] = fp64_error(specs, order, states, refs, err_steps)
+        out["error_vs_fp64"] = fp64_error(specs, order, states, refs, err_steps, refs32)
         v2 = job_value(len(specs), 1, args.steps, ms2)
         out["refined"] = {"refinement_sweeps": 1, "value": v2, "unit": UNIT, "ms_per_step": ms2 / args.steps,
                           "over_default": v2 / value, "sweep_mode": tune2["sweep_mode"],
