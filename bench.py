@@ -272,9 +272,31 @@ def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
     ms = timed_steps(batch, steps, warmup, contact)
     info = batch.info()
     value = n * steps / (ms / 1e3)
+    # the dominant kernel is the global solve (75 per step): its roofline, from
+    # the autotuner's time of the chosen sweeps on this batch and the
+    # algorithmic bytes of the oracle's factors of these meshes
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    nnz = {}
+    for sp in specs:
+        if sp.side not in nnz:
+            nnz[sp.side] = O.OracleSim(mesh(sp), O.init_params(), O.default_config()).factor_nnz()
+    alg = 2 * (8 * sum(nnz[sp.side] for sp in specs) + 12 * info["vertices"])
+    mode = tune["sweep_mode"]
+    key = str(tune["group_limit"]) if mode == "grouped" else str(tune["warp_item_limit"])
+    sweep_ms = tune["sweep_ms"][mode][key]
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    solves = 15 * 5  # PD iterations per AL pass x AL passes (at most; passes end early when converged)
+    roofline = {"bound": "hbm", "kernel": "the sweeps of one global solve", "algorithmic_bytes": alg,
+                "kernel_ms": sweep_ms, "achieved": alg / (sweep_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                "peak_source": "measured" if peaks else "fallback",
+                "solves_per_step_max": solves, "solve_share_of_step_max": min(1.0, solves * sweep_ms / (ms / steps))}
+    roofline["frac"] = roofline["achieved"] / peak
     out = {"value": value, "unit": UNIT, "instances": n, "steps": steps, "warmup": warmup,
            "ms_per_step": ms / steps, "vertices": info["vertices"], "triangles": info["triangles"],
-           "launches_per_step": batch.launches_per_step(), "sweep": tune["sweep_mode"],
+           "launches_per_step": batch.launches_per_step(), "sweep": tune["sweep_mode"], "roofline": roofline,
            "how": "sphere drapes with ground, sphere and self-contact barriers (IPC, AL <= 5 x 15 iterations, "
                   "d_hat 1 mm as a distance), grid sides and materials of the batched workload, CUDA events over "
                   "the timed steps"}

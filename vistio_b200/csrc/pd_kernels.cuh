@@ -496,23 +496,63 @@ __global__ void __launch_bounds__(256) k_gather(BatchDev B, int keep_rhs) {
   // none where every stencil is (-1, -1, 1, 1): -1 for the edge's ends, 1 for
   // the wings, the same products as the loaded weights
   // the garment's connectivity class's lists (shared by the garments of one
-  // mesh topology: read once for all of them, from L2 after the first)
+  // mesh topology: read once for all of them, from L2 after the first). The
+  // first kGatherBatch incidences of each list load all their codes, then
+  // all their contributions, before the first add (the loads overlap); the
+  // sums run in list order either way.
   const uint32_t l = g - I.vbase;
   const uint32_t* tcode = B.vtri + I.tinc_off;
   const uint32_t* hcode = B.vhinge + I.hinc_off;
-#pragma unroll 4
-  for (uint32_t e = __ldg(B.vtri_ptr + I.inc_ptr + l), ee = __ldg(B.vtri_ptr + I.inc_ptr + l + 1); e < ee; ++e) {
-    uint32_t code = __ldg(tcode + e);
-    const float* o = B.tri_out + 9ull * (I.tbase + (code >> 2)) + 3 * (code & 3u);
-    r.x += __ldg(o); r.y += __ldg(o + 1); r.z += __ldg(o + 2);
+  constexpr uint32_t kGatherBatch = 8;
+  {
+    const uint32_t e0 = __ldg(B.vtri_ptr + I.inc_ptr + l), e1 = __ldg(B.vtri_ptr + I.inc_ptr + l + 1);
+    const uint32_t nb = min(e1 - e0, kGatherBatch);
+    uint32_t code[kGatherBatch];
+    float3 c[kGatherBatch];
+#pragma unroll
+    for (uint32_t i = 0; i < kGatherBatch; ++i)
+      if (i < nb) code[i] = __ldg(tcode + e0 + i);
+#pragma unroll
+    for (uint32_t i = 0; i < kGatherBatch; ++i)
+      if (i < nb) {
+        const float* o = B.tri_out + 9ull * (I.tbase + (code[i] >> 2)) + 3 * (code[i] & 3u);
+        c[i] = make_float3(__ldg(o), __ldg(o + 1), __ldg(o + 2));
+      }
+#pragma unroll
+    for (uint32_t i = 0; i < kGatherBatch; ++i)
+      if (i < nb) { r.x += c[i].x; r.y += c[i].y; r.z += c[i].z; }
+    for (uint32_t e = e0 + nb; e < e1; ++e) {
+      const uint32_t cd = __ldg(tcode + e);
+      const float* o = B.tri_out + 9ull * (I.tbase + (cd >> 2)) + 3 * (cd & 3u);
+      r.x += __ldg(o); r.y += __ldg(o + 1); r.z += __ldg(o + 2);
+    }
   }
-#pragma unroll 4
-  for (uint32_t e = __ldg(B.vhinge_ptr + I.inc_ptr + l), ee = __ldg(B.vhinge_ptr + I.inc_ptr + l + 1); e < ee; ++e) {
-    uint32_t code = __ldg(hcode + e);
-    uint32_t h = I.hbase + (code >> 2), k = code & 3u;
-    float s = I.unit_stencils ? (k < 2u ? -1.f : 1.f) : __ldg(reinterpret_cast<const float*>(B.hinge_st + h) + k);
-    float4 o = __ldg(B.hinge_out + h);
-    r.x += s * o.x; r.y += s * o.y; r.z += s * o.z;
+  {
+    const uint32_t e0 = __ldg(B.vhinge_ptr + I.inc_ptr + l), e1 = __ldg(B.vhinge_ptr + I.inc_ptr + l + 1);
+    const uint32_t nb = min(e1 - e0, kGatherBatch);
+    uint32_t code[kGatherBatch];
+    float4 o[kGatherBatch];
+    float sw[kGatherBatch];
+#pragma unroll
+    for (uint32_t i = 0; i < kGatherBatch; ++i)
+      if (i < nb) code[i] = __ldg(hcode + e0 + i);
+#pragma unroll
+    for (uint32_t i = 0; i < kGatherBatch; ++i)
+      if (i < nb) {
+        const uint32_t h = I.hbase + (code[i] >> 2), k = code[i] & 3u;
+        sw[i] = I.unit_stencils ? (k < 2u ? -1.f : 1.f) : __ldg(reinterpret_cast<const float*>(B.hinge_st + h) + k);
+        o[i] = __ldg(B.hinge_out + h);
+      }
+#pragma unroll
+    for (uint32_t i = 0; i < kGatherBatch; ++i)
+      if (i < nb) { r.x += sw[i] * o[i].x; r.y += sw[i] * o[i].y; r.z += sw[i] * o[i].z; }
+    for (uint32_t e = e0 + nb; e < e1; ++e) {
+      const uint32_t cd = __ldg(hcode + e);
+      const uint32_t h = I.hbase + (cd >> 2), k = cd & 3u;
+      const float s = I.unit_stencils ? (k < 2u ? -1.f : 1.f) : __ldg(reinterpret_cast<const float*>(B.hinge_st + h) + k);
+      const float4 oo = __ldg(B.hinge_out + h);
+      r.x += s * oo.x; r.y += s * oo.y; r.z += s * oo.z;
+    }
   }
   if (P.ipc) {  // assemble_barrier_rhs (assembly.rs:272-282)
     float mu = R.mu;
@@ -1554,17 +1594,15 @@ __global__ void __launch_bounds__(kGThreads, 2) k_gsweep(BatchDev B, uint32_t ni
   const GLane L{gsm + warp * (kGCols * 3 * 32) + lane};
   const bool ipc = B.prm->ipc != 0;
   const uint2* items = DIR == 0 ? B.g_items_fwd : B.g_items_bwd;
-  // lane 0 takes the next item while the warp works on the current one (see
-  // k_sweep: the smallest unfinished item is always one a warp is working on)
-  uint32_t q = 0;
-  if (lane == 0) q = atomicAdd(B.g_queue, 1u);
-  q = __shfl_sync(0xffffffffu, q, 0);
-  while (q < nitems) {
-    uint32_t next = 0;
-    if (lane == 0) next = atomicAdd(B.g_queue, 1u);
+  // An item is taken when the warp is free: with few long items per warp,
+  // taking the next one ahead would hand the tail items to busy warps.
+  for (;;) {
+    uint32_t q = 0;
+    if (lane == 0) q = atomicAdd(B.g_queue, 1u);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= nitems) break;
     g_item<DIR>(B, items[q], L, lane, ipc);
     __syncwarp();
-    q = __shfl_sync(0xffffffffu, next, 0);
   }
   if (lane == 0) {
     __threadfence();
