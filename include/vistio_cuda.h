@@ -293,7 +293,9 @@ vistio_status vistio_batch_info(const vistio_batch* b, uint32_t* n_instances, ui
  * that warp-item limit). The fastest candidate is kept (*chosen_limit; the
  * kind from vistio_batch_get_sweep_mode, the group limit from
  * vistio_batch_get_group_limit). Without tuning: kind 2 if the batch has
- * garment groups, else kind 1, with the limits 6144. Captured step graphs are
+ * garment groups, else kind 1, with the limits 6144. For kinds 1 and 2 the
+ * chosen schedule is then timed with both compiled forms of the dependency-
+ * driven kernel (vistio_batch_get_sweep_blocks). Captured step graphs are
  * rebuilt on the next step. Synchronises the batch's stream. */
 vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* candidate_ms);
 /* Autotunes the shapes of the local steps on this batch (no reference
@@ -319,6 +321,15 @@ vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit);
 vistio_status vistio_batch_set_sweep_mode(vistio_batch* b, uint32_t mode);
 /* The sweep kind and warp-item limit in use. */
 vistio_status vistio_batch_get_sweep_mode(const vistio_batch* b, uint32_t* mode, uint32_t* warp_limit);
+/* The dependency-driven sweep kernel (kinds 1 and 2) is compiled for five
+ * resident blocks per SM (48 registers per thread) and for four (64, fewer
+ * spills); no reference counterpart. vistio_batch_tune times both with the
+ * schedule it chose and keeps the faster; without tuning, five. Both give
+ * the same results, bit for bit. get: the form in use and, in tuned_ms (2
+ * entries, may be NULL), the tuner's times of the five- and four-block forms
+ * (-1 before tuning or for kind 0). */
+vistio_status vistio_batch_set_sweep_blocks(vistio_batch* b, uint32_t blocks_per_sm);
+vistio_status vistio_batch_get_sweep_blocks(const vistio_batch* b, uint32_t* blocks_per_sm, float* tuned_ms);
 /* The device factorization done when the batch was created (the garments
  * whose solver config has host_factorization = 0): its kernel launches (one
  * per height of the supernodal trees per group of garments) and their device

@@ -321,27 +321,32 @@ def test_grouped_sweeps_bit_identical_to_dataflow_and_to_solo(refine):
     lane per garment at the bottom of their trees) give exactly the results
     of the per-garment dependency-driven sweeps, plain and with IPC, with and
     without a refinement sweep, and exactly what the garments give stepped
-    alone. A batch with groups starts in the grouped kind."""
+    alone; the dependency-driven kernel's two compiled forms (five and four
+    blocks per SM) agree bit for bit. A batch with groups starts in the
+    grouped kind."""
     assert len(set(GROUPED_SIDES)) == 7 and len(GROUPED_SIDES) == 99
     cfg = api.drape_config(max_iterations=8, al_max_iterations=3, barrier_d_hat=1e-3, barrier_kappa=1e4,
                            refinement_sweeps=refine)
     contact = api.Contact(has_ground=True, ground_height=0.3, kappa=1e4)
     res = {}
-    for mode, glimit in (("dataflow", None), ("grouped", 0), ("grouped", 256), ("grouped", 6144)):
+    for mode, glimit, blocks in (("dataflow", None, 5), ("grouped", 0, 5), ("grouped", 256, 5), ("grouped", 6144, 5),
+                                 ("dataflow", None, 4), ("grouped", 256, 4)):
         batch = api.Batch(grouped_batch_solvers(cfg, GROUPED_SIDES))
-        assert batch.sweep_mode()[0] == "grouped"
+        assert batch.sweep_mode()[0] == "grouped" and batch.sweep_blocks()[0] == 5
         batch.set_sweep_mode(mode)
+        batch.set_sweep_blocks(blocks)
+        assert batch.sweep_blocks()[0] == blocks
         if glimit is not None:
             batch.set_group_limit(glimit)
             assert batch.group_limit() == glimit
         batch.step(DT, 3)
         batch.step(DT, 3, contact=contact)
-        res[(mode, glimit)] = [batch.state(k)[0] for k in range(len(GROUPED_SIDES))]
+        res[(mode, glimit, blocks)] = [batch.state(k)[0] for k in range(len(GROUPED_SIDES))]
         batch.close()
     for key in res:
-        for k, (a, b) in enumerate(zip(res[("dataflow", None)], res[key])):
+        for k, (a, b) in enumerate(zip(res[("dataflow", None, 5)], res[key])):
             assert np.array_equal(a, b), (key, k, GROUPED_SIDES[k], float(np.abs(a - b).max()))
-    res["grouped"] = res[("grouped", 6144)]
+    res["grouped"] = res[("grouped", 6144, 5)]
     # garments of each group, stepped alone
     solo = grouped_batch_solvers(cfg, GROUPED_SIDES)
     for k in (0, 1, 2, 5, 7, 11):
@@ -384,6 +389,9 @@ def test_grouped_kind_needs_groups_and_tunes():
     t = batch.tune()
     print(t)
     assert set(t["sweep_ms"]) == {"levels", "dataflow", "grouped"}
+    assert t["sweep_blocks_per_sm"] in (4, 5)
+    if t["sweep_mode"] != "levels":  # the two compiled forms of the dependency-driven kernel were timed
+        assert all(v > 0 for v in t["sweep_blocks_ms"].values())
     assert all(v > 0 for m in t["sweep_ms"].values() for v in m.values())
     batch.step(DT, 2)
 

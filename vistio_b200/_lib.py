@@ -155,6 +155,8 @@ SIGNATURES = {
     "vistio_batch_set_warp_limit": (C.c_int, [_vp, C.c_uint32]),
     "vistio_batch_set_sweep_mode": (C.c_int, [_vp, C.c_uint32]),
     "vistio_batch_get_sweep_mode": (C.c_int, [_vp, _u32p, _u32p]),
+    "vistio_batch_set_sweep_blocks": (C.c_int, [_vp, C.c_uint32]),
+    "vistio_batch_get_sweep_blocks": (C.c_int, [_vp, _u32p, _fp]),
     "vistio_solver_clone": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
     "vistio_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
     "vistio_server_destroy": (C.c_int, [_vp]),

@@ -466,7 +466,9 @@ class Batch:
         grouped = {str(lim): float(ms[14 + i]) for i, lim in enumerate(self.GROUP_LIMITS) if ms[14 + i] >= 0}
         if grouped:
             sweep_ms["grouped"] = grouped
+        blocks, occ = self.sweep_blocks()
         return {"sweep_mode": self.sweep_mode()[0], "warp_item_limit": chosen.value,
+                "sweep_blocks_per_sm": blocks, "sweep_blocks_ms": occ,
                 "group_limit": self.group_limit() if grouped else None,
                 "sweep_ms": sweep_ms,
                 "triangles_per_thread": tri.value, "hinges_per_thread": hinge.value,
@@ -497,6 +499,17 @@ class Batch:
         8 or more garments of one mesh topology): the groups' tree bottoms
         one lane per garment, the rest dependency-driven."""
         L.check(L.lib().vistio_batch_set_sweep_mode(self.h, self.SWEEP_MODES.index(mode)), self.ctx.h)
+
+    def set_sweep_blocks(self, blocks_per_sm: int):
+        """Compiled form of the dependency-driven sweep kernel: 5 or 4
+        resident blocks per SM (bit-identical results)."""
+        L.check(L.lib().vistio_batch_set_sweep_blocks(self.h, int(blocks_per_sm)), self.ctx.h)
+
+    def sweep_blocks(self) -> tuple:
+        """(blocks per SM of the form in use, {form: the tuner's ms per solve})."""
+        v, ms = C.c_uint32(), (C.c_float * 2)()
+        L.check(L.lib().vistio_batch_get_sweep_blocks(self.h, C.byref(v), ms), self.ctx.h)
+        return v.value, {"5": float(ms[0]), "4": float(ms[1])}
 
     def sweep_mode(self) -> tuple:
         """(sweep kind, warp-item limit) in use."""

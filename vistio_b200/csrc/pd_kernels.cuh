@@ -1266,7 +1266,15 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
 // parent's backward or, at a root, for its own forward. So a garment's
 // backward sweep starts as soon as its own forward sweep ends, beside the
 // forward tail of the others. The last block out resets the queue.
-__global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_sweep(BatchDev B, uint32_t nfwd, uint32_t nbwd) {
+//
+// Compiled for two occupancies, MINB resident blocks per SM: five (48
+// registers, 68 bytes per thread spilled) or four (64 registers, 28 bytes).
+// With four, each unit is shorter; with five, more units are in flight. The autotuner
+// times both on the batch: on 512 sheets of 8 topologies they tie, on 64
+// contact drapes, whose solve follows the longest garments' chains, four
+// blocks shorten the solve by 6%.
+template <int MINB>
+__global__ void __launch_bounds__(32 * kSolveWarps, MINB) k_sweep(BatchDev B, uint32_t nfwd, uint32_t nbwd) {
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
   __shared__ uint32_t s_abort, s_unit[2];

@@ -35,7 +35,7 @@ struct vistio_ctx {
   std::mutex mu;
   int refs = 0;
   bool closed = false;
-  uint32_t sweep_blocks = 0;   // resident k_sweep blocks on this device (SMs x blocks per SM)
+  uint32_t sweep_blocks[2] = {0, 0};  // resident k_sweep blocks on this device (SMs x blocks per SM): five- and four-block forms
   uint32_t gsweep_blocks = 0;  // resident k_gsweep blocks
 };
 
@@ -168,6 +168,8 @@ struct vistio_batch {
   uint32_t warp_limit = kWarpItemLimit;             // s (s + m) limit of a warp item
   uint32_t tri_per = 2, hinge_per = 1;              // elements per thread of k_tri / k_hinge (autotuned)
   float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
+  float occ_ms[2] = {-1.f, -1.f};  // the autotuner's times of the two forms (ms per solve)
+  uint32_t sweep_occ = 5;  // blocks per SM of k_sweep's compiled form (5 or 4), the autotuner's choice
   // sweeps: 0 = one launch per level (k_level), 1 = dependency-driven (k_sweep),
   // 2 = garment groups' tree bottoms by k_gsweep, the rest by k_sweep
   uint32_t sweep_mode = 1;
@@ -1099,6 +1101,14 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
   return p;
 }
 
+// One k_sweep launch over the batch's units in the chosen compiled form.
+void launch_k_sweep(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
+  const uint32_t four = b->sweep_occ == 4 ? 1u : 0u;
+  const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks[four]);
+  if (four) k_sweep<4><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
+  else k_sweep<5><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
+}
+
 // Forward then backward sweep, level by level over the whole batch, in place
 // on dv.Y (right-hand side in, solution out). Returns the launches.
 uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
@@ -1110,16 +1120,14 @@ uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
     uint32_t n = 0;
     if (gf) { k_gsweep<0><<<gf, kGThreads, kGSmem, st>>>(dv, b->n_gitems_fwd); ++n; }
     if (b->n_units_fwd + b->n_units) {
-      const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks);
-      k_sweep<<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
+      launch_k_sweep(b, dv, st);
       ++n;
     }
     if (gb) { k_gsweep<1><<<gb, kGThreads, kGSmem, st>>>(dv, b->n_gitems_bwd); ++n; }
     return n;
   }
   if (b->sweep_mode == 1 && b->n_units) {
-    const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks);
-    k_sweep<<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
+    launch_k_sweep(b, dv, st);
     return 1;
   }
   uint32_t L = uint32_t(b->lvl_off.size()), n = 0;
@@ -1360,14 +1368,17 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   CU(cudaFuncSetAttribute(k_level<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_subtree<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_subtree<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
-  CU(cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_sweep<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_sweep<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_gsweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
   CU(cudaFuncSetAttribute(k_gsweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
   {
     int per_sm = 0, sms = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep, kSolveThreads, kSolveSmem));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    c->sweep_blocks = uint32_t(std::max(1, per_sm) * std::max(1, sms));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<5>, kSolveThreads, kSolveSmem));
+    c->sweep_blocks[0] = uint32_t(std::max(1, per_sm) * std::max(1, sms));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<4>, kSolveThreads, kSolveSmem));
+    c->sweep_blocks[1] = uint32_t(std::max(1, per_sm) * std::max(1, sms));
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gsweep<0>, kGThreads, kGSmem));
     c->gsweep_blocks = uint32_t(std::max(1, per_sm) * std::max(1, sms));
   }
@@ -1829,14 +1840,33 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
     if (c >= 7 && c < 14 && (c == 7 || ms < best1)) { best1 = ms; best1_limit = limit; }
     if (c == 0 || ms < best) { best = ms; best_limit = limit; best_mode = b->sweep_mode; best_glimit = glimit; }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   uint32_t status = 0;
   CU(cudaMemcpyAsync(&status, b->status.p, sizeof(status), cudaMemcpyDeviceToHost, st));
   b->sweep_mode = best_mode;
   if (b->n_groups) CU(schedule_groups(b, best_glimit, st));
   std::vector<uint32_t> items = schedule_levels(b, best_limit);
   CU(upload_schedule(b, items, st));
+  if (best_mode != 0) {
+    // the chosen schedule with k_sweep's two compiled forms (five and four
+    // blocks per SM): the faster is kept
+    float occ_ms[2] = {0.f, 0.f};
+    for (int v = 0; v < 2; ++v) {
+      b->sweep_occ = v ? 4u : 5u;
+      launch_sweeps(b, b->dev, st);  // warm-up
+      CU(cudaEventRecord(e0, st));
+      for (int r = 0; r < 3; ++r) launch_sweeps(b, b->dev, st);
+      CU(cudaEventRecord(e1, st));
+      CU(cudaEventSynchronize(e1));
+      CU(cudaEventElapsedTime(&occ_ms[v], e0, e1));
+      occ_ms[v] /= 3.f;
+    }
+    b->sweep_occ = occ_ms[1] < occ_ms[0] ? 4u : 5u;
+    best = std::min(occ_ms[0], occ_ms[1]);
+    b->occ_ms[0] = occ_ms[0];
+    b->occ_ms[1] = occ_ms[1];
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   CU(cudaStreamSynchronize(st));
   if (status & 4u) return fail(ctx, VISTIO_ERR_TIMEOUT, "a bounded wait of the sweeps gave up while tuning");
   b->tuned_ms = best;
@@ -1926,6 +1956,24 @@ vistio_status vistio_batch_set_sweep_mode(vistio_batch* b, uint32_t mode) {
   CU(upload_schedule(b, items, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
   return drop_graphs(b);
+}
+
+vistio_status vistio_batch_set_sweep_blocks(vistio_batch* b, uint32_t blocks_per_sm) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  if (blocks_per_sm != 4 && blocks_per_sm != 5)
+    return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "k_sweep is compiled for 4 or 5 blocks per SM");
+  b->sweep_occ = blocks_per_sm;
+  return drop_graphs(b);
+}
+
+vistio_status vistio_batch_get_sweep_blocks(const vistio_batch* b, uint32_t* blocks_per_sm, float* tuned_ms) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  if (blocks_per_sm) *blocks_per_sm = b->sweep_occ;
+  if (tuned_ms) {
+    tuned_ms[0] = b->occ_ms[0];
+    tuned_ms[1] = b->occ_ms[1];
+  }
+  return VISTIO_OK;
 }
 
 vistio_status vistio_batch_get_sweep_mode(const vistio_batch* b, uint32_t* mode, uint32_t* warp_limit) {
