@@ -324,7 +324,7 @@ vistio_status vistio_batch_get_sweep_mode(const vistio_batch* b, uint32_t* mode,
 /* The dependency-driven sweep kernel (kinds 1 and 2) is compiled for five
  * resident blocks per SM (48 registers per thread) and for four (64, fewer
  * spills); no reference counterpart. vistio_batch_tune times both with the
- * schedule it chose and keeps the faster; without tuning, five. Both give
+ * schedule it chose and keeps the faster; without tuning, four. Both give
  * the same results, bit for bit. get: the form in use and, in tuned_ms (2
  * entries, may be NULL), the tuner's times of the five- and four-block forms
  * (-1 before tuning or for kind 0). */

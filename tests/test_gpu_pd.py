@@ -332,7 +332,7 @@ def test_grouped_sweeps_bit_identical_to_dataflow_and_to_solo(refine):
     for mode, glimit, blocks in (("dataflow", None, 5), ("grouped", 0, 5), ("grouped", 256, 5), ("grouped", 6144, 5),
                                  ("dataflow", None, 4), ("grouped", 256, 4)):
         batch = api.Batch(grouped_batch_solvers(cfg, GROUPED_SIDES))
-        assert batch.sweep_mode()[0] == "grouped" and batch.sweep_blocks()[0] == 5
+        assert batch.sweep_mode()[0] == "grouped" and batch.sweep_blocks()[0] == 4
         batch.set_sweep_mode(mode)
         batch.set_sweep_blocks(blocks)
         assert batch.sweep_blocks()[0] == blocks

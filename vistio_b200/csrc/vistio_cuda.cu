@@ -169,7 +169,7 @@ struct vistio_batch {
   uint32_t tri_per = 2, hinge_per = 1;              // elements per thread of k_tri / k_hinge (autotuned)
   float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
   float occ_ms[2] = {-1.f, -1.f};  // the autotuner's times of the two forms (ms per solve)
-  uint32_t sweep_occ = 5;  // blocks per SM of k_sweep's compiled form (5 or 4), the autotuner's choice
+  uint32_t sweep_occ = 4;  // blocks per SM of k_sweep's compiled form (5 or 4), the autotuner's choice
   // sweeps: 0 = one launch per level (k_level), 1 = dependency-driven (k_sweep),
   // 2 = garment groups' tree bottoms by k_gsweep, the rest by k_sweep
   uint32_t sweep_mode = 1;
