@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--sustain-rate", type=float, default=16.0,
                     help="arrival rate (req/s) of the second served stream, one that one GPU sustains")
     ap.add_argument("--sustain-seconds", type=float, default=10.0, help="its arrival window")
+    ap.add_argument("--pin-sweep", default=None,
+                    help="after tuning, use this sweep configuration instead of the tuner's choice: "
+                         "KIND,WARP_LIMIT,GROUP_LIMIT,BLOCKS_PER_SM,TRIANGLES,HINGES (e.g. grouped,12288,64,4,2,2); "
+                         "for profiling runs, where the tuner's timings are distorted")
     ap.add_argument("--refine", type=int, default=None,
                     help="FP64 refinement sweeps of the global solve (default: the solver's default)")
     return ap.parse_args()
@@ -743,6 +747,15 @@ def main():
     symbolic = {"hits": sym1["hits"] - sym0["hits"], "misses": sym1["misses"] - sym0["misses"],
                 "host_threads": threads}
     tune = batch.tune()  # level schedule picked by timing this batch's sweeps
+    if args.pin_sweep:
+        kind, wl, gl, blocks, tri, hin = args.pin_sweep.split(",")
+        batch.set_sweep_mode(kind)
+        batch.set_warp_limit(int(wl))
+        if kind == "grouped":
+            batch.set_group_limit(int(gl))
+        batch.set_sweep_blocks(int(blocks))
+        batch.set_local_shape(int(tri), int(hin))
+        tune = dict(tune, pinned=args.pin_sweep, sweep_mode=kind)
     info = batch.info()
     V = info["vertices"]
     stream = torch.cuda.ExternalStream(batch.stream())
