@@ -47,6 +47,7 @@ __device__ __forceinline__ void warp_sum_u32(uint32_t& v) {
 // mode 1: the re-detect after the inner loop (writes grad_up / in_contact_up,
 //         reduces active count and max violation).
 __global__ void __launch_bounds__(256) k_detect(BatchDev B, int mode) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   const StepParams& P = *B.prm;
   InstRed& R = B.red[ch.x];
@@ -207,6 +208,7 @@ __global__ void __launch_bounds__(256) k_detect(BatchDev B, int mode) {
 // cylinder.rs:201-262, box_collider.rs:203-251)
 // and the backtracking sum grad . d over free vertices (pd_solver.rs:915-925).
 __global__ void __launch_bounds__(256) k_ccd(BatchDev B) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   const StepParams& P = *B.prm;
   InstRed& R = B.red[ch.x];
@@ -447,6 +449,7 @@ __global__ void __launch_bounds__(256) k_resolve(BatchDev B, ColliderDev C, uint
 
 // Step-size selection (pd_solver.rs:896-932) and x <- x + alpha d on free vertices.
 __global__ void __launch_bounds__(256) k_ipc_update(BatchDev B) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   InstRed& R = B.red[ch.x];
   if (R.al_done) return;
@@ -472,6 +475,7 @@ __global__ void __launch_bounds__(256) k_ipc_update(BatchDev B) {
 
 // Clears the re-detect reductions before the inner loop of an AL pass.
 __global__ void k_al_begin(BatchDev B, uint32_t ninst) {
+  pdl_begin();
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ninst) return;
   InstRed& R = B.red[k];
@@ -483,6 +487,7 @@ __global__ void k_al_begin(BatchDev B, uint32_t ninst) {
 // lambda += mu * grad_up on re-detected contacts when the AL pass did not
 // converge (pd_solver.rs:1005-1018).
 __global__ void __launch_bounds__(256) k_al_end(BatchDev B) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   const StepParams& P = *B.prm;
   InstRed& R = B.red[ch.x];
@@ -499,6 +504,7 @@ __global__ void __launch_bounds__(256) k_al_end(BatchDev B) {
 
 // Per instance: count the pass, record the active contacts, stop or grow mu.
 __global__ void k_al_finish(BatchDev B, uint32_t ninst) {
+  pdl_begin();
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ninst) return;
   const StepParams& P = *B.prm;
@@ -512,6 +518,7 @@ __global__ void k_al_finish(BatchDev B, uint32_t ninst) {
 
 // Zeroes the FP64 self-contact gradient accumulator before a detect.
 __global__ void __launch_bounds__(256) k_clear_grad(BatchDev B) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   if (B.red[ch.x].al_done) return;
   if ((int)threadIdx.x >= ch.z) return;

@@ -15,11 +15,47 @@
 // differences and FP32 sweeps lose accuracy relative to |d|, not to |x|.
 #pragma once
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "setup.h"
 
 namespace vistio {
+
+// Programmatic dependent launch. The step's kernels are launched with the
+// programmatic stream serialization attribute (launch_pdl on the host), so a
+// kernel's blocks may be scheduled while the kernel before it in the stream
+// is still running. Each such kernel calls pdl_begin() first: it waits until
+// the previous kernel has completed and its memory is visible, which orders
+// every earlier kernel too (each of them waited for its own predecessor). A
+// grid of at most kPdlEarlyBlocks blocks then lets the next kernel launch
+// right away, so that kernel's launch overlaps this one's work; larger grids
+// leave the SMs to their own blocks. In a kernel launched without the
+// attribute both instructions do nothing.
+constexpr uint32_t kPdlEarlyBlocks = 148;
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (gridDim.x * gridDim.y * gridDim.z <= kPdlEarlyBlocks) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launches a step kernel with the programmatic stream serialization
+// attribute (the kernel calls pdl_begin() first); records errors as a <<<>>>
+// launch would.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), uint32_t grid, uint32_t block, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 struct InstDev {
   uint32_t vbase, nv;
@@ -371,6 +407,7 @@ __device__ __forceinline__ void tri_project(const BatchDev& B, const InstDev& I,
 // one triangle per thread at five 256-thread blocks per SM.
 constexpr int kTriThreads = 128;
 __global__ void __launch_bounds__(kTriThreads, 8) k_tri(BatchDev B) {
+  pdl_begin();
   int4 ch = B.tri_chunks[blockIdx.x];
   const uint32_t i0 = threadIdx.x, i1 = threadIdx.x + kTriThreads;
   if ((int)i0 >= ch.z) return;
@@ -391,6 +428,7 @@ __global__ void __launch_bounds__(kTriThreads, 8) k_tri(BatchDev B) {
 // The same membrane step with one triangle per thread (a chunk of up to 256
 // triangles on 256 threads, four blocks per SM): the autotuner's other shape.
 __global__ void __launch_bounds__(256, 4) k_tri1(BatchDev B) {
+  pdl_begin();
   int4 ch = B.tri_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) return;
@@ -446,6 +484,7 @@ __device__ __noinline__ float4 hinge_project(float4 st, float2 wr, float3 p0, fl
 // stencils are all (-1, -1, 1, 1) skips their load (16 B per hinge), with the
 // same products.
 __global__ void __launch_bounds__(256) k_hinge(BatchDev B) {
+  pdl_begin();
   int4 ch = B.hinge_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) return;
@@ -459,6 +498,7 @@ __global__ void __launch_bounds__(256) k_hinge(BatchDev B) {
 // Two hinges per thread (128 threads over a chunk of up to 256), both hinges'
 // loads issued before either projection: the autotuner's other shape.
 __global__ void __launch_bounds__(128, 8) k_hinge2(BatchDev B) {
+  pdl_begin();
   int4 ch = B.hinge_chunks[blockIdx.x];
   const uint32_t i0 = threadIdx.x, i1 = threadIdx.x + 128;
   if ((int)i0 >= ch.z) return;
@@ -480,6 +520,7 @@ __global__ void __launch_bounds__(128, 8) k_hinge2(BatchDev B) {
 // terms [- (mu grad_i + lambda_i)], written in solve (permuted) order.
 // keep_rhs also stores r in R0 for a refinement of this iteration's solve.
 __global__ void __launch_bounds__(256) k_gather(BatchDev B, int keep_rhs) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   const InstDev I = B.inst[ch.x];
@@ -1104,6 +1145,7 @@ __device__ __forceinline__ SweepTeams make_teams(float4* smem4, uint64_t* s_bar,
 // kernel boundaries.
 template <int DIR>
 __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_level(BatchDev B, uint32_t off, uint32_t nblock, uint32_t nwarp) {
+  pdl_begin();
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
   __shared__ uint32_t s_abort;
@@ -1127,6 +1169,7 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_level(Bat
 // Bottom subtrees of every instance, one per warp.
 template <int DIR>
 __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_subtree(BatchDev B, uint32_t nitems) {
+  pdl_begin();
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
   __shared__ uint32_t s_abort;
@@ -1276,6 +1319,7 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
 // (the default).
 template <int MINB>
 __global__ void __launch_bounds__(32 * kSolveWarps, MINB) k_sweep(BatchDev B, uint32_t nfwd, uint32_t nbwd) {
+  pdl_begin();
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
   __shared__ uint32_t s_abort, s_unit[2];
@@ -1561,6 +1605,7 @@ __device__ __forceinline__ void g_item(const BatchDev& B, uint2 it, const GLane&
 // last warp out resets the queue.
 template <int DIR>
 __global__ void __launch_bounds__(kGThreads, 2) k_gsweep(BatchDev B, uint32_t nitems) {
+  pdl_begin();
   extern __shared__ float gsm[];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const GLane L{gsm + warp * (kGCols * 3 * 32) + lane};
@@ -1624,6 +1669,7 @@ __global__ void __launch_bounds__(256) k_gpack(BatchDev B, float* g_vals, const 
 }
 
 __global__ void k_red_reset(BatchDev B, uint32_t ninst) {
+  pdl_begin();
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ninst) return;
   InstRed& R = B.red[k];
@@ -1639,6 +1685,7 @@ __global__ void k_red_reset(BatchDev B, uint32_t ninst) {
 // instance's rows are numbered like its vertices, so the vertex chunks cover
 // them. The sweeps then solve A e = W in place and d + e replaces d.
 __global__ void __launch_bounds__(256) k_refine(BatchDev B) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) return;
@@ -1655,6 +1702,7 @@ __global__ void __launch_bounds__(256) k_refine(BatchDev B) {
 
 // d <- d + e between two refinement sweeps.
 __global__ void __launch_bounds__(256) k_accum(BatchDev B) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) return;
@@ -1691,6 +1739,7 @@ __device__ __forceinline__ void update_one(const BatchDev& B, const InstDev& I, 
 // vertices' loads issued before either update: 0.063 -> about 0.043 ms per
 // iteration on 4.05 M vertices (the solve phase 1.315 -> 1.295 ms).
 __global__ void __launch_bounds__(128) k_update(BatchDev B, int do_update, int add_w) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   const InstDev I = B.inst[ch.x];
   InstRed& R = B.red[ch.x];
@@ -1738,6 +1787,7 @@ __global__ void __launch_bounds__(256) k_pack_pos(float* __restrict__ xyz, const
 // save_previous + (IPC) velocity clamp + predict + x <- pred (state.rs:145-169,
 // pd_solver.rs:273-283 and 566-603).
 __global__ void __launch_bounds__(256) k_predict(BatchDev B) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   const InstDev I = B.inst[ch.x];
   const StepParams& P = *B.prm;
@@ -1785,6 +1835,7 @@ __global__ void __launch_bounds__(256) k_predict(BatchDev B) {
 // update_velocities, (IPC) inelastic velocity filter, ground velocities,
 // damping and Rayleigh damping (pd_solver.rs:447-466 and 1027-1147).
 __global__ void __launch_bounds__(256) k_finalize(BatchDev B) {
+  pdl_begin();
   int4 ch = B.vtx_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   const InstDev I = B.inst[ch.x];

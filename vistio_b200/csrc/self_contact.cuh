@@ -104,6 +104,7 @@ __device__ __forceinline__ uint32_t morton_spread10(uint32_t v) {
 // 10 bits per axis within the garment's centroid bounds, as a Morton code
 // below the garment index (so each garment stays in its own range).
 __global__ void __launch_bounds__(1024) k_self_keys(BatchDev B, SelfContactView S) {
+  pdl_begin();
   const SelfInst I = S.inst[blockIdx.x];
   __shared__ float red[6][32];
   float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(1024) k_self_keys(BatchDev B, SelfContactView 
 // (ranks within a block from warp match masks and per-warp digit counts).
 __global__ void __launch_bounds__(256) k_rs_hist(const uint64_t* __restrict__ keys, uint32_t n, uint32_t shift,
                                                  uint32_t* __restrict__ hist, uint32_t nblocks) {
+  pdl_begin();
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
@@ -163,6 +165,7 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t* __restrict__
                                                     uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                     uint32_t n, uint32_t shift, const uint32_t* __restrict__ offs,
                                                     uint32_t nblocks) {
+  pdl_begin();
   __shared__ uint32_t wcnt[8][256];
   __shared__ uint32_t woff[8][256];
   __shared__ uint32_t run[256];
@@ -203,6 +206,7 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t* __restrict__
 // Leaf boxes (bvh.rs:29-43, inflated by the margin) and the level-by-level
 // refit, one block per garment.
 __global__ void __launch_bounds__(1024) k_self_boxes(BatchDev B, SelfContactView S, float margin_arg) {
+  pdl_begin();
   const SelfInst I = S.inst[blockIdx.x];
   if (B.prm->ipc && B.red[blockIdx.x].al_done) return;
   const float margin = margin_arg >= 0.f ? margin_arg : B.prm->thickness;
@@ -286,6 +290,7 @@ __device__ void self_traverse(const SelfContactView& S, const SelfInst& I, uint3
 }
 
 __global__ void __launch_bounds__(256) k_self_count(BatchDev B, SelfContactView S) {
+  pdl_begin();
   int4 ch = B.tri_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) { S.cnt[ch.y + threadIdx.x] = 0; return; }
@@ -298,6 +303,7 @@ __global__ void __launch_bounds__(256) k_self_count(BatchDev B, SelfContactView 
 
 // Exclusive scan of the per-triangle counts (three phases).
 __global__ void __launch_bounds__(kScanBlock) k_scan_local(uint32_t* v, uint32_t n, uint32_t* block_sums) {
+  pdl_begin();
   __shared__ uint32_t sh[kScanBlock];
   uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
   uint32_t x = i < n ? v[i] : 0u;
@@ -313,6 +319,7 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_local(uint32_t* v, uint32_t
   if (threadIdx.x == kScanBlock - 1) block_sums[blockIdx.x] = sh[threadIdx.x];
 }
 __global__ void __launch_bounds__(kScanBlock) k_scan_sums(uint32_t* block_sums, uint32_t nb, uint32_t* total) {
+  pdl_begin();
   __shared__ uint32_t sh[kScanBlock];
   uint32_t carry = 0;
   for (uint32_t b0 = 0; b0 < nb; b0 += kScanBlock) {
@@ -334,11 +341,13 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_sums(uint32_t* block_sums, 
   if (threadIdx.x == 0) total[0] = carry;
 }
 __global__ void __launch_bounds__(kScanBlock) k_scan_add(uint32_t* v, uint32_t n, const uint32_t* block_sums) {
+  pdl_begin();
   uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
   if (i < n) v[i] += block_sums[blockIdx.x];
 }
 
 __global__ void __launch_bounds__(256) k_self_write(BatchDev B, SelfContactView S) {
+  pdl_begin();
   int4 ch = B.tri_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) return;
@@ -590,6 +599,7 @@ __device__ __forceinline__ bool ee_far(V3d<float> p0, V3d<float> p1, V3d<float> 
 }
 
 __global__ void __launch_bounds__(kGradThreads, 4) k_self_grad(BatchDev B, SelfContactView S, int mode) {
+  pdl_begin();
   __shared__ double acc_s[18 * kGradThreads];  // 36 KB: four blocks per SM
   const StepParams& P = *B.prm;
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
@@ -752,6 +762,7 @@ __device__ R vt_ccd(V3d<R> p0, V3d<R> p1, V3d<R> a0, V3d<R> a1, V3d<R> b0, V3d<R
 
 // compute_max_step_size over the last detect's pairs (ccd.rs:238-292).
 __global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactView S) {
+  pdl_begin();
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
     uint2 pr = S.pairs[k];
@@ -787,18 +798,18 @@ inline uint32_t self_ccd_launches() { return 1; }
 inline uint32_t launch_self_sort(const BatchDev& d, const SelfContactView& S, cudaStream_t st) {
   if (!S.leaf_tri) return 0;
   const uint32_t n = uint32_t(S.T);
-  k_self_keys<<<S.ninst, 1024, 0, st>>>(d, S);
+  launch_pdl(k_self_keys, S.ninst, 1024, 0, st, d, S);
   uint64_t* k0 = S.keys;
   uint64_t* k1 = S.keys_alt;
   uint32_t* v0 = S.order;
   uint32_t* v1 = S.order_alt;
   const uint32_t L = 256u * S.sort_blocks;
   for (uint32_t p = 0; p < S.sort_passes; ++p) {
-    k_rs_hist<<<S.sort_blocks, 256, 0, st>>>(k0, n, 8 * p, S.sort_hist, S.sort_blocks);
-    k_scan_local<<<S.sort_scan_blocks, kScanBlock, 0, st>>>(S.sort_hist, L, S.sort_sums);
-    k_scan_sums<<<1, kScanBlock, 0, st>>>(S.sort_sums, S.sort_scan_blocks, S.sort_sums + S.sort_scan_blocks);
-    k_scan_add<<<S.sort_scan_blocks, kScanBlock, 0, st>>>(S.sort_hist, L, S.sort_sums);
-    k_rs_scatter<<<S.sort_blocks, 256, 0, st>>>(k0, v0, k1, v1, n, 8 * p, S.sort_hist, S.sort_blocks);
+    launch_pdl(k_rs_hist, S.sort_blocks, 256, 0, st, k0, n, 8 * p, S.sort_hist, S.sort_blocks);
+    launch_pdl(k_scan_local, S.sort_scan_blocks, kScanBlock, 0, st, S.sort_hist, L, S.sort_sums);
+    launch_pdl(k_scan_sums, 1, kScanBlock, 0, st, S.sort_sums, S.sort_scan_blocks, S.sort_sums + S.sort_scan_blocks);
+    launch_pdl(k_scan_add, S.sort_scan_blocks, kScanBlock, 0, st, S.sort_hist, L, S.sort_sums);
+    launch_pdl(k_rs_scatter, S.sort_blocks, 256, 0, st, k0, v0, k1, v1, n, 8 * p, S.sort_hist, S.sort_blocks);
     std::swap(k0, k1);
     std::swap(v0, v1);
   }
@@ -808,20 +819,20 @@ inline uint32_t launch_self_sort(const BatchDev& d, const SelfContactView& S, cu
 // Returns the kernels launched.
 inline uint32_t launch_self_detect(const BatchDev& d, const SelfContactView& S, uint32_t n_vtx_chunks,
                                    uint32_t n_tri_chunks, int mode, cudaStream_t st) {
-  k_clear_grad<<<n_vtx_chunks, 256, 0, st>>>(d);
+  launch_pdl(k_clear_grad, n_vtx_chunks, 256, 0, st, d);
   const uint32_t ns = launch_self_sort(d, S, st);
-  k_self_boxes<<<S.ninst, 1024, 0, st>>>(d, S, -1.f);  // margin: StepParams::thickness
-  k_self_count<<<n_tri_chunks, 256, 0, st>>>(d, S);
-  k_scan_local<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);
-  k_scan_sums<<<1, kScanBlock, 0, st>>>(S.block_sums, S.scan_blocks, S.npairs);
-  k_scan_add<<<S.scan_blocks, kScanBlock, 0, st>>>(S.cnt, uint32_t(S.T), S.block_sums);
-  k_self_write<<<n_tri_chunks, 256, 0, st>>>(d, S);
-  k_self_grad<<<4 * 148, kGradThreads, 0, st>>>(d, S, mode);
+  launch_pdl(k_self_boxes, S.ninst, 1024, 0, st, d, S, -1.f);  // margin: StepParams::thickness
+  launch_pdl(k_self_count, n_tri_chunks, 256, 0, st, d, S);
+  launch_pdl(k_scan_local, S.scan_blocks, kScanBlock, 0, st, S.cnt, uint32_t(S.T), S.block_sums);
+  launch_pdl(k_scan_sums, 1, kScanBlock, 0, st, S.block_sums, S.scan_blocks, S.npairs);
+  launch_pdl(k_scan_add, S.scan_blocks, kScanBlock, 0, st, S.cnt, uint32_t(S.T), S.block_sums);
+  launch_pdl(k_self_write, n_tri_chunks, 256, 0, st, d, S);
+  launch_pdl(k_self_grad, 4 * 148, kGradThreads, 0, st, d, S, mode);
   return 8 + ns;
 }
 
 inline void launch_self_ccd(const BatchDev& d, const SelfContactView& S, cudaStream_t st) {
-  k_self_ccd<<<4 * 148, 256, 0, st>>>(d, S);
+  launch_pdl(k_self_ccd, 4 * 148, 256, 0, st, d, S);
 }
 
 vistio_status ensure_self_contact(const BatchDev& d, SelfContactDev& S, const std::vector<vistio_solver*>& solvers,

@@ -1105,8 +1105,8 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
 void launch_k_sweep(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
   const uint32_t four = b->sweep_occ == 4 ? 1u : 0u;
   const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks[four]);
-  if (four) k_sweep<4><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
-  else k_sweep<5><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_units_fwd, b->n_units);
+  if (four) launch_pdl(k_sweep<4>, grid, kSolveThreads, kSolveSmem, st, dv, b->n_units_fwd, b->n_units);
+  else launch_pdl(k_sweep<5>, grid, kSolveThreads, kSolveSmem, st, dv, b->n_units_fwd, b->n_units);
 }
 
 // Forward then backward sweep, level by level over the whole batch, in place
@@ -1118,12 +1118,12 @@ uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
     const uint32_t gf = std::min((b->n_gitems_fwd + kGWarps - 1) / kGWarps, b->ctx->gsweep_blocks);
     const uint32_t gb = std::min((b->n_gitems_bwd + kGWarps - 1) / kGWarps, b->ctx->gsweep_blocks);
     uint32_t n = 0;
-    if (gf) { k_gsweep<0><<<gf, kGThreads, kGSmem, st>>>(dv, b->n_gitems_fwd); ++n; }
+    if (gf) { launch_pdl(k_gsweep<0>, gf, kGThreads, kGSmem, st, dv, b->n_gitems_fwd); ++n; }
     if (b->n_units_fwd + b->n_units) {
       launch_k_sweep(b, dv, st);
       ++n;
     }
-    if (gb) { k_gsweep<1><<<gb, kGThreads, kGSmem, st>>>(dv, b->n_gitems_bwd); ++n; }
+    if (gb) { launch_pdl(k_gsweep<1>, gb, kGThreads, kGSmem, st, dv, b->n_gitems_bwd); ++n; }
     return n;
   }
   if (b->sweep_mode == 1 && b->n_units) {
@@ -1132,22 +1132,22 @@ uint32_t launch_sweeps(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
   }
   uint32_t L = uint32_t(b->lvl_off.size()), n = 0;
   const uint32_t sub_grid = (b->n_sub + kSolveWarps - 1) / kSolveWarps;
-  if (sub_grid) { k_subtree<0><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_sub); ++n; }
+  if (sub_grid) { launch_pdl(k_subtree<0>, sub_grid, kSolveThreads, kSolveSmem, st, dv, b->n_sub); ++n; }
   for (uint32_t l = 0; l < L; ++l) {
     uint32_t grid = b->lvl_nb[l] + (b->lvl_nw[l] + kSolveWarps - 1) / kSolveWarps;
-    if (grid) { k_level<0><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
+    if (grid) { launch_pdl(k_level<0>, grid, kSolveThreads, kSolveSmem, st, dv, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
   }
   for (int l = int(L) - 1; l >= 0; --l) {
     uint32_t grid = b->lvl_nb[l] + (b->lvl_nw[l] + kSolveWarps - 1) / kSolveWarps;
-    if (grid) { k_level<1><<<grid, kSolveThreads, kSolveSmem, st>>>(dv, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
+    if (grid) { launch_pdl(k_level<1>, grid, kSolveThreads, kSolveSmem, st, dv, b->lvl_off[l], b->lvl_nb[l], b->lvl_nw[l]); ++n; }
   }
-  if (sub_grid) { k_subtree<1><<<sub_grid, kSolveThreads, kSolveSmem, st>>>(dv, b->n_sub); ++n; }
+  if (sub_grid) { launch_pdl(k_subtree<1>, sub_grid, kSolveThreads, kSolveSmem, st, dv, b->n_sub); ++n; }
   return n;
 }
 
 // One FP64 refinement: W = R0 - A d, then the sweeps solve A e = W in place.
 uint32_t launch_refinement(vistio_batch* b, cudaStream_t st) {
-  k_refine<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+  launch_pdl(k_refine, b->n_vtx_chunks, kElemThreads, 0, st, b->dev);
   return 1 + launch_sweeps(b, b->dev_w, st);
 }
 
@@ -1155,33 +1155,33 @@ uint32_t launch_refinement(vistio_batch* b, cudaStream_t st) {
 // residual sums and (plain step) the position update.
 uint32_t launch_solve(vistio_batch* b, cudaStream_t st, int do_update, uint32_t refine) {
   uint32_t n = 2;
-  k_red_reset<<<(b->ninst + 127) / 128, 128, 0, st>>>(b->dev, b->ninst);
+  launch_pdl(k_red_reset, (b->ninst + 127) / 128, 128, 0, st, b->dev, b->ninst);
   n += launch_sweeps(b, b->dev, st);
   for (uint32_t k = 0; k < refine; ++k) {
-    if (k) { k_accum<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev); ++n; }
+    if (k) { launch_pdl(k_accum, b->n_vtx_chunks, kElemThreads, 0, st, b->dev); ++n; }
     n += launch_refinement(b, st);
   }
-  k_update<<<b->n_vtx_chunks, 128, 0, st>>>(b->dev, do_update, refine > 0);  // two vertices per thread
+  launch_pdl(k_update, b->n_vtx_chunks, 128, 0, st, b->dev, do_update, refine > 0);  // two vertices per thread
   return n;
 }
 
 // The local steps in the shapes the autotuner chose (elements per thread).
 void launch_membrane(vistio_batch* b, cudaStream_t st) {
   if (!b->n_tri_chunks) return;
-  if (b->tri_per == 2) k_tri<<<b->n_tri_chunks, kTriThreads, 0, st>>>(b->dev);
-  else k_tri1<<<b->n_tri_chunks, kElemThreads, 0, st>>>(b->dev);
+  if (b->tri_per == 2) launch_pdl(k_tri, b->n_tri_chunks, kTriThreads, 0, st, b->dev);
+  else launch_pdl(k_tri1, b->n_tri_chunks, kElemThreads, 0, st, b->dev);
 }
 void launch_bending(vistio_batch* b, cudaStream_t st) {
   if (!b->n_hinge_chunks) return;
-  if (b->hinge_per == 2) k_hinge2<<<b->n_hinge_chunks, kElemThreads / 2, 0, st>>>(b->dev);
-  else k_hinge<<<b->n_hinge_chunks, kElemThreads, 0, st>>>(b->dev);
+  if (b->hinge_per == 2) launch_pdl(k_hinge2, b->n_hinge_chunks, kElemThreads / 2, 0, st, b->dev);
+  else launch_pdl(k_hinge, b->n_hinge_chunks, kElemThreads, 0, st, b->dev);
 }
 
 uint32_t launch_plain_iteration(vistio_batch* b, cudaStream_t st, int do_update, uint32_t refine) {
   uint32_t n = 1;
   if (b->n_tri_chunks) { launch_membrane(b, st); ++n; }
   if (b->n_hinge_chunks) { launch_bending(b, st); ++n; }
-  k_gather<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, refine > 0);
+  launch_pdl(k_gather, b->n_vtx_chunks, kElemThreads, 0, st, b->dev, refine > 0);
   return n + launch_solve(b, st, do_update, refine);
 }
 
@@ -1192,7 +1192,7 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
   uint32_t iters = b->cfg.max_iterations;
   uint32_t small_grid = (b->ninst + 127) / 128;
   CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  k_predict<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+  launch_pdl(k_predict, b->n_vtx_chunks, kElemThreads, 0, st, b->dev);
   uint32_t L = 2;
   if (!ipc) {
     // Each PD iteration recomputes its residual from x, so a sweep's error is
@@ -1200,25 +1200,25 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
     for (uint32_t it = 0; it < iters; ++it) L += launch_plain_iteration(b, st, 1, it + 1 == iters ? b->refine : 0);
   } else {
     for (uint32_t al = 0; al < b->cfg.al_max_iterations; ++al) {
-      k_al_begin<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
+      launch_pdl(k_al_begin, small_grid, 128, 0, st, b->dev, b->ninst);
       if (self) L += launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 0, st);
-      k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 0);
+      launch_pdl(k_detect, b->n_vtx_chunks, kElemThreads, 0, st, b->dev, 0);
       for (uint32_t it = 0; it < iters; ++it) {
         // With backtracking (alpha < 1) part of each sweep's error stays in x:
         // every solve is refined.
         L += launch_plain_iteration(b, st, 0, b->refine) + 2;
         if (self) { launch_self_ccd(b->dev, b->self.view(), st); L += self_ccd_launches(); }
-        k_ccd<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
-        k_ipc_update<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+        launch_pdl(k_ccd, b->n_vtx_chunks, kElemThreads, 0, st, b->dev);
+        launch_pdl(k_ipc_update, b->n_vtx_chunks, kElemThreads, 0, st, b->dev);
       }
       if (self) L += launch_self_detect(b->dev, b->self.view(), b->n_vtx_chunks, b->n_tri_chunks, 1, st);
-      k_detect<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev, 1);
-      k_al_end<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
-      k_al_finish<<<small_grid, 128, 0, st>>>(b->dev, b->ninst);
+      launch_pdl(k_detect, b->n_vtx_chunks, kElemThreads, 0, st, b->dev, 1);
+      launch_pdl(k_al_end, b->n_vtx_chunks, kElemThreads, 0, st, b->dev);
+      launch_pdl(k_al_finish, small_grid, 128, 0, st, b->dev, b->ninst);
       L += 5;
     }
   }
-  k_finalize<<<b->n_vtx_chunks, kElemThreads, 0, st>>>(b->dev);
+  launch_pdl(k_finalize, b->n_vtx_chunks, kElemThreads, 0, st, b->dev);
   cudaError_t e = cudaStreamEndCapture(st, &g);
   if (e != cudaSuccess) return fail(ctx, VISTIO_ERR_GPU, std::string("graph capture: ") + cudaGetErrorString(e));
   e = cudaGraphInstantiate(out, g, 0);
