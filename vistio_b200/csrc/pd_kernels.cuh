@@ -1201,6 +1201,11 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_subtree(B
 // bounded; a wait that gives up sets status bit 4, and every later wait
 // returns at once, so a failing sweep ends quickly with the error recorded.
 //
+// Items per unit of bottom subtrees or warp supernodes: the block's eight
+// warps take them one at a time, each its next item as soon as it is done
+// with the last, so a unit lasts about two items rather than the slowest of
+// eight.
+constexpr uint32_t kUnitItems = 16;
 // SweepUnit (uint2): x = kind | count << 2; kind 0: `count` bottom subtrees
 // from sub_items[y]; kind 1: the top supernode y with the whole block; kind
 // 2: `count` top supernodes, one per warp, from lvl_items[y].
@@ -1255,7 +1260,7 @@ __device__ __forceinline__ void dep_leave(const BatchDev& B, uint32_t k, uint32_
 
 // One work unit of the dependency-driven sweeps (the whole block runs it).
 template <int DIR>
-__device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uint2 u, bool ipc) {
+__device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uint2 u, bool ipc, uint32_t* next) {
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t kind = u.x & 3u, count = u.x >> 2;
   if (kind == 1) {
@@ -1273,31 +1278,39 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
       __threadfence();
       dep_leave<DIR>(B, k, 0, 1);
     }
-  } else if (warp < count) {
-    if (kind == 0) {
-      const uint2 it = B.sub_items[u.y + warp];
-      if (ipc && B.red[B.sn[it.x].inst].al_done) return;
-      if (DIR == 1 && lane == 0) dep_enter<1>(B, it.y);
-      __syncwarp();
-      subtree_sweep<DIR>(B, t.wt, it.x, it.y);
-      __syncwarp();
-      if (DIR == 0 && lane == 0) {
-        __threadfence();
-        dep_leave<0>(B, it.y, 0, 1);
+  } else {
+    // warp w takes item w, then the unit's next free item until none is left
+    for (uint32_t i = warp; i < count;) {
+      if (kind == 0) {
+        const uint2 it = B.sub_items[u.y + i];
+        if (!(ipc && B.red[B.sn[it.x].inst].al_done)) {
+          if (DIR == 1 && lane == 0) dep_enter<1>(B, it.y);
+          __syncwarp();
+          subtree_sweep<DIR>(B, t.wt, it.x, it.y);
+          __syncwarp();
+          if (DIR == 0 && lane == 0) {
+            __threadfence();
+            dep_leave<0>(B, it.y, 0, 1);
+          }
+        }
+      } else {
+        const uint32_t k = (DIR == 0 ? B.df_items_fwd : B.lvl_items)[u.y + i];
+        const SnDev S = B.sn[k];
+        if (!(ipc && B.red[S.inst].al_done)) {
+          if (lane == 0) dep_enter<DIR>(B, k);
+          __syncwarp();
+          if (DIR == 0) sn_forward(B, t.wt, S);
+          else sn_backward(B, t.wt, S);
+          __syncwarp();
+          if (lane == 0) {
+            __threadfence();
+            dep_leave<DIR>(B, k, 0, 1);
+          }
+        }
       }
-    } else {
-      const uint32_t k = (DIR == 0 ? B.df_items_fwd : B.lvl_items)[u.y + warp];
-      const SnDev S = B.sn[k];
-      if (ipc && B.red[S.inst].al_done) return;
-      if (lane == 0) dep_enter<DIR>(B, k);
-      __syncwarp();
-      if (DIR == 0) sn_forward(B, t.wt, S);
-      else sn_backward(B, t.wt, S);
-      __syncwarp();
-      if (lane == 0) {
-        __threadfence();
-        dep_leave<DIR>(B, k, 0, 1);
-      }
+      uint32_t nxt = 0;
+      if (lane == 0) nxt = atomicAdd(next, 1u);
+      i = __shfl_sync(0xffffffffu, nxt, 0);
     }
   }
 }
@@ -1322,7 +1335,7 @@ __global__ void __launch_bounds__(32 * kSolveWarps, MINB) k_sweep(BatchDev B, ui
   pdl_begin();
   extern __shared__ float4 smem4[];
   __shared__ uint64_t s_bar[kSolveWarps + 1];
-  __shared__ uint32_t s_abort, s_unit[2];
+  __shared__ uint32_t s_abort, s_unit[2], s_next[2];
   SweepTeams t = make_teams(smem4, s_bar, &s_abort);
   const uint32_t tid = threadIdx.x;
   const bool ipc = B.prm->ipc != 0;
@@ -1331,15 +1344,19 @@ __global__ void __launch_bounds__(32 * kSolveWarps, MINB) k_sweep(BatchDev B, ui
   // holds one unit it has not started, which cannot deadlock: the smallest
   // unfinished unit is always one that a block is working on (a block takes
   // its next unit after its current one), and it waits only for smaller ones.
-  if (tid == 0) s_unit[0] = atomicAdd(B.df_queue, 1u);
+  if (tid == 0) {
+    s_unit[0] = atomicAdd(B.df_queue, 1u);
+    s_next[0] = kSolveWarps;  // the first item a warp takes after its own
+  }
   for (uint32_t it = 0;; ++it) {
     __syncthreads();  // every warp is done with the previous unit; s_unit[it & 1] is written
     const uint32_t q = s_unit[it & 1];
     if (q >= nfwd + nbwd) break;
     uint32_t next = 0;
     if (tid == 0) next = atomicAdd(B.df_queue, 1u);
-    if (q < nfwd) sweep_unit<0>(B, t, B.df_units_fwd[q], ipc);
-    else sweep_unit<1>(B, t, B.df_units[nbwd - 1 - (q - nfwd)], ipc);
+    if (tid == 0) s_next[(it + 1) & 1] = kSolveWarps;  // the next unit's counter (unused until the barrier)
+    if (q < nfwd) sweep_unit<0>(B, t, B.df_units_fwd[q], ipc, &s_next[it & 1]);
+    else sweep_unit<1>(B, t, B.df_units[nbwd - 1 - (q - nfwd)], ipc, &s_next[it & 1]);
     if (tid == 0) s_unit[(it + 1) & 1] = next;  // read by all after the next barrier
   }
   if (tid == 0) {

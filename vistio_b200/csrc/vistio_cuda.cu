@@ -275,13 +275,13 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
   // k_sweep units in forward order: bottom subtrees by eight, then each level's
   // block supernodes one by one and its warp supernodes by eight
   b->units_host.clear();
-  for (uint32_t q = 0; q < nsub; q += kSolveWarps)
-    b->units_host.push_back(make_uint2(0u | (std::min(kSolveWarps, nsub - q) << 2), q));
+  for (uint32_t q = 0; q < nsub; q += kUnitItems)
+    b->units_host.push_back(make_uint2(0u | (std::min(kUnitItems, nsub - q) << 2), q));
   for (uint32_t l = 0; l < L; ++l) {
     const uint32_t off = b->lvl_off[l], nb = b->lvl_nb[l], nw = b->lvl_nw[l];
     for (uint32_t i = 0; i < nb; ++i) b->units_host.push_back(make_uint2(1u | (1u << 2), items[off + i]));
-    for (uint32_t i = 0; i < nw; i += kSolveWarps)
-      b->units_host.push_back(make_uint2(2u | (std::min(kSolveWarps, nw - i) << 2), off + nb + i));
+    for (uint32_t i = 0; i < nw; i += kUnitItems)
+      b->units_host.push_back(make_uint2(2u | (std::min(kUnitItems, nw - i) << 2), off + nb + i));
   }
   b->n_units = uint32_t(b->units_host.size());
   // The forward sweep's critical path runs from the deepest supernodes of the
@@ -301,15 +301,15 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
     }
     b->units_fwd_host.clear();
     b->items_fwd_host.clear();
-    for (uint32_t q = 0; q < nsub; q += kSolveWarps)
-      b->units_fwd_host.push_back(make_uint2(0u | (std::min(kSolveWarps, nsub - q) << 2), q));
+    for (uint32_t q = 0; q < nsub; q += kUnitItems)
+      b->units_fwd_host.push_back(make_uint2(0u | (std::min(kUnitItems, nsub - q) << 2), q));
     for (uint32_t d = D; d-- > 0;) {
       std::stable_sort(dblk[d].begin(), dblk[d].end(), heavier);
       std::stable_sort(dwrp[d].begin(), dwrp[d].end(), heavier);
       for (uint32_t k : dblk[d]) b->units_fwd_host.push_back(make_uint2(1u | (1u << 2), k));
-      for (size_t i = 0; i < dwrp[d].size(); i += kSolveWarps) {
+      for (size_t i = 0; i < dwrp[d].size(); i += kUnitItems) {
         const uint32_t off = uint32_t(b->items_fwd_host.size());
-        const uint32_t cnt = uint32_t(std::min<size_t>(kSolveWarps, dwrp[d].size() - i));
+        const uint32_t cnt = uint32_t(std::min<size_t>(kUnitItems, dwrp[d].size() - i));
         b->items_fwd_host.insert(b->items_fwd_host.end(), dwrp[d].begin() + i, dwrp[d].begin() + i + cnt);
         b->units_fwd_host.push_back(make_uint2(2u | (cnt << 2), off));
       }
