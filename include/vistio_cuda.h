@@ -321,13 +321,14 @@ vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit);
 vistio_status vistio_batch_set_sweep_mode(vistio_batch* b, uint32_t mode);
 /* The sweep kind and warp-item limit in use. */
 vistio_status vistio_batch_get_sweep_mode(const vistio_batch* b, uint32_t* mode, uint32_t* warp_limit);
-/* The dependency-driven sweep kernel (kinds 1 and 2) is compiled for five
- * resident blocks per SM (48 registers per thread) and for four (64, fewer
- * spills); no reference counterpart. vistio_batch_tune times both with the
- * schedule it chose and keeps the faster; without tuning, four. Both give
- * the same results, bit for bit. get: the form in use and, in tuned_ms (2
- * entries, may be NULL), the tuner's times of the five- and four-block forms
- * (-1 before tuning or for kind 0). */
+/* The dependency-driven sweep kernel (kinds 1 and 2) is compiled in three
+ * forms, named by resident blocks per SM: 5 and 4 (eight-warp blocks, 48 and
+ * 64 registers per thread) and 2 (sixteen-warp blocks, whose units hold twice
+ * as many items); no reference counterpart. vistio_batch_tune times the three
+ * with the schedule it chose and keeps the fastest; without tuning, 2 for a
+ * batch of at most 8 garments, else 4. All give the same results, bit for
+ * bit. get: the form in use and, in tuned_ms (3 entries, may be NULL), the
+ * tuner's times of the forms 5, 4 and 2 (-1 before tuning or for kind 0). */
 vistio_status vistio_batch_set_sweep_blocks(vistio_batch* b, uint32_t blocks_per_sm);
 vistio_status vistio_batch_get_sweep_blocks(const vistio_batch* b, uint32_t* blocks_per_sm, float* tuned_ms);
 /* The device factorization done when the batch was created (the garments

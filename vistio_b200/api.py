@@ -501,15 +501,16 @@ class Batch:
         L.check(L.lib().vistio_batch_set_sweep_mode(self.h, self.SWEEP_MODES.index(mode)), self.ctx.h)
 
     def set_sweep_blocks(self, blocks_per_sm: int):
-        """Compiled form of the dependency-driven sweep kernel: 5 or 4
-        resident blocks per SM (bit-identical results)."""
+        """Compiled form of the dependency-driven sweep kernel, by resident
+        blocks per SM: 5 or 4 (eight-warp blocks) or 2 (sixteen-warp blocks);
+        bit-identical results."""
         L.check(L.lib().vistio_batch_set_sweep_blocks(self.h, int(blocks_per_sm)), self.ctx.h)
 
     def sweep_blocks(self) -> tuple:
         """(blocks per SM of the form in use, {form: the tuner's ms per solve})."""
-        v, ms = C.c_uint32(), (C.c_float * 2)()
+        v, ms = C.c_uint32(), (C.c_float * 3)()
         L.check(L.lib().vistio_batch_get_sweep_blocks(self.h, C.byref(v), ms), self.ctx.h)
-        return v.value, {"5": float(ms[0]), "4": float(ms[1])}
+        return v.value, {"5": float(ms[0]), "4": float(ms[1]), "2": float(ms[2])}
 
     def sweep_mode(self) -> tuple:
         """(sweep kind, warp-item limit) in use."""

@@ -1111,17 +1111,24 @@ __device__ __forceinline__ void subtree_sweep(const BatchDev& B, Team& tm, uint3
   for (uint32_t c = tm.rank; c < nc; c += tm.size) Yg[c0 + c] = acc[c];
 }
 
-// Shared-memory teams of one sweep kernel block: eight warp teams and, over
-// the same memory, one block team.
+// Shared-memory teams of one sweep kernel block: one team per warp and, over
+// the same memory, the block team, and bn: the block supernodes' backward
+// team, the first eight warps' worth of threads and buffer (in an eight-warp
+// block the same as bt, on its own mbarrier). The backward step of a block
+// supernode splits each column's sum over parts of the rows, and how depends
+// on the team's width and buffer; with bn it is the same in every compiled
+// form of k_sweep, and the results stay bit-identical. (The forward step's
+// sums do not depend on the team.)
 struct SweepTeams {
-  Team wt, bt;
+  Team wt, bt, bn;
 };
+template <uint32_t NW = kSolveWarps>
 __device__ __forceinline__ SweepTeams make_teams(float4* smem4, uint64_t* s_bar, uint32_t* s_abort) {
-  constexpr uint32_t NW = kSolveWarps, NT = 32 * kSolveWarps;
+  constexpr uint32_t NT = 32 * NW;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float* fbuf = reinterpret_cast<float*>(smem4);
   float4* vbuf = smem4 + NW * kWarpFloats / 4;
-  if (tid <= NW) mbar_init(&s_bar[tid]);
+  if (tid <= NW + 1) mbar_init(&s_bar[tid]);
   if (tid == 0) *s_abort = 0u;
   mbar_fence_init();
   __syncthreads();
@@ -1131,9 +1138,14 @@ __device__ __forceinline__ SweepTeams make_teams(float4* smem4, uint64_t* s_bar,
               false, &s_bar[warp], 0u, s_abort};
   // block team: all warps' buffers; the vector slots split kMaxSupernode /
   // kMaxSupernode / NT (xg doubles as the NT-entry reduction buffer).
-  static_assert(3 * kWarpVec * kSolveWarps >= 2 * kMaxSupernode + NT, "block-team vector slots");
+  static_assert(3 * kWarpVec * NW >= 2 * kMaxSupernode + NT, "block-team vector slots");
   t.bt = Team{tid, NT, fbuf, NW * kWarpFloats, vbuf, vbuf + kMaxSupernode, vbuf + 2 * kMaxSupernode, kMaxSupernode, NT,
               true, &s_bar[NW], 0u, s_abort};
+  // threads beyond the first eight warps take no part in bn's loops (their
+  // rank is beyond its size) but keep its barriers
+  constexpr uint32_t NR = 32 * kSolveWarps;
+  t.bn = Team{tid, NR, fbuf, kSolveWarps * kWarpFloats, vbuf, vbuf + kMaxSupernode, vbuf + 2 * kMaxSupernode,
+              kMaxSupernode, NR, true, &s_bar[NW + 1], 0u, s_abort};
   return t;
 }
 
@@ -1147,7 +1159,7 @@ template <int DIR>
 __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_level(BatchDev B, uint32_t off, uint32_t nblock, uint32_t nwarp) {
   pdl_begin();
   extern __shared__ float4 smem4[];
-  __shared__ uint64_t s_bar[kSolveWarps + 1];
+  __shared__ uint64_t s_bar[kSolveWarps + 2];
   __shared__ uint32_t s_abort;
   SweepTeams t = make_teams(smem4, s_bar, &s_abort);
   const bool ipc = B.prm->ipc != 0;
@@ -1171,7 +1183,7 @@ template <int DIR>
 __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_subtree(BatchDev B, uint32_t nitems) {
   pdl_begin();
   extern __shared__ float4 smem4[];
-  __shared__ uint64_t s_bar[kSolveWarps + 1];
+  __shared__ uint64_t s_bar[kSolveWarps + 2];
   __shared__ uint32_t s_abort;
   SweepTeams t = make_teams(smem4, s_bar, &s_abort);
   uint32_t q = blockIdx.x * kSolveWarps + (threadIdx.x >> 5);
@@ -1206,6 +1218,10 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveMinBlocks) k_subtree(B
 // with the last, so a unit lasts about two items rather than the slowest of
 // eight.
 constexpr uint32_t kUnitItems = 16;
+// The sixteen-warp form of k_sweep: its units hold twice as many items, and
+// untuned batches of at most this many garments use it.
+constexpr uint32_t kWideWarps = 16;
+constexpr uint32_t kWideMaxInstances = 8;
 // SweepUnit (uint2): x = kind | count << 2; kind 0: `count` bottom subtrees
 // from sub_items[y]; kind 1: the top supernode y with the whole block; kind
 // 2: `count` top supernodes, one per warp, from lvl_items[y].
@@ -1270,7 +1286,7 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
     if (tid == 0) dep_enter<DIR>(B, k);
     __syncthreads();
     if (DIR == 0) sn_forward(B, t.bt, S);
-    else sn_backward(B, t.bt, S);
+    else sn_backward(B, t.bn, S);
     // one fence after the barrier covers the whole block's writes (the fence
     // is cumulative over what the barrier ordered before it); then signal
     __syncthreads();
@@ -1323,20 +1339,25 @@ __device__ __forceinline__ void sweep_unit(const BatchDev& B, SweepTeams& t, uin
 // backward sweep starts as soon as its own forward sweep ends, beside the
 // forward tail of the others. The last block out resets the queue.
 //
-// Compiled for two occupancies, MINB resident blocks per SM: five (48
-// registers, 68 bytes per thread spilled) or four (64 registers, 28 bytes).
-// With four, each unit is shorter; with five, more units are in flight. The autotuner
-// times both on the batch: on 512 sheets of 8 topologies they tie, on 64
-// contact drapes, whose solve follows the longest garments' chains, four
-// blocks shorten the solve by 6%, and on single garments the step by 5-7%
-// (the default).
-template <int MINB>
-__global__ void __launch_bounds__(32 * kSolveWarps, MINB) k_sweep(BatchDev B, uint32_t nfwd, uint32_t nbwd) {
+// Compiled in three forms, NW warps per block and MINB resident blocks per
+// SM: eight warps at five blocks (48 registers, 68 bytes per thread spilled)
+// or four (64 registers, 28 bytes), and sixteen warps at two blocks (64
+// registers; units of twice as many items). With four eight-warp blocks each
+// unit is shorter than with five; with five, more units are in flight; with
+// sixteen warps a block supernode has twice the threads and staging buffer,
+// which shortens the chains of a single garment's tree. The autotuner times
+// the forms on the batch: on 512 sheets of 8 topologies the eight-warp forms
+// tie and sixteen warps are 14% slower; on 64 contact drapes four eight-warp
+// blocks are 6% faster than five; on single garments sixteen warps shorten
+// the step by 4-12%. Untuned batches take sixteen warps for at most
+// kWideMaxInstances garments, else four eight-warp blocks.
+template <int MINB, uint32_t NW = kSolveWarps>
+__global__ void __launch_bounds__(32 * NW, MINB) k_sweep(BatchDev B, uint32_t nfwd, uint32_t nbwd) {
   pdl_begin();
   extern __shared__ float4 smem4[];
-  __shared__ uint64_t s_bar[kSolveWarps + 1];
+  __shared__ uint64_t s_bar[NW + 2];
   __shared__ uint32_t s_abort, s_unit[2], s_next[2];
-  SweepTeams t = make_teams(smem4, s_bar, &s_abort);
+  SweepTeams t = make_teams<NW>(smem4, s_bar, &s_abort);
   const uint32_t tid = threadIdx.x;
   const bool ipc = B.prm->ipc != 0;
   // Thread 0 takes the next unit from the queue while the block works on the
@@ -1346,7 +1367,7 @@ __global__ void __launch_bounds__(32 * kSolveWarps, MINB) k_sweep(BatchDev B, ui
   // its next unit after its current one), and it waits only for smaller ones.
   if (tid == 0) {
     s_unit[0] = atomicAdd(B.df_queue, 1u);
-    s_next[0] = kSolveWarps;  // the first item a warp takes after its own
+    s_next[0] = NW;  // the first item a warp takes after its own
   }
   for (uint32_t it = 0;; ++it) {
     __syncthreads();  // every warp is done with the previous unit; s_unit[it & 1] is written
@@ -1354,7 +1375,7 @@ __global__ void __launch_bounds__(32 * kSolveWarps, MINB) k_sweep(BatchDev B, ui
     if (q >= nfwd + nbwd) break;
     uint32_t next = 0;
     if (tid == 0) next = atomicAdd(B.df_queue, 1u);
-    if (tid == 0) s_next[(it + 1) & 1] = kSolveWarps;  // the next unit's counter (unused until the barrier)
+    if (tid == 0) s_next[(it + 1) & 1] = NW;  // the next unit's counter (unused until the barrier)
     if (q < nfwd) sweep_unit<0>(B, t, B.df_units_fwd[q], ipc, &s_next[it & 1]);
     else sweep_unit<1>(B, t, B.df_units[nbwd - 1 - (q - nfwd)], ipc, &s_next[it & 1]);
     if (tid == 0) s_unit[(it + 1) & 1] = next;  // read by all after the next barrier

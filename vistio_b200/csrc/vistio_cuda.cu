@@ -35,7 +35,7 @@ struct vistio_ctx {
   std::mutex mu;
   int refs = 0;
   bool closed = false;
-  uint32_t sweep_blocks[2] = {0, 0};  // resident k_sweep blocks on this device (SMs x blocks per SM): five- and four-block forms
+  uint32_t sweep_blocks[3] = {0, 0, 0};  // resident k_sweep blocks on this device: the five- and four-block eight-warp forms, the sixteen-warp form
   uint32_t gsweep_blocks = 0;  // resident k_gsweep blocks
 };
 
@@ -82,6 +82,7 @@ namespace {
 
 constexpr int kElemThreads = 256;
 constexpr int kSolveThreads = 32 * kSolveWarps;
+constexpr uint32_t kWideSmem = kWideWarps * (kWarpFloats * 4 + 3 * kWarpVec * 16);
 
 thread_local std::string g_tls_error;
 
@@ -168,8 +169,11 @@ struct vistio_batch {
   uint32_t warp_limit = kWarpItemLimit;             // s (s + m) limit of a warp item
   uint32_t tri_per = 2, hinge_per = 1;              // elements per thread of k_tri / k_hinge (autotuned)
   float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
-  float occ_ms[2] = {-1.f, -1.f};  // the autotuner's times of the two forms (ms per solve)
-  uint32_t sweep_occ = 4;  // blocks per SM of k_sweep's compiled form (5 or 4), the autotuner's choice
+  float occ_ms[3] = {-1.f, -1.f, -1.f};  // the autotuner's times of the three forms (ms per solve)
+  // k_sweep's compiled form, by blocks per SM: 5 or 4 (eight warps), 2
+  // (sixteen warps, units of 2 kUnitItems items); the autotuner's choice
+  uint32_t sweep_occ = 4;
+  uint32_t unit_items = kUnitItems;  // items per subtree or warp-supernode unit of the schedule
   // sweeps: 0 = one launch per level (k_level), 1 = dependency-driven (k_sweep),
   // 2 = garment groups' tree bottoms by k_gsweep, the rest by k_sweep
   uint32_t sweep_mode = 1;
@@ -275,13 +279,14 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
   // k_sweep units in forward order: bottom subtrees by eight, then each level's
   // block supernodes one by one and its warp supernodes by eight
   b->units_host.clear();
-  for (uint32_t q = 0; q < nsub; q += kUnitItems)
-    b->units_host.push_back(make_uint2(0u | (std::min(kUnitItems, nsub - q) << 2), q));
+  const uint32_t UI = b->unit_items;
+  for (uint32_t q = 0; q < nsub; q += UI)
+    b->units_host.push_back(make_uint2(0u | (std::min(UI, nsub - q) << 2), q));
   for (uint32_t l = 0; l < L; ++l) {
     const uint32_t off = b->lvl_off[l], nb = b->lvl_nb[l], nw = b->lvl_nw[l];
     for (uint32_t i = 0; i < nb; ++i) b->units_host.push_back(make_uint2(1u | (1u << 2), items[off + i]));
-    for (uint32_t i = 0; i < nw; i += kUnitItems)
-      b->units_host.push_back(make_uint2(2u | (std::min(kUnitItems, nw - i) << 2), off + nb + i));
+    for (uint32_t i = 0; i < nw; i += UI)
+      b->units_host.push_back(make_uint2(2u | (std::min(UI, nw - i) << 2), off + nb + i));
   }
   b->n_units = uint32_t(b->units_host.size());
   // The forward sweep's critical path runs from the deepest supernodes of the
@@ -301,15 +306,15 @@ std::vector<uint32_t> schedule_levels(vistio_batch* b, uint32_t limit) {
     }
     b->units_fwd_host.clear();
     b->items_fwd_host.clear();
-    for (uint32_t q = 0; q < nsub; q += kUnitItems)
-      b->units_fwd_host.push_back(make_uint2(0u | (std::min(kUnitItems, nsub - q) << 2), q));
+    for (uint32_t q = 0; q < nsub; q += UI)
+      b->units_fwd_host.push_back(make_uint2(0u | (std::min(UI, nsub - q) << 2), q));
     for (uint32_t d = D; d-- > 0;) {
       std::stable_sort(dblk[d].begin(), dblk[d].end(), heavier);
       std::stable_sort(dwrp[d].begin(), dwrp[d].end(), heavier);
       for (uint32_t k : dblk[d]) b->units_fwd_host.push_back(make_uint2(1u | (1u << 2), k));
-      for (size_t i = 0; i < dwrp[d].size(); i += kUnitItems) {
+      for (size_t i = 0; i < dwrp[d].size(); i += UI) {
         const uint32_t off = uint32_t(b->items_fwd_host.size());
-        const uint32_t cnt = uint32_t(std::min<size_t>(kUnitItems, dwrp[d].size() - i));
+        const uint32_t cnt = uint32_t(std::min<size_t>(UI, dwrp[d].size() - i));
         b->items_fwd_host.insert(b->items_fwd_host.end(), dwrp[d].begin() + i, dwrp[d].begin() + i + cnt);
         b->units_fwd_host.push_back(make_uint2(2u | (cnt << 2), off));
       }
@@ -649,6 +654,10 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
   b->ctx_ref.bind(ctx);
   b->solvers.assign(solvers, solvers + n);
   b->ninst = n;
+  // untuned: sixteen-warp sweep blocks for a few garments (their solves are
+  // one tree's chains), four eight-warp blocks per SM otherwise
+  b->sweep_occ = n <= kWideMaxInstances ? 2u : 4u;
+  b->unit_items = b->sweep_occ == 2 ? 2 * kUnitItems : kUnitItems;
   b->cfg = solvers[0]->cfg;
   std::vector<InstDev> hi(n);
   std::vector<uint64_t> vb(n), vc(n), tb(n), tc(n), hb(n), hc(n);
@@ -1103,10 +1112,12 @@ StepParams make_params(const vistio_solver_config& c, float dt, const vistio_con
 
 // One k_sweep launch over the batch's units in the chosen compiled form.
 void launch_k_sweep(vistio_batch* b, const BatchDev& dv, cudaStream_t st) {
-  const uint32_t four = b->sweep_occ == 4 ? 1u : 0u;
-  const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks[four]);
-  if (four) launch_pdl(k_sweep<4>, grid, kSolveThreads, kSolveSmem, st, dv, b->n_units_fwd, b->n_units);
-  else launch_pdl(k_sweep<5>, grid, kSolveThreads, kSolveSmem, st, dv, b->n_units_fwd, b->n_units);
+  const uint32_t form = b->sweep_occ == 5 ? 0u : b->sweep_occ == 4 ? 1u : 2u;
+  const uint32_t grid = std::min(b->n_units_fwd + b->n_units, b->ctx->sweep_blocks[form]);
+  if (form == 0) launch_pdl(k_sweep<5>, grid, kSolveThreads, kSolveSmem, st, dv, b->n_units_fwd, b->n_units);
+  else if (form == 1) launch_pdl(k_sweep<4>, grid, kSolveThreads, kSolveSmem, st, dv, b->n_units_fwd, b->n_units);
+  else
+    launch_pdl(k_sweep<2, kWideWarps>, grid, 32 * kWideWarps, kWideSmem, st, dv, b->n_units_fwd, b->n_units);
 }
 
 // Forward then backward sweep, level by level over the whole batch, in place
@@ -1370,6 +1381,7 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
   CU(cudaFuncSetAttribute(k_subtree<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_sweep<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
   CU(cudaFuncSetAttribute(k_sweep<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+  CU(cudaFuncSetAttribute(k_sweep<2, kWideWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWideSmem));
   CU(cudaFuncSetAttribute(k_gsweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
   CU(cudaFuncSetAttribute(k_gsweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
   {
@@ -1379,6 +1391,8 @@ vistio_status vistio_ctx_create(int32_t device, vistio_ctx** out) {
     c->sweep_blocks[0] = uint32_t(std::max(1, per_sm) * std::max(1, sms));
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<4>, kSolveThreads, kSolveSmem));
     c->sweep_blocks[1] = uint32_t(std::max(1, per_sm) * std::max(1, sms));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<2, kWideWarps>, 32 * kWideWarps, kWideSmem));
+    c->sweep_blocks[2] = uint32_t(std::max(1, per_sm) * std::max(1, sms));
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gsweep<0>, kGThreads, kGSmem));
     c->gsweep_blocks = uint32_t(std::max(1, per_sm) * std::max(1, sms));
   }
@@ -1816,6 +1830,8 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
   float best = 0.f, best1 = 0.f;
   uint32_t best_limit = b->warp_limit, best_mode = b->sweep_mode, best_glimit = b->group_limit;
   uint32_t best1_limit = kWarpItemLimit;  // the fastest limit of kind 1: kind 2 runs its rest at it
+  b->sweep_occ = 4;
+  b->unit_items = kUnitItems;
   for (int c = 0; c < 21; ++c) {
     const uint32_t glimit = c >= 14 ? kGroupTuneLimits[c - 14] : b->group_limit;
     if (c >= 14 && (!b->n_groups || glimit > best1_limit)) {  // no groups, or a limit kind 1's rest could not match
@@ -1847,11 +1863,17 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
   std::vector<uint32_t> items = schedule_levels(b, best_limit);
   CU(upload_schedule(b, items, st));
   if (best_mode != 0) {
-    // the chosen schedule with k_sweep's two compiled forms (five and four
-    // blocks per SM): the faster is kept
-    float occ_ms[2] = {0.f, 0.f};
-    for (int v = 0; v < 2; ++v) {
-      b->sweep_occ = v ? 4u : 5u;
+    // the chosen schedule with k_sweep's three compiled forms (five and four
+    // eight-warp blocks per SM, two sixteen-warp blocks with units of twice
+    // the items): the fastest is kept
+    float occ_ms[3] = {0.f, 0.f, 0.f};
+    for (int v = 0; v < 3; ++v) {
+      b->sweep_occ = v == 0 ? 5u : v == 1 ? 4u : 2u;
+      if (v == 2) {
+        b->unit_items = 2 * kUnitItems;
+        std::vector<uint32_t> wide = schedule_levels(b, best_limit);
+        CU(upload_schedule(b, wide, st));
+      }
       launch_sweeps(b, b->dev, st);  // warm-up
       CU(cudaEventRecord(e0, st));
       for (int r = 0; r < 3; ++r) launch_sweeps(b, b->dev, st);
@@ -1860,10 +1882,19 @@ vistio_status vistio_batch_tune(vistio_batch* b, uint32_t* chosen_limit, float* 
       CU(cudaEventElapsedTime(&occ_ms[v], e0, e1));
       occ_ms[v] /= 3.f;
     }
-    b->sweep_occ = occ_ms[1] < occ_ms[0] ? 4u : 5u;
-    best = std::min(occ_ms[0], occ_ms[1]);
-    b->occ_ms[0] = occ_ms[0];
-    b->occ_ms[1] = occ_ms[1];
+    int bv = 0;
+    for (int v = 1; v < 3; ++v)
+      if (occ_ms[v] < occ_ms[bv]) bv = v;
+    b->sweep_occ = bv == 0 ? 5u : bv == 1 ? 4u : 2u;
+    if (bv != 2) {  // back to eight-warp units
+      b->unit_items = kUnitItems;
+      std::vector<uint32_t> narrow = schedule_levels(b, best_limit);
+      CU(upload_schedule(b, narrow, st));
+    }
+    best = occ_ms[bv];
+    for (int v = 0; v < 3; ++v) b->occ_ms[v] = occ_ms[v];
+  } else {
+    b->sweep_occ = 4;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1960,9 +1991,17 @@ vistio_status vistio_batch_set_sweep_mode(vistio_batch* b, uint32_t mode) {
 
 vistio_status vistio_batch_set_sweep_blocks(vistio_batch* b, uint32_t blocks_per_sm) {
   if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
-  if (blocks_per_sm != 4 && blocks_per_sm != 5)
-    return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "k_sweep is compiled for 4 or 5 blocks per SM");
+  if (blocks_per_sm != 2 && blocks_per_sm != 4 && blocks_per_sm != 5)
+    return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "k_sweep is compiled for 5 or 4 eight-warp blocks or 2 sixteen-warp blocks per SM");
+  vistio_ctx* ctx = b->ctx;
   b->sweep_occ = blocks_per_sm;
+  const uint32_t ui = blocks_per_sm == 2 ? 2 * kUnitItems : kUnitItems;
+  if (ui != b->unit_items) {
+    b->unit_items = ui;
+    std::vector<uint32_t> items = schedule_levels(b, b->warp_limit);
+    CU(upload_schedule(b, items, b->ctx->stream));
+    CU(cudaStreamSynchronize(b->ctx->stream));
+  }
   return drop_graphs(b);
 }
 
@@ -1972,6 +2011,7 @@ vistio_status vistio_batch_get_sweep_blocks(const vistio_batch* b, uint32_t* blo
   if (tuned_ms) {
     tuned_ms[0] = b->occ_ms[0];
     tuned_ms[1] = b->occ_ms[1];
+    tuned_ms[2] = b->occ_ms[2];
   }
   return VISTIO_OK;
 }
