@@ -202,6 +202,7 @@ struct vistio_batch {
   struct GTopoHost {
     std::vector<uint8_t> taken, insub;     // laid out for the groups; bottom-subtree supernode
     std::vector<uint32_t> depth, parent, cost;  // cost = s (s + m)
+    std::vector<uint64_t> sub_cost;             // factor entries of each bottom subtree
     uint32_t sn_off = 0, sub_base = 0, nsub = 0;
   };
   std::vector<GTopoHost> gtopo_host;
@@ -373,6 +374,13 @@ cudaError_t schedule_groups(vistio_batch* b, uint32_t limit, cudaStream_t st) {
       if (act[t][q] && !T.insub[q]) tops.push_back(TopItem{T.depth[q], q, g});
     for (uint32_t i = 0; i < T.nsub; ++i) fwd.push_back(make_uint2(g, (T.sub_base + i) << 1));
   }
+  // the bottom subtrees longest first: each warp runs about two items, so the
+  // last ones decide when the launch ends
+  std::stable_sort(fwd.begin(), fwd.end(), [&](const uint2& a, const uint2& c) {
+    const auto& Ta = b->gtopo_host[b->group_topo[a.x]];
+    const auto& Tc = b->gtopo_host[b->group_topo[c.x]];
+    return Ta.sub_cost[(a.y >> 1) - Ta.sub_base] > Tc.sub_cost[(c.y >> 1) - Tc.sub_base];
+  });
   std::stable_sort(tops.begin(), tops.end(), [](const TopItem& a, const TopItem& c) {
     return a.depth != c.depth ? a.depth > c.depth : a.q != c.q ? a.q < c.q : a.g < c.g;
   });
@@ -997,6 +1005,12 @@ vistio_status pack_batch(vistio_ctx* ctx, vistio_solver* const* solvers, uint32_
       for (const Supernode& X : F.sn) {
         h.parent.push_back(X.parent);
         h.cost.push_back(X.ncols * (X.ncols + X.nrows));
+      }
+      for (size_t q = 0; q < F.sub_first.size(); ++q) {
+        uint64_t c = 0;
+        for (uint32_t k = F.sub_first[q]; k <= F.sub_last[q]; ++k)
+          c += uint64_t(F.sn[k].ncols) * (F.sn[k].ncols + 1) / 2 + uint64_t(F.sn[k].nrows) * F.sn[k].ncols;
+        h.sub_cost.push_back(c);
       }
       b->gtopo_host.push_back(std::move(h));
     }
