@@ -228,7 +228,23 @@ def reference_arm(args):
 D_HAT_IPC = 1e-3  # m, a distance: barrier_d_hat = D_HAT_IPC^2, self-contact thickness 1.5 D_HAT_IPC
 
 
-def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
+def apply_pin(batch, tune, pin):
+    """Replaces the autotuner's choice by the sweep configuration `pin`
+    ("KIND,WARP_LIMIT,GROUP_LIMIT,BLOCKS_PER_SM,TRIANGLES,HINGES"), for
+    profiling runs whose tuner timings the profiler distorts."""
+    if not pin:
+        return tune
+    kind, wl, gl, blocks, tri, hin = pin.split(",")
+    batch.set_sweep_mode(kind)
+    batch.set_warp_limit(int(wl))
+    if kind == "grouped":
+        batch.set_group_limit(int(gl))
+    batch.set_sweep_blocks(int(blocks))
+    batch.set_local_shape(int(tri), int(hin))
+    return dict(tune, pinned=pin, sweep_mode=kind, sweep_blocks_per_sm=int(blocks))
+
+
+def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None, pin=None):
     """Batched contact drapes: `n` sphere drapes with the batched workload's grid
     sides and materials, each starting 1 mm above a sphere of radius 0.3 m (so
     the barriers are active from the first step), ground and sphere barriers
@@ -267,12 +283,14 @@ def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
         for side, k in first.items():
             sp = specs[k]
             prm = O.init_params(stiffness=sp.stretch, bend_stiffness=sp.bending, density_gsm=sp.density_gsm)
-            refs[k] = pool.submit(lambda m=mesh(sp), prm=prm: _oracle_run(_oracle(m, prm, oc, 1, ground=-0.3),
-                                                                          warmup + steps, DT, c)[1])
+            for prec in (1, 0):  # FP64, and the reference's FP32 for the spread of the runs
+                refs[(k, prec)] = pool.submit(
+                    lambda m=mesh(sp), prm=prm, prec=prec: _oracle_run(_oracle(m, prm, oc, prec, ground=-0.3),
+                                                                       warmup + steps, DT, c)[1])
     with cf.ThreadPoolExecutor(threads or (os.cpu_count() or 4)) as ex:
         solvers = list(ex.map(make, specs))
     batch = api.Batch(solvers)
-    tune = batch.tune()
+    tune = apply_pin(batch, batch.tune(), pin)
     ms = timed_steps(batch, steps, warmup, contact)
     info = batch.info()
     value = n * steps / (ms / 1e3)
@@ -288,9 +306,9 @@ def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
     alg = 2 * (8 * sum(nnz[sp.side] for sp in specs) + 12 * info["vertices"])
     mode = tune["sweep_mode"]
     key = str(tune["group_limit"]) if mode == "grouped" else str(tune["warp_item_limit"])
-    sweep_ms = tune["sweep_ms"][mode][key]
+    sweep_ms = tune["sweep_ms"].get(mode, {}).get(key, -1.0)
     occ_ms = tune["sweep_blocks_ms"].get(str(tune["sweep_blocks_per_sm"]), -1.0)
-    if occ_ms > 0:  # the chosen compiled form's time (the candidates ran the five-block form)
+    if occ_ms > 0 and "pinned" not in tune:  # the chosen compiled form's time (the candidates ran the five-block form)
         sweep_ms = occ_ms
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
@@ -301,16 +319,28 @@ def ipc_batch(n, steps=10, warmup=5, threads=None, pool=None):
                 "peak_source": "measured" if peaks else "fallback",
                 "solves_per_step_max": solves, "solve_share_of_step_max": min(1.0, solves * sweep_ms / (ms / steps))}
     roofline["frac"] = roofline["achieved"] / peak
+    if sweep_ms <= 0:  # a pinned configuration the tuner did not time
+        roofline.update(kernel_ms=None, achieved=None, frac=None, solve_share_of_step_max=None)
     out = {"value": value, "unit": UNIT, "instances": n, "steps": steps, "warmup": warmup,
            "ms_per_step": ms / steps, "vertices": info["vertices"], "triangles": info["triangles"],
-           "launches_per_step": batch.launches_per_step(), "sweep": tune["sweep_mode"], "sweep_blocks_per_sm": tune["sweep_blocks_per_sm"], "roofline": roofline,
+           "launches_per_step": batch.launches_per_step(), "sweep": tune["sweep_mode"], "sweep_blocks_per_sm": tune["sweep_blocks_per_sm"],
+           "autotune": {k: tune[k] for k in ("warp_item_limit", "group_limit", "triangles_per_thread",
+                                             "hinges_per_thread", "pinned") if k in tune},
+           "roofline": roofline,
            "how": "sphere drapes with ground, sphere and self-contact barriers (IPC, AL <= 5 x 15 iterations, "
                   "d_hat 1 mm as a distance), grid sides and materials of the batched workload, CUDA events over "
                   "the timed steps"}
     if pool is not None:
-        errs = {str(specs[k].side): float(np.abs(batch.state(k)[0] - refs[k].result()).max()) for k in refs}
+        errs = {str(specs[k].side): float(np.abs(batch.state(k)[0] - refs[(k, 1)].result()).max())
+                for k in first.values()}
+        errs32 = {str(specs[k].side): float(np.abs(refs[(k, 0)].result() - refs[(k, 1)].result()).max())
+                  for k in first.values()}
         out["error_vs_fp64"] = {"max_m": max(errs.values()), "per_side_m": errs, "steps": warmup + steps,
-                                "how": "first drape of each grid side vs the FP64 oracle run of the same steps"}
+                                "ref32_max_m": max(errs32.values()), "ref32_per_side_m": errs32,
+                                "how": "first drape of each grid side vs the FP64 oracle run of the same steps; "
+                                       "ref32: the oracle's restatement of the reference's FP32 step on the same "
+                                       "runs (the sheets bounce on the sphere, and rounding differences grow "
+                                       "after the first bounce in both)"}
         # plain: the same drapes, one garment per step call
         plain_steps, secs = 3, 0.0
         for k in first.values():
@@ -714,7 +744,8 @@ def main():
     api._default_ctx = api.Context(local)
     if args.ipc_only:
         if rank == 0:
-            print(json.dumps({"ipc": ipc_batch(args.ipc_instances, args.steps, args.warmup)}), flush=True)
+            print(json.dumps({"ipc": ipc_batch(args.ipc_instances, args.steps, args.warmup, pin=args.pin_sweep)}),
+                  flush=True)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -746,16 +777,7 @@ def main():
     sym1 = _api.symbolic_cache_info()
     symbolic = {"hits": sym1["hits"] - sym0["hits"], "misses": sym1["misses"] - sym0["misses"],
                 "host_threads": threads}
-    tune = batch.tune()  # level schedule picked by timing this batch's sweeps
-    if args.pin_sweep:
-        kind, wl, gl, blocks, tri, hin = args.pin_sweep.split(",")
-        batch.set_sweep_mode(kind)
-        batch.set_warp_limit(int(wl))
-        if kind == "grouped":
-            batch.set_group_limit(int(gl))
-        batch.set_sweep_blocks(int(blocks))
-        batch.set_local_shape(int(tri), int(hin))
-        tune = dict(tune, pinned=args.pin_sweep, sweep_mode=kind)
+    tune = apply_pin(batch, batch.tune(), args.pin_sweep)  # level schedule picked by timing this batch's sweeps
     info = batch.info()
     V = info["vertices"]
     stream = torch.cuda.ExternalStream(batch.stream())

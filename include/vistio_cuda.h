@@ -310,6 +310,15 @@ vistio_status vistio_batch_tune_local(vistio_batch* b, uint32_t* tri_per_thread,
                                       float* candidate_ms);
 /* Sets the local steps' elements per thread directly (1 or 2 each). */
 vistio_status vistio_batch_set_local_shape(vistio_batch* b, uint32_t tri_per_thread, uint32_t hinge_per_thread);
+/* How the self-contact CCD step bound (compute_max_step_size,
+ * crates/vistio-contact/src/ccd.rs:238-292) visits its vertex-triangle tests.
+ * on = 1 (default): the detect that opens each AL pass lists every test of
+ * its candidate pairs once (a vertex of A meets triangle B again in each
+ * other pair (A', B) with the vertex in A', about 2.6 times per test on a
+ * cloth mesh) and the pass's CCDs run over that list; 0: every test of every
+ * pair, as the reference does. The minimum, and so every step, is
+ * bit-identical either way. No reference counterpart. */
+vistio_status vistio_batch_set_self_ccd_dedup(vistio_batch* b, uint32_t on);
 /* Sets / reads the group limit of sweep kind 2 (see vistio_batch_tune; at
  * most 6144; the batch must have garment groups). No reference counterpart. */
 vistio_status vistio_batch_set_group_limit(vistio_batch* b, uint32_t limit);

@@ -292,6 +292,94 @@ def test_self_contact_step_matches(iters, al):
     assert e <= 1e-5, (e, e32)
 
 
+def crossing_sheets(n=10, size=0.1, squeeze=0.25):
+    """Two square sheets in one mesh: a flat one at y = 0.5, and above it a
+    second whose rest shape is a plane tilted 17 degrees through it (its low
+    edge 1 cm below the first sheet), started squeezed to `squeeze` of its
+    size about its centre, clear of the first sheet. Springing back along its
+    plane drives its low side through the first sheet within the first PD
+    iteration, so the self CCD must bound that step."""
+    px, py, _, tris = scenarios.quad_grid(n, n, size, size)
+    nv = len(px)
+    bottom = np.stack([px, np.full(nv, 0.5, np.float32), py], 1)
+    rest_top = np.stack([px, 0.49 + 0.3 * (px + size / 2), py], 1)
+    c = rest_top.mean(0)
+    top = c + squeeze * (rest_top - c)
+    rest = np.concatenate([bottom, rest_top]).astype(np.float32)
+    state = np.concatenate([bottom, top]).astype(np.float32)
+    t = np.concatenate([tris, tris + nv]).astype(np.uint32)
+    mesh = scenarios.Mesh(rest[:, 0].copy(), rest[:, 1].copy(), rest[:, 2].copy(), t, np.zeros(2 * nv, np.uint8))
+    assert state[nv:, 1].min() > 0.5 + 1e-3  # clear of the first sheet at the start
+    return mesh, state
+
+
+def test_self_ccd_test_list_bit_identical_to_every_pair_test():
+    """The self CCD over its deduplicated vertex-triangle tests (each test of
+    the candidate pairs once, the default) against every test of every pair,
+    as compute_max_step_size runs them (ccd.rs:238-292): a batch of crossing
+    sheets (the self CCD bounds their steps), folded ribbons and sphere drapes
+    steps bit-identically both ways."""
+    d_hat = 5e-4
+    contact = api.Contact(has_ground=True, ground_height=-0.3, has_sphere=True, sphere_center=(0.0, 0.0, 0.0),
+                          sphere_radius=0.3, self_collision=True, kappa=1e3, thickness=1.5 * d_hat)
+    cfg = api.drape_config(max_iterations=8, al_max_iterations=3, barrier_d_hat=d_hat * d_hat, barrier_kappa=1e3)
+    setup = api.SetupDesc(stiffness=1e3, bend_stiffness=1e-4, density_gsm=150.0)
+    meshes, states = [], []
+    for n in (10, 13):
+        m, st = crossing_sheets(n)
+        meshes.append(m)
+        states.append(st)
+    for k in range(2):
+        pos, tris = folded_ribbon(cols=6, rows=40, gap=0.003, seed=k)
+        meshes.append(scenarios.Mesh(pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy(), tris,
+                                     np.zeros(len(pos), np.uint8)))
+        states.append(None)
+    for side in (16, 23):
+        meshes.append(scenarios.sphere_drape(side=side, length=1.5, height=0.301))
+        states.append(None)
+
+    def run(dedup, nsteps=6):
+        solvers = [api.ProjectiveDynamicsSolver().init_explicit(m, cfg, setup, pinned=m.pinned) for m in meshes]
+        batch = api.Batch(solvers)
+        batch.set_self_ccd_dedup(dedup)
+        for k, st in enumerate(states):
+            if st is not None:
+                batch.set_state(k, st)
+        out = []
+        for _ in range(nsteps):
+            batch.step(DT, 1, contact)
+            out.append([batch.state(k)[0].copy() for k in range(len(meshes))])
+        batch.close()
+        for s_ in solvers:
+            s_.close()
+        return out
+
+    a, b = run(True), run(False)
+    for sa, sb in zip(a, b):
+        for pa, pb in zip(sa, sb):
+            assert np.array_equal(pa, pb)
+    # the self CCD bounds the first PD iteration of the crossing sheets: their
+    # first step, stopped after that iteration, takes a step below 1 (the CCD
+    # scales its bound by 0.8), and both forms land on the same positions
+    cfg1 = api.drape_config(max_iterations=1, al_max_iterations=1, barrier_d_hat=d_hat * d_hat, barrier_kappa=1e3)
+    solo = api.ProjectiveDynamicsSolver().init_explicit(meshes[0], cfg1, setup, pinned=meshes[0].pinned)
+    solo.set_state(states[0])
+    alpha = solo.step_with_ipc(DT, contact).last_alpha
+    solo.close()
+    assert alpha < 0.9, alpha
+    first = []
+    for dedup in (True, False):
+        solo = api.ProjectiveDynamicsSolver().init_explicit(meshes[0], cfg1, setup, pinned=meshes[0].pinned)
+        batch = api.Batch([solo])
+        batch.set_self_ccd_dedup(dedup)
+        batch.set_state(0, states[0])
+        batch.step(DT, 1, contact)
+        first.append(batch.state(0)[0])
+        batch.close()
+        solo.close()
+    assert np.array_equal(first[0], first[1])
+
+
 def steps_from_oracle(gpu, ref, c, contact, nsteps, dt=DT):
     """nsteps GPU steps, each from the FP64 oracle's state; returns the worst
     relative error and the last GPU step result."""

@@ -150,6 +150,7 @@ SIGNATURES = {
     "vistio_batch_tune": (C.c_int, [_vp, _u32p, _fp]),
     "vistio_batch_tune_local": (C.c_int, [_vp, _u32p, _u32p, _fp]),
     "vistio_batch_set_local_shape": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
+    "vistio_batch_set_self_ccd_dedup": (C.c_int, [_vp, C.c_uint32]),
     "vistio_batch_set_group_limit": (C.c_int, [_vp, C.c_uint32]),
     "vistio_batch_get_group_limit": (C.c_int, [_vp, _u32p]),
     "vistio_batch_set_warp_limit": (C.c_int, [_vp, C.c_uint32]),

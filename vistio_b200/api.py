@@ -490,6 +490,12 @@ class Batch:
         L.check(L.lib().vistio_batch_set_local_shape(self.h, int(triangles_per_thread), int(hinges_per_thread)),
                 self.ctx.h)
 
+    def set_self_ccd_dedup(self, on: bool):
+        """Self-contact CCD over each vertex-triangle test once (True, the
+        default) or over every test of every candidate pair (False); the step
+        is bit-identical either way."""
+        L.check(L.lib().vistio_batch_set_self_ccd_dedup(self.h, 1 if on else 0), self.ctx.h)
+
     def set_warp_limit(self, limit: int):
         L.check(L.lib().vistio_batch_set_warp_limit(self.h, int(limit)), self.ctx.h)
 

@@ -60,6 +60,18 @@ struct SelfContactView {
   uint32_t* sort_hist;   // 256 digit counts per sort block, then their offsets
   uint32_t* sort_sums;   // scan block sums of sort_hist (+1: the total)
   uint32_t sort_blocks, sort_scan_blocks, sort_passes;
+  // The self CCD's vertex-triangle tests, each once. A candidate pair (A, B)
+  // tests the vertices of A against B and those of B against A, and a vertex
+  // v of A meets B again in every other pair (A', B) with v in A': about 2.6
+  // times per test on a cloth mesh. The list keeps (v, B) only from the pair
+  // whose A is the lowest-numbered triangle around v with a box overlapping
+  // B's, which is the first pair the broad phase holds for that test. Built
+  // by the detect that opens an AL pass; the pass's CCDs read it.
+  uint32_t* leaf_of;     // global triangle -> its leaf in its garment's tree (null: no list)
+  uint2* vt;             // (vertex, triangle), global ids
+  uint32_t* nvt;         // [0] tests, [1] overflow: the CCD then runs over the pairs
+  uint64_t vt_cap;
+  int32_t vt_on;         // build and use the list (0: every test of every pair)
 };
 
 // Host-side owner of those buffers (never passed to a kernel). They are
@@ -77,11 +89,13 @@ struct SelfContactDev : SelfContactView {
                     static_cast<void*>(pairs), static_cast<void*>(npairs), static_cast<void*>(adj_ptr),
                     static_cast<void*>(adj), static_cast<void*>(keys), static_cast<void*>(keys_alt),
                     static_cast<void*>(order), static_cast<void*>(order_alt), static_cast<void*>(sort_hist),
-                    static_cast<void*>(sort_sums)})
+                    static_cast<void*>(sort_sums), static_cast<void*>(leaf_of), static_cast<void*>(vt),
+                    static_cast<void*>(nvt)})
       if (q) cudaFreeAsync(q, stream);
     inst = nullptr; tri_inst = nullptr; box_min = box_max = nullptr; cnt = block_sums = nullptr;
     pairs = nullptr; npairs = nullptr; adj_ptr = adj = nullptr; ready = false;
     keys = keys_alt = nullptr; order = order_alt = leaf_tri = sort_hist = sort_sums = nullptr;
+    leaf_of = nullptr; vt = nullptr; nvt = nullptr; vt_cap = 0;
   }
   ~SelfContactDev() { release(); }
 };
@@ -207,6 +221,8 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t* __restrict__
 // refit, one block per garment.
 __global__ void __launch_bounds__(1024) k_self_boxes(BatchDev B, SelfContactView S, float margin_arg) {
   pdl_begin();
+  if (blockIdx.x == 0 && threadIdx.x == 0) S.npairs[0] = 0u;  // k_self_pairs counts from zero
+  if (blockIdx.x == 0 && threadIdx.x < 2 && S.nvt) S.nvt[threadIdx.x] = 0u;
   const SelfInst I = S.inst[blockIdx.x];
   if (B.prm->ipc && B.red[blockIdx.x].al_done) return;
   const float margin = margin_arg >= 0.f ? margin_arg : B.prm->thickness;
@@ -214,6 +230,7 @@ __global__ void __launch_bounds__(1024) k_self_boxes(BatchDev B, SelfContactView
   float4* mx = S.box_max + I.box_base;
   for (uint32_t i = threadIdx.x; i < I.nt; i += blockDim.x) {
     const uint32_t tri = S.leaf_tri ? S.leaf_tri[I.tbase + i] : I.tbase + i;
+    if (S.leaf_of) S.leaf_of[tri] = i;
     uint4 id = B.tri_idx[tri];
     float4 a = B.pos[id.x], b = B.pos[id.y], c = B.pos[id.z];
     mn[i] = make_float4(fminf(fminf(a.x, b.x), c.x) - margin, fminf(fminf(a.y, b.y), c.y) - margin,
@@ -249,8 +266,8 @@ __device__ __forceinline__ bool box_overlap(float4 amn, float4 amx, float4 bmn, 
 // Traversal for leaf i: visits subtrees holding leaves > i whose boxes overlap.
 // mode 0 counts, mode 1 writes at the scanned offset.
 template <int MODE>
-__device__ void self_traverse(const SelfContactView& S, const SelfInst& I, uint32_t i, uint32_t* count_out,
-                              uint2* out, uint32_t cap) {
+__device__ uint32_t self_traverse(const SelfContactView& S, const SelfInst& I, uint32_t i, uint32_t* count_out,
+                                  uint2* out, uint32_t cap) {
   const float4* mn = S.box_min + I.box_base;
   const float4* mx = S.box_max + I.box_base;
   float4 qmn = mn[i], qmx = mx[i];
@@ -287,6 +304,7 @@ __device__ void self_traverse(const SelfContactView& S, const SelfInst& I, uint3
     stack[sp++] = ((l - 1) << 26) | (2 * k);
   }
   if (MODE == 0) *count_out = found;
+  return found;
 }
 
 __global__ void __launch_bounds__(256) k_self_count(BatchDev B, SelfContactView S) {
@@ -358,6 +376,114 @@ __global__ void __launch_bounds__(256) k_self_write(BatchDev B, SelfContactView 
   if (threadIdx.x == 0 && S.npairs[0] > S.pair_cap) {
     S.npairs[1] = 1;
     atomicOr(B.status, 2u);  // candidate pairs exceeded the buffer
+  }
+}
+
+// The candidate pairs in one pass over the tree (the batch detect's form; the
+// pair order is not fixed, and nothing downstream depends on it). A thread
+// keeps its first kPairBuf pairs in a local buffer while it walks the tree,
+// its warp takes slots for all of them with one atomic, and a thread that
+// found more walks the tree again to write them all.
+constexpr uint32_t kPairBuf = 24;
+__global__ void __launch_bounds__(256) k_self_pairs(BatchDev B, SelfContactView S) {
+  pdl_begin();
+  const int4 ch = B.tri_chunks[blockIdx.x];
+  const bool live = (int)threadIdx.x < ch.z && !(B.prm->ipc && B.red[ch.x].al_done);
+  const uint32_t lane = threadIdx.x & 31u;
+  uint2 buf[kPairBuf];
+  uint32_t found = 0, i = 0;
+  SelfInst I;
+  if (live) {
+    I = S.inst[ch.x];
+    i = uint32_t(ch.y) + threadIdx.x - I.tbase;
+    uint32_t zero = 0;
+    found = self_traverse<1>(S, I, i, &zero, buf, kPairBuf);
+  }
+  uint32_t incl = found;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= uint32_t(o)) incl += y;
+  }
+  uint32_t base = 0;
+  if (lane == 31u && incl) base = atomicAdd(S.npairs, incl);
+  base = __shfl_sync(0xffffffffu, base, 31) + incl - found;
+  if (!live || !found) return;
+  const uint64_t cap = S.pair_cap;
+  if (uint64_t(base) + found > cap) {
+    S.npairs[1] = 1;
+    atomicOr(B.status, 2u);  // candidate pairs exceeded the buffer
+  }
+  if (found <= kPairBuf) {
+    for (uint32_t j = 0; j < found; ++j)
+      if (uint64_t(base) + j < cap) S.pairs[base + j] = buf[j];
+  } else {
+    self_traverse<1>(S, I, i, &base, S.pairs, uint32_t(cap));
+  }
+}
+
+// The deduplicated vertex-triangle CCD tests of this detect's pairs (see
+// SelfContactView::vt). A test (v, B) of pair (A, B) is kept unless a
+// triangle A' < A around v has a box overlapping B's: the broad phase then
+// holds the pair (A', B) too (it lists every pair of overlapping leaf boxes),
+// and that pair, or one before it, keeps the test. The CCD's minimum over the
+// list is the minimum over every test of every pair, bit for bit.
+__global__ void __launch_bounds__(256) k_self_vt(BatchDev B, SelfContactView S) {
+  pdl_begin();
+  const uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < np; k0 += stride) {
+    const uint32_t k = k0 + lane;
+    uint2 keep[6];
+    uint32_t c = 0;
+    if (k < np) {
+      const uint2 pr = S.pairs[k];
+      const uint32_t inst = S.tri_inst[pr.x];
+      const InstDev I = B.inst[inst];
+      const uint32_t box_base = S.inst[inst].box_base;
+      const uint4 A = B.tri_idx[pr.x], Bt = B.tri_idx[pr.y];
+      const uint32_t av[3] = {A.x, A.y, A.z}, bv[3] = {Bt.x, Bt.y, Bt.z};
+      const uint32_t* tcode = B.vtri + I.tinc_off;
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const uint32_t* X = side == 0 ? av : bv;
+        const uint32_t* Yt = side == 0 ? bv : av;
+        const uint32_t xt = side == 0 ? pr.x : pr.y, yt = side == 0 ? pr.y : pr.x;
+        const uint32_t yl = box_base + S.leaf_of[yt];
+        const float4 ymn = S.box_min[yl], ymx = S.box_max[yl];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const uint32_t v = X[q];
+          if (v == Yt[0] || v == Yt[1] || v == Yt[2]) continue;
+          bool first = true;
+          const uint32_t l = v - I.vbase;
+          for (uint32_t e = __ldg(B.vtri_ptr + I.inc_ptr + l), ee = __ldg(B.vtri_ptr + I.inc_ptr + l + 1);
+               e < ee && first; ++e) {
+            const uint32_t t2 = I.tbase + (__ldg(tcode + e) >> 2);
+            if (t2 >= xt) continue;
+            const uint32_t o = box_base + S.leaf_of[t2];
+            if (box_overlap(S.box_min[o], S.box_max[o], ymn, ymx)) first = false;
+          }
+          if (first) keep[c++] = make_uint2(v, yt);
+        }
+      }
+    }
+    // warp-aggregated slots: one atomic per warp
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= uint32_t(o)) incl += y;
+    }
+    uint32_t base = 0;
+    if (lane == 31u && incl) base = atomicAdd(S.nvt, incl);
+    base = __shfl_sync(0xffffffffu, base, 31) + incl - c;
+    if (base + c > S.vt_cap) {
+      S.nvt[1] = 1u;
+    } else {
+      for (uint32_t j = 0; j < c; ++j) S.vt[base + j] = keep[j];
+    }
   }
 }
 
@@ -763,6 +889,25 @@ __device__ R vt_ccd(V3d<R> p0, V3d<R> p1, V3d<R> a0, V3d<R> a1, V3d<R> b0, V3d<R
 // compute_max_step_size over the last detect's pairs (ccd.rs:238-292).
 __global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactView S) {
   pdl_begin();
+  if (S.vt_on && S.nvt[1] == 0u) {  // the deduplicated tests
+    const uint32_t nt = min(S.nvt[0], uint32_t(S.vt_cap));
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+      const uint2 tst = S.vt[k];
+      const uint32_t inst = S.tri_inst[tst.y];
+      InstRed& R = B.red[inst];
+      if (R.al_done) continue;
+      const InstDev I = B.inst[inst];
+      const uint4 T = B.tri_idx[tst.y];
+      auto P0 = [&](uint32_t v) { return ld3(B.pos, v); };
+      auto P1 = [&](uint32_t v) {
+        float4 x = B.pos[v], d = B.Y[I.vbase + B.perm_local[v]];
+        return mk<float>(x.x + d.x, x.y + d.y, x.z + d.z);
+      };
+      const float t = vt_ccd<float>(P0(tst.x), P1(tst.x), P0(T.x), P1(T.x), P0(T.y), P1(T.y), P0(T.z), P1(T.z));
+      if (t <= 1.f) atomicMin(&R.toi_bits, __float_as_uint(t));
+    }
+    return;
+  }
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
     uint2 pr = S.pairs[k];
@@ -822,13 +967,14 @@ inline uint32_t launch_self_detect(const BatchDev& d, const SelfContactView& S, 
   launch_pdl(k_clear_grad, n_vtx_chunks, 256, 0, st, d);
   const uint32_t ns = launch_self_sort(d, S, st);
   launch_pdl(k_self_boxes, S.ninst, 1024, 0, st, d, S, -1.f);  // margin: StepParams::thickness
-  launch_pdl(k_self_count, n_tri_chunks, 256, 0, st, d, S);
-  launch_pdl(k_scan_local, S.scan_blocks, kScanBlock, 0, st, S.cnt, uint32_t(S.T), S.block_sums);
-  launch_pdl(k_scan_sums, 1, kScanBlock, 0, st, S.block_sums, S.scan_blocks, S.npairs);
-  launch_pdl(k_scan_add, S.scan_blocks, kScanBlock, 0, st, S.cnt, uint32_t(S.T), S.block_sums);
-  launch_pdl(k_self_write, n_tri_chunks, 256, 0, st, d, S);
+  launch_pdl(k_self_pairs, n_tri_chunks, 256, 0, st, d, S);
+  uint32_t nl = 4 + ns;
+  if (S.vt_on && mode == 0) {  // the pass's CCD tests
+    launch_pdl(k_self_vt, 4 * 148, 256, 0, st, d, S);
+    ++nl;
+  }
   launch_pdl(k_self_grad, 4 * 148, kGradThreads, 0, st, d, S, mode);
-  return 8 + ns;
+  return nl;
 }
 
 inline void launch_self_ccd(const BatchDev& d, const SelfContactView& S, cudaStream_t st) {

@@ -168,6 +168,7 @@ struct vistio_batch {
   std::vector<uint64_t> sn_key;
   uint32_t warp_limit = kWarpItemLimit;             // s (s + m) limit of a warp item
   uint32_t tri_per = 2, hinge_per = 1;              // elements per thread of k_tri / k_hinge (autotuned)
+  uint32_t self_ccd_dedup = 1;                      // self CCD over each vertex-triangle test once
   float tuned_ms = 0.f;                             // sweep time of the tuned schedule (0: not tuned)
   float occ_ms[3] = {-1.f, -1.f, -1.f};  // the autotuner's times of the three forms (ms per solve)
   // k_sweep's compiled form, by blocks per SM: 5 or 4 (eight warps), 2
@@ -1266,6 +1267,7 @@ vistio_status batch_run(vistio_batch* b, float dt, uint32_t nsteps, const vistio
     }
     vistio_status s = ensure_self_contact(b->dev, b->self, b->solvers, b->vbase, b->T, st, &ctx->last_error);
     if (s != VISTIO_OK) return s;
+    b->self.vt_on = int32_t(b->self_ccd_dedup);
   }
   StepParams p = make_params(b->cfg, dt, ct);
   CU(cudaMemcpyAsync(b->prm.p, &p, sizeof(p), cudaMemcpyHostToDevice, st));
@@ -1981,6 +1983,14 @@ vistio_status vistio_batch_set_local_shape(vistio_batch* b, uint32_t tri_per_thr
   return drop_graphs(b);
 }
 
+vistio_status vistio_batch_set_self_ccd_dedup(vistio_batch* b, uint32_t on) {
+  if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
+  if (on > 1) return fail(b->ctx, VISTIO_ERR_INVALID_CONFIG, "on must be 0 or 1");
+  b->self_ccd_dedup = on;
+  b->self.vt_on = int32_t(on);
+  return drop_graphs(b);
+}
+
 vistio_status vistio_batch_set_warp_limit(vistio_batch* b, uint32_t limit) {
   if (!b) return fail(nullptr, VISTIO_ERR_INVALID_CONFIG, "null batch");
   vistio_ctx* ctx = b->ctx;
@@ -2340,12 +2350,20 @@ vistio_status self_build(SelfContactDev& S, const std::vector<std::pair<const ui
     SA(S.sort_sums, (S.sort_scan_blocks + 1ull) * 4);
     S.leaf_tri = S.sort_passes % 2 == 0 ? S.order : S.order_alt;  // where the last pass leaves the order
   }
+  // the self CCD's deduplicated tests: as many as the pair capacity (a cloth
+  // mesh has about 1.6 per pair); beyond it the CCD runs over the pairs
+  S.vt_cap = std::min<uint64_t>(S.pair_cap, 0xffffffffull);
+  SA(S.leaf_of, std::max<uint64_t>(T, 1) * 4);
+  SA(S.vt, S.vt_cap * sizeof(uint2));
+  SA(S.nvt, 8);
 #undef SA
   if ((e = cudaMemcpyAsync(S.inst, si.data(), n * sizeof(SelfInst), cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
   if (T && (e = cudaMemcpyAsync(S.tri_inst, tri_inst.data(), T * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
   if ((e = cudaMemcpyAsync(S.adj_ptr, aptr.data(), (V + 1) * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
   if (!adj.empty() && (e = cudaMemcpyAsync(S.adj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return bad(e, "copy");
   if ((e = cudaMemsetAsync(S.npairs, 0, 8, st)) != cudaSuccess) return bad(e, "memset");
+  if ((e = cudaMemsetAsync(S.nvt, 0, 8, st)) != cudaSuccess) return bad(e, "memset");
+  if ((e = cudaMemsetAsync(S.leaf_of, 0, std::max<uint64_t>(T, 1) * 4, st)) != cudaSuccess) return bad(e, "memset");
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return bad(e, "sync");
   S.ready = true;
   return VISTIO_OK;
