@@ -887,27 +887,33 @@ __device__ R vt_ccd(V3d<R> p0, V3d<R> p1, V3d<R> a0, V3d<R> a1, V3d<R> b0, V3d<R
 }
 
 // compute_max_step_size over the last detect's pairs (ccd.rs:238-292).
+// Over the pass's listed tests (SelfContactView::vt), one thread per test; a
+// kernel of its own, so that it keeps the registers of one test (six blocks
+// per SM). Nothing to do when the list overflowed (k_self_ccd runs then).
+__global__ void __launch_bounds__(256, 6) k_self_ccd_list(BatchDev B, SelfContactView S) {
+  pdl_begin();
+  if (S.nvt[1] != 0u) return;
+  const uint32_t nt = min(S.nvt[0], uint32_t(S.vt_cap));
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+    const uint2 tst = S.vt[k];
+    const uint32_t inst = S.tri_inst[tst.y];
+    InstRed& R = B.red[inst];
+    if (R.al_done) continue;
+    const uint32_t vbase = B.inst[inst].vbase;
+    const uint4 T = B.tri_idx[tst.y];
+    auto P0 = [&](uint32_t v) { return ld3(B.pos, v); };
+    auto P1 = [&](uint32_t v) {
+      float4 x = B.pos[v], d = B.Y[vbase + B.perm_local[v]];
+      return mk<float>(x.x + d.x, x.y + d.y, x.z + d.z);
+    };
+    const float t = vt_ccd<float>(P0(tst.x), P1(tst.x), P0(T.x), P1(T.x), P0(T.y), P1(T.y), P0(T.z), P1(T.z));
+    if (t <= 1.f) atomicMin(&R.toi_bits, __float_as_uint(t));
+  }
+}
+
 __global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactView S) {
   pdl_begin();
-  if (S.vt_on && S.nvt[1] == 0u) {  // the deduplicated tests
-    const uint32_t nt = min(S.nvt[0], uint32_t(S.vt_cap));
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
-      const uint2 tst = S.vt[k];
-      const uint32_t inst = S.tri_inst[tst.y];
-      InstRed& R = B.red[inst];
-      if (R.al_done) continue;
-      const InstDev I = B.inst[inst];
-      const uint4 T = B.tri_idx[tst.y];
-      auto P0 = [&](uint32_t v) { return ld3(B.pos, v); };
-      auto P1 = [&](uint32_t v) {
-        float4 x = B.pos[v], d = B.Y[I.vbase + B.perm_local[v]];
-        return mk<float>(x.x + d.x, x.y + d.y, x.z + d.z);
-      };
-      const float t = vt_ccd<float>(P0(tst.x), P1(tst.x), P0(T.x), P1(T.x), P0(T.y), P1(T.y), P0(T.z), P1(T.z));
-      if (t <= 1.f) atomicMin(&R.toi_bits, __float_as_uint(t));
-    }
-    return;
-  }
+  if (S.vt_on && S.nvt[1] == 0u) return;  // k_self_ccd_list has the tests
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
     uint2 pr = S.pairs[k];
@@ -937,7 +943,7 @@ __global__ void __launch_bounds__(256) k_self_ccd(BatchDev B, SelfContactView S)
 }
 
 // ---------------------------------------------------------------- host side
-inline uint32_t self_ccd_launches() { return 1; }
+inline uint32_t self_ccd_launches(const SelfContactView& S) { return S.vt_on ? 2 : 1; }
 
 // The LBVH leaf order: Morton keys, then sort_passes radix passes (5 launches each).
 inline uint32_t launch_self_sort(const BatchDev& d, const SelfContactView& S, cudaStream_t st) {
@@ -978,6 +984,7 @@ inline uint32_t launch_self_detect(const BatchDev& d, const SelfContactView& S, 
 }
 
 inline void launch_self_ccd(const BatchDev& d, const SelfContactView& S, cudaStream_t st) {
+  if (S.vt_on) launch_pdl(k_self_ccd_list, 6 * 148, 256, 0, st, d, S);
   launch_pdl(k_self_ccd, 4 * 148, 256, 0, st, d, S);
 }
 

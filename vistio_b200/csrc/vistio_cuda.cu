@@ -1233,7 +1233,7 @@ vistio_status capture(vistio_batch* b, bool ipc, bool self, cudaGraphExec_t* out
         // With backtracking (alpha < 1) part of each sweep's error stays in x:
         // every solve is refined.
         L += launch_plain_iteration(b, st, 0, b->refine) + 2;
-        if (self) { launch_self_ccd(b->dev, b->self.view(), st); L += self_ccd_launches(); }
+        if (self) { launch_self_ccd(b->dev, b->self.view(), st); L += self_ccd_launches(b->self.view()); }
         launch_pdl(k_ccd, b->n_vtx_chunks, kElemThreads, 0, st, b->dev);
         launch_pdl(k_ipc_update, b->n_vtx_chunks, kElemThreads, 0, st, b->dev);
       }
