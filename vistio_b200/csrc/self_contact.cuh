@@ -119,7 +119,7 @@ __device__ __forceinline__ uint32_t morton_spread10(uint32_t v) {
 // below the garment index (so each garment stays in its own range).
 __global__ void __launch_bounds__(1024) k_self_keys(BatchDev B, SelfContactView S) {
   pdl_begin();
-  const SelfInst I = S.inst[blockIdx.x];
+  const SelfInst& I = S.inst[blockIdx.x];
   __shared__ float red[6][32];
   float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
   auto centroid = [&](uint32_t i) {
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(1024) k_self_boxes(BatchDev B, SelfContactView
   pdl_begin();
   if (blockIdx.x == 0 && threadIdx.x == 0) S.npairs[0] = 0u;  // k_self_pairs counts from zero
   if (blockIdx.x == 0 && threadIdx.x < 2 && S.nvt) S.nvt[threadIdx.x] = 0u;
-  const SelfInst I = S.inst[blockIdx.x];
+  const SelfInst& I = S.inst[blockIdx.x];
   if (B.prm->ipc && B.red[blockIdx.x].al_done) return;
   const float margin = margin_arg >= 0.f ? margin_arg : B.prm->thickness;
   float4* mn = S.box_min + I.box_base;
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(256) k_self_count(BatchDev B, SelfContactView 
   int4 ch = B.tri_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) { S.cnt[ch.y + threadIdx.x] = 0; return; }
-  const SelfInst I = S.inst[ch.x];
+  const SelfInst& I = S.inst[ch.x];
   uint32_t t = uint32_t(ch.y) + threadIdx.x;
   uint32_t c = 0;
   self_traverse<0>(S, I, t - I.tbase, &c, nullptr, 0);
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(256) k_self_write(BatchDev B, SelfContactView 
   int4 ch = B.tri_chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   if (B.prm->ipc && B.red[ch.x].al_done) return;
-  const SelfInst I = S.inst[ch.x];
+  const SelfInst& I = S.inst[ch.x];
   uint32_t t = uint32_t(ch.y) + threadIdx.x;
   uint32_t off = S.cnt[t];
   self_traverse<1>(S, I, t - I.tbase, &off, S.pairs, uint32_t(S.pair_cap));
@@ -392,9 +392,8 @@ __global__ void __launch_bounds__(256) k_self_pairs(BatchDev B, SelfContactView 
   const uint32_t lane = threadIdx.x & 31u;
   uint2 buf[kPairBuf];
   uint32_t found = 0, i = 0;
-  SelfInst I;
+  const SelfInst& I = S.inst[ch.x];  // read in place (cached): the block's threads share it
   if (live) {
-    I = S.inst[ch.x];
     i = uint32_t(ch.y) + threadIdx.x - I.tbase;
     uint32_t zero = 0;
     found = self_traverse<1>(S, I, i, &zero, buf, kPairBuf);
