@@ -723,9 +723,12 @@ __device__ __forceinline__ bool ee_far(V3d<float> p0, V3d<float> p1, V3d<float> 
   return gx * gx + gy * gy + gz * gz >= screen;
 }
 
-__global__ void __launch_bounds__(kGradThreads, 4) k_self_grad(BatchDev B, SelfContactView S, int mode) {
+// Three blocks per SM (80 registers, 110 bytes of spill): against four (64
+// registers, 174 bytes of spill) the 64-drape contact step 37.25 -> 37.02 ms;
+// two (128 registers, no spill) 37.58 ms.
+__global__ void __launch_bounds__(kGradThreads, 3) k_self_grad(BatchDev B, SelfContactView S, int mode) {
   pdl_begin();
-  __shared__ double acc_s[18 * kGradThreads];  // 36 KB: four blocks per SM
+  __shared__ double acc_s[18 * kGradThreads];  // 36 KB per block
   const StepParams& P = *B.prm;
   uint32_t np = min(S.npairs[0], uint32_t(S.pair_cap));
   double4* G = B.gacc;
@@ -978,7 +981,7 @@ inline uint32_t launch_self_detect(const BatchDev& d, const SelfContactView& S, 
     launch_pdl(k_self_vt, 4 * 148, 256, 0, st, d, S);
     ++nl;
   }
-  launch_pdl(k_self_grad, 4 * 148, kGradThreads, 0, st, d, S, mode);
+  launch_pdl(k_self_grad, 3 * 148, kGradThreads, 0, st, d, S, mode);
   return nl;
 }
 
