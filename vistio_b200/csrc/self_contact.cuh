@@ -978,7 +978,7 @@ inline uint32_t launch_self_detect(const BatchDev& d, const SelfContactView& S, 
   launch_pdl(k_self_pairs, n_tri_chunks, 256, 0, st, d, S);
   uint32_t nl = 4 + ns;
   if (S.vt_on && mode == 0) {  // the pass's CCD tests
-    launch_pdl(k_self_vt, 4 * 148, 256, 0, st, d, S);
+    launch_pdl(k_self_vt, 6 * 148, 256, 0, st, d, S);  // 40 registers: six blocks per SM
     ++nl;
   }
   launch_pdl(k_self_grad, 3 * 148, kGradThreads, 0, st, d, S, mode);
